@@ -1,0 +1,188 @@
+/*
+ * gofish_b200.h -- C ABI of the B200 (sm_100a) GO_Fish forward Wright-Fisher engine and the
+ * Spectrum site-frequency-spectrum path.
+ *
+ * Plain C types only (pointers, sizes, ints, floats): no CUDA or C++ types cross this boundary, so
+ * the library can be bound from C, C++ (the header front-end in include/3P/), ctypes or any FFI.
+ * Every entry point returns a gf_status; gf_engine_last_error() holds the message of the last
+ * failure on that engine.  Nothing in the library calls exit().
+ *
+ * Each declaration cites the reference interface it replaces, as `file:line` within
+ * ParallelPopGen 3P v0.3.2.
+ */
+#ifndef GOFISH_B200_H_
+#define GOFISH_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Largest number of populations one simulation may hold.  The reference has no fixed bound; the
+ * per-generation parameter block below is a fixed-size struct so it can be passed by value to the
+ * drift kernel. */
+#define GF_MAX_POPULATIONS 16
+
+/* Largest generation number the engine accepts: on the device a mutation's origin generation and
+ * origin population share one 32-bit word (24 + 7 bits); the origin thread ID keeps its own word. */
+#define GF_MAX_GENERATION ((1 << 24) - 1)
+
+typedef enum gf_status {
+  GF_OK = 0,
+  GF_ERR_INVALID_ARGUMENT = 1, /* a parameter is out of range (check_sim_parameters, go_fish_impl.cuh:431-452) */
+  GF_ERR_CUDA = 2,             /* a CUDA runtime call failed (cudaCheckErrors, shared.cuh:24) */
+  GF_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
+  GF_ERR_CAPACITY = 4,         /* a documented size limit was exceeded */
+  GF_ERR_STATE = 5,            /* call out of order, e.g. gf_sim_run before a gf_sim_begin_* */
+  GF_ERR_DEVICE = 6,           /* a kernel reported a fault through the engine's device status word */
+  GF_ERR_NO_DEVICE = 7         /* no CUDA device, or the requested ordinal does not exist */
+} gf_status;
+
+typedef struct gf_engine gf_engine;
+
+/* ---------------------------------------------------------------------------------------------
+ * Engine lifecycle.  An engine owns one device, one CUDA stream and the device buffers of one
+ * simulation at a time.  Replaces set_cuda_device (shared.cuh:27-37) and the stream/event set-up
+ * of GO_Fish::run_sim (go_fish_impl.cuh:561-587).
+ *   device       CUDA ordinal, or -1 for the current device.
+ *   cuda_stream  a cudaStream_t to run on, or NULL to let the engine create its own.
+ * ------------------------------------------------------------------------------------------- */
+gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out_engine);
+void gf_engine_destroy(gf_engine* engine);
+const char* gf_engine_last_error(const gf_engine* engine);
+/* CUDA ordinal the engine runs on (set_cuda_device reports it back, shared.cuh:35). */
+int32_t gf_engine_device(const gf_engine* engine);
+const char* gf_status_string(gf_status status);
+/* Library version, "major.minor.patch". */
+const char* gf_version(void);
+
+/* Simulation constants (allele_trajectories::sim_constants, go_fish_data_struct.h:57-70). */
+typedef struct gf_sim_config {
+  int32_t seed1;            /* Philox key word 0 */
+  int32_t seed2;            /* Philox key word 1 */
+  float num_sites;          /* L */
+  int32_t num_populations;  /* P, 1 .. GF_MAX_POPULATIONS */
+  int32_t compact_interval; /* 0 = never compact */
+  int32_t reserve_mutations;/* initial capacity hint in mutations (0 = automatic) */
+} gf_sim_config;
+
+/* Per-population model values at one generation, evaluated by the caller from its model functions
+ * (Sim_Model functors).  Selection must be affine in frequency at a fixed population and
+ * generation: s(freq) = sel_slope * freq + sel_intercept, which covers every selection model the
+ * reference ships (template_inline_simulation_functors.cuh:46-158). */
+typedef struct gf_population_params {
+  int32_t Nchrom_e;      /* effective chromosomes 2N/(1+F) (go_fish_impl.cuh:659); 0 = not simulated */
+  int32_t drift;         /* 1: run migration/selection/drift for this population this generation */
+  int32_t alive;         /* demography(pop, generation) > 0, used by the compaction flag (:156) */
+  int32_t mutate;        /* 1: draw new mutations for this population (calc_new_mutations_Index :462) */
+  float mu;              /* per-site mutation rate */
+  float F;               /* inbreeding coefficient */
+  float h;               /* dominance coefficient */
+  float sel_slope;       /* selection coefficient slope in frequency */
+  float sel_intercept;   /* selection coefficient at frequency 0 */
+} gf_population_params;
+
+/* One generation (the body of the run_sim loop, go_fish_impl.cuh:645-714). */
+typedef struct gf_generation {
+  int32_t generation;
+  int32_t compact;   /* compact after this generation (:705) */
+  int32_t preserve;  /* mark survivors of this compaction as preserved (:686, scatter_arrays) */
+  int32_t reserved;
+  gf_population_params pop[GF_MAX_POPULATIONS];
+  /* migration[from * GF_MAX_POPULATIONS + to]: proportion of chromosomes in `to` from `from`
+   * (Functor_migration, go_fish.cuh:238). */
+  float migration[GF_MAX_POPULATIONS * GF_MAX_POPULATIONS];
+} gf_generation;
+
+/* Begin a simulation from an empty mutation array at `start_generation`
+ * (init_blank_prev_run, blank branch: go_fish_impl.cuh:335-349). */
+gf_status gf_sim_begin_blank(gf_engine* engine, const gf_sim_config* config, int32_t start_generation);
+
+/* Begin a simulation from host arrays (init_blank_prev_run, resume branch: go_fish_impl.cuh:339-365).
+ *   freq       [num_populations][num_mutations] row-major frequencies
+ *   mut_ids    [num_mutations][4] int32 = (origin_generation, origin_population, origin_threadID, reserved);
+ *              a negative threadID marks a preserved mutation
+ *   extinct    [num_populations] 0/1 (may be NULL)
+ *   preserve   1: mark every loaded mutation preserved (preserve_prev_run_mutations, go_fish_impl.cu:191-194) */
+gf_status gf_sim_begin_from_state(gf_engine* engine, const gf_sim_config* config, int32_t start_generation,
+                                  const float* freq, const int32_t* mut_ids, int32_t num_mutations,
+                                  const uint8_t* extinct, int32_t preserve);
+
+/* Per-population inputs of the mutation-selection-equilibrium start (initialize_mse,
+ * go_fish_impl.cuh:242-332).  Selection is affine in frequency, as in gf_population_params. */
+typedef struct gf_mse_population {
+  int32_t N_ind;         /* demography(pop, 0) */
+  int32_t Nchrom_e;      /* 2 * N_ind / (1 + F) */
+  float mu;
+  float F;
+  float h;
+  float sel_slope;
+  float sel_intercept;
+} gf_mse_population;
+
+/* Begin at mutation-selection equilibrium at generation 0 (initialize_mse).  Neutral populations
+ * use lambda(x) = 2 mu L / x exactly as the reference; selected ones integrate the MSE density with
+ * a fixed-order (deterministic) scan.  preserve = preserve(0) | sample(0). */
+gf_status gf_sim_begin_mse(gf_engine* engine, const gf_sim_config* config, const gf_mse_population* pops,
+                           int32_t preserve);
+
+/* Run `num_generations` consecutive generations (run_sim loop body, go_fish_impl.cuh:645-714:
+ * fused migration/selection/drift + new mutations, then compaction where gens[i].compact is set).
+ * Asynchronous: returns once the work is queued on the engine's stream. */
+gf_status gf_sim_run(gf_engine* engine, const gf_generation* gens, int32_t num_generations);
+
+/* Current number of mutations in the array (h_mutations_Index).  Synchronizes the stream. */
+gf_status gf_sim_num_mutations(gf_engine* engine, int32_t* out_num_mutations);
+
+/* Copy the current state to host memory (store_time_sample, go_fish_impl.cuh:477-501).
+ *   freq_out   [num_populations][num_mutations] (may be NULL)
+ *   ids_out    [num_mutations][4] int32 mutID layout (may be NULL)
+ *   max_mutations  capacity of the caller's arrays, in mutations
+ * Synchronizes the stream. */
+gf_status gf_sim_read_state(gf_engine* engine, float* freq_out, int32_t* ids_out, int32_t max_mutations,
+                            int32_t* out_num_mutations);
+
+/* Device pointer to the current frequency rows ([P][stride] floats) and their row stride, for
+ * device-side consumers (valid until the next gf_sim_* call). */
+gf_status gf_sim_device_state(gf_engine* engine, const float** out_freq, int32_t* out_row_stride,
+                              int32_t* out_num_mutations);
+
+/* Host-side new-mutation count of one population in one generation, exactly as the reference draws
+ * it on the host (calc_new_mutations_Index, go_fish_impl.cuh:454-467, ApproxRandPois1
+ * shared.cuh:251-256): max(Poisson~(mu * Nchrom_e * L), 0) with counter (1, generation, pop, 0). */
+int32_t gf_new_mutation_count(int32_t seed1, int32_t seed2, float mu, int32_t Nchrom_e, float num_sites,
+                              int32_t generation, int32_t population);
+
+/* ---------------------------------------------------------------------------------------------
+ * Spectrum (spectrum.h:24-43, spectrum.cu:153-294).  Inputs are one population row of a host time
+ * sample, as the reference's functions take it; outputs are host arrays.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Population frequency histogram (Spectrum::population_frequency_histogram, spectrum.cu:153-210):
+ * out[k] = number of mutations with round(Nchrom_e * freq) == k (k == Nchrom_e folds into 0),
+ * plus (num_sites - num_mutations) in out[0].  out has Nchrom_e floats. */
+gf_status gf_population_histogram(gf_engine* engine, const float* freq, int32_t num_mutations, int32_t Nchrom_e,
+                                  float num_sites, float* out);
+
+/* Binomially projected SFS of sample size n (Spectrum::site_frequency_spectrum, spectrum.cu:213-294):
+ * out[k] = sum over mutations segregating in this population (0 < p < 1) of C(n,k) p^k (1-p)^(n-k)
+ * for k = 1 .. n-1; out[0] collects k = 0 and k = n, every non-segregating mutation and
+ * (num_sites - num_mutations).  Requires 1 <= n < Nchrom_e.  out has n floats. */
+gf_status gf_site_frequency_spectrum(gf_engine* engine, const float* freq, int32_t num_mutations,
+                                     int32_t Nchrom_e, int32_t n, float num_sites, float* out);
+
+/* The same two functions on a device-resident frequency row (no host copies). */
+gf_status gf_population_histogram_device(gf_engine* engine, const float* d_freq, int32_t num_mutations,
+                                         int32_t Nchrom_e, float num_sites, float* d_out);
+gf_status gf_site_frequency_spectrum_device(gf_engine* engine, const float* d_freq, int32_t num_mutations,
+                                            int32_t Nchrom_e, int32_t n, float num_sites, float* d_out);
+
+/* Synchronize the engine's stream and report any pending device-side fault. */
+gf_status gf_engine_synchronize(gf_engine* engine);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOFISH_B200_H_ */

@@ -1,0 +1,1076 @@
+// GO_Fish plain engine for one B200: device state, the per-generation kernels and the host loop.
+//
+// Device state (all rows have the same stride `capacity`, a multiple of 1024 slots):
+//   freq[2]      [P][capacity] fp32, ping-pong between generations (d_prev_freq / d_mutations_freq,
+//                go_fish_impl.cuh:183-199)
+//   id_gp[2]     origin generation | origin population << 24       (mutID.x, mutID.y)
+//   id_tid[2]    origin threadID, negative = preserved              (mutID.z)
+//   flags        1 bit per slot: survives the next compaction
+//   tile_count / tile_offset   survivors per 1024-slot tile and their exclusive prefix
+//   d_count      [0], [1] mutation count ping-pong (written by the device, never synchronized on
+//                except for state reads), [2] device status word
+//
+// One generation = one fused kernel (migration -> selection -> drift for every population of a
+// mutation quad, the new-mutation fill of the appended slots, and -- on compaction generations --
+// the survival bitmask and per-tile survivor counts).  A compaction adds a one-block scan of the
+// tile counts and a stable scatter.  There is no cudaMalloc and no host synchronization inside the
+// generation loop: the host tracks an upper bound on the mutation count and tightens it from
+// asynchronous read-backs of each compaction's survivor count.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+
+#include "gf_internal.h"
+#include "gf_rng.cuh"
+
+namespace gf {
+
+// ------------------------------------------------------------------------------------------------
+// error helpers
+// ------------------------------------------------------------------------------------------------
+gf_status fail(Engine* e, gf_status st, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (e) e->last_error = buf;
+  return st;
+}
+
+gf_status cuda_fail(Engine* e, cudaError_t err, const char* what) {
+  const gf_status st = (err == cudaErrorMemoryAllocation) ? GF_ERR_OUT_OF_MEMORY : GF_ERR_CUDA;
+  return fail(e, st, "CUDA error %d (%s) in %s", static_cast<int>(err), cudaGetErrorString(err), what);
+}
+
+gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need) {
+  if (*have >= need && *ptr) return GF_OK;
+  if (*ptr) {
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    GF_CUDA(e, cudaFree(*ptr));
+    *ptr = nullptr;
+    *have = 0;
+  }
+  const size_t bytes = std::max<size_t>(need, 256);
+  GF_CUDA(e, cudaMalloc(ptr, bytes));
+  *have = bytes;
+  return GF_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// per-slot model arithmetic (the expressions of migration_selection_drift, go_fish_impl.cuh:93-124)
+// ------------------------------------------------------------------------------------------------
+
+// Frequency after selection (go_fish_impl.cuh:105 / :119).  With s == 0 the expression reduces to
+// x exactly, which the NEUTRAL instantiation uses directly.
+template <bool NEUTRAL>
+__device__ __forceinline__ float selected_freq(float x, float sa, float sb, float F, float h) {
+  if (NEUTRAL) return x;
+  const float s = fmaxf(sa * x + sb, -1.f);
+  return (s * x * x + x + (F + h - h * F) * s * x * (1 - x)) /
+         (x * x * s + (F + 2 * h - 2 * h * F) * s * x * (1 - x) + 1);
+}
+
+// Drift of one quad lane: returns the new count j in [0, N].  Lost (x == 0) and, for N > 6, fixed
+// (x == 1) slots have a certain outcome (0 and N) and skip the sampler.
+__device__ __forceinline__ int drift_lane(uint32_t bits, float xs, int N) {
+  if (xs == 0.f) return 0;
+  if (xs == 1.f && N > 6) return N;
+  const float mean = xs * N;
+  const float var = (1.0f - xs) * mean;
+  return binom_draw_lane(bits, mean, var, static_cast<float>(N));
+}
+
+// Drift of one scalar-tail slot: counter (slot + 2, generation, pop, 0), variance evaluated in
+// double as the reference's scalar tail does (go_fish_impl.cuh:121).
+__device__ __forceinline__ int drift_tail(int seed1, int seed2, int slot, int generation, int pop, float xs, int N) {
+  if (xs == 0.f) return 0;
+  if (xs == 1.f && N > 6) return N;
+  const float mean = xs * N;
+  const float var = static_cast<float>((1.0 - static_cast<double>(xs)) * static_cast<double>(mean));
+  const uint4 r = philox(seed1, seed2, slot + 2, generation, pop, 0);
+  return binom_draw_tail(r.x, mean, var, static_cast<float>(N));
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return max(lo, min(v, hi)); }
+
+// ------------------------------------------------------------------------------------------------
+// the fused generation kernel
+// ------------------------------------------------------------------------------------------------
+// PT: 1 = single-population specialization, 0 = any P <= kMaxPops.
+// NEUTRAL: every drifted population has s(x) == 0.
+// FLAG: compaction generation -- also write the survival bitmask and tile counts.
+template <int PT, bool NEUTRAL, bool FLAG>
+__global__ void __launch_bounds__(kDriftThreads)
+    drift_kernel(const float* __restrict__ prev, float* __restrict__ next, int* __restrict__ id_gp,
+                 int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
+                 int* __restrict__ d_count, long long stride, int slot_in, int slot_out, int launch_slots,
+                 const GenArgs a) {
+  const int M_in = d_count[slot_in];
+  const int total = M_in + a.new_total;
+  const int q = blockIdx.x * kDriftThreads + threadIdx.x;  // quad index
+  const int base = q * 4;
+  const int nquads = M_in >> 2;
+  const int P = (PT > 0) ? PT : a.num_pops;
+  const int g = a.generation;
+  unsigned keep = 0;  // bit j: slot base + j survives the compaction
+
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d_count[slot_out] = total;
+    if (total > launch_slots) atomicExch(d_count + 2, kFaultCapacity);
+  }
+
+  if (q < nquads) {
+    // ---- full quad: one Philox block per population, lanes x,y,z,w = slots base .. base+3 ----
+    unsigned zero = 0xFu, one = 0xFu;
+#pragma unroll 1
+    for (int p = 0; p < P; ++p) {
+      if (!((a.drift_mask >> p) & 1)) continue;
+      float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int k = 0; k < P; ++k) {
+        const float m = a.mig[k * P + p];
+        const float4 v = __ldg(reinterpret_cast<const float4*>(prev + k * stride + base));
+        xm.x += m * v.x;
+        xm.y += m * v.y;
+        xm.z += m * v.z;
+        xm.w += m * v.w;
+      }
+      const float F = a.F[p], h = a.h[p], sa = a.sel_a[p], sb = a.sel_b[p];
+      const int N = a.Nc[p];
+      float4 o;
+      if (N <= 0) {
+        // extinction generation: the population's row is cleared
+        o = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+        const float x0 = selected_freq<NEUTRAL>(xm.x, sa, sb, F, h);
+        const float x1 = selected_freq<NEUTRAL>(xm.y, sa, sb, F, h);
+        const float x2 = selected_freq<NEUTRAL>(xm.z, sa, sb, F, h);
+        const float x3 = selected_freq<NEUTRAL>(xm.w, sa, sb, F, h);
+        const bool certain = (x0 == 0.f || (x0 == 1.f && N > 6)) && (x1 == 0.f || (x1 == 1.f && N > 6)) &&
+                             (x2 == 0.f || (x2 == 1.f && N > 6)) && (x3 == 0.f || (x3 == 1.f && N > 6));
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);
+        if (!certain) r = philox(a.seed1, a.seed2, q + 2, g, p, 0);
+        const float Nf = static_cast<float>(N);
+        o.x = static_cast<float>(clampi(drift_lane(r.x, x0, N), 0, N)) / Nf;
+        o.y = static_cast<float>(clampi(drift_lane(r.y, x1, N), 0, N)) / Nf;
+        o.z = static_cast<float>(clampi(drift_lane(r.z, x2, N), 0, N)) / Nf;
+        o.w = static_cast<float>(clampi(drift_lane(r.w, x3, N), 0, N)) / Nf;
+      }
+      *reinterpret_cast<float4*>(next + p * stride + base) = o;
+      if (FLAG && ((a.alive_mask >> p) & 1)) {
+        zero &= (o.x <= 0.f ? 1u : 0u) | (o.y <= 0.f ? 2u : 0u) | (o.z <= 0.f ? 4u : 0u) | (o.w <= 0.f ? 8u : 0u);
+        one &= (o.x >= 1.f ? 1u : 0u) | (o.y >= 1.f ? 2u : 0u) | (o.z >= 1.f ? 4u : 0u) | (o.w >= 1.f ? 8u : 0u);
+      }
+    }
+    if (FLAG) {
+      keep = ~(zero | one) & 0xFu;
+      if (a.check_preserved) {
+        const int4 t = *reinterpret_cast<const int4*>(id_tid + base);
+        keep |= (t.x < 0 ? 1u : 0u) | (t.y < 0 ? 2u : 0u) | (t.z < 0 ? 4u : 0u) | (t.w < 0 ? 8u : 0u);
+      }
+    }
+  } else if (base < total) {
+    // ---- scalar tail (slots past the last whole quad) and the new-mutation fill ----
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+      const int e = base + j;
+      if (e >= total) break;
+      unsigned zero = 1u, one = 1u;
+      if (e < M_in) {
+        for (int p = 0; p < P; ++p) {
+          if (!((a.drift_mask >> p) & 1)) continue;
+          float xm = 0.f;
+          for (int k = 0; k < P; ++k) xm += a.mig[k * P + p] * prev[k * stride + e];
+          const int N = a.Nc[p];
+          float o = 0.f;
+          if (N > 0) {
+            const float xs = selected_freq<NEUTRAL>(xm, a.sel_a[p], a.sel_b[p], a.F[p], a.h[p]);
+            o = static_cast<float>(clampi(drift_tail(a.seed1, a.seed2, e, g, p, xs, N), 0, N)) /
+                static_cast<float>(N);
+          }
+          next[p * stride + e] = o;
+          if (FLAG && ((a.alive_mask >> p) & 1)) {
+            zero &= (o <= 0.f);
+            one &= (o >= 1.f);
+          }
+        }
+        if (FLAG) keep |= ((!(zero | one)) || (a.check_preserved && id_tid[e] < 0)) ? (1u << j) : 0u;
+      } else {
+        // new mutation (add_new_mutations, go_fish_impl.cu:138-145): row p = 1/Nc, others 0
+        const int r = e - M_in;
+        int p = 0;
+        while (p + 1 < P && r >= a.new_offset[p + 1]) ++p;
+        const int tid = r - a.new_offset[p] + 1;
+        for (int k = 0; k < P; ++k) {
+          const float v = (k == p) ? a.new_freq[p] : 0.f;
+          next[k * stride + e] = v;
+          if (FLAG && ((a.alive_mask >> k) & 1)) {
+            zero &= (v <= 0.f);
+            one &= (v >= 1.f);
+          }
+        }
+        id_gp[e] = g | (p << 24);
+        id_tid[e] = tid;
+        if (FLAG) keep |= (!(zero | one)) ? (1u << j) : 0u;
+      }
+    }
+  }
+
+  if (FLAG) {
+    // 8 consecutive threads own the 32 slots of one flag word.
+    const int lane = threadIdx.x & 31;
+    unsigned word = (keep & 0xFu) << ((lane & 7) * 4);
+    word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);
+    word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);
+    word |= __shfl_xor_sync(0xFFFFFFFFu, word, 4);
+    if ((lane & 7) == 0) flags[base >> 5] = word;
+    // survivors of the tile
+    __shared__ unsigned s_warp[kDriftThreads / 32];
+    unsigned c = __popc(keep & 0xFu);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if (lane == 0) s_warp[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned t = 0;
+#pragma unroll
+      for (int w = 0; w < kDriftThreads / 32; ++w) t += s_warp[w];
+      tile_count[blockIdx.x] = t;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// single-block exclusive scan of uint32 counts (replaces cub::DeviceScan, go_fish_impl.cuh:389-391)
+// ------------------------------------------------------------------------------------------------
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_exclusive_kernel(const unsigned* __restrict__ in, unsigned* __restrict__ out, int n, int* total_out) {
+  __shared__ unsigned s_warp[kScanThreads / 32];
+  __shared__ unsigned s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += kScanThreads * kScanItems) {
+    unsigned v[kScanItems];
+    unsigned tsum = 0;
+    const int first = base + threadIdx.x * kScanItems;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      const int idx = first + k;
+      v[k] = (idx < n) ? in[idx] : 0u;
+      tsum += v[k];
+    }
+    unsigned incl = tsum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned w = s_warp[lane];
+      unsigned wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      s_warp[lane] = wi - w;  // exclusive prefix of warp sums
+    }
+    __syncthreads();
+    unsigned run = s_carry + s_warp[warp] + incl - tsum;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      const int idx = first + k;
+      if (idx < n) out[idx] = run;
+      run += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == kScanThreads - 1) s_carry = run;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = static_cast<int>(s_carry);
+}
+
+// ------------------------------------------------------------------------------------------------
+// stable scatter of surviving slots (scatter_arrays, go_fish_impl.cu:147-189), staged through
+// shared memory so that every tile writes its survivors as one contiguous, coalesced run
+// ------------------------------------------------------------------------------------------------
+template <bool PRESERVE>
+__global__ void __launch_bounds__(kDriftThreads)
+    scatter_kernel(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ gp_src,
+                   const int* __restrict__ tid_src, int* __restrict__ gp_dst, int* __restrict__ tid_dst,
+                   const unsigned* __restrict__ flags, const unsigned* __restrict__ tile_offset, long long stride,
+                   int P) {
+  __shared__ unsigned s_words[32];
+  __shared__ unsigned s_prefix[32];
+  __shared__ float s_stage[kTileSlots];
+  const int t = threadIdx.x;
+  const long long tile = blockIdx.x;
+  if (t < 32) {
+    const unsigned w = flags[tile * 32 + t];
+    s_words[t] = w;
+    const unsigned c = __popc(w);
+    unsigned incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (t >= o) incl += y;
+    }
+    s_prefix[t] = incl - c;
+  }
+  __syncthreads();
+  const int w = t >> 3, sh = (t & 7) * 4;
+  const unsigned word = s_words[w];
+  const unsigned nib = (word >> sh) & 0xFu;
+  const int local = static_cast<int>(s_prefix[w] + __popc(word & ((1u << sh) - 1u)));
+  const int count = static_cast<int>(s_prefix[31] + __popc(s_words[31]));
+  const long long out_base = tile_offset[tile];
+  const long long in_base = tile * kTileSlots + 4 * t;
+
+  for (int r = 0; r < P; ++r) {
+    if (nib) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(src + r * stride + in_base));
+      int k = local;
+      if (nib & 1u) s_stage[k++] = v.x;
+      if (nib & 2u) s_stage[k++] = v.y;
+      if (nib & 4u) s_stage[k++] = v.z;
+      if (nib & 8u) s_stage[k++] = v.w;
+    }
+    __syncthreads();
+    for (int k = t; k < count; k += kDriftThreads) dst[r * stride + out_base + k] = s_stage[k];
+    __syncthreads();
+  }
+  int* s_istage = reinterpret_cast<int*>(s_stage);
+  for (int arr = 0; arr < 2; ++arr) {
+    const int* s = arr ? tid_src : gp_src;
+    int* d = arr ? tid_dst : gp_dst;
+    if (nib) {
+      const int4 v = __ldg(reinterpret_cast<const int4*>(s + in_base));
+      int k = local;
+      auto mark = [&](int x) { return (arr && PRESERVE) ? -abs(x) : x; };
+      if (nib & 1u) s_istage[k++] = mark(v.x);
+      if (nib & 2u) s_istage[k++] = mark(v.y);
+      if (nib & 4u) s_istage[k++] = mark(v.z);
+      if (nib & 8u) s_istage[k++] = mark(v.w);
+    }
+    __syncthreads();
+    for (int k = t; k < count; k += kDriftThreads) d[out_base + k] = s_istage[k];
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// state load / read helpers
+// ------------------------------------------------------------------------------------------------
+__global__ void mark_preserved_kernel(int* __restrict__ tid, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x) tid[i] = -abs(tid[i]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// mutation-selection-equilibrium start (initialize_mse and friends, go_fish_impl.cuh:20-71, 201-332)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float mse_density(float i, int N, float F, float h, float s) {
+  return exp(2 * N * s * i * ((2 * h + (1 - 2 * h) * i) * (1 - F) + 2 * F) / (1 + F));
+}
+
+// Trapezoid slices of the MSE integrand from frequency 1 down to 0 (calculate_area + trapezoidal_upper
+// + mse_integrand, go_fish_impl.cuh:24-53).
+__global__ void mse_area_kernel(float* __restrict__ area, int num_freq, float step, int N_ind, float F, float h,
+                                float sa, float sb) {
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < num_freq; id += blockDim.x * gridDim.x) {
+    const float a = static_cast<float>(1.0 - id * step);
+    const float b = a - step;
+    const float s1 = fmaxf(sa * a + sb, -1.f);
+    const float s2 = fmaxf(sa * b + sb, -1.f);
+    const float f1 = mse_density(a, N_ind, F, h, -1 * s1);
+    const float f2 = mse_density(b, N_ind, F, h, -1 * s2);
+    area[id] = step * (f1 + f2) / 2;
+  }
+}
+
+// Deterministic inclusive scan of the slices in double precision, stored reversed as float:
+// integral[id] = sum_{k <= num_freq-1-id} area[k] (the reference scans in float with CUB and then
+// reverses, go_fish_impl.cuh:213-221; its float summation order is not fixed).
+__global__ void __launch_bounds__(1024) mse_integral_kernel(const float* __restrict__ area, float* __restrict__ integral,
+                                                            int num_freq) {
+  __shared__ double s_warp[32];
+  __shared__ double s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0.0;
+  __syncthreads();
+  for (int base = 0; base < num_freq; base += 1024) {
+    const int idx = base + threadIdx.x;
+    const double v = idx < num_freq ? static_cast<double>(area[idx]) : 0.0;
+    double incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const double w = s_warp[lane];
+      double wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      s_warp[lane] = wi - w;
+    }
+    __syncthreads();
+    const double total = s_carry + s_warp[warp] + incl;
+    if (idx < num_freq) integral[num_freq - 1 - idx] = static_cast<float>(total);
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry = total;
+    __syncthreads();
+  }
+}
+
+// Poisson count of mutations in each frequency class (initialize_mse_frequency_array,
+// go_fish_impl.cuh:58-71); counter (0, class, pop, 0).
+__global__ void mse_count_kernel(unsigned* __restrict__ counts, const float* __restrict__ integral, int offset,
+                                 float mu, int N_ind, int Nchrom, float L, float sa, float sb, float F, float h,
+                                 int seed1, int seed2, int pop, int use_integral) {
+  const float mse_total = use_integral ? integral[0] : 0.f;
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < Nchrom - 1; id += blockDim.x * gridDim.x) {
+    const float i = (id + 1.f) / Nchrom;
+    const float j = ((Nchrom - id) + 1.f) / Nchrom;
+    const float s = sa * i + sb;
+    float lambda;
+    if (s == 0) {
+      lambda = 2 * mu * L / i;
+    } else {
+      lambda = 2 * mu * L * (mse_density(i, N_ind, F, h, s) * integral[id]) / (mse_total * i * j);
+    }
+    counts[offset + id] = static_cast<unsigned>(max(pois_draw(lambda, lambda, L * Nchrom, seed1, seed2, 0, id, pop), 0));
+  }
+}
+
+struct MseClassRange {
+  int first_class[kMaxPops + 1];  // global class index where each population's classes start
+  int Nc[kMaxPops];
+};
+
+// Expand class counts into mutation slots (initialize_mse_mutation_array + mse_set_mutID,
+// go_fish_impl.cu:45-70): slot k of class (pop, id) gets frequency (id + 1) / Nc in row pop,
+// 0 in the other rows, and ID (0, pop, +-(k + 1), 0).
+__global__ void mse_fill_kernel(float* __restrict__ freq, int* __restrict__ id_gp, int* __restrict__ id_tid,
+                                const unsigned* __restrict__ starts, int num_classes, int M0, long long stride,
+                                int P, int preserve, const MseClassRange cr) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M0; k += blockDim.x * gridDim.x) {
+    // last class whose start <= k
+    int lo = 0, hi = num_classes - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (static_cast<int>(starts[mid]) <= k) lo = mid; else hi = mid - 1;
+    }
+    int pop = 0;
+    while (pop + 1 < P && lo >= cr.first_class[pop + 1]) ++pop;
+    const int idy = lo - cr.first_class[pop];
+    const float f = (idy + 1.f) / cr.Nc[pop];
+    for (int r = 0; r < P; ++r) freq[r * stride + k] = (r == pop) ? f : 0.f;
+    id_gp[k] = 0 | (pop << 24);
+    id_tid[k] = preserve ? -(k + 1) : (k + 1);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+static long long align_up(long long v, long long a) { return (v + a - 1) / a * a; }
+
+static void release_sim(Engine* e) {
+  for (int b = 0; b < 2; ++b) {
+    if (e->freq[b]) cudaFree(e->freq[b]);
+    if (e->id_gp[b]) cudaFree(e->id_gp[b]);
+    if (e->id_tid[b]) cudaFree(e->id_tid[b]);
+    e->freq[b] = nullptr;
+    e->id_gp[b] = nullptr;
+    e->id_tid[b] = nullptr;
+  }
+  if (e->flags) cudaFree(e->flags);
+  if (e->tile_count) cudaFree(e->tile_count);
+  if (e->tile_offset) cudaFree(e->tile_offset);
+  e->flags = nullptr;
+  e->tile_count = nullptr;
+  e->tile_offset = nullptr;
+  for (auto& pc : e->pending) e->free_events.push_back(pc.event);
+  e->pending.clear();
+  e->capacity = 0;
+  e->active = false;
+}
+
+// Allocate (zeroed) arrays of `cap` slots.  When `keep` > 0, the first `keep` slots of the current
+// buffers are carried over.
+static gf_status set_capacity(Engine* e, long long cap, long long keep) {
+  cap = align_up(std::max<long long>(cap, kSlotAlign), kSlotAlign);
+  if (cap > (1LL << 31) - kSlotAlign) return fail(e, GF_ERR_CAPACITY, "mutation capacity %lld exceeds 2^31 slots", cap);
+  const int P = e->P;
+  float* nf[2] = {nullptr, nullptr};
+  int* ngp[2] = {nullptr, nullptr};
+  int* ntid[2] = {nullptr, nullptr};
+  unsigned *nflags = nullptr, *ncount = nullptr, *noffset = nullptr;
+  const long long ntiles = cap / kTileSlots;
+  cudaError_t err = cudaSuccess;
+  for (int b = 0; b < 2 && err == cudaSuccess; ++b) {
+    err = cudaMallocAsync(&nf[b], sizeof(float) * P * cap, e->stream);
+    if (err == cudaSuccess) err = cudaMallocAsync(&ngp[b], sizeof(int) * cap, e->stream);
+    if (err == cudaSuccess) err = cudaMallocAsync(&ntid[b], sizeof(int) * cap, e->stream);
+  }
+  if (err == cudaSuccess) err = cudaMallocAsync(&nflags, sizeof(unsigned) * (cap / 32), e->stream);
+  if (err == cudaSuccess) err = cudaMallocAsync(&ncount, sizeof(unsigned) * ntiles, e->stream);
+  if (err == cudaSuccess) err = cudaMallocAsync(&noffset, sizeof(unsigned) * ntiles, e->stream);
+  if (err != cudaSuccess) {
+    for (int b = 0; b < 2; ++b) {
+      if (nf[b]) cudaFreeAsync(nf[b], e->stream);
+      if (ngp[b]) cudaFreeAsync(ngp[b], e->stream);
+      if (ntid[b]) cudaFreeAsync(ntid[b], e->stream);
+    }
+    if (nflags) cudaFreeAsync(nflags, e->stream);
+    if (ncount) cudaFreeAsync(ncount, e->stream);
+    cudaGetLastError();
+    return cuda_fail(e, err, "allocating the mutation arrays");
+  }
+  for (int b = 0; b < 2; ++b) {
+    GF_CUDA(e, cudaMemsetAsync(nf[b], 0, sizeof(float) * P * cap, e->stream));
+    GF_CUDA(e, cudaMemsetAsync(ngp[b], 0, sizeof(int) * cap, e->stream));
+    GF_CUDA(e, cudaMemsetAsync(ntid[b], 0, sizeof(int) * cap, e->stream));
+  }
+  if (keep > 0 && e->capacity > 0) {
+    GF_CUDA(e, cudaMemcpy2DAsync(nf[e->cur], sizeof(float) * cap, e->freq[e->cur], sizeof(float) * e->capacity,
+                                 sizeof(float) * keep, P, cudaMemcpyDeviceToDevice, e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(ngp[e->id_cur], e->id_gp[e->id_cur], sizeof(int) * keep, cudaMemcpyDeviceToDevice,
+                               e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(ntid[e->id_cur], e->id_tid[e->id_cur], sizeof(int) * keep, cudaMemcpyDeviceToDevice,
+                               e->stream));
+  }
+  for (int b = 0; b < 2; ++b) {
+    if (e->freq[b]) cudaFreeAsync(e->freq[b], e->stream);
+    if (e->id_gp[b]) cudaFreeAsync(e->id_gp[b], e->stream);
+    if (e->id_tid[b]) cudaFreeAsync(e->id_tid[b], e->stream);
+    e->freq[b] = nf[b];
+    e->id_gp[b] = ngp[b];
+    e->id_tid[b] = ntid[b];
+  }
+  if (e->flags) cudaFreeAsync(e->flags, e->stream);
+  if (e->tile_count) cudaFreeAsync(e->tile_count, e->stream);
+  if (e->tile_offset) cudaFreeAsync(e->tile_offset, e->stream);
+  e->flags = nflags;
+  e->tile_count = ncount;
+  e->tile_offset = noffset;
+  e->capacity = cap;
+  return GF_OK;
+}
+
+static gf_status check_device_fault(Engine* e) {
+  int fault = 0;
+  GF_CUDA(e, cudaMemcpyAsync(&fault, e->d_count + 2, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  if (fault != kFaultNone) {
+    return fail(e, GF_ERR_DEVICE, "device status word reports fault %d (%s)", fault,
+                fault == kFaultCapacity ? "mutation array capacity exceeded" : "bounded wait expired");
+  }
+  return GF_OK;
+}
+
+static gf_status begin_common(Engine* e, const gf_sim_config* c, long long initial_mutations) {
+  if (!c) return fail(e, GF_ERR_INVALID_ARGUMENT, "config is NULL");
+  if (c->num_populations < 1 || c->num_populations > kMaxPops)
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "num_populations %d outside [1, %d]", c->num_populations, kMaxPops);
+  if (!(c->num_sites > 0.f)) return fail(e, GF_ERR_INVALID_ARGUMENT, "num_sites must be > 0");
+  if (c->compact_interval < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "compact_interval must be >= 0");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  release_sim(e);
+  e->P = c->num_populations;
+  e->seed1 = c->seed1;
+  e->seed2 = c->seed2;
+  e->num_sites = c->num_sites;
+  e->compact_interval = c->compact_interval;
+  e->any_preserved = false;
+  e->step_index = 0;
+  e->cur = 0;
+  e->id_cur = 0;
+  const long long want = std::max<long long>({static_cast<long long>(c->reserve_mutations),
+                                               2 * initial_mutations + 65536, 65536});
+  gf_status st = set_capacity(e, want, 0);
+  if (st != GF_OK) return st;
+  GF_CUDA(e, cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream));
+  e->M_upper = initial_mutations;
+  e->M_exact = true;
+  e->active = true;
+  return GF_OK;
+}
+
+// Retire completed survivor-count read-backs, tightening the host's upper bound.
+static void poll_pending(Engine* e, bool wait_all) {
+  while (!e->pending.empty()) {
+    PendingCount& pc = e->pending.front();
+    if (wait_all) {
+      cudaEventSynchronize(pc.event);
+    } else if (cudaEventQuery(pc.event) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    const long long exact = e->h_pinned[pc.slot] + pc.added;
+    if (e->pending.size() == 1 && exact <= e->M_upper) {
+      e->M_upper = exact;
+      e->M_exact = true;
+    }
+    e->free_events.push_back(pc.event);
+    e->pending.pop_front();
+  }
+}
+
+static gf_status get_event(Engine* e, cudaEvent_t* ev) {
+  if (!e->free_events.empty()) {
+    *ev = e->free_events.back();
+    e->free_events.pop_back();
+    return GF_OK;
+  }
+  GF_CUDA(e, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  return GF_OK;
+}
+
+int host_new_mutation_count(int seed1, int seed2, float mu, int Nchrom_e, float num_sites, int generation, int pop) {
+  // calc_new_mutations_Index (go_fish_impl.cuh:454-467), evaluated on the host like the reference.
+  const float lambda = mu * Nchrom_e * num_sites;
+  if (Nchrom_e == 0 || lambda == 0) return 0;
+  return std::max(pois_draw(lambda, lambda, Nchrom_e * num_sites, seed1, seed2, 1, generation, pop), 0);
+}
+
+template <int PT, bool NEUTRAL, bool FLAG>
+static void launch_drift_t(Engine* e, int blocks, int launch_slots, int slot_in, int slot_out, const GenArgs& a) {
+  drift_kernel<PT, NEUTRAL, FLAG><<<blocks, kDriftThreads, 0, e->stream>>>(
+      e->freq[e->cur], e->freq[e->cur ^ 1], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->flags, e->tile_count,
+      e->d_count, e->capacity, slot_in, slot_out, launch_slots, a);
+}
+
+static void launch_drift(Engine* e, int blocks, int launch_slots, int slot_in, int slot_out, const GenArgs& a,
+                         bool single, bool neutral, bool flag) {
+  if (single) {
+    if (neutral) {
+      flag ? launch_drift_t<1, true, true>(e, blocks, launch_slots, slot_in, slot_out, a)
+           : launch_drift_t<1, true, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+    } else {
+      flag ? launch_drift_t<1, false, true>(e, blocks, launch_slots, slot_in, slot_out, a)
+           : launch_drift_t<1, false, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+    }
+  } else {
+    if (neutral) {
+      flag ? launch_drift_t<0, true, true>(e, blocks, launch_slots, slot_in, slot_out, a)
+           : launch_drift_t<0, true, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+    } else {
+      flag ? launch_drift_t<0, false, true>(e, blocks, launch_slots, slot_in, slot_out, a)
+           : launch_drift_t<0, false, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+    }
+  }
+}
+
+static gf_status run_generation(Engine* e, const gf_generation& gen) {
+  const int P = e->P;
+  if (gen.generation < 0 || gen.generation > GF_MAX_GENERATION)
+    return fail(e, GF_ERR_CAPACITY, "generation %d outside [0, %d]", gen.generation, GF_MAX_GENERATION);
+  GenArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.generation = gen.generation;
+  a.num_pops = P;
+  a.seed1 = e->seed1;
+  a.seed2 = e->seed2;
+  bool neutral = true;
+  long long new_total = 0;
+  a.new_offset[0] = 0;
+  for (int p = 0; p < P; ++p) {
+    const gf_population_params& pp = gen.pop[p];
+    if (pp.Nchrom_e < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "generation %d population %d: Nchrom_e < 0", gen.generation, p);
+    if (pp.alive && !pp.drift)
+      return fail(e, GF_ERR_INVALID_ARGUMENT, "generation %d population %d: alive population must be drifted", gen.generation, p);
+    if (pp.drift) a.drift_mask |= 1 << p;
+    if (pp.alive) a.alive_mask |= 1 << p;
+    a.Nc[p] = pp.Nchrom_e;
+    a.F[p] = pp.F;
+    a.h[p] = pp.h;
+    a.sel_a[p] = pp.sel_slope;
+    a.sel_b[p] = pp.sel_intercept;
+    if (pp.drift && (pp.sel_slope != 0.f || pp.sel_intercept != 0.f)) neutral = false;
+    int count = 0;
+    if (pp.mutate && pp.Nchrom_e > 0) {
+      count = host_new_mutation_count(e->seed1, e->seed2, pp.mu, pp.Nchrom_e, e->num_sites, gen.generation, p);
+      a.new_freq[p] = 1.f / pp.Nchrom_e;
+    }
+    new_total += count;
+    a.new_offset[p + 1] = static_cast<int>(std::min<long long>(new_total, 1LL << 30));
+    for (int k = 0; k < P; ++k) a.mig[k * P + p] = gen.migration[k * kMaxPops + p];
+  }
+  for (int p = P; p <= kMaxPops; ++p) a.new_offset[p] = a.new_offset[P];
+  a.new_total = static_cast<int>(new_total);
+  a.flag = (gen.compact || gen.preserve) && e->compact_interval > 0;
+  a.check_preserved = e->any_preserved ? 1 : 0;
+
+  poll_pending(e, false);
+  long long need = e->M_upper + new_total;
+  if (need > e->capacity) {
+    poll_pending(e, true);
+    need = e->M_upper + new_total;
+    if (need > e->capacity) {
+      // exact count, then grow
+      int M = 0;
+      GF_CUDA(e, cudaMemcpyAsync(&M, e->d_count + (e->step_index & 1), sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+      GF_CUDA(e, cudaStreamSynchronize(e->stream));
+      e->M_upper = M;
+      need = M + new_total;
+      if (need > e->capacity) {
+        gf_status st = set_capacity(e, std::max<long long>(need + need / 2, e->capacity * 3 / 2), M);
+        if (st != GF_OK) return st;
+      }
+    }
+  }
+  const int launch_slots = static_cast<int>(align_up(std::max<long long>(need, 1), kTileSlots));
+  const int blocks = launch_slots / kTileSlots;
+  const int slot_in = static_cast<int>(e->step_index & 1);
+  const int slot_out = slot_in ^ 1;
+  launch_drift(e, blocks, launch_slots, slot_in, slot_out, a, P == 1, neutral, a.flag != 0);
+  GF_CUDA(e, cudaGetLastError());
+  e->M_upper = need;
+  for (auto& pc : e->pending) pc.added += new_total;
+
+  if (a.flag) {
+    scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(e->tile_count, e->tile_offset, blocks,
+                                                              e->d_count + slot_out);
+    GF_CUDA(e, cudaGetLastError());
+    const int src = e->cur ^ 1;
+    if (gen.preserve) {
+      scatter_kernel<true><<<blocks, kDriftThreads, 0, e->stream>>>(
+          e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
+          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P);
+      e->any_preserved = true;
+    } else {
+      scatter_kernel<false><<<blocks, kDriftThreads, 0, e->stream>>>(
+          e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
+          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P);
+    }
+    GF_CUDA(e, cudaGetLastError());
+    e->id_cur ^= 1;
+    // asynchronous read-back of the survivor count
+    PendingCount pc;
+    gf_status st = get_event(e, &pc.event);
+    if (st != GF_OK) return st;
+    pc.slot = e->next_slot;
+    e->next_slot = (e->next_slot + 1) % e->pinned_slots;
+    pc.added = 0;
+    GF_CUDA(e, cudaMemcpyAsync(e->h_pinned + pc.slot, e->d_count + slot_out, sizeof(int), cudaMemcpyDeviceToHost,
+                               e->stream));
+    GF_CUDA(e, cudaEventRecord(pc.event, e->stream));
+    if (static_cast<int>(e->pending.size()) >= e->pinned_slots - 1) poll_pending(e, true);
+    e->pending.push_back(pc);
+    e->M_exact = false;
+  } else {
+    e->cur ^= 1;
+  }
+  e->step_index++;
+  return GF_OK;
+}
+
+static gf_status current_count(Engine* e, int* M) {
+  GF_CUDA(e, cudaMemcpyAsync(M, e->d_count + (e->step_index & 1), sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  gf_status st = check_device_fault(e);
+  if (st != GF_OK) return st;
+  poll_pending(e, true);
+  e->M_upper = *M;
+  e->M_exact = true;
+  return GF_OK;
+}
+
+}  // namespace gf
+
+// ==================================================================================================
+// C ABI
+// ==================================================================================================
+using namespace gf;
+
+
+extern "C" {
+
+const char* gf_version(void) { return "0.1.0"; }
+
+const char* gf_status_string(gf_status s) {
+  switch (s) {
+    case GF_OK: return "ok";
+    case GF_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case GF_ERR_CUDA: return "CUDA error";
+    case GF_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case GF_ERR_CAPACITY: return "capacity limit exceeded";
+    case GF_ERR_STATE: return "invalid call order";
+    case GF_ERR_DEVICE: return "device-side fault";
+    case GF_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
+  if (!out) return GF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return GF_ERR_NO_DEVICE;
+  }
+  if (device < 0) {
+    if (cudaGetDevice(&device) != cudaSuccess) return GF_ERR_NO_DEVICE;
+  }
+  if (device >= n) return GF_ERR_NO_DEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return GF_ERR_NO_DEVICE;
+  gf_engine* g = new gf_engine();
+  Engine* e = &g->impl;
+  e->device = device;
+  if (cuda_stream) {
+    e->stream = static_cast<cudaStream_t>(cuda_stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete g;
+      return GF_ERR_CUDA;
+    }
+    e->own_stream = true;
+  }
+  if (cudaMalloc(&e->d_count, sizeof(int) * 4) != cudaSuccess ||
+      cudaMallocHost(&e->h_pinned, sizeof(int) * e->pinned_slots) != cudaSuccess) {
+    if (e->d_count) cudaFree(e->d_count);
+    if (e->own_stream) cudaStreamDestroy(e->stream);
+    delete g;
+    return GF_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream);
+  *out = g;
+  return GF_OK;
+}
+
+void gf_engine_destroy(gf_engine* g) {
+  if (!g) return;
+  Engine* e = &g->impl;
+  cudaSetDevice(e->device);
+  cudaStreamSynchronize(e->stream);
+  release_sim(e);
+  for (auto ev : e->free_events) cudaEventDestroy(ev);
+  if (e->spec_scratch) cudaFree(e->spec_scratch);
+  if (e->spec_in) cudaFree(e->spec_in);
+  if (e->spec_out) cudaFree(e->spec_out);
+  if (e->d_count) cudaFree(e->d_count);
+  if (e->h_pinned) cudaFreeHost(e->h_pinned);
+  if (e->own_stream) cudaStreamDestroy(e->stream);
+  delete g;
+}
+
+const char* gf_engine_last_error(const gf_engine* g) { return g ? g->impl.last_error.c_str() : "engine is NULL"; }
+
+int32_t gf_engine_device(const gf_engine* g) { return g ? g->impl.device : -1; }
+
+gf_status gf_engine_synchronize(gf_engine* g) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  GF_CUDA(e, cudaSetDevice(e->device));
+  return check_device_fault(e);
+}
+
+int32_t gf_new_mutation_count(int32_t seed1, int32_t seed2, float mu, int32_t Nchrom_e, float num_sites,
+                              int32_t generation, int32_t population) {
+  return host_new_mutation_count(seed1, seed2, mu, Nchrom_e, num_sites, generation, population);
+}
+
+gf_status gf_sim_begin_blank(gf_engine* g, const gf_sim_config* c, int32_t start_generation) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  (void)start_generation;
+  return begin_common(e, c, 0);
+}
+
+gf_status gf_sim_begin_from_state(gf_engine* g, const gf_sim_config* c, int32_t start_generation, const float* freq,
+                                  const int32_t* mut_ids, int32_t num_mutations, const uint8_t* extinct,
+                                  int32_t preserve) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  (void)start_generation;
+  (void)extinct;
+  if (num_mutations < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "num_mutations < 0");
+  if (num_mutations > 0 && (!freq || !mut_ids)) return fail(e, GF_ERR_INVALID_ARGUMENT, "freq / mut_ids is NULL");
+  gf_status st = begin_common(e, c, num_mutations);
+  if (st != GF_OK) return st;
+  if (num_mutations == 0) return GF_OK;
+  const int P = e->P;
+  GF_CUDA(e, cudaMemcpy2DAsync(e->freq[e->cur], sizeof(float) * e->capacity, freq, sizeof(float) * num_mutations,
+                               sizeof(float) * num_mutations, P, cudaMemcpyHostToDevice, e->stream));
+  std::vector<int> gp(num_mutations), tid(num_mutations);
+  bool any_neg = false;
+  for (int i = 0; i < num_mutations; ++i) {
+    const int gen0 = mut_ids[4 * i + 0], pop0 = mut_ids[4 * i + 1];
+    if (gen0 < 0 || gen0 > GF_MAX_GENERATION || pop0 < 0 || pop0 >= 128)
+      return fail(e, GF_ERR_CAPACITY, "mutation %d: origin generation %d / population %d outside the packed ID range", i,
+                  gen0, pop0);
+    gp[i] = gen0 | (pop0 << 24);
+    tid[i] = preserve ? -std::abs(mut_ids[4 * i + 2]) : mut_ids[4 * i + 2];
+    any_neg |= tid[i] < 0;
+  }
+  GF_CUDA(e, cudaMemcpyAsync(e->id_gp[e->id_cur], gp.data(), sizeof(int) * num_mutations, cudaMemcpyHostToDevice, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(e->id_tid[e->id_cur], tid.data(), sizeof(int) * num_mutations, cudaMemcpyHostToDevice, e->stream));
+  const int M = num_mutations;
+  GF_CUDA(e, cudaMemcpyAsync(e->d_count, &M, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));  // host vectors go out of scope
+  e->any_preserved = any_neg;
+  return GF_OK;
+}
+
+gf_status gf_sim_begin_mse(gf_engine* g, const gf_sim_config* c, const gf_mse_population* pops, int32_t preserve) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!c || !pops) return fail(e, GF_ERR_INVALID_ARGUMENT, "config / pops is NULL");
+  if (c->num_populations < 1 || c->num_populations > kMaxPops)
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "num_populations %d outside [1, %d]", c->num_populations, kMaxPops);
+  const int P = c->num_populations;
+  MseClassRange cr;
+  std::memset(&cr, 0, sizeof(cr));
+  long long num_classes = 0;
+  for (int p = 0; p < P; ++p) {
+    cr.first_class[p] = static_cast<int>(num_classes);
+    cr.Nc[p] = pops[p].Nchrom_e;
+    if (pops[p].Nchrom_e > 1) num_classes += pops[p].Nchrom_e - 1;
+  }
+  for (int p = P; p <= kMaxPops; ++p) cr.first_class[p] = static_cast<int>(num_classes);
+  GF_CUDA(e, cudaSetDevice(e->device));
+  // class counts, then their exclusive scan; the total is read back once (as the reference does)
+  unsigned* d_counts = nullptr;
+  unsigned* d_starts = nullptr;
+  float* d_area = nullptr;
+  float* d_integral = nullptr;
+  int* d_total = nullptr;
+  const long long ncls = std::max<long long>(num_classes, 1);
+  long long max_nc = 1;
+  for (int p = 0; p < P; ++p) max_nc = std::max<long long>(max_nc, pops[p].Nchrom_e);
+  GF_CUDA(e, cudaMalloc(&d_counts, sizeof(unsigned) * ncls));
+  GF_CUDA(e, cudaMalloc(&d_starts, sizeof(unsigned) * ncls));
+  GF_CUDA(e, cudaMalloc(&d_area, sizeof(float) * max_nc));
+  GF_CUDA(e, cudaMalloc(&d_integral, sizeof(float) * max_nc));
+  GF_CUDA(e, cudaMalloc(&d_total, sizeof(int)));
+  GF_CUDA(e, cudaMemsetAsync(d_counts, 0, sizeof(unsigned) * ncls, e->stream));
+  for (int p = 0; p < P; ++p) {
+    const gf_mse_population& mp = pops[p];
+    const int Nc = mp.Nchrom_e;
+    if (Nc <= 1) continue;
+    const bool selected = (mp.sel_slope != 0.f || mp.sel_intercept != 0.f);
+    if (selected) {
+      mse_area_kernel<<<148, 1024, 0, e->stream>>>(d_area, Nc, 1.0f / Nc, mp.N_ind, mp.F, mp.h, mp.sel_slope,
+                                                    mp.sel_intercept);
+      mse_integral_kernel<<<1, 1024, 0, e->stream>>>(d_area, d_integral, Nc);
+    }
+    mse_count_kernel<<<std::max(1, std::min(1184, (Nc + 255) / 256)), 256, 0, e->stream>>>(
+        d_counts, d_integral, cr.first_class[p], mp.mu, mp.N_ind, Nc, c->num_sites, mp.sel_slope, mp.sel_intercept,
+        mp.F, mp.h, c->seed1, c->seed2, p, selected ? 1 : 0);
+    GF_CUDA(e, cudaGetLastError());
+  }
+  scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(d_counts, d_starts, static_cast<int>(num_classes), d_total);
+  GF_CUDA(e, cudaGetLastError());
+  int M0 = 0;
+  GF_CUDA(e, cudaMemcpyAsync(&M0, d_total, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  gf_status st = begin_common(e, c, M0);
+  if (st == GF_OK && M0 > 0) {
+    mse_fill_kernel<<<std::max(1, std::min(148 * 8, (M0 + 255) / 256)), 256, 0, e->stream>>>(
+        e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], d_starts, static_cast<int>(num_classes), M0,
+        e->capacity, P, preserve ? 1 : 0, cr);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) st = cuda_fail(e, err, "mse_fill_kernel");
+    if (st == GF_OK) {
+      err = cudaMemcpyAsync(e->d_count, &M0, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+      if (err != cudaSuccess) st = cuda_fail(e, err, "cudaMemcpyAsync");
+    }
+    e->any_preserved = preserve != 0;
+  }
+  cudaStreamSynchronize(e->stream);
+  cudaFree(d_counts);
+  cudaFree(d_starts);
+  cudaFree(d_area);
+  cudaFree(d_integral);
+  cudaFree(d_total);
+  return st;
+}
+
+gf_status gf_sim_run(gf_engine* g, const gf_generation* gens, int32_t n) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!e->active) return fail(e, GF_ERR_STATE, "gf_sim_run before gf_sim_begin_*");
+  if (n < 0 || (n > 0 && !gens)) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad generation table");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  for (int i = 0; i < n; ++i) {
+    gf_status st = run_generation(e, gens[i]);
+    if (st != GF_OK) return st;
+  }
+  return GF_OK;
+}
+
+gf_status gf_sim_num_mutations(gf_engine* g, int32_t* out) {
+  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  int M = 0;
+  gf_status st = current_count(e, &M);
+  if (st != GF_OK) return st;
+  *out = M;
+  return GF_OK;
+}
+
+gf_status gf_sim_read_state(gf_engine* g, float* freq_out, int32_t* ids_out, int32_t max_mutations,
+                            int32_t* out_num) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  int M = 0;
+  gf_status st = current_count(e, &M);
+  if (st != GF_OK) return st;
+  if (out_num) *out_num = M;
+  if (M > max_mutations) return fail(e, GF_ERR_CAPACITY, "state holds %d mutations, caller buffer %d", M, max_mutations);
+  if (M == 0) return GF_OK;
+  if (freq_out) {
+    GF_CUDA(e, cudaMemcpy2DAsync(freq_out, sizeof(float) * M, e->freq[e->cur], sizeof(float) * e->capacity,
+                                 sizeof(float) * M, e->P, cudaMemcpyDeviceToHost, e->stream));
+  }
+  if (ids_out) {
+    std::vector<int> gp(M), tid(M);
+    GF_CUDA(e, cudaMemcpyAsync(gp.data(), e->id_gp[e->id_cur], sizeof(int) * M, cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(tid.data(), e->id_tid[e->id_cur], sizeof(int) * M, cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    for (int i = 0; i < M; ++i) {
+      ids_out[4 * i + 0] = gp[i] & 0xFFFFFF;
+      ids_out[4 * i + 1] = gp[i] >> 24;
+      ids_out[4 * i + 2] = tid[i];
+      ids_out[4 * i + 3] = 0;
+    }
+  }
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return GF_OK;
+}
+
+gf_status gf_sim_device_state(gf_engine* g, const float** out_freq, int32_t* out_stride, int32_t* out_num) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  int M = 0;
+  gf_status st = current_count(e, &M);
+  if (st != GF_OK) return st;
+  if (out_freq) *out_freq = e->freq[e->cur];
+  if (out_stride) *out_stride = static_cast<int32_t>(e->capacity);
+  if (out_num) *out_num = M;
+  return GF_OK;
+}
+
+}  // extern "C"

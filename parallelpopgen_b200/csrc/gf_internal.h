@@ -1,0 +1,119 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <deque>
+#include <string>
+#include <vector>
+
+#include "../../include/gofish_b200.h"
+
+namespace gf {
+
+constexpr int kMaxPops = GF_MAX_POPULATIONS;
+// One drift thread owns one quad of mutations (4 consecutive slots) -- the reference's counter layout
+// draws one Philox block per quad.  A tile is the 1024 slots of one 256-thread block, and is also
+// the unit of the compaction scan.
+constexpr int kDriftThreads = 256;
+constexpr int kTileSlots = kDriftThreads * 4;
+// Row stride granularity of the device arrays, in slots: keeps every row 128-byte aligned so quad
+// loads and stores are 16-byte aligned and whole tiles map to whole 32-bit flag words.
+constexpr int kSlotAlign = kTileSlots;
+
+// Device status word codes (bounded waits and range checks report here instead of trapping).
+enum DeviceFault : int {
+  kFaultNone = 0,
+  kFaultCapacity = 1,  // a kernel was asked to write beyond the allocated rows
+  kFaultScanTimeout = 2,
+};
+
+// Per-generation kernel arguments (passed by value; ~1.3 KB).
+struct GenArgs {
+  int generation;
+  int num_pops;
+  int seed1, seed2;
+  int new_total;                 // new mutations appended this generation, all populations
+  int new_offset[kMaxPops + 1];  // exclusive prefix of the per-population new counts
+  float new_freq[kMaxPops];      // 1.f / Nchrom_e, computed on the host as the reference does
+  int Nc[kMaxPops];              // Nchrom_e used by the drift of each population
+  float F[kMaxPops], h[kMaxPops];
+  float sel_a[kMaxPops], sel_b[kMaxPops];
+  int drift_mask;                // bit p: population p is drifted this generation
+  int alive_mask;                // bit p: demography(p, generation) > 0 (compaction flag)
+  int flag;                      // 1: write compaction flags and tile counts for this generation
+  int check_preserved;           // 1: some mutation may carry the preserved mark
+  float mig[kMaxPops * kMaxPops];  // [from * num_pops + to]
+};
+
+struct PendingCount {
+  cudaEvent_t event;
+  int slot;           // index into the pinned readback array
+  long long added;    // new mutations appended after this compaction
+};
+
+struct Engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+
+  // simulation constants
+  bool active = false;
+  int P = 1;
+  int seed1 = 0, seed2 = 0;
+  float num_sites = 0.f;
+  int compact_interval = 0;
+  bool any_preserved = false;
+  long long step_index = 0;  // generations run since begin (selects the count ping-pong slot)
+
+  // device arrays; capacity = row stride in slots
+  long long capacity = 0;
+  float* freq[2] = {nullptr, nullptr};      // [P][capacity]
+  int* id_gp[2] = {nullptr, nullptr};       // origin generation | origin population << 24
+  int* id_tid[2] = {nullptr, nullptr};      // origin threadID; negative = preserved
+  int id_cur = 0;                           // ID buffer of the current generation (swaps on compaction)
+  unsigned* flags = nullptr;                // compaction bitmask, 1 bit per slot
+  unsigned* tile_count = nullptr;           // survivors per tile
+  unsigned* tile_offset = nullptr;          // exclusive prefix of tile_count
+  int cur = 0;                              // buffer holding the current generation
+  int* d_count = nullptr;                   // [0],[1]: mutation count ping-pong; [2]: device status
+  int* h_pinned = nullptr;                  // pinned readback slots
+  int pinned_slots = 64;
+  int next_slot = 0;
+
+  // host tracking of the mutation count
+  long long M_upper = 0;   // upper bound on the current count (exact when nothing is pending)
+  bool M_exact = true;
+  std::deque<PendingCount> pending;
+  std::vector<cudaEvent_t> free_events;
+
+  // spectrum scratch
+  void* spec_scratch = nullptr;
+  size_t spec_scratch_bytes = 0;
+  float* spec_in = nullptr;
+  size_t spec_in_bytes = 0;
+  float* spec_out = nullptr;
+  size_t spec_out_bytes = 0;
+};
+
+// Error helpers: record a message on the engine and return the status.
+gf_status fail(Engine* e, gf_status st, const char* fmt, ...);
+gf_status cuda_fail(Engine* e, cudaError_t err, const char* what);
+
+#define GF_CUDA(e, call)                                      \
+  do {                                                        \
+    cudaError_t _err = (call);                                \
+    if (_err != cudaSuccess) return ::gf::cuda_fail((e), _err, #call); \
+  } while (0)
+
+gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
+
+}  // namespace gf
+
+// The opaque handle of the C ABI.
+struct gf_engine {
+  gf::Engine impl;
+};

@@ -1,0 +1,393 @@
+// Spectrum: population frequency histogram and binomially projected site frequency spectrum
+// (Spectrum::population_frequency_histogram / site_frequency_spectrum, spectrum.cu:74-294 of the
+// reference).
+//
+// Both start from one integer histogram of allele counts j = round(Nc * p) over j in [0, Nc]
+// (population_hist, spectrum.cu:74-83), built with a block-private shared-memory histogram for the
+// low-count bins -- where a neutral SFS puts most of its mass -- and global atomics above them.
+//
+// The SFS then projects the histogram instead of every mutation: sum_i f(p_i) = sum_j c_j f(p_j),
+// O(n * Nc) terms instead of the reference's O(n * M) (binom<1024>, spectrum.cu:111-139).  This is
+// exact because engine frequencies are float(j) / Nc: the histogram kernel recomputes p_j with the
+// same division and flags any mutation whose frequency differs from its class value, in which case
+// the direct per-mutation projection runs instead.  Terms are evaluated in double precision from an
+// exact log-binomial table and reduced in a fixed order, so the result is deterministic (the
+// reference's float atomics are not, spectrum.cu:271-272).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "gf_internal.h"
+
+namespace gf {
+
+constexpr int kHistThreads = 512;
+constexpr int kSmemBins = 40960;  // 160 KB of shared counters per block
+
+// counts[j] for j in [0, Nc]; mismatch[0] != 0 if some frequency is not float(j) / Nc.
+__global__ void __launch_bounds__(kHistThreads)
+    hist_kernel(const float* __restrict__ freq, int M, int Nc, unsigned* __restrict__ counts,
+                unsigned* __restrict__ mismatch, int smem_bins) {
+  extern __shared__ unsigned s_bins[];
+  for (int b = threadIdx.x; b < smem_bins; b += blockDim.x) s_bins[b] = 0;
+  __syncthreads();
+  unsigned bad = 0;
+  const float Nf = static_cast<float>(Nc);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += blockDim.x * gridDim.x) {
+    const float p = freq[i];
+    int j = static_cast<int>(round(Nc * p));
+    if (j < 0) j = 0;
+    if (j > Nc) j = Nc;
+    if (static_cast<float>(j) / Nf != p) bad = 1;
+    if (j < smem_bins) {
+      // warp-aggregated: one shared atomic per distinct bin in the warp
+      const unsigned active = __activemask();
+      const unsigned peers = __match_any_sync(active, j);
+      const int leader = __ffs(peers) - 1;
+      if ((threadIdx.x & 31) == leader) atomicAdd(&s_bins[j], __popc(peers));
+    } else {
+      atomicAdd(&counts[j], 1u);
+    }
+  }
+  if (bad) atomicOr(mismatch, 1u);
+  __syncthreads();
+  for (int b = threadIdx.x; b < smem_bins; b += blockDim.x) {
+    const unsigned v = s_bins[b];
+    if (v) atomicAdd(&counts[b], v);
+  }
+}
+
+// population_frequency_histogram output: out[k] = count of k (k in [1, Nc)), out[0] = count of 0,
+// of Nc (fixed folds into 0) and of the (num_sites - M) monomorphic sites, in uint32 arithmetic as
+// the reference accumulates it (spectrum.cu:78-82).
+__global__ void hist_to_float_kernel(const unsigned* __restrict__ counts, int Nc, unsigned extra0, float* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Nc; k += blockDim.x * gridDim.x) {
+    unsigned v = counts[k];
+    if (k == 0) v = v + counts[Nc] + extra0;
+    out[k] = static_cast<float>(v);
+  }
+}
+
+constexpr int kProjThreads = 256;
+constexpr int kProjChunk = 256;
+
+// Partial projections: block b covers classes [j0, j1) and writes partial[b][k] for k in [0, n].
+__global__ void __launch_bounds__(kProjThreads)
+    project_hist_kernel(const unsigned* __restrict__ counts, int Nc, int n, const double* __restrict__ lgc,
+                        double* __restrict__ partial, int classes_per_block) {
+  __shared__ double s_lp[kProjChunk];
+  __shared__ double s_lq[kProjChunk];
+  __shared__ double s_c[kProjChunk];
+  __shared__ int s_any;
+  const int j0 = blockIdx.x * classes_per_block;
+  const int j1 = min(Nc + 1, j0 + classes_per_block);
+  const float Nf = static_cast<float>(Nc);
+  const int levels = n + 1;
+  const int kper = (levels + kProjThreads - 1) / kProjThreads;  // levels per thread
+  double acc[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) acc[u] = 0.0;
+  for (int c0 = j0; c0 < j1; c0 += kProjChunk) {
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < kProjChunk; t += blockDim.x) {
+      const int j = c0 + t;
+      double c = 0.0, lp = 0.0, lq = 0.0;
+      if (j < j1) {
+        const float p = static_cast<float>(j) / Nf;
+        const unsigned cnt = counts[j];
+        if (cnt && p > 0.f && p < 1.f) {
+          c = static_cast<double>(cnt);
+          lp = log(static_cast<double>(p));
+          lq = log1p(-static_cast<double>(p));
+          s_any = 1;
+        }
+      }
+      s_c[t] = c;
+      s_lp[t] = lp;
+      s_lq[t] = lq;
+    }
+    __syncthreads();
+    if (s_any) {
+      const int cend = min(kProjChunk, j1 - c0);
+      for (int t = 0; t < cend; ++t) {
+        const double c = s_c[t];
+        if (c == 0.0) continue;
+        const double lp = s_lp[t], lq = s_lq[t];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (u >= kper) break;
+          const int k = threadIdx.x + u * kProjThreads;
+          if (k < levels) acc[u] += c * exp(lgc[k] + k * lp + (n - k) * lq);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    if (u >= kper) break;
+    const int k = threadIdx.x + u * kProjThreads;
+    if (k < levels) partial[static_cast<long long>(blockIdx.x) * levels + k] = acc[u];
+  }
+}
+
+// Direct projection of every mutation (used when frequencies are not on the 1/Nc grid).
+__global__ void __launch_bounds__(kProjThreads)
+    project_direct_kernel(const float* __restrict__ freq, int M, int n, const double* __restrict__ lgc,
+                          double* __restrict__ partial, int per_block, unsigned* __restrict__ nonseg) {
+  __shared__ double s_lp[kProjChunk];
+  __shared__ double s_lq[kProjChunk];
+  __shared__ double s_c[kProjChunk];
+  const int i0 = blockIdx.x * per_block;
+  const int i1 = min(M, i0 + per_block);
+  const int levels = n + 1;
+  const int kper = (levels + kProjThreads - 1) / kProjThreads;
+  double acc[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) acc[u] = 0.0;
+  unsigned ns = 0;
+  for (int c0 = i0; c0 < i1; c0 += kProjChunk) {
+    for (int t = threadIdx.x; t < kProjChunk; t += blockDim.x) {
+      const int i = c0 + t;
+      double c = 0.0, lp = 0.0, lq = 0.0;
+      if (i < i1) {
+        const float p = freq[i];
+        if (p > 0.f && p < 1.f) {
+          c = 1.0;
+          lp = log(static_cast<double>(p));
+          lq = log1p(-static_cast<double>(p));
+        } else {
+          ++ns;
+        }
+      }
+      s_c[t] = c;
+      s_lp[t] = lp;
+      s_lq[t] = lq;
+    }
+    __syncthreads();
+    const int cend = min(kProjChunk, i1 - c0);
+    for (int t = 0; t < cend; ++t) {
+      if (s_c[t] == 0.0) continue;
+      const double lp = s_lp[t], lq = s_lq[t];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (u >= kper) break;
+        const int k = threadIdx.x + u * kProjThreads;
+        if (k < levels) acc[u] += exp(lgc[k] + k * lp + (n - k) * lq);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    if (u >= kper) break;
+    const int k = threadIdx.x + u * kProjThreads;
+    if (k < levels) partial[static_cast<long long>(blockIdx.x) * levels + k] = acc[u];
+  }
+  if (ns) atomicAdd(nonseg, ns);
+}
+
+// Fixed-order reduction of the partials into float bins; k == n and every non-segregating mutation
+// fold into bin 0, plus the (num_sites - M) monomorphic sites (spectrum.cu:130-138).
+__global__ void sfs_finish_kernel(const double* __restrict__ partial, int nblocks, int n, double extra0,
+                                  const unsigned* __restrict__ nonseg_count, float* __restrict__ out) {
+  const int levels = n + 1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += blockDim.x * gridDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[static_cast<long long>(b) * levels + k];
+    if (k == 0) {
+      double top = 0.0;
+      for (int b = 0; b < nblocks; ++b) top += partial[static_cast<long long>(b) * levels + n];
+      s += top + extra0 + static_cast<double>(*nonseg_count);
+    }
+    out[k] = static_cast<float>(s);
+  }
+}
+
+// Non-segregating count from the histogram: classes whose p_j is not in (0, 1).
+__global__ void nonseg_from_hist_kernel(const unsigned* __restrict__ counts, int Nc, unsigned* __restrict__ out) {
+  __shared__ unsigned s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  const float Nf = static_cast<float>(Nc);
+  unsigned local = 0;
+  for (int j = threadIdx.x; j <= Nc; j += blockDim.x) {
+    // only j == 0 and j == Nc can leave (0, 1); test them with the same division as the projection
+    if (j != 0 && j != Nc) continue;
+    const float p = static_cast<float>(j) / Nf;
+    if (!(p > 0.f && p < 1.f)) local += counts[j];
+  }
+  atomicAdd(&s, local);
+  __syncthreads();
+  if (threadIdx.x == 0) *out = s;
+}
+
+// ------------------------------------------------------------------------------------------------
+// host drivers
+// ------------------------------------------------------------------------------------------------
+struct SpecLayout {
+  size_t counts_off, mismatch_off, nonseg_off, lgc_off, partial_off, total;
+};
+
+static size_t al256(size_t v) { return (v + 255) / 256 * 256; }
+
+static int hist_blocks(int M) { return std::max(1, std::min(148 * 2, (M + kHistThreads - 1) / kHistThreads)); }
+
+// Histogram into the scratch `counts` ([Nc + 1] uint32) and `mismatch` words.
+static gf_status run_hist(Engine* e, const float* d_freq, int M, int Nc, unsigned* counts, unsigned* mismatch) {
+  GF_CUDA(e, cudaMemsetAsync(counts, 0, sizeof(unsigned) * (Nc + 1), e->stream));
+  GF_CUDA(e, cudaMemsetAsync(mismatch, 0, sizeof(unsigned), e->stream));
+  if (M <= 0) return GF_OK;
+  const int smem_bins = std::min(kSmemBins, Nc + 1);
+  const size_t smem = sizeof(unsigned) * smem_bins;
+  GF_CUDA(e, cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(sizeof(unsigned) * kSmemBins)));
+  hist_kernel<<<hist_blocks(M), kHistThreads, smem, e->stream>>>(d_freq, M, Nc, counts, mismatch, smem_bins);
+  GF_CUDA(e, cudaGetLastError());
+  return GF_OK;
+}
+
+static std::vector<double> log_binomial_row(int n) {
+  std::vector<double> lgc(n + 1);
+  const double ln = std::lgamma(n + 1.0);
+  for (int k = 0; k <= n; ++k) lgc[k] = ln - std::lgamma(k + 1.0) - std::lgamma(n - k + 1.0);
+  return lgc;
+}
+
+gf_status population_histogram_device(Engine* e, const float* d_freq, int M, int Nc, float num_sites, float* d_out) {
+  if (Nc <= 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "Nchrom_e must be > 0");
+  if (M < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "num_mutations < 0");
+  const size_t need = al256(sizeof(unsigned) * (Nc + 1)) + 256;
+  gf_status st = ensure_scratch(e, &e->spec_scratch, &e->spec_scratch_bytes, need);
+  if (st != GF_OK) return st;
+  unsigned* counts = static_cast<unsigned*>(e->spec_scratch);
+  unsigned* mismatch = reinterpret_cast<unsigned*>(static_cast<char*>(e->spec_scratch) + al256(sizeof(unsigned) * (Nc + 1)));
+  st = run_hist(e, d_freq, M, Nc, counts, mismatch);
+  if (st != GF_OK) return st;
+  const unsigned extra0 = static_cast<unsigned>(static_cast<int>(num_sites) - M);
+  hist_to_float_kernel<<<std::max(1, std::min(1024, (Nc + 255) / 256)), 256, 0, e->stream>>>(counts, Nc, extra0, d_out);
+  GF_CUDA(e, cudaGetLastError());
+  return GF_OK;
+}
+
+gf_status site_frequency_spectrum_device(Engine* e, const float* d_freq, int M, int Nc, int n, float num_sites,
+                                         float* d_out) {
+  if (n <= 0 || n >= Nc)
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "sample_size %d out of range [1, population_size %d)", n, Nc);
+  if (M < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "num_mutations < 0");
+  if (n + 1 > 8 * kProjThreads) return fail(e, GF_ERR_CAPACITY, "sample_size %d above the supported %d", n, 8 * kProjThreads - 1);
+  const int levels = n + 1;
+  // partial blocks: enough to fill the GPU, bounded so the partial buffer stays small
+  const int hist_nblocks = std::max(1, std::min(592, (Nc + 1 + 255) / 256));
+  const int classes_per_block = (Nc + 1 + hist_nblocks - 1) / hist_nblocks;
+  const int direct_nblocks = std::max(1, std::min(592, (M + 1023) / 1024));
+  const int nblocks = std::max(hist_nblocks, direct_nblocks);
+  SpecLayout L;
+  L.counts_off = 0;
+  L.mismatch_off = al256(sizeof(unsigned) * (Nc + 1));
+  L.nonseg_off = L.mismatch_off + 256;
+  L.lgc_off = L.nonseg_off + 256;
+  L.partial_off = L.lgc_off + al256(sizeof(double) * levels);
+  L.total = L.partial_off + al256(sizeof(double) * levels * nblocks);
+  gf_status st = ensure_scratch(e, &e->spec_scratch, &e->spec_scratch_bytes, L.total);
+  if (st != GF_OK) return st;
+  char* base = static_cast<char*>(e->spec_scratch);
+  unsigned* counts = reinterpret_cast<unsigned*>(base + L.counts_off);
+  unsigned* mismatch = reinterpret_cast<unsigned*>(base + L.mismatch_off);
+  unsigned* nonseg = reinterpret_cast<unsigned*>(base + L.nonseg_off);
+  double* lgc = reinterpret_cast<double*>(base + L.lgc_off);
+  double* partial = reinterpret_cast<double*>(base + L.partial_off);
+  const std::vector<double> h_lgc = log_binomial_row(n);
+  GF_CUDA(e, cudaMemcpyAsync(lgc, h_lgc.data(), sizeof(double) * levels, cudaMemcpyHostToDevice, e->stream));
+  st = run_hist(e, d_freq, M, Nc, counts, mismatch);
+  if (st != GF_OK) return st;
+  unsigned h_mismatch = 0;
+  GF_CUDA(e, cudaMemcpyAsync(&h_mismatch, mismatch, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  const double extra0 = static_cast<double>(num_sites - M);
+  int used_blocks;
+  if (!h_mismatch) {
+    nonseg_from_hist_kernel<<<1, 256, 0, e->stream>>>(counts, Nc, nonseg);
+    project_hist_kernel<<<hist_nblocks, kProjThreads, 0, e->stream>>>(counts, Nc, n, lgc, partial, classes_per_block);
+    used_blocks = hist_nblocks;
+  } else {
+    GF_CUDA(e, cudaMemsetAsync(nonseg, 0, sizeof(unsigned), e->stream));
+    const int per_block = (M + direct_nblocks - 1) / direct_nblocks;
+    project_direct_kernel<<<direct_nblocks, kProjThreads, 0, e->stream>>>(d_freq, M, n, lgc, partial, std::max(per_block, 1),
+                                                                           nonseg);
+    used_blocks = direct_nblocks;
+  }
+  GF_CUDA(e, cudaGetLastError());
+  sfs_finish_kernel<<<std::max(1, (n + 255) / 256), 256, 0, e->stream>>>(partial, used_blocks, n, extra0, nonseg, d_out);
+  GF_CUDA(e, cudaGetLastError());
+  return GF_OK;
+}
+
+static gf_status stage_input(Engine* e, const float* h_freq, int M, const float** d_freq) {
+  gf_status st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_in), &e->spec_in_bytes,
+                                sizeof(float) * std::max(M, 1));
+  if (st != GF_OK) return st;
+  if (M > 0) GF_CUDA(e, cudaMemcpyAsync(e->spec_in, h_freq, sizeof(float) * M, cudaMemcpyHostToDevice, e->stream));
+  *d_freq = e->spec_in;
+  return GF_OK;
+}
+
+}  // namespace gf
+
+using namespace gf;
+
+extern "C" {
+
+gf_status gf_population_histogram_device(gf_engine* g, const float* d_freq, int32_t M, int32_t Nc, float L, float* d_out) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  GF_CUDA(e, cudaSetDevice(e->device));
+  return population_histogram_device(e, d_freq, M, Nc, L, d_out);
+}
+
+gf_status gf_site_frequency_spectrum_device(gf_engine* g, const float* d_freq, int32_t M, int32_t Nc, int32_t n, float L,
+                                            float* d_out) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  GF_CUDA(e, cudaSetDevice(e->device));
+  return site_frequency_spectrum_device(e, d_freq, M, Nc, n, L, d_out);
+}
+
+gf_status gf_population_histogram(gf_engine* g, const float* freq, int32_t M, int32_t Nc, float L, float* out) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!out || (M > 0 && !freq)) return fail(e, GF_ERR_INVALID_ARGUMENT, "NULL buffer");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  const float* d_freq = nullptr;
+  gf_status st = stage_input(e, freq, M, &d_freq);
+  if (st != GF_OK) return st;
+  st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_out), &e->spec_out_bytes, sizeof(float) * std::max(Nc, 1));
+  if (st != GF_OK) return st;
+  st = population_histogram_device(e, d_freq, M, Nc, L, e->spec_out);
+  if (st != GF_OK) return st;
+  GF_CUDA(e, cudaMemcpyAsync(out, e->spec_out, sizeof(float) * Nc, cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return GF_OK;
+}
+
+gf_status gf_site_frequency_spectrum(gf_engine* g, const float* freq, int32_t M, int32_t Nc, int32_t n, float L, float* out) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!out || (M > 0 && !freq)) return fail(e, GF_ERR_INVALID_ARGUMENT, "NULL buffer");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  const float* d_freq = nullptr;
+  gf_status st = stage_input(e, freq, M, &d_freq);
+  if (st != GF_OK) return st;
+  st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_out), &e->spec_out_bytes, sizeof(float) * std::max(n, 1));
+  if (st != GF_OK) return st;
+  st = site_frequency_spectrum_device(e, d_freq, M, Nc, n, L, e->spec_out);
+  if (st != GF_OK) return st;
+  GF_CUDA(e, cudaMemcpyAsync(out, e->spec_out, sizeof(float) * n, cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return GF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,263 @@
+// Simulation scenarios written only against the public GO_Fish / Sim_Model / Spectrum API.
+//
+// The same source is compiled twice: against the reference's own headers (oracle/ref_driver.cu,
+// nvcc, for the bit-exact oracle run on the GPU) and against this library's drop-in headers
+// (tests/cpp/gofish_driver.cpp, plain g++), so the two programs differ only in the library behind
+// the API.  Each scenario takes key=value parameters and the driver writes every time sample, the
+// mutation IDs and the requested spectra to one binary dump (format in dump_results below; reader in
+// tests/gfdump.py).
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "go_fish.cuh"
+#include "spectrum.h"
+
+#ifdef __CUDACC__
+#define SCN_HD __host__ __device__
+#else
+#define SCN_HD
+#endif
+
+namespace scn {
+
+struct Args {
+  std::map<std::string, std::string> kv;
+  Args(int argc, char** argv, int first) {
+    for (int i = first; i < argc; ++i) {
+      std::string s(argv[i]);
+      const size_t eq = s.find('=');
+      if (eq != std::string::npos) kv[s.substr(0, eq)] = s.substr(eq + 1);
+    }
+  }
+  double num(const char* k, double def) const {
+    auto it = kv.find(k);
+    return it == kv.end() ? def : std::strtod(it->second.c_str(), nullptr);
+  }
+  long long integer(const char* k, long long def) const {
+    auto it = kv.find(k);
+    return it == kv.end() ? def : std::strtoll(it->second.c_str(), nullptr, 0);
+  }
+  std::string str(const char* k, const char* def) const {
+    auto it = kv.find(k);
+    return it == kv.end() ? std::string(def) : it->second;
+  }
+};
+
+// take a time sample every `k` generations after `start` (and never at `start` itself)
+struct every_k {
+  int k;
+  int start;
+  every_k(int k = 0, int start = 0) : k(k), start(start) {}
+  bool operator()(const int g) const { return k > 0 && g > start && ((g - start) % k) == 0; }
+};
+
+// Three populations: pop 0 is the ancestor (N0 individuals), pop 1 splits off at split1 and pop 2 at
+// split2, each founded by N0 individuals drawn from pop 0 and growing logistically at `rate` to its
+// own carrying capacity.
+struct split_demography {
+  int N0;
+  float rate;
+  int split1, split2;
+  int K0, K1, K2;
+  SCN_HD int logistic(int K, int t) const {
+    const float term = expf(rate * t);
+    return (int)roundf(static_cast<float>(K) * N0 * term / (K + N0 * (term - 1)));
+  }
+  SCN_HD int operator()(const int pop, const int gen) const {
+    if (pop == 0) return logistic(K0, gen);
+    if (pop == 1) return gen >= split1 ? logistic(K1, gen - split1) : 0;
+    return gen >= split2 ? logistic(K2, gen - split2) : 0;
+  }
+};
+
+// At a population's split generation all of its chromosomes come from pop 0; otherwise existing
+// populations exchange migrants symmetrically at rate m.
+struct split_migration {
+  float m;
+  int split1, split2;
+  SCN_HD bool exists(int pop, int gen) const { return pop == 0 || (pop == 1 ? gen >= split1 : gen >= split2); }
+  SCN_HD bool founding(int pop, int gen) const { return (pop == 1 && gen == split1) || (pop == 2 && gen == split2); }
+  SCN_HD float operator()(const int from, const int to, const int gen) const {
+    if (!exists(to, gen)) return from == to ? 1.f : 0.f;
+    if (founding(to, gen)) return from == 0 ? 1.f : 0.f;
+    if (!exists(from, gen) || founding(from, gen)) return 0.f;
+    int live = 0;
+    for (int p = 0; p < 3; ++p) live += (exists(p, gen) && !founding(p, gen)) ? 1 : 0;
+    if (from == to) return 1.f - (live - 1) * m;
+    return m;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// scenario "wf": one population (or several identical ones), constant size, constant selection
+// ---------------------------------------------------------------------------------------------
+inline void scenario_wf(GO_Fish::allele_trajectories& a, const Args& args) {
+  using namespace Sim_Model;
+  a.sim_input_constants.seed1 = static_cast<int>(args.integer("seed1", 0xbeef));
+  a.sim_input_constants.seed2 = static_cast<int>(args.integer("seed2", 0xdecaf));
+  a.sim_input_constants.num_generations = static_cast<int>(args.integer("gens", 1000));
+  a.sim_input_constants.num_sites = static_cast<float>(args.num("L", 2e7));
+  a.sim_input_constants.num_populations = static_cast<int>(args.integer("pops", 1));
+  a.sim_input_constants.init_mse = args.integer("mse", 1) != 0;
+  a.sim_input_constants.compact_interval = static_cast<int>(args.integer("compact", 35));
+  const int P = a.sim_input_constants.num_populations;
+  F_mu_h_constant mutation(static_cast<float>(args.num("mu", 1e-9)));
+  F_mu_h_constant inbreeding(static_cast<float>(args.num("F", 0.0)));
+  demography_constant demography(static_cast<int>(args.integer("N", 10000)));
+  migration_constant_equal migration(static_cast<float>(args.num("m", 0.0)), P);
+  selection_constant selection(static_cast<float>(args.num("gamma", 0.0)), demography, inbreeding);
+  F_mu_h_constant dominance(static_cast<float>(args.num("h", 0.5)));
+  every_k sample(static_cast<int>(args.integer("sample_every", 0)), 0);
+  GO_Fish::run_sim(a, mutation, demography, migration, selection, inbreeding, dominance, bool_off(), sample);
+}
+
+// ---------------------------------------------------------------------------------------------
+// scenario "compilation": two inbred populations (N = 1000, F = 1) with migration 0.005 start
+// blank, run a burn-in with weakly deleterious mutations (s = -1/1000), then continue for `gens2`
+// generations from the burn-in's final sample with beneficial selection (s = +20/1000) in
+// population 1, sampling the starting generation.
+// ---------------------------------------------------------------------------------------------
+inline void scenario_compilation(GO_Fish::allele_trajectories& a, const Args& args) {
+  using namespace Sim_Model;
+  a.sim_input_constants.seed1 = static_cast<int>(args.integer("seed1", 0xbeeff00d));
+  a.sim_input_constants.seed2 = static_cast<int>(args.integer("seed2", 0xdecafbad));
+  a.sim_input_constants.num_sites = static_cast<float>(args.num("L", 2e8));
+  a.sim_input_constants.num_populations = 2;
+  a.sim_input_constants.init_mse = false;
+  F_mu_h_constant mutation(1e-9f);
+  F_mu_h_constant inbreeding(1.f);
+  demography_constant demography(1000);
+  migration_constant_equal migration(static_cast<float>(args.num("m", 0.005)), 2);
+  selection_constant deleterious(-1.f / 1000.f);
+  F_mu_h_constant dominance(0.f);
+  a.sim_input_constants.compact_interval = static_cast<int>(args.integer("compact", 100));
+  a.sim_input_constants.num_generations = static_cast<int>(args.integer("gens1", 20000));
+  GO_Fish::run_sim(a, mutation, demography, migration, deleterious, inbreeding, dominance, bool_off(), bool_off());
+  bool_pulse<bool_off, bool_on> sample_start(bool_off(), bool_on(), 0, a.sim_input_constants.num_generations);
+  a.sim_input_constants.num_generations = static_cast<int>(args.integer("gens2", 1000));
+  a.sim_input_constants.prev_sim_sample = 0;
+  selection_constant beneficial(20.f / 1000.f);
+  selection_population_specific<selection_constant, selection_constant> selection(deleterious, beneficial, 1);
+  GO_Fish::run_sim(a, mutation, demography, migration, selection, inbreeding, dominance, bool_off(), sample_start, a);
+}
+
+// ---------------------------------------------------------------------------------------------
+// scenario "split3": three populations split from an ancestor, grow logistically, exchange
+// migrants, and switch selection from gamma1 to gamma2 at `switch_gen`; population 2 is inbred.
+// ---------------------------------------------------------------------------------------------
+inline void scenario_split3(GO_Fish::allele_trajectories& a, const Args& args) {
+  using namespace Sim_Model;
+  a.sim_input_constants.seed1 = static_cast<int>(args.integer("seed1", 0xbeef));
+  a.sim_input_constants.seed2 = static_cast<int>(args.integer("seed2", 0xdecaf));
+  a.sim_input_constants.num_generations = static_cast<int>(args.integer("gens", 5000));
+  a.sim_input_constants.num_sites = static_cast<float>(args.num("L", 2e8));
+  a.sim_input_constants.num_populations = 3;
+  a.sim_input_constants.init_mse = args.integer("mse", 1) != 0;
+  a.sim_input_constants.compact_interval = static_cast<int>(args.integer("compact", 35));
+  split_demography dem;
+  dem.N0 = static_cast<int>(args.integer("N0", 10000));
+  dem.rate = static_cast<float>(args.num("rate", 0.005));
+  dem.split1 = static_cast<int>(args.integer("split1", 1));
+  dem.split2 = static_cast<int>(args.integer("split2", 2000));
+  dem.K0 = static_cast<int>(args.integer("K0", 100000));
+  dem.K1 = static_cast<int>(args.integer("K1", 200000));
+  dem.K2 = static_cast<int>(args.integer("K2", 500000));
+  split_migration mig;
+  mig.m = static_cast<float>(args.num("m", 1e-4));
+  mig.split1 = dem.split1;
+  mig.split2 = dem.split2;
+  F_mu_h_constant mutation(static_cast<float>(args.num("mu", 1e-9)));
+  F_mu_h_population_specific<F_mu_h_constant, F_mu_h_constant> inbreeding(
+      F_mu_h_constant(0.f), F_mu_h_constant(static_cast<float>(args.num("F2", 0.1))), 2);
+  selection_piecewise<selection_constant, selection_constant> selection(
+      selection_constant(static_cast<float>(args.num("gamma1", -5.0)), dem, inbreeding),
+      selection_constant(static_cast<float>(args.num("gamma2", 2.0)), dem, inbreeding),
+      static_cast<int>(args.integer("switch_gen", 3000)));
+  F_mu_h_constant dominance(static_cast<float>(args.num("h", 0.3)));
+  every_k sample(static_cast<int>(args.integer("sample_every", 500)), 0);
+  GO_Fish::run_sim(a, mutation, dem, mig, selection, inbreeding, dominance, bool_off(), sample);
+}
+
+inline bool run_scenario(const std::string& name, GO_Fish::allele_trajectories& a, const Args& args) {
+  if (name == "wf") scenario_wf(a, args);
+  else if (name == "compilation") scenario_compilation(a, args);
+  else if (name == "split3") scenario_split3(a, args);
+  else return false;
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// binary dump: int32 little-endian words and float32 arrays
+//   'GFD1' P S
+//   per sample: generation M Nc[P] extinct[P] freq[P*M]
+//   A ids[A*4]
+//   K, then K spectra: sample pop kind(0 = SFS, 1 = histogram) n len values[len]
+// ---------------------------------------------------------------------------------------------
+inline void put(FILE* f, int32_t v) { std::fwrite(&v, sizeof(v), 1, f); }
+
+inline void dump_results(GO_Fish::allele_trajectories& a, const Args& args, const char* path) {
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    std::perror(path);
+    std::exit(2);
+  }
+  const int P = a.num_populations();
+  const int S = a.num_time_samples();
+  std::fwrite("GFD1", 1, 4, f);
+  put(f, P);
+  put(f, S);
+  for (int s = 0; s < S; ++s) {
+    const int M = a.num_mutations_time_sample(s);
+    put(f, a.sampled_generation(s));
+    put(f, M);
+    for (int p = 0; p < P; ++p) put(f, a.effective_number_of_chromosomes(s, p));
+    for (int p = 0; p < P; ++p) put(f, a.extinct(s, p) ? 1 : 0);
+    std::vector<float> row(static_cast<size_t>(M));
+    for (int p = 0; p < P; ++p) {
+      for (int i = 0; i < M; ++i) row[i] = a.frequency(s, p, i);
+      if (M) std::fwrite(row.data(), sizeof(float), M, f);
+    }
+  }
+  const int A = a.maximal_num_mutations();
+  put(f, A);
+  for (int i = 0; i < A; ++i) {
+    const GO_Fish::mutID id = a.mutation_ID(i);
+    put(f, id.origin_generation);
+    put(f, id.origin_population);
+    put(f, id.origin_threadID);
+    put(f, id.reserved);
+  }
+  const int n = static_cast<int>(args.integer("sfs_n", 0));
+  const bool hist = args.integer("hist", 0) != 0;
+  std::vector<std::vector<int>> specs;
+  for (int s = 0; s < S; ++s)
+    for (int p = 0; p < P; ++p) {
+      const int Nc = a.effective_number_of_chromosomes(s, p);
+      if (Nc <= 1) continue;
+      if (n > 0 && n < Nc) specs.push_back({s, p, 0, n});
+      if (hist) specs.push_back({s, p, 1, Nc});
+    }
+  put(f, static_cast<int32_t>(specs.size()));
+  for (const auto& sp : specs) {
+    Spectrum::SFS sfs;
+    if (sp[2] == 0) Spectrum::site_frequency_spectrum(sfs, a, sp[0], sp[1], sp[3]);
+    else Spectrum::population_frequency_histogram(sfs, a, sp[0], sp[1]);
+    const int len = sfs.sample_size[0];
+    put(f, sp[0]);
+    put(f, sp[1]);
+    put(f, sp[2]);
+    put(f, sp[3]);
+    put(f, len);
+    std::fwrite(sfs.frequency_spectrum, sizeof(float), len, f);
+  }
+  std::fclose(f);
+}
+
+}  // namespace scn

@@ -1,0 +1,210 @@
+"""GPU parity of the sm_100a engine against the reference run on the same GPU (oracle/_ref) and the CPU
+oracle (oracle/).
+
+Bar: bit-exact against the reference for every integer allele count, frequency, mutation ID and
+histogram bin; the projected SFS within 2e-4 relative per bin of the reference (whose float atomics
+are order-dependent) and within 1e-5 of the oracle's double-precision projection.  Against the CPU
+oracle, drawn counts agree except for draws near a rounding boundary: CUDA's fast-math normcdfinv
+carries a few 1e-5 of relative error, which the oracle's double-precision inverse does not, so a
+normal-branch draw with standard deviation sd lands one count apart with probability ~1e-5 * sd.
+The tolerance is: every difference is one count, and at most 1% of draws differ.
+"""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gfdump import Dump
+from parallelpopgen_b200 import ConstantModel, Engine, constant_generations
+
+import oracle.oracle as orc  # noqa: E402  (checker)
+
+pytestmark = pytest.mark.gpu
+
+SEED1, SEED2 = 0xBEEF, 0xDECAF
+
+
+def run_engine_one_generation(freq: np.ndarray, *, N: int, F=0.0, h=0.5, s=0.0, slope=0.0, gen=1,
+                              seed1=SEED1, seed2=SEED2) -> np.ndarray:
+    with Engine() as e:
+        e.begin_from_state(freq, None, seed1=seed1, seed2=seed2, num_sites=1e6, compact_interval=0)
+        model = ConstantModel(N=1, F=F, h=h, s=s)
+        g = constant_generations(model, gen, 1, compact_interval=0, mutate=False)
+        g["pop"]["Nchrom_e"][:, 0] = N
+        g["pop"]["sel_slope"][:, 0] = slope
+        e.run(g)
+        out, _ = e.read_state(with_ids=False)
+    return out[0]
+
+
+def freq_grid(N: int, M: int, rng: np.random.Generator) -> np.ndarray:
+    """Frequencies j/N (engine values) covering lost, fixed, rare, common and near-fixed classes."""
+    j = np.concatenate([
+        np.array([0, 1, 2, 3, N - 3, N - 2, N - 1, N, N // 2]),
+        rng.integers(0, N + 1, size=M - 9),
+        rng.integers(0, min(N, 12) + 1, size=0),
+    ])[:M]
+    return (j.astype(np.float32) / np.float32(N)).astype(np.float32)
+
+
+DRIFT_CASES = [
+    # N, F, h, s, slope, M
+    (20000, 0.0, 0.5, 0.0, 0.0, 200003),
+    (20000, 0.0, 0.5, -0.00025, 0.0, 100001),
+    (400000, 0.0, 0.5, -0.0000125, 0.0, 200002),
+    (1000, 1.0, 0.0, -0.001, 0.0, 50001),
+    (1000, 0.1, 0.3, 0.002, 0.0, 50000),
+    (99, 0.0, 0.5, 0.0, 0.0, 20003),
+    (50, 0.0, 0.2, -0.05, 0.0, 20001),
+    (100, 0.0, 0.5, 0.01, 0.0, 20002),
+    (2000, 0.0, 0.5, -0.001, 0.004, 40001),
+]
+
+
+@pytest.mark.parametrize("N,F,h,s,slope,M", DRIFT_CASES)
+def test_one_generation_matches_reference_kernel(ref_driver, tmp_path, N, F, h, s, slope, M):
+    """Same input row through the reference's migration_selection_drift and the fused kernel."""
+    rng = np.random.default_rng(N * 7 + M)
+    x = freq_grid(N, M, rng)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        f.write(np.int32(M).tobytes())
+        f.write(x.tobytes())
+    out = tmp_path / "out.bin"
+    args = [f"N={N}", f"F={F}", f"h={h}", f"s={s}", f"slope={slope}", "gen=7", f"seed1={SEED1}", f"seed2={SEED2}"]
+    subprocess.run([str(ref_driver), "drift1", str(inp), str(out), *args], check=True)
+    ref = np.fromfile(out, dtype=np.float32)
+    mine = run_engine_one_generation(x, N=N, F=F, h=h, s=s, slope=slope, gen=7)
+    bad = np.flatnonzero(ref.view(np.uint32) != mine.view(np.uint32))
+    assert bad.size == 0, f"{bad.size} of {M} slots differ; first {bad[:5]}: ref {ref[bad[:5]]} mine {mine[bad[:5]]}"
+
+
+@pytest.mark.parametrize("N,F,h,s,slope,M", DRIFT_CASES[:6])
+def test_one_generation_matches_oracle(N, F, h, s, slope, M):
+    rng = np.random.default_rng(N * 11 + M)
+    x = freq_grid(N, M, rng)
+    mine = run_engine_one_generation(x, N=N, F=F, h=h, s=s, slope=slope, gen=3)
+    ref = orc.drift(x, generation=3, seed1=SEED1, seed2=SEED2, Nc=N, F=F, h=h, sel_intercept=s, sel_slope=slope)[0]
+    cm = np.rint(mine.astype(np.float64) * N)
+    cr = np.rint(ref.astype(np.float64) * N)
+    diff = np.abs(cm - cr)
+    assert diff.max() <= 1, f"max count difference {diff.max()}"
+    assert (diff > 0).mean() <= 1e-2, f"{(diff > 0).sum()} of {M} draws differ"
+
+
+def run_driver(driver: Path, scenario: str, out: Path, args: list[str]) -> Dump:
+    r = subprocess.run([str(driver), scenario, str(out), *args], check=True, capture_output=True, text=True)
+    return Dump(out)
+
+
+def assert_dumps_equal(a: Dump, b: Dump, sfs_rtol=2e-4):
+    assert a.P == b.P
+    assert len(a.samples) == len(b.samples)
+    for sa, sb in zip(a.samples, b.samples):
+        assert sa["generation"] == sb["generation"]
+        assert sa["M"] == sb["M"], f"generation {sa['generation']}: {sa['M']} vs {sb['M']} mutations"
+        assert np.array_equal(sa["Nc"], sb["Nc"]) and np.array_equal(sa["extinct"], sb["extinct"])
+        bad = np.flatnonzero(sa["freq"].view(np.uint32).ravel() != sb["freq"].view(np.uint32).ravel())
+        assert bad.size == 0, f"generation {sa['generation']}: {bad.size} frequencies differ"
+    assert np.array_equal(a.ids, b.ids)
+    assert a.spectra.keys() == b.spectra.keys()
+    for k in a.spectra:
+        x, y = a.spectra[k].astype(np.float64), b.spectra[k].astype(np.float64)
+        if k[2] == "hist":
+            assert np.array_equal(x, y), k
+        else:
+            np.testing.assert_allclose(x, y, rtol=sfs_rtol, atol=1e-3, err_msg=str(k))
+
+
+WF_CFG1 = ["N=10000", "L=2e7", "gens=1000", "compact=35", "mse=1", "sfs_n=100", "hist=1", "sample_every=250"]
+
+
+def test_cfg1_neutral_matches_reference(gofish_driver, ref_driver, tmp_path):
+    """1 pop, N=1e4, L=2e7, neutral, MSE start, 1000 generations (the CPU-runnable configuration)."""
+    mine = run_driver(gofish_driver, "wf", tmp_path / "mine.bin", WF_CFG1)
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *WF_CFG1], check=True, capture_output=True)
+    ref = Dump(tmp_path / "ref.bin")
+    assert mine.samples[-1]["M"] > 1000
+    assert_dumps_equal(mine, ref)
+
+
+@pytest.mark.parametrize("extra", [
+    ["gamma=-10", "h=0.5", "mse=0", "gens=3000", "compact=25"],
+    ["gamma=5", "h=0.3", "F=0.1", "mse=0", "gens=2000", "compact=10"],
+    ["N=40", "mse=0", "gens=3000", "L=2e8"],
+    ["pops=2", "m=0.01", "mse=1", "gens=500"],
+])
+def test_wf_variants_match_reference(gofish_driver, ref_driver, tmp_path, extra):
+    args = ["N=5000", "L=1e7", "sfs_n=50", "hist=1", "sample_every=0", *extra]
+    mine = run_driver(gofish_driver, "wf", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *args], check=True, capture_output=True)
+    assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
+
+
+def test_resume_and_preserve_match_reference(gofish_driver, ref_driver, tmp_path):
+    """Two inbred populations: blank start, burn-in, resume from the burn-in sample, sampling the start."""
+    args = ["gens1=3000", "gens2=500", "L=2e7", "sfs_n=20", "hist=1"]
+    mine = run_driver(gofish_driver, "compilation", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "compilation", str(tmp_path / "ref.bin"), *args], check=True,
+                   capture_output=True)
+    assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
+
+
+def test_split3_matches_reference(gofish_driver, ref_driver, tmp_path):
+    """Three populations with splits, logistic growth, migration, piecewise selection, inbreeding."""
+    args = ["L=2e6", "gens=700", "split2=300", "switch_gen=400", "sample_every=100", "K0=20000", "K1=30000",
+            "K2=40000", "N0=5000", "mse=0", "sfs_n=30", "hist=1"]
+    mine = run_driver(gofish_driver, "split3", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "split3", str(tmp_path / "ref.bin"), *args], check=True,
+                   capture_output=True)
+    assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
+
+
+def test_compaction_matches_oracle():
+    """Stable compaction of a state with lost, fixed and preserved slots equals the oracle's."""
+    rng = np.random.default_rng(5)
+    P, M, N = 2, 30001, 1000
+    j = rng.integers(0, N + 1, size=(P, M))
+    j[:, rng.random(M) < 0.3] = 0
+    j[:, rng.random(M) < 0.1] = N
+    freq = (j.astype(np.float32) / np.float32(N)).astype(np.float32)
+    ids = np.zeros((M, 4), dtype=np.int32)
+    ids[:, 0] = rng.integers(0, 5000, size=M)
+    ids[:, 1] = rng.integers(0, P, size=M)
+    ids[:, 2] = np.arange(1, M + 1)
+    ids[rng.random(M) < 0.05, 2] *= -1
+    with Engine() as e:
+        e.begin_from_state(freq, ids, seed1=1, seed2=2, num_sites=1e7, compact_interval=1)
+        model = ConstantModel(N=N // 2, P=P)
+        g = constant_generations(model, 1, 1, compact_interval=1, mutate=False)
+        g["pop"]["drift"][:, :P] = 0   # no drift: compaction of the loaded state only
+        g["pop"]["alive"][:, :P] = 0
+        g["pop"]["alive"][:, 0] = 0
+        e.run(g)
+        got_f, got_ids = e.read_state()
+    # with no alive population nothing is segregating: only preserved slots survive
+    want_f, want_ids = orc.compact(freq, ids, alive=[0, 0])
+    assert np.array_equal(got_ids, want_ids)
+    assert np.array_equal(got_f.view(np.uint32), want_f.view(np.uint32))
+
+
+def test_histogram_and_sfs_match_oracle():
+    rng = np.random.default_rng(9)
+    Nc, M, L = 20000, 300000, 2e7
+    j = np.minimum(rng.geometric(0.0005, size=M), Nc)
+    j[rng.random(M) < 0.02] = 0
+    x = (j.astype(np.float32) / np.float32(Nc)).astype(np.float32)
+    with Engine() as e:
+        h = e.population_histogram(x, Nc, L)
+        np.testing.assert_array_equal(h, orc.histogram(x, Nc, L))
+        for n in (2, 100, 1000):
+            got = e.site_frequency_spectrum(x, Nc, n, L).astype(np.float64)
+            want = orc.sfs(x, n, L)
+            np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-4)
+        # frequencies off the 1/Nc grid take the direct projection
+        y = rng.random(5000).astype(np.float32)
+        got = e.site_frequency_spectrum(y, Nc, 64, L).astype(np.float64)
+        np.testing.assert_allclose(got, orc.sfs(y, 64, L), rtol=1e-5, atol=1e-4)
