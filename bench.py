@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Headline benchmark: GO_Fish plain engine, mutation-generations/s on B200.
+
+Workload (one "step"): the large single-population configuration -- N = 200,000 diploids
+(Nchrom_e = 400,000), mu = 1e-9, h = 0.5, F = 0, L = 5e8 sites with purifying selection
+gamma = 2Ns = -10 on half of the sites and the other half neutral, mutation-selection-equilibrium
+start, 10,000 generations with compaction every 25, then the site frequency spectrum of a sample of
+n = 1,000.  Selection acts per (population, generation, frequency) in GO_Fish, so "gamma on 50% of
+new mutations" is run exactly as two independent simulations of L = 2.5e8 sites each (neutral and
+gamma = -10), which is the same model under the Poisson-random-field independence of sites.
+
+Metric: mutation-generations/s = sum over generations of the mutation slots the drift pass updated,
+divided by device time.  `value` times the whole step on the device (MSE initialization, every
+generation, compactions, SFS) with the engine's inputs built on the host beforehand; `e2e` repeats the
+step through the C ABI with host buffers, reading the final frequencies, mutation IDs and the SFS back
+to host memory inside the timed region.  Synthetic inputs: the simulation draws its own state.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the CPU restatement of the same per-generation update (oracle/, all host
+threads) on a bounded sample of the same workload; the reference ships no CPU path of its own.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_IND = 200_000
+MU = 1e-9
+L_HALF = 2.5e8
+GENS = 10_000
+COMPACT = 25
+SFS_N = 1000
+GAMMA_SEL = -10.0
+H = 0.5
+SEED1, SEED2 = 0xBEEF, 0xDECAF
+ALG_BYTES_PER_MUTGEN = 8  # P = 1: read one fp32 frequency, write one fp32 frequency
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in out.stdout.strip().split(",")]
+                if len(f) >= 7:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------------------------
+# B200 arm
+# ------------------------------------------------------------------------------------------------
+def build_halves(rank: int, gens_per_sim: int = GENS):
+    from parallelpopgen_b200 import ConstantModel, constant_generations
+    halves = []
+    for k, gamma in enumerate((0.0, GAMMA_SEL)):
+        s = ConstantModel.s_from_gamma(gamma, N_IND, 0.0) if gamma else 0.0
+        model = ConstantModel(N=N_IND, F=0.0, h=H, s=s, mu=MU)
+        gens = constant_generations(model, 1, gens_per_sim, COMPACT)
+        halves.append({"model": model, "gens": gens, "seed1": SEED1 + 2 * (2 * rank + k), "seed2": SEED2 - 2 * (2 * rank + k)})
+    return halves
+
+
+def run_b200(args, rank, local_rank, world):
+    import torch
+    from parallelpopgen_b200 import Engine
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    eng = Engine(device=local_rank, stream=stream.cuda_stream)
+    halves = build_halves(rank, args.gens)
+    Nc = halves[0]["model"].Nchrom_e
+    d_sfs = torch.empty(SFS_N, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    reserve = 12_000_000
+
+    def device_step():
+        """The step on device-resident state; returns mutation-generations."""
+        mg = 0.0
+        for hv in halves:
+            eng.begin_mse(hv["model"].mse_pops(), seed1=hv["seed1"], seed2=hv["seed2"], num_sites=L_HALF,
+                          compact_interval=COMPACT, reserve=reserve)
+            eng.run(hv["gens"])
+            d_freq, stride, M = eng.device_state()
+            eng.site_frequency_spectrum_device(d_freq, M, Nc, SFS_N, L_HALF, d_sfs.data_ptr())
+            mg += eng.stats()["mutation_generations"]
+        return mg
+
+    def e2e_step():
+        """The step through the C ABI with host buffers: final frequencies, IDs and SFS to host."""
+        mg = 0.0
+        h2d = d2h = 0
+        for hv in halves:
+            eng.begin_mse(hv["model"].mse_pops(), seed1=hv["seed1"], seed2=hv["seed2"], num_sites=L_HALF,
+                          compact_interval=COMPACT, reserve=reserve)
+            eng.run(hv["gens"])
+            h2d += hv["gens"].nbytes
+            freq, ids = eng.read_state(with_ids=True)
+            d2h += freq.nbytes + ids.nbytes
+            sfs = eng.site_frequency_spectrum(freq[0], Nc, SFS_N, L_HALF)
+            h2d += freq[0].nbytes
+            d2h += sfs.nbytes
+            mg += eng.stats()["mutation_generations"]
+        return mg, h2d, d2h
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        device_step()
+        e2e_step()
+    barrier()
+
+    # ---- value: device time of the whole step ----
+    launches0 = eng.stats()["kernel_launches"]
+    times = []
+    mg_total = 0.0
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            stream.synchronize()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            mg_total += device_step()
+            ev1.record(stream)
+            ev1.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+    launches = (eng.stats()["kernel_launches"] - launches0) // max(args.steps, 1) * args.steps
+    barrier()
+    ms_total = float(sum(times))
+
+    # ---- roofline: one more step with every drift launch bracketed by CUDA events ----
+    with torch.cuda.stream(stream):
+        flush.fill_(1.0)
+    stream.synchronize()
+    eng.set_profiling(True)
+    eng.read_profile()
+    prof_mg = device_step()
+    prof = eng.read_profile()
+    eng.set_profiling(False)
+    barrier()
+
+    # ---- e2e: host buffers, copies inside the timed region ----
+    e2e_times, e2e_mg, h2d_b, d2h_b = [], 0.0, 0, 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        stream.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        mg, h2d, d2h = e2e_step()
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_times.append(ev0.elapsed_time(ev1))
+        e2e_mg += mg
+        h2d_b, d2h_b = h2d, d2h
+    barrier()
+
+    # max time over ranks, total work over ranks
+    if world > 1:
+        t = torch.tensor([ms_total, float(sum(e2e_times))], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        w = torch.tensor([mg_total, e2e_mg], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+        ms_total, e2e_ms = float(t[0]), float(t[1])
+        mg_all, e2e_mg_all = float(w[0]), float(w[1])
+    else:
+        e2e_ms = float(sum(e2e_times))
+        mg_all, e2e_mg_all = mg_total, e2e_mg
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    drift_bytes = ALG_BYTES_PER_MUTGEN * prof_mg  # the profiled step's drift launches
+    achieved = drift_bytes / (prof["drift_ms"] * 1e-3) / 1e9 if prof["drift_ms"] > 0 else None
+    traffic = None
+    tfile = ROOT / "profiles" / "drift_traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get("dram_bytes_per_mutation_generation")
+            if traffic is not None:
+                traffic = traffic * prof_mg / max(prof["drift_launches"], 1)
+        except Exception:
+            traffic = None
+    cpu = cpu_baseline_sample(threads=os.cpu_count() or 1) if not args.skip_cpu_baseline else None
+    value = mg_all / (ms_total * 1e-3)
+    line = {
+        "metric": "mutation-generations/s",
+        "value": value,
+        "unit": "mutation-generations/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (the simulation draws its own mutation-selection-equilibrium start)",
+        "config": {
+            "workload": "GO_Fish single population N=200,000 (Nchrom_e 400,000), mu 1e-9, L=5e8 as 2 x 2.5e8 "
+                        "(neutral + gamma=-10, h=0.5), MSE start, 10,000 generations, compact every 25, SFS n=1000",
+            "generations_per_step": 2 * args.gens,
+            "mutation_generations_per_step": mg_total / args.steps,
+            "l2": "256 MB buffer written between steps (L2 is 126 MB); the 10-40 MB working set of one "
+                  "simulation is L2-resident inside a step",
+            "parallelism": f"replicas x{world} (independent seeds per rank, no collective)",
+        },
+        "e2e": {
+            "value": e2e_mg_all / (e2e_ms * 1e-3),
+            "unit": "mutation-generations/s",
+            "h2d_bytes_per_step": int(h2d_b),
+            "d2h_bytes_per_step": int(d2h_b),
+            "ms_per_step": e2e_ms / args.steps,
+        },
+        "gpu_launches": int(launches),
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "drift_kernel (fused migration/selection/drift + new mutations + compaction flags)",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "peak_source": peak_kind,
+            "traffic": traffic,
+            "drift_ms_per_step": prof["drift_ms"],
+            "drift_launches_per_step": prof["drift_launches"],
+            "drift_us_per_launch": 1e3 * prof["drift_ms"] / max(prof["drift_launches"], 1),
+            "compact_ms_per_step": prof["compact_ms"],
+            "bytes_per_mutation_generation": ALG_BYTES_PER_MUTGEN,
+        },
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU restatement (oracle) -- the reference arm and the cpu_baseline
+# ------------------------------------------------------------------------------------------------
+def equilibrium_state(rng, Nc, L, mu):
+    i = np.arange(1, Nc)
+    counts = rng.poisson(2 * mu * L / (i / Nc))
+    return np.repeat((i.astype(np.float32) / np.float32(Nc)).astype(np.float32), counts)
+
+
+def cpu_sample(threads: int, gens: int, seed: int = 1):
+    import oracle.oracle as orc  # CPU restatement: the timed baseline, never the product
+    Nc = 2 * N_IND
+    x = equilibrium_state(np.random.default_rng(seed), Nc, L_HALF, MU)
+    t0 = time.perf_counter()
+    _, _, mg = orc.run_single(x, first_gen=0, num_gens=gens, Nc=Nc, F=0.0, h=H, s=0.0, mu=MU, num_sites=L_HALF,
+                              seed1=SEED1, seed2=SEED2, compact_interval=COMPACT, capacity=2 * len(x) + 4_000_000,
+                              threads=threads)
+    dt = time.perf_counter() - t0
+    return mg, dt
+
+
+def cpu_baseline_sample(threads: int, gens: int = 40):
+    mg, dt = cpu_sample(threads, gens)
+    return {"value": mg / dt, "unit": "mutation-generations/s", "cores": threads, "kind": "port",
+            "sample": f"{gens} generations of the neutral half (Nchrom_e 400,000, L 2.5e8, ~2.7M mutations) "
+                      f"from a synthetic equilibrium state; {dt:.1f} s of CPU time"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    gens = 20
+    for _ in range(args.warmup):
+        cpu_sample(threads, 2)
+    total_mg, total_s = 0.0, 0.0
+    for k in range(args.steps):
+        mg, dt = cpu_sample(threads, gens, seed=k + 1)
+        total_mg += mg
+        total_s += dt
+    v = total_mg / total_s
+    print(json.dumps({
+        "metric": "mutation-generations/s", "value": v, "unit": "mutation-generations/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "GO_Fish single population N=200,000 (Nchrom_e 400,000), mu 1e-9, L=5e8 as 2 x 2.5e8 "
+                               "(neutral + gamma=-10, h=0.5), MSE start, 10,000 generations, compact every 25, "
+                               "SFS n=1000", "parallelism": "CPU threads"},
+        "cpu_baseline": {"value": v, "unit": "mutation-generations/s", "cores": threads, "kind": "port",
+                         "sample": f"{gens} generations of the neutral half per step (~2.7M mutations), "
+                                   "CPU restatement of the reference's per-generation update (the reference "
+                                   "ships no CPU implementation of this path)"},
+        "e2e": {"value": v, "unit": "mutation-generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--gens", type=int, default=GENS,
+                    help="generations per simulation (profiling captures use a shorter run)")
+    args = ap.parse_args()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import torch
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_b200(args, rank, local_rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

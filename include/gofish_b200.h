@@ -181,6 +181,41 @@ gf_status gf_site_frequency_spectrum_device(gf_engine* engine, const float* d_fr
 /* Synchronize the engine's stream and report any pending device-side fault. */
 gf_status gf_engine_synchronize(gf_engine* engine);
 
+/* ---------------------------------------------------------------------------------------------
+ * Measurement (no reference counterpart: the reference's examples time whole run_sim calls with
+ * cudaEvents, examples/example_speed/run.cu:29-45).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct gf_sim_stats {
+  double mutation_generations; /* sum over generations of the slots the drift pass updated */
+  int64_t generations;         /* generations run since the simulation began */
+  int64_t compactions;
+  int64_t kernel_launches;     /* kernels this engine launched since it was created */
+} gf_sim_stats;
+
+/* Counters of the current simulation.  Synchronizes the stream. */
+gf_status gf_sim_stats_read(gf_engine* engine, gf_sim_stats* out);
+
+/* Launch choices of the drift pass (results do not depend on them). */
+typedef struct gf_tuning {
+  int32_t draw_strategy; /* 0: each thread draws its own four lanes; 1: warp-cooperative draws, grouped by
+                            sampler branch */
+  int32_t blocks_per_sm; /* resident drift blocks per SM (0: the occupancy maximum) */
+} gf_tuning;
+gf_status gf_engine_set_tuning(gf_engine* engine, const gf_tuning* tuning);
+gf_status gf_engine_get_tuning(const gf_engine* engine, gf_tuning* tuning);
+
+/* When enabled, the engine brackets every drift launch and every compaction (scan + scatter) with
+ * CUDA events on its stream; gf_engine_read_profile() returns the accumulated device times and
+ * resets them.  Disabled by default. */
+gf_status gf_engine_set_profiling(gf_engine* engine, int32_t enable);
+typedef struct gf_kernel_times {
+  double drift_ms;
+  int64_t drift_launches;
+  double compact_ms;
+  int64_t compactions;
+} gf_kernel_times;
+gf_status gf_engine_read_profile(gf_engine* engine, gf_kernel_times* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,20 @@ MSE_DTYPE = np.dtype([
 assert POP_DTYPE.itemsize == 36 and GEN_DTYPE.itemsize == 16 + 16 * 36 + 1024 and MSE_DTYPE.itemsize == 28
 
 
+class SimStats(ctypes.Structure):
+    _fields_ = [("mutation_generations", ctypes.c_double), ("generations", ctypes.c_int64),
+                ("compactions", ctypes.c_int64), ("kernel_launches", ctypes.c_int64)]
+
+
+class KernelTimes(ctypes.Structure):
+    _fields_ = [("drift_ms", ctypes.c_double), ("drift_launches", ctypes.c_int64),
+                ("compact_ms", ctypes.c_double), ("compactions", ctypes.c_int64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("draw_strategy", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32)]
+
+
 class SimConfig(ctypes.Structure):
     _fields_ = [
         ("seed1", ctypes.c_int32), ("seed2", ctypes.c_int32), ("num_sites", ctypes.c_float),
@@ -78,6 +92,11 @@ SIGNATURES = {
     "gf_site_frequency_spectrum": (_I, [_P, _P, _I, _I, _I, _F, _P]),
     "gf_population_histogram_device": (_I, [_P, _P, _I, _I, _F, _P]),
     "gf_site_frequency_spectrum_device": (_I, [_P, _P, _I, _I, _I, _F, _P]),
+    "gf_sim_stats_read": (_I, [_P, ctypes.POINTER(SimStats)]),
+    "gf_engine_set_profiling": (_I, [_P, _I]),
+    "gf_engine_set_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),
+    "gf_engine_get_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),
+    "gf_engine_read_profile": (_I, [_P, ctypes.POINTER(KernelTimes)]),
 }
 
 _lib = None

@@ -35,22 +35,28 @@ def _run(cmd: list[str]) -> None:
     subprocess.run(cmd, check=True)
 
 
-def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, verbose_ptxas: bool = False, defines: list[str] | None = None,
+          out: Path | None = None, build_dir: Path | None = None) -> Path:
+    """Compile csrc/*.cu into one shared library (default: libgofish_b200.so next to this file).
+    `defines` (e.g. ["GF_DRIFT_MIN_BLOCKS=6"]) and `out`/`build_dir` build a variant elsewhere."""
+    bdir = build_dir or BUILD
+    lib = out or LIB
+    dflags = [f"-D{d}" for d in (defines or [])]
+    bdir.mkdir(parents=True, exist_ok=True)
     sources = sorted(CSRC.glob("*.cu"))
     hdr_mtime = max((h.stat().st_mtime for h in _headers()), default=0.0)
     objects = []
     rebuilt = False
     for src in sources:
-        obj = BUILD / (src.stem + ".o")
+        obj = bdir / (src.stem + ".o")
         objects.append(obj)
         if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_mtime):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-            _run([NVCC, *ARCH, *CFLAGS, *extra, "-c", str(src), "-o", str(obj)])
+            _run([NVCC, *ARCH, *CFLAGS, *dflags, *extra, "-c", str(src), "-o", str(obj)])
             rebuilt = True
-    if force or rebuilt or not LIB.exists():
-        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objects), "-lcudart"])
-    return LIB
+    if force or rebuilt or not lib.exists():
+        _run([NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objects), "-lcudart"])
+    return lib
 
 
 if __name__ == "__main__":

@@ -100,145 +100,258 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return max(lo, mi
 // ------------------------------------------------------------------------------------------------
 // the fused generation kernel
 // ------------------------------------------------------------------------------------------------
+// Work items of one warp: the draws of its 128 slots that need the sampler, compacted so that every
+// round of 32 lanes runs the same branch of the sampler.  Normal-approximation items fill the
+// arrays from the front, sequential-search items from the back.
+struct WarpDraws {
+  uint32_t bits[128];
+  float mean[128];
+  float var[128];
+  int res[128];
+  unsigned char slot[128];
+};
+
+// Draws of the four lanes of one quad.  COOP = false: each thread draws its own lanes.  COOP = true:
+// the warp pools its work items and draws them branch by branch (all 32 lanes of the warp must call
+// this together).  Both give identical results: the same function of the same (bits, mean, var, N).
+// Resident drift blocks per SM the register allocation must allow (6: at most 40 registers; the
+// kernel is latency-bound, and 6 resident blocks beat 4 by ~4% with no spills).
+#ifndef GF_DRIFT_MIN_BLOCKS
+#define GF_DRIFT_MIN_BLOCKS 6
+#endif
+constexpr int kDriftMinBlocks = GF_DRIFT_MIN_BLOCKS;
+
+// The quad-lane sampler is inlined; the reference compiles its counterpart out of line in another
+// translation unit (shared.cu:10-18).  Both forms give bit-identical draws on sm_100a (checked against
+// the reference kernel for every sampler branch), and inlining is ~8% faster.  GF_DRAW_OUT_OF_LINE
+// restores the out-of-line call.
+#ifdef GF_DRAW_OUT_OF_LINE
+#define GF_LANE_DRAW binom_draw_lane
+#else
+#define GF_LANE_DRAW binom_draw_body
+#endif
+
+template <bool COOP>
+__device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsigned need, int N, int lane,
+                                          WarpDraws* w, int res[4]) {
+  const float Nf = static_cast<float>(N);
+  const uint32_t rb[4] = {r.x, r.y, r.z, r.w};
+  if (!COOP) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
+    return;
+  }
+  const unsigned lt = (1u << lane) - 1u;
+  int nN = 0, nS = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const bool has = (need >> j) & 1u;
+    const float mean = xs[j] * N;
+    const float var = (1.0f - xs[j]) * mean;
+    const bool search = has && (mean <= kMeanBoundary || mean >= Nf - kMeanBoundary);
+    const bool normal = has && !search;
+    const unsigned bN = __ballot_sync(0xFFFFFFFFu, normal);
+    const unsigned bS = __ballot_sync(0xFFFFFFFFu, search);
+    int k = -1;
+    if (normal) k = nN + __popc(bN & lt);
+    if (search) k = 127 - (nS + __popc(bS & lt));
+    if (k >= 0) {
+      w->bits[k] = rb[j];
+      w->mean[k] = mean;
+      w->var[k] = var;
+      w->slot[k] = static_cast<unsigned char>(4 * lane + j);
+    }
+    nN += __popc(bN);
+    nS += __popc(bS);
+  }
+  __syncwarp();
+  for (int k = lane; k < nN; k += 32) w->res[w->slot[k]] = binom_draw_lane(w->bits[k], w->mean[k], w->var[k], Nf);
+  for (int k = lane; k < nS; k += 32) {
+    const int kk = 127 - k;
+    w->res[w->slot[kk]] = binom_draw_lane(w->bits[kk], w->mean[kk], w->var[kk], Nf);
+  }
+  __syncwarp();
+  if (need) {
+    const int4 rr = reinterpret_cast<const int4*>(w->res)[lane];
+    if (need & 1u) res[0] = rr.x;
+    if (need & 2u) res[1] = rr.y;
+    if (need & 4u) res[2] = rr.z;
+    if (need & 8u) res[3] = rr.w;
+  }
+  __syncwarp();
+}
+
 // PT: 1 = single-population specialization, 0 = any P <= kMaxPops.
 // NEUTRAL: every drifted population has s(x) == 0.
 // FLAG: compaction generation -- also write the survival bitmask and tile counts.
-template <int PT, bool NEUTRAL, bool FLAG>
-__global__ void __launch_bounds__(kDriftThreads)
+// COOP: warp-cooperative draws (see draw_quad).
+// The grid is sized by occupancy and strides over the 1024-slot tiles of the current generation,
+// whose number the kernel derives from the device-side mutation count.
+template <int PT, bool NEUTRAL, bool FLAG, bool COOP>
+__global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
     drift_kernel(const float* __restrict__ prev, float* __restrict__ next, int* __restrict__ id_gp,
                  int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
-                 int* __restrict__ d_count, long long stride, int slot_in, int slot_out, int launch_slots,
-                 const GenArgs a) {
+                 int* __restrict__ d_count, unsigned long long* __restrict__ stats, long long stride, int slot_in,
+                 int slot_out, long long capacity, const GenArgs* __restrict__ table) {
+  __shared__ GenArgs a;
+  __shared__ WarpDraws s_draws[COOP ? kDriftThreads / 32 : 1];
+  __shared__ unsigned s_warp[kDriftThreads / 32];
+  {
+    const int* src = reinterpret_cast<const int*>(table);
+    int* dst = reinterpret_cast<int*>(&a);
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(GenArgs) / 4); i += kDriftThreads) dst[i] = src[i];
+  }
+  __syncthreads();
   const int M_in = d_count[slot_in];
-  const int total = M_in + a.new_total;
-  const int q = blockIdx.x * kDriftThreads + threadIdx.x;  // quad index
-  const int base = q * 4;
+  int total = M_in + a.new_total;
+  if (total > capacity) total = static_cast<int>(capacity);  // reported below; never written past the rows
+  const int ntiles = (total + kTileSlots - 1) / kTileSlots;
   const int nquads = M_in >> 2;
   const int P = (PT > 0) ? PT : a.num_pops;
   const int g = a.generation;
-  unsigned keep = 0;  // bit j: slot base + j survives the compaction
+  const int lane = threadIdx.x & 31;
+  WarpDraws* w = &s_draws[COOP ? (threadIdx.x >> 5) : 0];
 
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     d_count[slot_out] = total;
-    if (total > launch_slots) atomicExch(d_count + 2, kFaultCapacity);
+    d_count[3] = total;
+    if (M_in + a.new_total > capacity) atomicExch(d_count + 2, kFaultCapacity);
+    stats[0] += static_cast<unsigned long long>(M_in);
+    stats[1] += 1ull;
   }
 
-  if (q < nquads) {
-    // ---- full quad: one Philox block per population, lanes x,y,z,w = slots base .. base+3 ----
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int q = tile * kDriftThreads + threadIdx.x;  // quad index
+    const int base = q * 4;
+    const bool quad = q < nquads;
+    unsigned keep = 0;  // bit j: slot base + j survives the compaction
+
+    // ---- whole quads: one Philox block per population, lanes x,y,z,w = slots base .. base+3 ----
     unsigned zero = 0xFu, one = 0xFu;
 #pragma unroll 1
     for (int p = 0; p < P; ++p) {
       if (!((a.drift_mask >> p) & 1)) continue;
-      float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (int k = 0; k < P; ++k) {
-        const float m = a.mig[k * P + p];
-        const float4 v = __ldg(reinterpret_cast<const float4*>(prev + k * stride + base));
-        xm.x += m * v.x;
-        xm.y += m * v.y;
-        xm.z += m * v.z;
-        xm.w += m * v.w;
-      }
-      const float F = a.F[p], h = a.h[p], sa = a.sel_a[p], sb = a.sel_b[p];
       const int N = a.Nc[p];
-      float4 o;
-      if (N <= 0) {
-        // extinction generation: the population's row is cleared
-        o = make_float4(0.f, 0.f, 0.f, 0.f);
-      } else {
-        const float x0 = selected_freq<NEUTRAL>(xm.x, sa, sb, F, h);
-        const float x1 = selected_freq<NEUTRAL>(xm.y, sa, sb, F, h);
-        const float x2 = selected_freq<NEUTRAL>(xm.z, sa, sb, F, h);
-        const float x3 = selected_freq<NEUTRAL>(xm.w, sa, sb, F, h);
-        const bool certain = (x0 == 0.f || (x0 == 1.f && N > 6)) && (x1 == 0.f || (x1 == 1.f && N > 6)) &&
-                             (x2 == 0.f || (x2 == 1.f && N > 6)) && (x3 == 0.f || (x3 == 1.f && N > 6));
+      float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (N > 0) {  // N == 0: extinction generation, the population's row is cleared
+        float xs[4] = {0.f, 0.f, 0.f, 0.f};
+        if (quad) {
+          float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int k = 0; k < P; ++k) {
+            const float m = a.mig[k * P + p];
+            const float4 v = __ldg(reinterpret_cast<const float4*>(prev + k * stride + base));
+            xm.x += m * v.x;
+            xm.y += m * v.y;
+            xm.z += m * v.z;
+            xm.w += m * v.w;
+          }
+          const float F = a.F[p], h = a.h[p], sa = a.sel_a[p], sb = a.sel_b[p];
+          xs[0] = selected_freq<NEUTRAL>(xm.x, sa, sb, F, h);
+          xs[1] = selected_freq<NEUTRAL>(xm.y, sa, sb, F, h);
+          xs[2] = selected_freq<NEUTRAL>(xm.z, sa, sb, F, h);
+          xs[3] = selected_freq<NEUTRAL>(xm.w, sa, sb, F, h);
+        }
+        // lost (x == 0) and, for N > 6, fixed (x == 1) slots have a certain outcome
+        int res[4];
+        unsigned need = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          res[j] = (xs[j] == 1.f && N > 6) ? N : 0;
+          if (quad && !(xs[j] == 0.f || (xs[j] == 1.f && N > 6))) need |= 1u << j;
+        }
         uint4 r = make_uint4(0u, 0u, 0u, 0u);
-        if (!certain) r = philox(a.seed1, a.seed2, q + 2, g, p, 0);
+        if (need) r = philox(a.seed1, a.seed2, q + 2, g, p, 0);
+        draw_quad<COOP>(xs, r, need, N, lane, w, res);
         const float Nf = static_cast<float>(N);
-        o.x = static_cast<float>(clampi(drift_lane(r.x, x0, N), 0, N)) / Nf;
-        o.y = static_cast<float>(clampi(drift_lane(r.y, x1, N), 0, N)) / Nf;
-        o.z = static_cast<float>(clampi(drift_lane(r.z, x2, N), 0, N)) / Nf;
-        o.w = static_cast<float>(clampi(drift_lane(r.w, x3, N), 0, N)) / Nf;
+        o.x = static_cast<float>(clampi(res[0], 0, N)) / Nf;
+        o.y = static_cast<float>(clampi(res[1], 0, N)) / Nf;
+        o.z = static_cast<float>(clampi(res[2], 0, N)) / Nf;
+        o.w = static_cast<float>(clampi(res[3], 0, N)) / Nf;
       }
-      *reinterpret_cast<float4*>(next + p * stride + base) = o;
-      if (FLAG && ((a.alive_mask >> p) & 1)) {
-        zero &= (o.x <= 0.f ? 1u : 0u) | (o.y <= 0.f ? 2u : 0u) | (o.z <= 0.f ? 4u : 0u) | (o.w <= 0.f ? 8u : 0u);
-        one &= (o.x >= 1.f ? 1u : 0u) | (o.y >= 1.f ? 2u : 0u) | (o.z >= 1.f ? 4u : 0u) | (o.w >= 1.f ? 8u : 0u);
+      if (quad) {
+        *reinterpret_cast<float4*>(next + p * stride + base) = o;
+        if (FLAG && ((a.alive_mask >> p) & 1)) {
+          zero &= (o.x <= 0.f ? 1u : 0u) | (o.y <= 0.f ? 2u : 0u) | (o.z <= 0.f ? 4u : 0u) | (o.w <= 0.f ? 8u : 0u);
+          one &= (o.x >= 1.f ? 1u : 0u) | (o.y >= 1.f ? 2u : 0u) | (o.z >= 1.f ? 4u : 0u) | (o.w >= 1.f ? 8u : 0u);
+        }
       }
     }
-    if (FLAG) {
+    if (FLAG && quad) {
       keep = ~(zero | one) & 0xFu;
       if (a.check_preserved) {
         const int4 t = *reinterpret_cast<const int4*>(id_tid + base);
         keep |= (t.x < 0 ? 1u : 0u) | (t.y < 0 ? 2u : 0u) | (t.z < 0 ? 4u : 0u) | (t.w < 0 ? 8u : 0u);
       }
     }
-  } else if (base < total) {
-    // ---- scalar tail (slots past the last whole quad) and the new-mutation fill ----
+
+    if (!quad && base < total) {
+      // ---- scalar tail (slots past the last whole quad) and the new-mutation fill ----
 #pragma unroll 1
-    for (int j = 0; j < 4; ++j) {
-      const int e = base + j;
-      if (e >= total) break;
-      unsigned zero = 1u, one = 1u;
-      if (e < M_in) {
-        for (int p = 0; p < P; ++p) {
-          if (!((a.drift_mask >> p) & 1)) continue;
-          float xm = 0.f;
-          for (int k = 0; k < P; ++k) xm += a.mig[k * P + p] * prev[k * stride + e];
-          const int N = a.Nc[p];
-          float o = 0.f;
-          if (N > 0) {
-            const float xs = selected_freq<NEUTRAL>(xm, a.sel_a[p], a.sel_b[p], a.F[p], a.h[p]);
-            o = static_cast<float>(clampi(drift_tail(a.seed1, a.seed2, e, g, p, xs, N), 0, N)) /
-                static_cast<float>(N);
+      for (int j = 0; j < 4; ++j) {
+        const int e = base + j;
+        if (e >= total) break;
+        unsigned z1 = 1u, o1 = 1u;
+        if (e < M_in) {
+          for (int p = 0; p < P; ++p) {
+            if (!((a.drift_mask >> p) & 1)) continue;
+            float xm = 0.f;
+            for (int k = 0; k < P; ++k) xm += a.mig[k * P + p] * prev[k * stride + e];
+            const int N = a.Nc[p];
+            float o = 0.f;
+            if (N > 0) {
+              const float xs = selected_freq<NEUTRAL>(xm, a.sel_a[p], a.sel_b[p], a.F[p], a.h[p]);
+              o = static_cast<float>(clampi(drift_tail(a.seed1, a.seed2, e, g, p, xs, N), 0, N)) /
+                  static_cast<float>(N);
+            }
+            next[p * stride + e] = o;
+            if (FLAG && ((a.alive_mask >> p) & 1)) {
+              z1 &= (o <= 0.f);
+              o1 &= (o >= 1.f);
+            }
           }
-          next[p * stride + e] = o;
-          if (FLAG && ((a.alive_mask >> p) & 1)) {
-            zero &= (o <= 0.f);
-            one &= (o >= 1.f);
+          if (FLAG) keep |= ((!(z1 | o1)) || (a.check_preserved && id_tid[e] < 0)) ? (1u << j) : 0u;
+        } else {
+          // new mutation (add_new_mutations, go_fish_impl.cu:138-145): row p = 1/Nc, others 0
+          const int r = e - M_in;
+          int p = 0;
+          while (p + 1 < P && r >= a.new_offset[p + 1]) ++p;
+          const int tid = r - a.new_offset[p] + 1;
+          for (int k = 0; k < P; ++k) {
+            const float v = (k == p) ? a.new_freq[p] : 0.f;
+            next[k * stride + e] = v;
+            if (FLAG && ((a.alive_mask >> k) & 1)) {
+              z1 &= (v <= 0.f);
+              o1 &= (v >= 1.f);
+            }
           }
+          id_gp[e] = g | (p << 24);
+          id_tid[e] = tid;
+          if (FLAG) keep |= (!(z1 | o1)) ? (1u << j) : 0u;
         }
-        if (FLAG) keep |= ((!(zero | one)) || (a.check_preserved && id_tid[e] < 0)) ? (1u << j) : 0u;
-      } else {
-        // new mutation (add_new_mutations, go_fish_impl.cu:138-145): row p = 1/Nc, others 0
-        const int r = e - M_in;
-        int p = 0;
-        while (p + 1 < P && r >= a.new_offset[p + 1]) ++p;
-        const int tid = r - a.new_offset[p] + 1;
-        for (int k = 0; k < P; ++k) {
-          const float v = (k == p) ? a.new_freq[p] : 0.f;
-          next[k * stride + e] = v;
-          if (FLAG && ((a.alive_mask >> k) & 1)) {
-            zero &= (v <= 0.f);
-            one &= (v >= 1.f);
-          }
-        }
-        id_gp[e] = g | (p << 24);
-        id_tid[e] = tid;
-        if (FLAG) keep |= (!(zero | one)) ? (1u << j) : 0u;
       }
     }
-  }
 
-  if (FLAG) {
-    // 8 consecutive threads own the 32 slots of one flag word.
-    const int lane = threadIdx.x & 31;
-    unsigned word = (keep & 0xFu) << ((lane & 7) * 4);
-    word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);
-    word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);
-    word |= __shfl_xor_sync(0xFFFFFFFFu, word, 4);
-    if ((lane & 7) == 0) flags[base >> 5] = word;
-    // survivors of the tile
-    __shared__ unsigned s_warp[kDriftThreads / 32];
-    unsigned c = __popc(keep & 0xFu);
+    if (FLAG) {
+      // 8 consecutive threads own the 32 slots of one flag word.
+      unsigned word = (keep & 0xFu) << ((lane & 7) * 4);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 4);
+      if ((lane & 7) == 0) flags[base >> 5] = word;
+      // survivors of the tile
+      unsigned c = __popc(keep & 0xFu);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
-    if (lane == 0) s_warp[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned t = 0;
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+      if (lane == 0) s_warp[threadIdx.x >> 5] = c;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned t = 0;
 #pragma unroll
-      for (int w = 0; w < kDriftThreads / 32; ++w) t += s_warp[w];
-      tile_count[blockIdx.x] = t;
+        for (int wi = 0; wi < kDriftThreads / 32; ++wi) t += s_warp[wi];
+        tile_count[tile] = t;
+      }
+      __syncthreads();
     }
   }
 }
@@ -249,10 +362,14 @@ __global__ void __launch_bounds__(kDriftThreads)
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
 
+// n_from_slots: if not null, n = ceil(*n_from_slots / 1024) -- the tile count of a generation whose
+// slot count only the device knows.
 __global__ void __launch_bounds__(kScanThreads)
-    scan_exclusive_kernel(const unsigned* __restrict__ in, unsigned* __restrict__ out, int n, int* total_out) {
+    scan_exclusive_kernel(const unsigned* __restrict__ in, unsigned* __restrict__ out, int n, int* total_out,
+                          const int* __restrict__ n_from_slots) {
   __shared__ unsigned s_warp[kScanThreads / 32];
   __shared__ unsigned s_carry;
+  if (n_from_slots) n = (*n_from_slots + kTileSlots - 1) / kTileSlots;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
@@ -308,12 +425,13 @@ __global__ void __launch_bounds__(kDriftThreads)
     scatter_kernel(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ gp_src,
                    const int* __restrict__ tid_src, int* __restrict__ gp_dst, int* __restrict__ tid_dst,
                    const unsigned* __restrict__ flags, const unsigned* __restrict__ tile_offset, long long stride,
-                   int P) {
+                   int P, const int* __restrict__ d_slots) {
   __shared__ unsigned s_words[32];
   __shared__ unsigned s_prefix[32];
   __shared__ float s_stage[kTileSlots];
   const int t = threadIdx.x;
-  const long long tile = blockIdx.x;
+  const long long ntiles = (*d_slots + kTileSlots - 1) / kTileSlots;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
   if (t < 32) {
     const unsigned w = flags[tile * 32 + t];
     s_words[t] = w;
@@ -364,6 +482,7 @@ __global__ void __launch_bounds__(kDriftThreads)
     __syncthreads();
     for (int k = t; k < count; k += kDriftThreads) d[out_base + k] = s_istage[k];
     __syncthreads();
+  }
   }
 }
 
@@ -606,6 +725,8 @@ static gf_status begin_common(Engine* e, const gf_sim_config* c, long long initi
   gf_status st = set_capacity(e, want, 0);
   if (st != GF_OK) return st;
   GF_CUDA(e, cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream));
+  GF_CUDA(e, cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream));
+  e->compactions = 0;
   e->M_upper = initial_mutations;
   e->M_exact = true;
   e->active = true;
@@ -649,39 +770,73 @@ int host_new_mutation_count(int seed1, int seed2, float mu, int Nchrom_e, float 
   return std::max(pois_draw(lambda, lambda, Nchrom_e * num_sites, seed1, seed2, 1, generation, pop), 0);
 }
 
-template <int PT, bool NEUTRAL, bool FLAG>
-static void launch_drift_t(Engine* e, int blocks, int launch_slots, int slot_in, int slot_out, const GenArgs& a) {
-  drift_kernel<PT, NEUTRAL, FLAG><<<blocks, kDriftThreads, 0, e->stream>>>(
-      e->freq[e->cur], e->freq[e->cur ^ 1], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->flags, e->tile_count,
-      e->d_count, e->capacity, slot_in, slot_out, launch_slots, a);
+template <int PT, bool NEUTRAL, bool FLAG, bool COOP>
+static void launch_drift_t(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a) {
+  static int occupancy = 0;
+  auto kernel = drift_kernel<PT, NEUTRAL, FLAG, COOP>;
+  if (occupancy == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kernel, kDriftThreads, 0) != cudaSuccess ||
+        occupancy < 1) {
+      cudaGetLastError();
+      occupancy = 1;
+    }
+  }
+  const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
+  const int blocks = std::max(1, std::min(tiles_bound, e->num_sms * per_sm));
+  kernel<<<blocks, kDriftThreads, 0, e->stream>>>(e->freq[e->cur], e->freq[e->cur ^ 1], e->id_gp[e->id_cur],
+                                                  e->id_tid[e->id_cur], e->flags, e->tile_count, e->d_count,
+                                                  e->d_stats, e->capacity, slot_in, slot_out, e->capacity, a);
 }
 
-static void launch_drift(Engine* e, int blocks, int launch_slots, int slot_in, int slot_out, const GenArgs& a,
-                         bool single, bool neutral, bool flag) {
+template <int PT, bool NEUTRAL, bool FLAG>
+static void launch_drift_c(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a) {
+  if (e->draw_coop) launch_drift_t<PT, NEUTRAL, FLAG, true>(e, tiles_bound, slot_in, slot_out, a);
+  else launch_drift_t<PT, NEUTRAL, FLAG, false>(e, tiles_bound, slot_in, slot_out, a);
+}
+
+static void launch_drift(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a, bool single,
+                         bool neutral, bool flag) {
   if (single) {
     if (neutral) {
-      flag ? launch_drift_t<1, true, true>(e, blocks, launch_slots, slot_in, slot_out, a)
-           : launch_drift_t<1, true, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+      flag ? launch_drift_c<1, true, true>(e, tiles_bound, slot_in, slot_out, a)
+           : launch_drift_c<1, true, false>(e, tiles_bound, slot_in, slot_out, a);
     } else {
-      flag ? launch_drift_t<1, false, true>(e, blocks, launch_slots, slot_in, slot_out, a)
-           : launch_drift_t<1, false, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+      flag ? launch_drift_c<1, false, true>(e, tiles_bound, slot_in, slot_out, a)
+           : launch_drift_c<1, false, false>(e, tiles_bound, slot_in, slot_out, a);
     }
   } else {
     if (neutral) {
-      flag ? launch_drift_t<0, true, true>(e, blocks, launch_slots, slot_in, slot_out, a)
-           : launch_drift_t<0, true, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+      flag ? launch_drift_c<0, true, true>(e, tiles_bound, slot_in, slot_out, a)
+           : launch_drift_c<0, true, false>(e, tiles_bound, slot_in, slot_out, a);
     } else {
-      flag ? launch_drift_t<0, false, true>(e, blocks, launch_slots, slot_in, slot_out, a)
-           : launch_drift_t<0, false, false>(e, blocks, launch_slots, slot_in, slot_out, a);
+      flag ? launch_drift_c<0, false, true>(e, tiles_bound, slot_in, slot_out, a)
+           : launch_drift_c<0, false, false>(e, tiles_bound, slot_in, slot_out, a);
     }
   }
 }
 
-static gf_status run_generation(Engine* e, const gf_generation& gen) {
+static cudaEvent_t prof_event(Engine* e) {
+  if (!e->prof_pool.empty()) {
+    cudaEvent_t ev = e->prof_pool.back();
+    e->prof_pool.pop_back();
+    return ev;
+  }
+  cudaEvent_t ev = nullptr;
+  cudaEventCreate(&ev);
+  return ev;
+}
+
+// Host evaluation of one generation record into kernel arguments: validation, the host-side
+// new-mutation draws (calc_new_mutations_Index) and the per-population parameter arrays.
+struct GenHost {
+  bool neutral;
+  bool preserve;
+};
+
+static gf_status build_args(Engine* e, const gf_generation& gen, GenArgs& a, GenHost& gh) {
   const int P = e->P;
   if (gen.generation < 0 || gen.generation > GF_MAX_GENERATION)
     return fail(e, GF_ERR_CAPACITY, "generation %d outside [0, %d]", gen.generation, GF_MAX_GENERATION);
-  GenArgs a;
   std::memset(&a, 0, sizeof(a));
   a.generation = gen.generation;
   a.num_pops = P;
@@ -709,15 +864,29 @@ static gf_status run_generation(Engine* e, const gf_generation& gen) {
       a.new_freq[p] = 1.f / pp.Nchrom_e;
     }
     new_total += count;
-    a.new_offset[p + 1] = static_cast<int>(std::min<long long>(new_total, 1LL << 30));
+    if (new_total > (1LL << 30)) return fail(e, GF_ERR_CAPACITY, "generation %d: %lld new mutations", gen.generation, new_total);
+    a.new_offset[p + 1] = static_cast<int>(new_total);
     for (int k = 0; k < P; ++k) a.mig[k * P + p] = gen.migration[k * kMaxPops + p];
   }
   for (int p = P; p <= kMaxPops; ++p) a.new_offset[p] = a.new_offset[P];
   a.new_total = static_cast<int>(new_total);
   a.flag = (gen.compact || gen.preserve) && e->compact_interval > 0;
-  a.check_preserved = e->any_preserved ? 1 : 0;
+  gh.neutral = neutral;
+  gh.preserve = gen.preserve != 0;
+  return GF_OK;
+}
 
-  poll_pending(e, false);
+// Launch one generation whose arguments are `h` on the host and `d` in the device table.
+static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int index, const GenHost& gh) {
+  const int P = e->P;
+  const long long new_total = h.new_total;
+  if (!e->pending.empty()) poll_pending(e, false);
+  // the preserved check is decided when the generation launches (earlier compactions may set it)
+  if (h.flag && e->any_preserved && !h.check_preserved) {
+    h.check_preserved = 1;
+    GF_CUDA(e, cudaMemcpyAsync(&d_table[index].check_preserved, &h.check_preserved, sizeof(int),
+                               cudaMemcpyHostToDevice, e->stream));
+  }
   long long need = e->M_upper + new_total;
   if (need > e->capacity) {
     poll_pending(e, true);
@@ -735,33 +904,56 @@ static gf_status run_generation(Engine* e, const gf_generation& gen) {
       }
     }
   }
-  const int launch_slots = static_cast<int>(align_up(std::max<long long>(need, 1), kTileSlots));
-  const int blocks = launch_slots / kTileSlots;
+  const int tiles_bound = static_cast<int>(align_up(std::max<long long>(need, 1), kTileSlots) / kTileSlots);
   const int slot_in = static_cast<int>(e->step_index & 1);
   const int slot_out = slot_in ^ 1;
-  launch_drift(e, blocks, launch_slots, slot_in, slot_out, a, P == 1, neutral, a.flag != 0);
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    ev0 = prof_event(e);
+    ev1 = prof_event(e);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  launch_drift(e, tiles_bound, slot_in, slot_out, d_table + index, P == 1, gh.neutral, h.flag != 0);
   GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 1;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_drift.emplace_back(ev0, ev1);
+  }
   e->M_upper = need;
   for (auto& pc : e->pending) pc.added += new_total;
 
-  if (a.flag) {
-    scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(e->tile_count, e->tile_offset, blocks,
-                                                              e->d_count + slot_out);
+  if (h.flag) {
+    if (e->profiling) {
+      ev0 = prof_event(e);
+      ev1 = prof_event(e);
+      GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+    }
+    scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(e->tile_count, e->tile_offset, 0,
+                                                              e->d_count + slot_out, e->d_count + 3);
+    const int sblocks = std::max(1, std::min(tiles_bound, e->num_sms * 8));
     GF_CUDA(e, cudaGetLastError());
     const int src = e->cur ^ 1;
-    if (gen.preserve) {
-      scatter_kernel<true><<<blocks, kDriftThreads, 0, e->stream>>>(
+    if (gh.preserve) {
+      scatter_kernel<true><<<sblocks, kDriftThreads, 0, e->stream>>>(
           e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
-          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P);
+          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P, e->d_count + 3);
       e->any_preserved = true;
     } else {
-      scatter_kernel<false><<<blocks, kDriftThreads, 0, e->stream>>>(
+      scatter_kernel<false><<<sblocks, kDriftThreads, 0, e->stream>>>(
           e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
-          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P);
+          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P, e->d_count + 3);
     }
     GF_CUDA(e, cudaGetLastError());
+    e->kernel_launches += 2;
+    e->compactions += 1;
+    if (e->profiling) {
+      GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+      e->prof_compact.emplace_back(ev0, ev1);
+    }
     e->id_cur ^= 1;
     // asynchronous read-back of the survivor count
+    poll_pending(e, false);
     PendingCount pc;
     gf_status st = get_event(e, &pc.event);
     if (st != GF_OK) return st;
@@ -778,6 +970,38 @@ static gf_status run_generation(Engine* e, const gf_generation& gen) {
     e->cur ^= 1;
   }
   e->step_index++;
+  return GF_OK;
+}
+
+// Run a batch of generations: evaluate all records on the host, upload them as one table, launch.
+static gf_status run_batch(Engine* e, const gf_generation* gens, int n) {
+  const int b = e->table_next;
+  e->table_next ^= 1;
+  if (e->table_done[b]) GF_CUDA(e, cudaEventSynchronize(e->table_done[b]));  // the GPU is done with buffer b
+  else GF_CUDA(e, cudaEventCreateWithFlags(&e->table_done[b], cudaEventDisableTiming));
+  if (e->table_cap[b] < static_cast<size_t>(n)) {
+    const size_t cap = std::max<size_t>(n, 256);
+    if (e->d_table[b]) GF_CUDA(e, cudaFree(e->d_table[b]));
+    if (e->h_table[b]) GF_CUDA(e, cudaFreeHost(e->h_table[b]));
+    e->d_table[b] = nullptr;
+    e->h_table[b] = nullptr;
+    e->table_cap[b] = 0;
+    GF_CUDA(e, cudaMalloc(&e->d_table[b], sizeof(GenArgs) * cap));
+    GF_CUDA(e, cudaMallocHost(&e->h_table[b], sizeof(GenArgs) * cap));
+    e->table_cap[b] = cap;
+  }
+  std::vector<GenHost> gh(n);
+  for (int i = 0; i < n; ++i) {
+    gf_status st = build_args(e, gens[i], e->h_table[b][i], gh[i]);
+    if (st != GF_OK) return st;
+    e->h_table[b][i].check_preserved = e->any_preserved ? 1 : 0;
+  }
+  GF_CUDA(e, cudaMemcpyAsync(e->d_table[b], e->h_table[b], sizeof(GenArgs) * n, cudaMemcpyHostToDevice, e->stream));
+  for (int i = 0; i < n; ++i) {
+    gf_status st = launch_generation(e, e->h_table[b][i], e->d_table[b], i, gh[i]);
+    if (st != GF_OK) return st;
+  }
+  GF_CUDA(e, cudaEventRecord(e->table_done[b], e->stream));
   return GF_OK;
 }
 
@@ -833,6 +1057,10 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
   gf_engine* g = new gf_engine();
   Engine* e = &g->impl;
   e->device = device;
+  if (cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || e->num_sms < 1) {
+    cudaGetLastError();
+    e->num_sms = 148;
+  }
   if (cuda_stream) {
     e->stream = static_cast<cudaStream_t>(cuda_stream);
   } else {
@@ -843,6 +1071,7 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
     e->own_stream = true;
   }
   if (cudaMalloc(&e->d_count, sizeof(int) * 4) != cudaSuccess ||
+      cudaMalloc(&e->d_stats, sizeof(unsigned long long) * 2) != cudaSuccess ||
       cudaMallocHost(&e->h_pinned, sizeof(int) * e->pinned_slots) != cudaSuccess) {
     if (e->d_count) cudaFree(e->d_count);
     if (e->own_stream) cudaStreamDestroy(e->stream);
@@ -850,6 +1079,7 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
     return GF_ERR_OUT_OF_MEMORY;
   }
   cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream);
+  cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream);
   *out = g;
   return GF_OK;
 }
@@ -865,6 +1095,15 @@ void gf_engine_destroy(gf_engine* g) {
   if (e->spec_in) cudaFree(e->spec_in);
   if (e->spec_out) cudaFree(e->spec_out);
   if (e->d_count) cudaFree(e->d_count);
+  if (e->d_stats) cudaFree(e->d_stats);
+  for (int b = 0; b < 2; ++b) {
+    if (e->d_table[b]) cudaFree(e->d_table[b]);
+    if (e->h_table[b]) cudaFreeHost(e->h_table[b]);
+    if (e->table_done[b]) cudaEventDestroy(e->table_done[b]);
+  }
+  for (auto& pr : e->prof_drift) e->prof_pool.insert(e->prof_pool.end(), {pr.first, pr.second});
+  for (auto& pr : e->prof_compact) e->prof_pool.insert(e->prof_pool.end(), {pr.first, pr.second});
+  for (auto ev : e->prof_pool) cudaEventDestroy(ev);
   if (e->h_pinned) cudaFreeHost(e->h_pinned);
   if (e->own_stream) cudaStreamDestroy(e->stream);
   delete g;
@@ -974,8 +1213,11 @@ gf_status gf_sim_begin_mse(gf_engine* g, const gf_sim_config* c, const gf_mse_po
         d_counts, d_integral, cr.first_class[p], mp.mu, mp.N_ind, Nc, c->num_sites, mp.sel_slope, mp.sel_intercept,
         mp.F, mp.h, c->seed1, c->seed2, p, selected ? 1 : 0);
     GF_CUDA(e, cudaGetLastError());
+    e->kernel_launches += selected ? 3 : 1;
   }
-  scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(d_counts, d_starts, static_cast<int>(num_classes), d_total);
+  e->kernel_launches += 2;  // class scan + slot fill
+  scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(d_counts, d_starts, static_cast<int>(num_classes), d_total,
+                                                            nullptr);
   GF_CUDA(e, cudaGetLastError());
   int M0 = 0;
   GF_CUDA(e, cudaMemcpyAsync(&M0, d_total, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
@@ -1008,11 +1250,8 @@ gf_status gf_sim_run(gf_engine* g, const gf_generation* gens, int32_t n) {
   if (!e->active) return fail(e, GF_ERR_STATE, "gf_sim_run before gf_sim_begin_*");
   if (n < 0 || (n > 0 && !gens)) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad generation table");
   GF_CUDA(e, cudaSetDevice(e->device));
-  for (int i = 0; i < n; ++i) {
-    gf_status st = run_generation(e, gens[i]);
-    if (st != GF_OK) return st;
-  }
-  return GF_OK;
+  if (n == 0) return GF_OK;
+  return run_batch(e, gens, n);
 }
 
 gf_status gf_sim_num_mutations(gf_engine* g, int32_t* out) {
@@ -1057,6 +1296,67 @@ gf_status gf_sim_read_state(gf_engine* g, float* freq_out, int32_t* ids_out, int
   }
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
   return GF_OK;
+}
+
+gf_status gf_sim_stats_read(gf_engine* g, gf_sim_stats* out) {
+  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  GF_CUDA(e, cudaSetDevice(e->device));
+  unsigned long long st[2] = {0, 0};
+  GF_CUDA(e, cudaMemcpyAsync(st, e->d_stats, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  out->mutation_generations = static_cast<double>(st[0]);
+  out->generations = static_cast<int64_t>(st[1]);
+  out->compactions = e->compactions;
+  out->kernel_launches = e->kernel_launches;
+  return GF_OK;
+}
+
+gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
+  if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (t->draw_strategy < 0 || t->draw_strategy > 1 || t->blocks_per_sm < 0)
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1}, blocks_per_sm >= 0");
+  e->draw_coop = t->draw_strategy;
+  e->blocks_per_sm = t->blocks_per_sm;
+  return GF_OK;
+}
+
+gf_status gf_engine_get_tuning(const gf_engine* g, gf_tuning* t) {
+  if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
+  t->draw_strategy = g->impl.draw_coop;
+  t->blocks_per_sm = g->impl.blocks_per_sm;
+  return GF_OK;
+}
+
+gf_status gf_engine_set_profiling(gf_engine* g, int32_t enable) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  g->impl.profiling = enable != 0;
+  return GF_OK;
+}
+
+gf_status gf_engine_read_profile(gf_engine* g, gf_kernel_times* out) {
+  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  GF_CUDA(e, cudaSetDevice(e->device));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  auto sum = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, double* ms, int64_t* n) -> gf_status {
+    double t = 0;
+    for (auto& pr : v) {
+      float x = 0.f;
+      GF_CUDA(e, cudaEventElapsedTime(&x, pr.first, pr.second));
+      t += x;
+      e->prof_pool.push_back(pr.first);
+      e->prof_pool.push_back(pr.second);
+    }
+    *ms = t;
+    *n = static_cast<int64_t>(v.size());
+    v.clear();
+    return GF_OK;
+  };
+  gf_status st = sum(e->prof_drift, &out->drift_ms, &out->drift_launches);
+  if (st != GF_OK) return st;
+  return sum(e->prof_compact, &out->compact_ms, &out->compactions);
 }
 
 gf_status gf_sim_device_state(gf_engine* g, const float** out_freq, int32_t* out_stride, int32_t* out_num) {

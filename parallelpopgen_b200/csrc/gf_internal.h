@@ -56,6 +56,9 @@ struct PendingCount {
 
 struct Engine {
   int device = 0;
+  int num_sms = 148;
+  int draw_coop = 0;       // 1: warp-cooperative draws
+  int blocks_per_sm = 0;   // drift grid limit per SM (0: occupancy maximum)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string last_error;
@@ -89,6 +92,21 @@ struct Engine {
   bool M_exact = true;
   std::deque<PendingCount> pending;
   std::vector<cudaEvent_t> free_events;
+
+  // per-generation parameter tables (double-buffered: the host fills one while the GPU reads the other)
+  GenArgs* d_table[2] = {nullptr, nullptr};
+  GenArgs* h_table[2] = {nullptr, nullptr};
+  size_t table_cap[2] = {0, 0};
+  cudaEvent_t table_done[2] = {nullptr, nullptr};
+  int table_next = 0;
+
+  // measurement
+  unsigned long long* d_stats = nullptr;  // [0] sum of drift slots, [1] generations
+  long long compactions = 0;
+  long long kernel_launches = 0;
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_drift, prof_compact;
+  std::vector<cudaEvent_t> prof_pool;
 
   // spectrum scratch
   void* spec_scratch = nullptr;

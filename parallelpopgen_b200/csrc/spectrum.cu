@@ -247,6 +247,7 @@ static gf_status run_hist(Engine* e, const float* d_freq, int M, int Nc, unsigne
                                   static_cast<int>(sizeof(unsigned) * kSmemBins)));
   hist_kernel<<<hist_blocks(M), kHistThreads, smem, e->stream>>>(d_freq, M, Nc, counts, mismatch, smem_bins);
   GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 1;
   return GF_OK;
 }
 
@@ -270,6 +271,7 @@ gf_status population_histogram_device(Engine* e, const float* d_freq, int M, int
   const unsigned extra0 = static_cast<unsigned>(static_cast<int>(num_sites) - M);
   hist_to_float_kernel<<<std::max(1, std::min(1024, (Nc + 255) / 256)), 256, 0, e->stream>>>(counts, Nc, extra0, d_out);
   GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 1;
   return GF_OK;
 }
 
@@ -323,6 +325,7 @@ gf_status site_frequency_spectrum_device(Engine* e, const float* d_freq, int M, 
   GF_CUDA(e, cudaGetLastError());
   sfs_finish_kernel<<<std::max(1, (n + 255) / 256), 256, 0, e->stream>>>(partial, used_blocks, n, extra0, nonseg, d_out);
   GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += h_mismatch ? 2 : 3;
   return GF_OK;
 }
 

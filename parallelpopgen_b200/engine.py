@@ -111,6 +111,30 @@ class Engine:
         self._check(self.lib.gf_sim_device_state(self.h, ctypes.byref(p), ctypes.byref(stride), ctypes.byref(m)))
         return p.value, stride.value, m.value
 
+    def stats(self) -> dict:
+        st = _capi.SimStats()
+        self._check(self.lib.gf_sim_stats_read(self.h, ctypes.byref(st)))
+        return {"mutation_generations": st.mutation_generations, "generations": st.generations,
+                "compactions": st.compactions, "kernel_launches": st.kernel_launches}
+
+    def set_tuning(self, draw_strategy: int = 0, blocks_per_sm: int = 0) -> None:
+        t = _capi.Tuning(int(draw_strategy), int(blocks_per_sm))
+        self._check(self.lib.gf_engine_set_tuning(self.h, ctypes.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = _capi.Tuning()
+        self._check(self.lib.gf_engine_get_tuning(self.h, ctypes.byref(t)))
+        return {"draw_strategy": t.draw_strategy, "blocks_per_sm": t.blocks_per_sm}
+
+    def set_profiling(self, enable: bool) -> None:
+        self._check(self.lib.gf_engine_set_profiling(self.h, int(enable)))
+
+    def read_profile(self) -> dict:
+        kt = _capi.KernelTimes()
+        self._check(self.lib.gf_engine_read_profile(self.h, ctypes.byref(kt)))
+        return {"drift_ms": kt.drift_ms, "drift_launches": kt.drift_launches, "compact_ms": kt.compact_ms,
+                "compactions": kt.compactions}
+
     def synchronize(self) -> None:
         self._check(self.lib.gf_engine_synchronize(self.h))
 
