@@ -104,6 +104,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def reduce_over_ranks(max_values, sum_values, world: int, device=None):
+    """Max over ranks of the timing values and sum over ranks of the work values (replicas: the only
+    cross-rank exchange of this benchmark; the simulations themselves share nothing)."""
+    if world <= 1:
+        return [float(x) for x in max_values], [float(x) for x in sum_values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(max_values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    w = torch.tensor(list(sum_values), dtype=torch.float64, device=device)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return t.tolist(), w.tolist()
+
+
 # ------------------------------------------------------------------------------------------------
 # B200 arm
 # ------------------------------------------------------------------------------------------------
@@ -220,16 +234,8 @@ def run_b200(args, rank, local_rank, world):
     barrier()
 
     # max time over ranks, total work over ranks
-    if world > 1:
-        t = torch.tensor([ms_total, float(sum(e2e_times))], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        w = torch.tensor([mg_total, e2e_mg], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
-        ms_total, e2e_ms = float(t[0]), float(t[1])
-        mg_all, e2e_mg_all = float(w[0]), float(w[1])
-    else:
-        e2e_ms = float(sum(e2e_times))
-        mg_all, e2e_mg_all = mg_total, e2e_mg
+    (ms_total, e2e_ms), (mg_all, e2e_mg_all) = reduce_over_ranks([ms_total, float(sum(e2e_times))],
+                                                                 [mg_total, e2e_mg], world, device=dev)
 
     if rank != 0:
         return

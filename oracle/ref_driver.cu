@@ -166,6 +166,10 @@ int main(int argc, char** argv) {
   if (mode == "hostrng") return mode_hostrng(argv[2]);
   if (mode == "draws" && argc >= 4) return mode_draws(argv[2], argv[3]);
   if (mode == "drift1" && argc >= 4) return mode_drift1(argv[2], argv[3], scn::Args(argc, argv, 4));
+  if (mode == "dadi") {  // ref_driver dadi <out.txt> key=value...
+    scn::dadi_table(scn::Args(argc, argv, 3), argv[2]);
+    return 0;
+  }
   if (mode == "sim" && argc >= 4) {
     scn::Args args(argc, argv, 4);
     GO_Fish::allele_trajectories a;

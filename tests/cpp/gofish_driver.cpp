@@ -3,6 +3,7 @@
 //   gofish_driver <scenario> <out.bin> key=value ...
 #include <chrono>
 #include <cstdio>
+#include <string>
 
 #include "scenarios.h"
 
@@ -12,6 +13,13 @@ int main(int argc, char** argv) {
     return 2;
   }
   scn::Args args(argc, argv, 3);
+  if (std::string(argv[1]) == "dadi") {  // replicate table of the two-population validation model
+    const auto t0 = std::chrono::steady_clock::now();
+    scn::dadi_table(args, argv[2]);
+    const auto t1 = std::chrono::steady_clock::now();
+    std::printf("sim_ms %.3f\n", std::chrono::duration<double, std::milli>(t1 - t0).count());
+    return 0;
+  }
   GO_Fish::allele_trajectories a;
   const auto t0 = std::chrono::steady_clock::now();
   if (!scn::run_scenario(argv[1], a, args)) {

@@ -185,6 +185,82 @@ inline void scenario_split3(GO_Fish::allele_trajectories& a, const Args& args) {
   GO_Fish::run_sim(a, mutation, dem, mig, selection, inbreeding, dominance, bool_off(), sample);
 }
 
+// ---------------------------------------------------------------------------------------------
+// scenario "dadi": the two-population model the reference validates against a diffusion solution
+// (examples/example_dadi/run.cu): population 0 starts at mutation-selection equilibrium with N
+// individuals and doubles at generation 1; population 1 splits off at generation 100 with 0.05 N
+// individuals drawn from population 0 and grows exponentially to 5 N by generation 1000; migration
+// 1/(2N) between them from generation 101; gamma = -4, h = 0.5, F = 0, mu = 1e-9, L = 2e9,
+// compaction every 30.  Replicate j uses seeds (0xbeeff00d + 2j, 0xdecafbad - 2j).  The SFS is
+// population 1's, n = 1001, at the final generation.
+// ---------------------------------------------------------------------------------------------
+inline void scenario_dadi(GO_Fish::allele_trajectories& b, const Args& args, int rep) {
+  typedef Sim_Model::demography_constant dem_const;
+  typedef Sim_Model::demography_population_specific<dem_const, dem_const> dem_pop_const;
+  typedef Sim_Model::demography_piecewise<dem_pop_const, dem_pop_const> init_expansion;
+  typedef Sim_Model::demography_exponential_growth exp_growth;
+  typedef Sim_Model::demography_population_specific<dem_const, exp_growth> dem_pop_const_exp;
+  typedef Sim_Model::migration_constant_equal mig_const;
+  typedef Sim_Model::migration_constant_directional<mig_const> mig_dir;
+  typedef Sim_Model::migration_constant_directional<mig_dir> mig_split;
+  typedef Sim_Model::migration_piecewise<mig_const, mig_split> split_pop0;
+  b.sim_input_constants.num_populations = 2;
+  b.sim_input_constants.num_generations = 1001;
+  Sim_Model::F_mu_h_constant codominant(0.5f);
+  Sim_Model::F_mu_h_constant outbred(0.f);
+  Sim_Model::F_mu_h_constant mutation(1e-9f);
+  const int N = static_cast<int>(args.integer("N", 10000));
+  dem_const pop0(N), pop1(0), pop0_final(2 * N);
+  dem_pop_const gen0(pop0, pop1, 1), gen1(pop0_final, pop1, 1);
+  init_expansion gen_0_1(gen0, gen1, 1);
+  exp_growth pop1_growth(std::log(100.f) / 900.f, static_cast<int>(0.05 * N), 100);
+  dem_pop_const_exp gen100(pop0_final, pop1_growth, 1);
+  Sim_Model::demography_piecewise<init_expansion, dem_pop_const_exp> demography(gen_0_1, gen100, 100);
+  mig_const none;
+  mig_dir no_pop1(0.f, 1, 1, none);
+  mig_split found_pop1(1.f, 0, 1, no_pop1);
+  split_pop0 split(none, found_pop1, 100);
+  mig_const equal(1.f / (2.f * N), 2);
+  Sim_Model::migration_piecewise<split_pop0, mig_const> migration(split, equal, 101);
+  Sim_Model::selection_constant weak_del(-4.f, demography, outbred);
+  b.sim_input_constants.compact_interval = static_cast<int>(args.integer("compact", 30));
+  b.sim_input_constants.num_sites = static_cast<float>(args.num("L", 2e9));
+  b.sim_input_constants.seed1 = static_cast<int>(0xbeeff00d + 2 * rep);
+  b.sim_input_constants.seed2 = static_cast<int>(0xdecafbad - 2 * rep);
+  GO_Fish::run_sim(b, mutation, demography, migration, weak_del, outbred, codominant, Sim_Model::bool_off(),
+                   Sim_Model::bool_off());
+}
+
+// Runs `reps` replicates of scenario "dadi" and writes, per allele count i = 1 .. n-1, the mean and
+// standard deviation over replicates of SFS[i] / (num_sites - SFS[0]) (the reference example's
+// table), then one line per replicate with its raw SFS.
+inline void dadi_table(const Args& args, const char* path) {
+  const int reps = static_cast<int>(args.integer("reps", 50));
+  const int n = static_cast<int>(args.integer("sfs_n", 1001));
+  std::vector<std::vector<float>> res(reps, std::vector<float>(n));
+  GO_Fish::allele_trajectories b;
+  Spectrum::SFS sfs;
+  for (int j = 0; j < reps; ++j) {
+    scenario_dadi(b, args, j);
+    Spectrum::site_frequency_spectrum(sfs, b, 0, 1, n);
+    for (int i = 0; i < n; ++i) res[j][i] = sfs.frequency_spectrum[i];
+  }
+  FILE* f = std::fopen(path, "w");
+  const double L = static_cast<double>(b.num_sites());
+  for (int i = 1; i < n; ++i) {
+    double avg = 0, var = 0;
+    for (int j = 0; j < reps; ++j) avg += res[j][i] / (reps * (L - res[j][0]));
+    for (int j = 0; j < reps; ++j) var += std::pow(res[j][i] / (L - res[j][0]) - avg, 2) / (reps - 1);
+    std::fprintf(f, "%d\t%.9g\t%.9g\n", i, avg, std::sqrt(var));
+  }
+  for (int j = 0; j < reps; ++j) {
+    std::fprintf(f, "rep%d", j);
+    for (int i = 0; i < n; ++i) std::fprintf(f, "\t%.9g", res[j][i]);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+}
+
 inline bool run_scenario(const std::string& name, GO_Fish::allele_trajectories& a, const Args& args) {
   if (name == "wf") scenario_wf(a, args);
   else if (name == "compilation") scenario_compilation(a, args);

@@ -1,0 +1,88 @@
+"""Host-side logic without a GPU: the per-generation records the engine receives, the compaction
+schedule of run_sim, the float semantics of model parameters, and the benchmark's replica plumbing
+across two processes (gloo)."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from parallelpopgen_b200 import ConstantModel, constant_generations
+from parallelpopgen_b200._capi import GEN_DTYPE, MAX_POPULATIONS
+
+
+def reference_schedule(start: int, final: int, ci: int) -> list[int]:
+    """Compaction generations of the run_sim loop (go_fish_impl.cuh:643-706) without preserve/sample."""
+    out, nxt = [], start + ci
+    for g in range(start + 1, final + 1):
+        if (g == nxt or g == final) and ci > 0:
+            out.append(g)
+            nxt = g + ci
+    return out
+
+
+@pytest.mark.parametrize("start,count,ci", [(0, 1000, 35), (0, 10000, 25), (20000, 1000, 100), (0, 7, 0), (5, 3, 1)])
+def test_compaction_schedule_matches_run_sim(start, count, ci):
+    g = constant_generations(ConstantModel(N=1000), start + 1, count, ci)
+    got = list(g["generation"][g["compact"] == 1])
+    assert got == reference_schedule(start, start + count, ci)
+    assert list(g["generation"]) == list(range(start + 1, start + count + 1))
+
+
+def test_generation_records_carry_the_model():
+    m = ConstantModel(N=1234, F=0.25, h=0.3, s=-0.001, mu=2e-9, P=3, m=0.01)
+    g = constant_generations(m, 1, 4, 2)
+    assert g.dtype == GEN_DTYPE
+    pops = g["pop"]
+    assert (pops["Nchrom_e"][:, :3] == m.Nchrom_e).all() and (pops["Nchrom_e"][:, 3:] == 0).all()
+    assert (pops["drift"][:, :3] == 1).all() and (pops["alive"][:, :3] == 1).all()
+    assert np.allclose(pops["sel_intercept"][:, :3], -0.001)
+    mig = g["migration"][0].reshape(MAX_POPULATIONS, MAX_POPULATIONS)
+    assert mig[0, 0] == np.float32(1) - np.float32(2) * np.float32(0.01)
+    assert mig[0, 1] == np.float32(0.01) and mig[3, 3] == 0
+
+
+def test_effective_chromosomes_and_gamma_use_float_arithmetic():
+    # 2 * N / (1 + F) in float, truncated (go_fish_impl.cuh:659)
+    assert ConstantModel(N=200000).Nchrom_e == 400000
+    assert ConstantModel(N=1000, F=1.0).Nchrom_e == 1000
+    assert ConstantModel(N=10000, F=0.1).Nchrom_e == int(np.float32(20000) / np.float32(1.1))
+    s = ConstantModel.s_from_gamma(-10.0, 200000, 0.0)
+    assert s == float(np.float32(-10.0) / np.float32(400000.0))
+
+
+def _free_port() -> int:
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def _replica_worker(rank, world, port, out):
+    import torch.distributed as dist
+
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mx, sm = bench.reduce_over_ranks([10.0 + rank, 5.0 * rank], [1e9 * (rank + 1), 7.0], world)
+        seeds = [(h["seed1"], h["seed2"]) for h in bench.build_halves(rank, 3)]
+        out[rank] = (mx, sm, seeds)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_replicas_reduce_over_two_gloo_ranks():
+    world = 2
+    port = _free_port()
+    out = mp.Manager().dict()
+    mp.spawn(_replica_worker, args=(world, port, out), nprocs=world, join=True)
+    for r in range(world):
+        mx, sm, _ = out[r]
+        assert mx == [11.0, 5.0]          # max over ranks of the timings
+        assert sm == [3e9, 14.0]          # total work of all replicas
+    # every rank simulates its own replicas: no seed pair repeats across ranks or halves
+    seeds = [s for r in range(world) for s in out[r][2]]
+    assert len(set(seeds)) == len(seeds) == 4
