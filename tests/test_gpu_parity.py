@@ -161,15 +161,17 @@ def test_resume_and_preserve_match_reference(gofish_driver, ref_driver, tmp_path
 
 
 def test_split3_matches_reference(gofish_driver, ref_driver, tmp_path):
-    """Three populations with splits, logistic growth, migration, piecewise selection, inbreeding.
+    """Three populations founded from an ancestor, logistic growth, founding and symmetric migration,
+    piecewise selection, inbreeding in one population, time samples with preservation.
 
-    The first time sample comes after population 2 has split off: before any sample the reference's
-    rows of a not-yet-existing population hold recycled device memory, and once preserved IDs
-    (negative threadIDs, NaN bit patterns as floats) have been freed and recycled into such a row,
-    the reference's migration sum 0 * NaN corrupts live populations.  This engine keeps such rows
-    at zero; the comparison covers the schedule on which the reference is well defined."""
-    args = ["L=2e6", "gens=900", "split2=300", "switch_gen=500", "sample_every=400", "K0=20000", "K1=30000",
-            "K2=40000", "N0=5000", "mse=0", "sfs_n=30", "hist=1"]
+    Both daughter populations are founded at generation 1.  While a population does not exist yet,
+    the reference never writes its rows, which then hold recycled device memory (freed flag words or
+    preserved IDs read as floats can be NaN), and its migration sum multiplies them by a zero rate:
+    0 * NaN corrupts live populations, so the reference's result depends on allocator history.  This
+    engine keeps such rows at zero; the bit-exact comparison uses a schedule on which the reference is
+    well defined."""
+    args = ["L=2e6", "gens=900", "split1=1", "split2=1", "switch_gen=500", "sample_every=200", "K0=20000",
+            "K1=30000", "K2=40000", "N0=5000", "mse=1", "sfs_n=30", "hist=1"]
     mine = run_driver(gofish_driver, "split3", tmp_path / "mine.bin", args)
     subprocess.run([str(ref_driver), "sim", "split3", str(tmp_path / "ref.bin"), *args], check=True,
                    capture_output=True)
