@@ -178,6 +178,29 @@ gf_status gf_population_histogram_device(gf_engine* engine, const float* d_freq,
 gf_status gf_site_frequency_spectrum_device(gf_engine* engine, const float* d_freq, int32_t num_mutations,
                                             int32_t Nchrom_e, int32_t n, float num_sites, float* d_out);
 
+/* Projected SFS that allocates no device memory (no counterpart in the reference).
+ *
+ * Same result as gf_site_frequency_spectrum_device, for callers that cannot call cudaMalloc: code
+ * embedded in a framework that owns the GPU's memory budget (a caching allocator or a pre-reserved
+ * pool that a library's own cudaMalloc would bypass, and that can fail mid-run), and code on a
+ * latency-critical path, where cudaMalloc / cudaFree would synchronize the device.  It needs no
+ * gf_engine: inputs and output are the caller's device buffers, work goes on `cuda_stream` (NULL: the
+ * legacy default stream) of the current device, and the only scratch is one file-scope device array
+ * of GF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the process exits.
+ *   Limits: Nchrom_e <= GF_NOALLOC_MAX_NCHROM, 1 <= n < Nchrom_e, n <= GF_NOALLOC_MAX_SAMPLE; larger
+ *   sizes return GF_ERR_CAPACITY.
+ *   The first call on a device looks the scratch array's address up (cudaGetSymbolAddress); make that
+ *   first call before capturing a stream into a CUDA graph.
+ *   All calls on a device share the scratch array: calls whose GPU work overlaps (two streams, two
+ *   host threads) race; serialize them.  Each call clears what it accumulates into.
+ *   The call synchronizes `cuda_stream` once (it reads back whether every frequency lies on the
+ *   1/Nchrom_e grid).  Status codes only: there is no engine to hold a message. */
+#define GF_NOALLOC_MAX_NCHROM (1 << 20)
+#define GF_NOALLOC_MAX_SAMPLE 1023
+#define GF_NOALLOC_SCRATCH_BYTES (4194560 + 256 + 8192 + 2097152)
+gf_status gf_site_frequency_spectrum_noalloc(const float* d_freq, int32_t num_mutations, int32_t Nchrom_e, int32_t n,
+                                             float num_sites, float* d_out, void* cuda_stream);
+
 /* Synchronize the engine's stream and report any pending device-side fault. */
 gf_status gf_engine_synchronize(gf_engine* engine);
 

@@ -92,6 +92,7 @@ SIGNATURES = {
     "gf_site_frequency_spectrum": (_I, [_P, _P, _I, _I, _I, _F, _P]),
     "gf_population_histogram_device": (_I, [_P, _P, _I, _I, _F, _P]),
     "gf_site_frequency_spectrum_device": (_I, [_P, _P, _I, _I, _I, _F, _P]),
+    "gf_site_frequency_spectrum_noalloc": (_I, [_P, _I, _I, _I, _F, _P, _P]),
     "gf_sim_stats_read": (_I, [_P, ctypes.POINTER(SimStats)]),
     "gf_engine_set_profiling": (_I, [_P, _I]),
     "gf_engine_set_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),

@@ -394,3 +394,128 @@ gf_status gf_site_frequency_spectrum(gf_engine* g, const float* freq, int32_t M,
 }
 
 }  // extern "C"
+
+// ==================================================================================================
+// SFS without allocation.
+//
+// For callers that must not allocate device memory: code running inside a framework that owns the
+// GPU's memory budget (a caching allocator or a pre-reserved pool, where a library's own cudaMalloc
+// would bypass the budget and can fail mid-run), and code on a latency-critical path, where
+// cudaMalloc / cudaFree would synchronize the device and stall work queued on other streams.  This
+// entry point takes its scratch from one file-scope __device__ array instead of engine-owned
+// allocations, and needs no gf_engine.
+//
+// The array is part of the library image: every GPU that loads libgofish_b200.so holds it
+// (GF_NOALLOC_SCRATCH_BYTES, about 6.3 MB) until the process exits.  All calls on a device share it
+// and it keeps the previous call's contents, so calls whose GPU work overlaps (concurrent streams, or
+// several host threads) race and must be serialized by the caller.
+// ==================================================================================================
+
+#include <mutex>
+
+namespace gf {
+
+constexpr size_t kNoAllocCountsOff = 0;
+constexpr size_t kNoAllocFlagsOff = (sizeof(unsigned) * (GF_NOALLOC_MAX_NCHROM + 1) + 255) / 256 * 256;
+constexpr size_t kNoAllocLgcOff = kNoAllocFlagsOff + 256;
+constexpr size_t kNoAllocPartialOff = kNoAllocLgcOff + sizeof(double) * (GF_NOALLOC_MAX_SAMPLE + 1);
+constexpr int kNoAllocMaxBlocks = 256;
+constexpr size_t kNoAllocBytes =
+    kNoAllocPartialOff + sizeof(double) * static_cast<size_t>(kNoAllocMaxBlocks) * (GF_NOALLOC_MAX_SAMPLE + 1);
+static_assert(kNoAllocBytes == GF_NOALLOC_SCRATCH_BYTES, "GF_NOALLOC_SCRATCH_BYTES out of date");
+
+// Scratch of gf_site_frequency_spectrum_noalloc: [counts | mismatch, nonseg | log C(n,k) | partials]
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// log C(n, k) for k = 0 .. n, computed on the device so the call needs no host staging buffer
+__global__ void log_binomial_kernel(double* __restrict__ lgc, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k <= n) lgc[k] = lgamma(n + 1.0) - lgamma(k + 1.0) - lgamma(n - k + 1.0);
+}
+
+// Device address of the scratch array on `device`, looked up once per device.  In host code the
+// array's name only stands for the symbol; kernels must be given this address.
+static gf_status noalloc_scratch(int device, unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* addr[64] = {nullptr};
+  if (device < 0 || device >= 64) return GF_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess || !p) {
+      cudaGetLastError();
+      return GF_ERR_CUDA;
+    }
+    addr[device] = static_cast<unsigned char*>(p);
+  }
+  *out = addr[device];
+  return GF_OK;
+}
+
+#define GF_NA_CUDA(call)                     \
+  do {                                       \
+    if ((call) != cudaSuccess) {             \
+      cudaGetLastError();                    \
+      return GF_ERR_CUDA;                    \
+    }                                        \
+  } while (0)
+
+}  // namespace gf
+
+extern "C" {
+
+gf_status gf_site_frequency_spectrum_noalloc(const float* d_freq, int32_t M, int32_t Nc, int32_t n, float num_sites,
+                                             float* d_out, void* cuda_stream) {
+  using namespace gf;
+  if (!d_out || (M > 0 && !d_freq) || M < 0) return GF_ERR_INVALID_ARGUMENT;
+  if (n <= 0 || n >= Nc) return GF_ERR_INVALID_ARGUMENT;
+  if (Nc > GF_NOALLOC_MAX_NCHROM || n > GF_NOALLOC_MAX_SAMPLE) return GF_ERR_CAPACITY;
+  int device = 0;
+  GF_NA_CUDA(cudaGetDevice(&device));
+  unsigned char* base = nullptr;
+  const gf_status st = noalloc_scratch(device, &base);
+  if (st != GF_OK) return st;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  unsigned* counts = reinterpret_cast<unsigned*>(base + kNoAllocCountsOff);
+  unsigned* mismatch = reinterpret_cast<unsigned*>(base + kNoAllocFlagsOff);
+  unsigned* nonseg = mismatch + 1;
+  double* lgc = reinterpret_cast<double*>(base + kNoAllocLgcOff);
+  double* partial = reinterpret_cast<double*>(base + kNoAllocPartialOff);
+  const int levels = n + 1;
+  // the array keeps the previous call's contents: everything accumulated into starts from zero here
+  GF_NA_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned) * (Nc + 1), stream));
+  GF_NA_CUDA(cudaMemsetAsync(mismatch, 0, sizeof(unsigned) * 2, stream));
+  log_binomial_kernel<<<(levels + 255) / 256, 256, 0, stream>>>(lgc, n);
+  GF_NA_CUDA(cudaGetLastError());
+  if (M > 0) {
+    const int smem_bins = std::min(kSmemBins, Nc + 1);
+    GF_NA_CUDA(cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(sizeof(unsigned) * kSmemBins)));
+    hist_kernel<<<hist_blocks(M), kHistThreads, sizeof(unsigned) * smem_bins, stream>>>(d_freq, M, Nc, counts,
+                                                                                       mismatch, smem_bins);
+    GF_NA_CUDA(cudaGetLastError());
+  }
+  unsigned h_mismatch = 0;
+  GF_NA_CUDA(cudaMemcpyAsync(&h_mismatch, mismatch, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+  GF_NA_CUDA(cudaStreamSynchronize(stream));
+  int used_blocks;
+  if (!h_mismatch) {
+    const int nb = std::max(1, std::min(kNoAllocMaxBlocks, (Nc + 1 + 255) / 256));
+    const int per_block = (Nc + 1 + nb - 1) / nb;
+    nonseg_from_hist_kernel<<<1, 256, 0, stream>>>(counts, Nc, nonseg);
+    project_hist_kernel<<<nb, kProjThreads, 0, stream>>>(counts, Nc, n, lgc, partial, per_block);
+    used_blocks = nb;
+  } else {
+    const int nb = std::max(1, std::min(kNoAllocMaxBlocks, (M + 1023) / 1024));
+    const int per_block = std::max(1, (M + nb - 1) / nb);
+    project_direct_kernel<<<nb, kProjThreads, 0, stream>>>(d_freq, M, n, lgc, partial, per_block, nonseg);
+    used_blocks = nb;
+  }
+  GF_NA_CUDA(cudaGetLastError());
+  sfs_finish_kernel<<<std::max(1, (n + 255) / 256), 256, 0, stream>>>(partial, used_blocks, n,
+                                                                      static_cast<double>(num_sites - M), nonseg, d_out);
+  GF_NA_CUDA(cudaGetLastError());
+  return GF_OK;
+}
+}  // extern "C"
