@@ -223,6 +223,8 @@ typedef struct gf_tuning {
   int32_t draw_strategy; /* 0: each thread draws its own four lanes; 1: warp-cooperative draws, grouped by
                             sampler branch */
   int32_t blocks_per_sm; /* resident drift blocks per SM (0: the occupancy maximum) */
+  int32_t windows;       /* 1 (default): single-population generations between compactions run as one
+                            window launch; 0: one launch per generation */
 } gf_tuning;
 gf_status gf_engine_set_tuning(gf_engine* engine, const gf_tuning* tuning);
 gf_status gf_engine_get_tuning(const gf_engine* engine, gf_tuning* tuning);

@@ -57,7 +57,7 @@ class KernelTimes(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("draw_strategy", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32)]
+    _fields_ = [("draw_strategy", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("windows", ctypes.c_int32)]
 
 
 class SimConfig(ctypes.Structure):

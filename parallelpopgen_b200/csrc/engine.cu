@@ -25,6 +25,7 @@
 
 #include "gf_internal.h"
 #include "gf_rng.cuh"
+#include "gf_drift.cuh"
 
 namespace gf {
 
@@ -61,43 +62,6 @@ gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// per-slot model arithmetic (the expressions of migration_selection_drift, go_fish_impl.cuh:93-124)
-// ------------------------------------------------------------------------------------------------
-
-// Frequency after selection (go_fish_impl.cuh:105 / :119).  With s == 0 the expression reduces to
-// x exactly, which the NEUTRAL instantiation uses directly.
-template <bool NEUTRAL>
-__device__ __forceinline__ float selected_freq(float x, float sa, float sb, float F, float h) {
-  if (NEUTRAL) return x;
-  const float s = fmaxf(sa * x + sb, -1.f);
-  return (s * x * x + x + (F + h - h * F) * s * x * (1 - x)) /
-         (x * x * s + (F + 2 * h - 2 * h * F) * s * x * (1 - x) + 1);
-}
-
-// Drift of one quad lane: returns the new count j in [0, N].  Lost (x == 0) and, for N > 6, fixed
-// (x == 1) slots have a certain outcome (0 and N) and skip the sampler.
-__device__ __forceinline__ int drift_lane(uint32_t bits, float xs, int N) {
-  if (xs == 0.f) return 0;
-  if (xs == 1.f && N > 6) return N;
-  const float mean = xs * N;
-  const float var = (1.0f - xs) * mean;
-  return binom_draw_lane(bits, mean, var, static_cast<float>(N));
-}
-
-// Drift of one scalar-tail slot: counter (slot + 2, generation, pop, 0), variance evaluated in
-// double as the reference's scalar tail does (go_fish_impl.cuh:121).
-__device__ __forceinline__ int drift_tail(int seed1, int seed2, int slot, int generation, int pop, float xs, int N) {
-  if (xs == 0.f) return 0;
-  if (xs == 1.f && N > 6) return N;
-  const float mean = xs * N;
-  const float var = static_cast<float>((1.0 - static_cast<double>(xs)) * static_cast<double>(mean));
-  const uint4 r = philox(seed1, seed2, slot + 2, generation, pop, 0);
-  return binom_draw_tail(r.x, mean, var, static_cast<float>(N));
-}
-
-__device__ __forceinline__ int clampi(int v, int lo, int hi) { return max(lo, min(v, hi)); }
-
-// ------------------------------------------------------------------------------------------------
 // the fused generation kernel
 // ------------------------------------------------------------------------------------------------
 // Work items of one warp: the draws of its 128 slots that need the sampler, compacted so that every
@@ -114,22 +78,7 @@ struct WarpDraws {
 // Draws of the four lanes of one quad.  COOP = false: each thread draws its own lanes.  COOP = true:
 // the warp pools its work items and draws them branch by branch (all 32 lanes of the warp must call
 // this together).  Both give identical results: the same function of the same (bits, mean, var, N).
-// Resident drift blocks per SM the register allocation must allow (6: at most 40 registers; the
-// kernel is latency-bound, and 6 resident blocks beat 4 by ~4% with no spills).
-#ifndef GF_DRIFT_MIN_BLOCKS
-#define GF_DRIFT_MIN_BLOCKS 6
-#endif
 constexpr int kDriftMinBlocks = GF_DRIFT_MIN_BLOCKS;
-
-// The quad-lane sampler is inlined; the reference compiles its counterpart out of line in another
-// translation unit (shared.cu:10-18).  Both forms give bit-identical draws on sm_100a (checked against
-// the reference kernel for every sampler branch), and inlining is ~8% faster.  GF_DRAW_OUT_OF_LINE
-// restores the out-of-line call.
-#ifdef GF_DRAW_OUT_OF_LINE
-#define GF_LANE_DRAW binom_draw_lane
-#else
-#define GF_LANE_DRAW binom_draw_body
-#endif
 
 template <bool COOP>
 __device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsigned need, int N, int lane,
@@ -718,6 +667,7 @@ static gf_status begin_common(Engine* e, const gf_sim_config* c, long long initi
   e->compact_interval = c->compact_interval;
   e->any_preserved = false;
   e->step_index = 0;
+  e->count_slot = 0;
   e->cur = 0;
   e->id_cur = 0;
   const long long want = std::max<long long>({static_cast<long long>(c->reserve_mutations),
@@ -894,7 +844,7 @@ static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int 
     if (need > e->capacity) {
       // exact count, then grow
       int M = 0;
-      GF_CUDA(e, cudaMemcpyAsync(&M, e->d_count + (e->step_index & 1), sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+      GF_CUDA(e, cudaMemcpyAsync(&M, e->d_count + e->count_slot, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
       GF_CUDA(e, cudaStreamSynchronize(e->stream));
       e->M_upper = M;
       need = M + new_total;
@@ -905,7 +855,7 @@ static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int 
     }
   }
   const int tiles_bound = static_cast<int>(align_up(std::max<long long>(need, 1), kTileSlots) / kTileSlots);
-  const int slot_in = static_cast<int>(e->step_index & 1);
+  const int slot_in = e->count_slot;
   const int slot_out = slot_in ^ 1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (e->profiling) {
@@ -970,6 +920,127 @@ static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int 
     e->cur ^= 1;
   }
   e->step_index++;
+  e->count_slot ^= 1;
+  return GF_OK;
+}
+
+// Make room for `need` slots: tighten the host bound from finished read-backs, then from an exact
+// (synchronizing) read of the count, and grow the arrays if still short.
+static gf_status ensure_capacity(Engine* e, long long new_slots, long long* need_out) {
+  long long need = e->M_upper + new_slots;
+  if (need > e->capacity) {
+    poll_pending(e, true);
+    need = e->M_upper + new_slots;
+    if (need > e->capacity) {
+      int M = 0;
+      GF_CUDA(e, cudaMemcpyAsync(&M, e->d_count + e->count_slot, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+      GF_CUDA(e, cudaStreamSynchronize(e->stream));
+      e->M_upper = M;
+      need = M + new_slots;
+      if (need > e->capacity) {
+        gf_status st = set_capacity(e, std::max<long long>(need + need / 2, e->capacity * 3 / 2), M);
+        if (st != GF_OK) return st;
+      }
+    }
+  }
+  *need_out = need;
+  return GF_OK;
+}
+
+// Queue the asynchronous read-back of the survivor count in d_count[slot].
+static gf_status push_readback(Engine* e, int slot) {
+  poll_pending(e, false);
+  PendingCount pc;
+  gf_status st = get_event(e, &pc.event);
+  if (st != GF_OK) return st;
+  pc.slot = e->next_slot;
+  e->next_slot = (e->next_slot + 1) % e->pinned_slots;
+  pc.added = 0;
+  GF_CUDA(e, cudaMemcpyAsync(e->h_pinned + pc.slot, e->d_count + slot, sizeof(int), cudaMemcpyDeviceToHost,
+                             e->stream));
+  GF_CUDA(e, cudaEventRecord(pc.event, e->stream));
+  if (static_cast<int>(e->pending.size()) >= e->pinned_slots - 1) poll_pending(e, true);
+  e->pending.push_back(pc);
+  e->M_exact = false;
+  return GF_OK;
+}
+
+// Single-population generations a window may hold: drifted, no migration factor other than 1.
+static bool window_eligible(const Engine* e, const gf_generation& g) {
+  return e->use_windows && e->P == 1 && g.pop[0].drift == 1 && g.migration[0] == 1.0f;
+}
+
+constexpr int kMaxWindow = 128;
+
+// Run generations [first, first + count) of the batch as one window launch.
+static gf_status launch_window(Engine* e, int b, int first, int count, const GenHost* gh) {
+  WinRep& R = e->h_wrep[b][first];
+  long long news = 0;
+  for (int k = 0; k < count; ++k) news += e->h_wgen[b][first + k].new_count;
+  long long need = 0;
+  gf_status st = ensure_capacity(e, news, &need);
+  if (st != GF_OK) return st;
+  const GenArgs& last = e->h_table[b][first + count - 1];
+  R.base = 0;
+  R.capacity = e->capacity;
+  R.rec = first;
+  R.ngen = count;
+  R.tile0 = 0;
+  R.ntiles = static_cast<int>(align_up(std::max<long long>(need, 1), kTileSlots) / kTileSlots);
+  R.seed1 = e->seed1;
+  R.seed2 = e->seed2;
+  R.check_preserved = e->any_preserved ? 1 : 0;
+  R.compact = last.flag ? 1 : 0;
+  R.preserve = (last.flag && gh[first + count - 1].preserve) ? 1 : 0;
+  R.rep = 0;
+  GF_CUDA(e, cudaMemcpyAsync(e->d_wrep[b] + first, &R, sizeof(WinRep), cudaMemcpyHostToDevice, e->stream));
+  const int slot = e->count_slot;
+  WindowLaunch w;
+  w.A = e->freq[e->cur];
+  w.B = e->freq[e->cur ^ 1];
+  w.id_gp_cur = e->id_gp[e->id_cur];
+  w.id_tid_cur = e->id_tid[e->id_cur];
+  w.id_gp_next = e->id_gp[e->id_cur ^ 1];
+  w.id_tid_next = e->id_tid[e->id_cur ^ 1];
+  w.flags = e->flags;
+  w.tile_count = e->tile_count;
+  w.tile_offset = e->tile_offset;
+  w.M_in = e->d_count + slot;
+  w.M_end = e->d_count + 3;
+  w.M_next = e->d_count + (slot ^ 1);
+  w.M_out = e->d_count + (slot ^ 1);
+  w.reps = e->d_wrep[b] + first;
+  w.nreps = 1;
+  w.recs = e->d_wgen[b];
+  w.total_tiles = R.ntiles;
+  w.any_compact = R.compact != 0;
+  w.stats = e->d_stats;
+  w.fault = e->d_count + 2;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    ev0 = prof_event(e);
+    ev1 = prof_event(e);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  st = window_run(e, w, e->freq[e->cur]);
+  if (st != GF_OK) return st;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_drift.emplace_back(ev0, ev1);
+  }
+  e->M_upper = need;
+  for (auto& pc : e->pending) pc.added += news;
+  e->count_slot ^= 1;
+  e->step_index += count;
+  if (R.compact) {
+    if (R.preserve) e->any_preserved = true;
+    e->id_cur ^= 1;
+    e->compactions += 1;
+    st = push_readback(e, e->count_slot);
+    if (st != GF_OK) return st;
+  } else {
+    e->cur ^= 1;
+  }
   return GF_OK;
 }
 
@@ -990,23 +1061,70 @@ static gf_status run_batch(Engine* e, const gf_generation* gens, int n) {
     GF_CUDA(e, cudaMallocHost(&e->h_table[b], sizeof(GenArgs) * cap));
     e->table_cap[b] = cap;
   }
+  const bool windows = e->use_windows && e->P == 1;
+  if (windows && e->wtable_cap[b] < static_cast<size_t>(n)) {
+    const size_t cap = std::max<size_t>(n, 256);
+    if (e->d_wgen[b]) GF_CUDA(e, cudaFree(e->d_wgen[b]));
+    if (e->h_wgen[b]) GF_CUDA(e, cudaFreeHost(e->h_wgen[b]));
+    if (e->d_wrep[b]) GF_CUDA(e, cudaFree(e->d_wrep[b]));
+    if (e->h_wrep[b]) GF_CUDA(e, cudaFreeHost(e->h_wrep[b]));
+    e->d_wgen[b] = nullptr;
+    e->h_wgen[b] = nullptr;
+    e->d_wrep[b] = nullptr;
+    e->h_wrep[b] = nullptr;
+    e->wtable_cap[b] = 0;
+    GF_CUDA(e, cudaMalloc(&e->d_wgen[b], sizeof(WinGen) * cap));
+    GF_CUDA(e, cudaMallocHost(&e->h_wgen[b], sizeof(WinGen) * cap));
+    GF_CUDA(e, cudaMalloc(&e->d_wrep[b], sizeof(WinRep) * cap));
+    GF_CUDA(e, cudaMallocHost(&e->h_wrep[b], sizeof(WinRep) * cap));
+    e->wtable_cap[b] = cap;
+  }
   std::vector<GenHost> gh(n);
   for (int i = 0; i < n; ++i) {
     gf_status st = build_args(e, gens[i], e->h_table[b][i], gh[i]);
     if (st != GF_OK) return st;
     e->h_table[b][i].check_preserved = e->any_preserved ? 1 : 0;
+    if (windows) {
+      const GenArgs& a = e->h_table[b][i];
+      WinGen& wg = e->h_wgen[b][i];
+      wg.generation = a.generation;
+      wg.Nc = a.Nc[0];
+      wg.new_count = a.new_total;
+      wg.new_freq = a.new_freq[0];
+      wg.F = a.F[0];
+      wg.h = a.h[0];
+      wg.sel_a = a.sel_a[0];
+      wg.sel_b = a.sel_b[0];
+      wg.alive = a.alive_mask & 1;
+    }
   }
   GF_CUDA(e, cudaMemcpyAsync(e->d_table[b], e->h_table[b], sizeof(GenArgs) * n, cudaMemcpyHostToDevice, e->stream));
-  for (int i = 0; i < n; ++i) {
-    gf_status st = launch_generation(e, e->h_table[b][i], e->d_table[b], i, gh[i]);
-    if (st != GF_OK) return st;
+  if (windows)
+    GF_CUDA(e, cudaMemcpyAsync(e->d_wgen[b], e->h_wgen[b], sizeof(WinGen) * n, cudaMemcpyHostToDevice, e->stream));
+  int i = 0;
+  while (i < n) {
+    if (windows && window_eligible(e, gens[i])) {
+      int j = i;
+      while (j < n && j - i < kMaxWindow && window_eligible(e, gens[j])) {
+        const bool ends = e->h_table[b][j].flag != 0;
+        ++j;
+        if (ends) break;
+      }
+      gf_status st = launch_window(e, b, i, j - i, gh.data());
+      if (st != GF_OK) return st;
+      i = j;
+    } else {
+      gf_status st = launch_generation(e, e->h_table[b][i], e->d_table[b], i, gh[i]);
+      if (st != GF_OK) return st;
+      ++i;
+    }
   }
   GF_CUDA(e, cudaEventRecord(e->table_done[b], e->stream));
   return GF_OK;
 }
 
 static gf_status current_count(Engine* e, int* M) {
-  GF_CUDA(e, cudaMemcpyAsync(M, e->d_count + (e->step_index & 1), sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(M, e->d_count + e->count_slot, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
   gf_status st = check_device_fault(e);
   if (st != GF_OK) return st;
   poll_pending(e, true);
@@ -1100,6 +1218,10 @@ void gf_engine_destroy(gf_engine* g) {
     if (e->d_table[b]) cudaFree(e->d_table[b]);
     if (e->h_table[b]) cudaFreeHost(e->h_table[b]);
     if (e->table_done[b]) cudaEventDestroy(e->table_done[b]);
+    if (e->d_wgen[b]) cudaFree(e->d_wgen[b]);
+    if (e->h_wgen[b]) cudaFreeHost(e->h_wgen[b]);
+    if (e->d_wrep[b]) cudaFree(e->d_wrep[b]);
+    if (e->h_wrep[b]) cudaFreeHost(e->h_wrep[b]);
   }
   for (auto& pr : e->prof_drift) e->prof_pool.insert(e->prof_pool.end(), {pr.first, pr.second});
   for (auto& pr : e->prof_compact) e->prof_pool.insert(e->prof_pool.end(), {pr.first, pr.second});
@@ -1315,10 +1437,11 @@ gf_status gf_sim_stats_read(gf_engine* g, gf_sim_stats* out) {
 gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
   if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
   Engine* e = &g->impl;
-  if (t->draw_strategy < 0 || t->draw_strategy > 1 || t->blocks_per_sm < 0)
-    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1}, blocks_per_sm >= 0");
+  if (t->draw_strategy < 0 || t->draw_strategy > 1 || t->blocks_per_sm < 0 || t->windows < 0 || t->windows > 1)
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1}, blocks_per_sm >= 0, windows in {0, 1}");
   e->draw_coop = t->draw_strategy;
   e->blocks_per_sm = t->blocks_per_sm;
+  e->use_windows = t->windows != 0;
   return GF_OK;
 }
 
@@ -1326,6 +1449,7 @@ gf_status gf_engine_get_tuning(const gf_engine* g, gf_tuning* t) {
   if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
   t->draw_strategy = g->impl.draw_coop;
   t->blocks_per_sm = g->impl.blocks_per_sm;
+  t->windows = g->impl.use_windows ? 1 : 0;
   return GF_OK;
 }
 

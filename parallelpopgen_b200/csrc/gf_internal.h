@@ -48,6 +48,56 @@ struct GenArgs {
   float mig[kMaxPops * kMaxPops];  // [from * num_pops + to]
 };
 
+// One generation of one single-population replicate, as the window kernel reads it (36 B).
+struct WinGen {
+  int generation;
+  int Nc;          // Nchrom_e of the drift (0: extinction generation, the row is cleared)
+  int new_count;   // new mutations appended after the drift (host draw)
+  float new_freq;  // 1.f / Nchrom_e, computed on the host
+  float F, h, sel_a, sel_b;
+  int alive;       // demography(pop, generation) > 0 (compaction flag of the window's last generation)
+};
+
+// One replicate's window in a window launch (56 B).  A replicate owns the arena slots
+// [base, base + capacity) of every per-slot array; base is a multiple of 1024.
+struct WinRep {
+  long long base;
+  long long capacity;
+  int rec;              // first WinGen record of the window
+  int ngen;             // generations in the window (>= 1)
+  int tile0;            // first launch tile of the replicate
+  int ntiles;           // launch tiles of the replicate (covers its end-of-window count)
+  int seed1, seed2;
+  int check_preserved;  // some slot may carry the preserved mark
+  int compact;          // flags after the last generation; compaction follows
+  int preserve;         // the compaction marks survivors preserved
+  int rep;              // index into the per-replicate count arrays
+};
+
+// Pointers and sizes of one window launch plus its optional compaction.
+struct WindowLaunch {
+  const float* A;          // state at the window start
+  float* B;                // state at the window end
+  int* id_gp_cur;          // IDs (new mutations are written here)
+  int* id_tid_cur;
+  int* id_gp_next;         // compaction output of the IDs
+  int* id_tid_next;
+  unsigned* flags;
+  unsigned* tile_count;
+  unsigned* tile_offset;
+  const int* M_in;         // [rep] counts at the window start
+  int* M_end;              // [rep] counts at the window end (before compaction)
+  int* M_next;             // [rep] counts for the next window when not compacting (may alias nothing)
+  int* M_out;              // [rep] counts after compaction
+  const WinRep* reps;      // device
+  int nreps;
+  const WinGen* recs;      // device
+  int total_tiles;
+  bool any_compact;
+  unsigned long long* stats;
+  int* fault;
+};
+
 struct PendingCount {
   cudaEvent_t event;
   int slot;           // index into the pinned readback array
@@ -70,7 +120,8 @@ struct Engine {
   float num_sites = 0.f;
   int compact_interval = 0;
   bool any_preserved = false;
-  long long step_index = 0;  // generations run since begin (selects the count ping-pong slot)
+  long long step_index = 0;  // generations run since begin
+  int count_slot = 0;        // d_count slot holding the current mutation count
 
   // device arrays; capacity = row stride in slots
   long long capacity = 0;
@@ -99,6 +150,13 @@ struct Engine {
   size_t table_cap[2] = {0, 0};
   cudaEvent_t table_done[2] = {nullptr, nullptr};
   int table_next = 0;
+  // window records of the single-population path (same double-buffering as the tables above)
+  WinGen* d_wgen[2] = {nullptr, nullptr};
+  WinGen* h_wgen[2] = {nullptr, nullptr};
+  WinRep* d_wrep[2] = {nullptr, nullptr};
+  WinRep* h_wrep[2] = {nullptr, nullptr};
+  size_t wtable_cap[2] = {0, 0};
+  bool use_windows = true;   // single-population runs use the window kernel
 
   // measurement
   unsigned long long* d_stats = nullptr;  // [0] sum of drift slots, [1] generations
@@ -128,6 +186,9 @@ gf_status cuda_fail(Engine* e, cudaError_t err, const char* what);
   } while (0)
 
 gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
+
+// Window launch (+ segmented compaction into compact_dst), window.cu.
+gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst);
 
 }  // namespace gf
 

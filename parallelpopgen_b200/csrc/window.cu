@@ -1,0 +1,347 @@
+// Windowed drift: every generation of a compaction window in one launch.
+//
+// Between two compactions a mutation keeps its slot, and its update in generation g depends only
+// on its own frequency, the generation's parameters, the slot index and the mutation count M_g at
+// the start of g (which decides the quad / scalar-tail counter layout, go_fish_impl.cuh:97-123).
+// M_g = M_start + the host-drawn new-mutation counts of the earlier generations of the window, so
+// one thread can carry its quad through all generations in registers: read the row once, drift it
+// W times with exactly the per-generation arithmetic (gf_drift.cuh), let slots born inside the
+// window start at 1/Nc in their birth generation (add_new_mutations, go_fish_impl.cu:138-145), and
+// write the row once with the survival flags of the last generation.  A launch covers any number of
+// single-population replicates, each in its own 1024-aligned arena segment with its own window
+// length, seeds and parameters: the plain engine uses it with one replicate, the batched engine with
+// thousands.  Results are bit-identical to running the per-generation kernel W times.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "gf_drift.cuh"
+#include "gf_internal.h"
+
+namespace gf {
+
+constexpr int kWinThreads = 256;
+constexpr int kWinTile = kWinThreads * 4;
+
+// replicate owning launch tile `gt` (last replicate whose tile0 <= gt)
+__device__ __forceinline__ int find_rep(const WinRep* __restrict__ reps, int nreps, int gt) {
+  int lo = 0, hi = nreps - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (reps[mid].tile0 <= gt) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kWinThreads, GF_DRIFT_MIN_BLOCKS)
+    window_kernel(const float* __restrict__ A, float* __restrict__ B, int* __restrict__ id_gp,
+                  int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
+                  const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
+                  const WinRep* __restrict__ reps, int nreps, const WinGen* __restrict__ recs, int total_tiles,
+                  unsigned long long* __restrict__ stats, int* __restrict__ fault) {
+  __shared__ int s_rep;
+  __shared__ unsigned s_warp[kWinThreads / 32];
+  const int lane = threadIdx.x & 31;
+  for (int gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
+    if (threadIdx.x == 0) s_rep = find_rep(reps, nreps, gt);
+    __syncthreads();
+    const WinRep R = reps[s_rep];
+    __syncthreads();
+    const int t = gt - R.tile0;
+    const int q = t * kWinThreads + threadIdx.x;  // quad within the replicate
+    const int s0 = 4 * q;
+    const int cap = static_cast<int>(R.capacity);
+    const int M0 = M_in[R.rep];
+    float* const rowB = B + R.base;
+    const float* const rowA = A + R.base;
+    int* const gp = id_gp + R.base;
+    int* const tid = id_tid + R.base;
+
+    float x[4];
+    if (s0 + 3 < M0) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(rowA + s0));
+      x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[j] = (s0 + j < M0) ? rowA[s0 + j] : 0.f;
+    }
+
+    int M = M0;
+    int alive = 1;
+#pragma unroll 1
+    for (int k = 0; k < R.ngen; ++k) {
+      const WinGen G = recs[R.rec + k];
+      const int N = G.Nc;
+      const int g = G.generation;
+      alive = G.alive;
+      if (s0 < M) {
+        if (N <= 0) {
+          // extinction generation: the population's row is cleared
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (s0 + j < M) x[j] = 0.f;
+        } else if (q < (M >> 2)) {
+          // whole quad: Philox (q + 2, g, 0, 0), lanes x, y, z, w
+          const bool neutral = (G.sel_a == 0.f && G.sel_b == 0.f);
+          float xs[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            xs[j] = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
+                            : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
+          int res[4];
+          unsigned need = 0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            res[j] = (xs[j] == 1.f && N > 6) ? N : 0;
+            if (!(xs[j] == 0.f || (xs[j] == 1.f && N > 6))) need |= 1u << j;
+          }
+          if (need) {
+            const uint4 r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
+            const uint32_t rb[4] = {r.x, r.y, r.z, r.w};
+            const float Nf = static_cast<float>(N);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
+          }
+          const float Nf = static_cast<float>(N);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) x[j] = static_cast<float>(clampi(res[j], 0, N)) / Nf;
+        } else {
+          // scalar tail: Philox (slot + 2, g, 0, 0) lane x, variance in double
+          const bool neutral = (G.sel_a == 0.f && G.sel_b == 0.f);
+#pragma unroll 1
+          for (int j = 0; j < 4; ++j) {
+            const int e = s0 + j;
+            if (e >= M) break;
+            const float xs = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
+                                     : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
+            x[j] = static_cast<float>(clampi(drift_tail(R.seed1, R.seed2, e, g, 0, xs, N), 0, N)) /
+                   static_cast<float>(N);
+          }
+        }
+      }
+      // births: slots [M, M + new_count) start at 1/Nc with ID (g, 0, slot - M + 1)
+      const int Mn = M + G.new_count;
+      if (s0 + 3 >= M && s0 < Mn) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int e = s0 + j;
+          if (e >= M && e < Mn && e < cap) {
+            x[j] = G.new_freq;
+            gp[e] = g;
+            tid[e] = e - M + 1;
+          }
+        }
+      }
+      M = Mn;
+    }
+    const int Mw = min(M, cap);
+    if (s0 + 3 < Mw) {
+      *reinterpret_cast<float4*>(rowB + s0) = make_float4(x[0], x[1], x[2], x[3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (s0 + j < Mw) rowB[s0 + j] = x[j];
+    }
+
+    if (R.compact) {
+      // flag_segregating_mutations for one population: keep unless lost or fixed (when alive), or
+      // if preserved
+      unsigned keep = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int e = s0 + j;
+        if (e >= Mw) continue;
+        // lost or fixed in the (only) population -- or the population is not alive -- removes it
+        bool k = alive && !(x[j] <= 0.f || x[j] >= 1.f);
+        if (R.check_preserved && e < M0 && tid[e] < 0) k = true;
+        if (k) keep |= 1u << j;
+      }
+      unsigned word = keep << ((lane & 7) * 4);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 4);
+      if ((lane & 7) == 0) flags[(R.base + s0) >> 5] = word;
+      unsigned c = __popc(keep);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+      if (lane == 0) s_warp[threadIdx.x >> 5] = c;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned tot = 0;
+#pragma unroll
+        for (int w = 0; w < kWinThreads / 32; ++w) tot += s_warp[w];
+        tile_count[R.base / kWinTile + t] = tot;
+      }
+      __syncthreads();
+    }
+
+    if (t == 0 && threadIdx.x == 0) {
+      // window bookkeeping, once per replicate
+      unsigned long long mg = 0;
+      int m = M0;
+      for (int k = 0; k < R.ngen; ++k) {
+        mg += static_cast<unsigned long long>(m);
+        m += recs[R.rec + k].new_count;
+      }
+      atomicAdd(stats, mg);
+      atomicAdd(stats + 1, static_cast<unsigned long long>(R.ngen));
+      if (M > cap) atomicExch(fault, kFaultCapacity);
+      M_end[R.rep] = Mw;
+      if (M_next && !R.compact) M_next[R.rep] = Mw;
+    }
+  }
+}
+
+// One block per replicate: exclusive scan of its tile survivor counts, compacted count.
+constexpr int kSegScanThreads = 1024;
+__global__ void __launch_bounds__(kSegScanThreads)
+    seg_scan_kernel(const unsigned* __restrict__ tile_count, unsigned* __restrict__ tile_offset,
+                    const WinRep* __restrict__ reps, const int* __restrict__ M_end, int* __restrict__ M_out) {
+  const WinRep R = reps[blockIdx.x];
+  if (!R.compact) return;
+  __shared__ unsigned s_warp[kSegScanThreads / 32];
+  __shared__ unsigned s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = (M_end[R.rep] + kWinTile - 1) / kWinTile;
+  const long long t0 = R.base / kWinTile;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += kSegScanThreads) {
+    const int i = base + threadIdx.x;
+    const unsigned v = i < n ? tile_count[t0 + i] : 0u;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned wv = s_warp[lane];
+      unsigned wi = wv;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      s_warp[lane] = wi - wv;
+    }
+    __syncthreads();
+    const unsigned excl = s_carry + s_warp[warp] + incl - v;
+    if (i < n) tile_offset[t0 + i] = excl;
+    __syncthreads();
+    if (threadIdx.x == kSegScanThreads - 1) s_carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) M_out[R.rep] = static_cast<int>(s_carry);
+}
+
+// Stable scatter of every compacting replicate's survivors (scatter_arrays, go_fish_impl.cu:147-189),
+// staged through shared memory into one contiguous run per tile.
+__global__ void __launch_bounds__(kWinThreads)
+    seg_scatter_kernel(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ gp_src,
+                       const int* __restrict__ tid_src, int* __restrict__ gp_dst, int* __restrict__ tid_dst,
+                       const unsigned* __restrict__ flags, const unsigned* __restrict__ tile_offset,
+                       const WinRep* __restrict__ reps, int nreps, const int* __restrict__ M_end, int total_tiles) {
+  __shared__ int s_rep;
+  __shared__ unsigned s_words[32];
+  __shared__ unsigned s_prefix[32];
+  __shared__ float s_stage[kWinTile];
+  const int t = threadIdx.x;
+  for (int gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
+    if (t == 0) s_rep = find_rep(reps, nreps, gt);
+    __syncthreads();
+    const WinRep R = reps[s_rep];
+    __syncthreads();
+    const int tile = gt - R.tile0;
+    const int ntiles = (M_end[R.rep] + kWinTile - 1) / kWinTile;
+    if (!R.compact || tile >= ntiles) continue;  // block-uniform
+    const long long atile = R.base / kWinTile + tile;
+    if (t < 32) {
+      const unsigned w = flags[atile * 32 + t];
+      s_words[t] = w;
+      const unsigned c = __popc(w);
+      unsigned incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (t >= o) incl += y;
+      }
+      s_prefix[t] = incl - c;
+    }
+    __syncthreads();
+    const int w = t >> 3, sh = (t & 7) * 4;
+    const unsigned word = s_words[w];
+    const unsigned nib = (word >> sh) & 0xFu;
+    const int local = static_cast<int>(s_prefix[w] + __popc(word & ((1u << sh) - 1u)));
+    const int count = static_cast<int>(s_prefix[31] + __popc(s_words[31]));
+    const long long out0 = R.base + tile_offset[atile];
+    const long long in0 = R.base + static_cast<long long>(tile) * kWinTile + 4 * t;
+    if (nib) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(src + in0));
+      int k = local;
+      if (nib & 1u) s_stage[k++] = v.x;
+      if (nib & 2u) s_stage[k++] = v.y;
+      if (nib & 4u) s_stage[k++] = v.z;
+      if (nib & 8u) s_stage[k++] = v.w;
+    }
+    __syncthreads();
+    for (int k = t; k < count; k += kWinThreads) dst[out0 + k] = s_stage[k];
+    __syncthreads();
+    int* s_istage = reinterpret_cast<int*>(s_stage);
+    for (int arr = 0; arr < 2; ++arr) {
+      const int* s = arr ? tid_src : gp_src;
+      int* d = arr ? tid_dst : gp_dst;
+      if (nib) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(s + in0));
+        int k = local;
+        const bool mark = arr && R.preserve;
+        if (nib & 1u) s_istage[k++] = mark ? -abs(v.x) : v.x;
+        if (nib & 2u) s_istage[k++] = mark ? -abs(v.y) : v.y;
+        if (nib & 4u) s_istage[k++] = mark ? -abs(v.z) : v.z;
+        if (nib & 8u) s_istage[k++] = mark ? -abs(v.w) : v.w;
+      }
+      __syncthreads();
+      for (int k = t; k < count; k += kWinThreads) d[out0 + k] = s_istage[k];
+      __syncthreads();
+    }
+  }
+}
+
+// Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
+// and scatter into `compact_dst` (the other state buffer).
+gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
+  static int occupancy = 0;
+  if (occupancy == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, window_kernel, kWinThreads, 0) != cudaSuccess ||
+        occupancy < 1) {
+      cudaGetLastError();
+      occupancy = 1;
+    }
+  }
+  const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
+  const int blocks = std::max(1, std::min(w.total_tiles, e->num_sms * per_sm));
+  window_kernel<<<blocks, kWinThreads, 0, e->stream>>>(w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count,
+                                                       w.M_in, w.M_end, w.M_next, w.reps, w.nreps, w.recs,
+                                                       w.total_tiles, w.stats, w.fault);
+  GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 1;
+  if (w.any_compact) {
+    seg_scan_kernel<<<w.nreps, kSegScanThreads, 0, e->stream>>>(w.tile_count, w.tile_offset, w.reps, w.M_end,
+                                                                w.M_out);
+    GF_CUDA(e, cudaGetLastError());
+    const int sblocks = std::max(1, std::min(w.total_tiles, e->num_sms * 8));
+    seg_scatter_kernel<<<sblocks, kWinThreads, 0, e->stream>>>(w.B, compact_dst, w.id_gp_cur, w.id_tid_cur,
+                                                               w.id_gp_next, w.id_tid_next, w.flags,
+                                                               w.tile_offset, w.reps, w.nreps, w.M_end,
+                                                               w.total_tiles);
+    GF_CUDA(e, cudaGetLastError());
+    e->kernel_launches += 2;
+  }
+  return GF_OK;
+}
+
+}  // namespace gf

@@ -117,14 +117,14 @@ class Engine:
         return {"mutation_generations": st.mutation_generations, "generations": st.generations,
                 "compactions": st.compactions, "kernel_launches": st.kernel_launches}
 
-    def set_tuning(self, draw_strategy: int = 0, blocks_per_sm: int = 0) -> None:
-        t = _capi.Tuning(int(draw_strategy), int(blocks_per_sm))
+    def set_tuning(self, draw_strategy: int = 0, blocks_per_sm: int = 0, windows: int = 1) -> None:
+        t = _capi.Tuning(int(draw_strategy), int(blocks_per_sm), int(windows))
         self._check(self.lib.gf_engine_set_tuning(self.h, ctypes.byref(t)))
 
     def get_tuning(self) -> dict:
         t = _capi.Tuning()
         self._check(self.lib.gf_engine_get_tuning(self.h, ctypes.byref(t)))
-        return {"draw_strategy": t.draw_strategy, "blocks_per_sm": t.blocks_per_sm}
+        return {"draw_strategy": t.draw_strategy, "blocks_per_sm": t.blocks_per_sm, "windows": t.windows}
 
     def set_profiling(self, enable: bool) -> None:
         self._check(self.lib.gf_engine_set_profiling(self.h, int(enable)))

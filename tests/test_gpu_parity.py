@@ -237,3 +237,28 @@ def test_histogram_and_sfs_match_oracle():
         y = rng.random(5000).astype(np.float32)
         got = e.site_frequency_spectrum(y, Nc, 64, L).astype(np.float64)
         np.testing.assert_allclose(got, orc.sfs(y, 64, L), rtol=1e-5, atol=1e-4)
+
+
+@pytest.mark.parametrize("gamma,ci,mse", [(0.0, 25, True), (-10.0, 25, True), (4.0, 7, False), (0.0, 0, True)])
+def test_window_path_equals_per_generation_path(gamma, ci, mse):
+    """Single-population generations run as window launches by default; the per-generation kernel
+    must give the same state bit for bit (including compactions, births and IDs)."""
+    N = 3000
+    s = ConstantModel.s_from_gamma(gamma, N, 0.0) if gamma else 0.0
+    model = ConstantModel(N=N, s=s, mu=2e-8, h=0.3)
+    gens = constant_generations(model, 1, 300, ci)
+    out = []
+    for windows in (1, 0):
+        with Engine() as e:
+            e.set_tuning(windows=windows)
+            if mse:
+                e.begin_mse(model.mse_pops(), seed1=7, seed2=9, num_sites=2e6, compact_interval=ci)
+            else:
+                e.begin_blank(seed1=7, seed2=9, num_sites=2e6, compact_interval=ci)
+            e.run(gens)
+            out.append(e.read_state() + (e.stats()["mutation_generations"],))
+    (f1, i1, m1), (f0, i0, m0) = out
+    assert f1.shape == f0.shape and f1.shape[1] > 100
+    assert np.array_equal(f1.view(np.uint32), f0.view(np.uint32))
+    assert np.array_equal(i1, i0)
+    assert m1 == m0
