@@ -155,6 +155,52 @@ int32_t gf_new_mutation_count(int32_t seed1, int32_t seed2, float mu, int32_t Nc
                               int32_t generation, int32_t population);
 
 /* ---------------------------------------------------------------------------------------------
+ * Batched replicates (no reference counterpart: the reference runs one simulation per run_sim call,
+ * go_fish_impl.cuh:553-730).  Thousands of independent single-population simulations with their own
+ * sizes, demographies, selection, seeds and run lengths advance together: each super-step runs one
+ * compaction window of every unfinished replicate in one launch of the window kernel, followed by a
+ * segmented compaction.  Replicate r's result is bit-identical to a plain gf_sim_* run with the same
+ * seeds, model and compaction schedule (MSE start, compaction every compact_interval generations and
+ * at the final one).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct gf_replicate {
+  int32_t seed1, seed2;
+  float num_sites;          /* L */
+  float mu;                 /* per-site mutation rate */
+  float F, h;               /* inbreeding, dominance */
+  float sel_slope, sel_intercept; /* selection s(freq) = slope * freq + intercept */
+  int32_t N0;               /* individuals at generation 0 */
+  float growth_rate;        /* N(g) = round(N0 * exp(growth_rate * g)), as demography_exponential_growth */
+  int32_t N_min, N_max;     /* ... clamped to [N_min, N_max] (N_min >= 1) */
+  int32_t num_generations;  /* generations to run after the MSE start */
+  int32_t compact_interval; /* >= 1 */
+} gf_replicate;
+
+/* Population size of replicate `rep` at `generation` (the clamped exponential above, evaluated on the
+ * host in float like Sim_Model::demography_exponential_growth), for building the equivalent plain run. */
+int32_t gf_replicate_population(const gf_replicate* rep, int32_t generation);
+
+/* Begin R replicates at mutation-selection equilibrium (initialize_mse for each). */
+gf_status gf_batch_begin(gf_engine* engine, const gf_replicate* reps, int32_t num_replicates);
+/* Run super-steps until every replicate has finished (max_super_steps <= 0) or for at most
+ * max_super_steps; *out_active (may be NULL) receives the number of unfinished replicates. */
+gf_status gf_batch_run(gf_engine* engine, int32_t max_super_steps, int32_t* out_active);
+/* Current state of replicate r (frequencies [M], IDs [M][4]), its count and generation. */
+gf_status gf_batch_read_state(gf_engine* engine, int32_t r, float* freq_out, int32_t* ids_out, int32_t max_mutations,
+                              int32_t* out_num_mutations, int32_t* out_generation);
+/* Projected SFS of sample size n of every replicate's current state, host out[r * n + k]. */
+gf_status gf_batch_sfs(gf_engine* engine, int32_t n, float* out);
+typedef struct gf_batch_stats {
+  double mutation_generations; /* all replicates, all generations */
+  int64_t generations;         /* sum over replicates */
+  int64_t super_steps;
+  int32_t replicates;
+  int32_t active;
+  int64_t arena_slots;         /* device slots reserved for all replicates */
+} gf_batch_stats;
+gf_status gf_batch_stats_read(gf_engine* engine, gf_batch_stats* out);
+
+/* ---------------------------------------------------------------------------------------------
  * Spectrum (spectrum.h:24-43, spectrum.cu:153-294).  Inputs are one population row of a host time
  * sample, as the reference's functions take it; outputs are host arrays.
  * ------------------------------------------------------------------------------------------- */

@@ -60,6 +60,20 @@ class Tuning(ctypes.Structure):
     _fields_ = [("draw_strategy", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("windows", ctypes.c_int32)]
 
 
+class Replicate(ctypes.Structure):
+    _fields_ = [("seed1", ctypes.c_int32), ("seed2", ctypes.c_int32), ("num_sites", ctypes.c_float),
+                ("mu", ctypes.c_float), ("F", ctypes.c_float), ("h", ctypes.c_float),
+                ("sel_slope", ctypes.c_float), ("sel_intercept", ctypes.c_float), ("N0", ctypes.c_int32),
+                ("growth_rate", ctypes.c_float), ("N_min", ctypes.c_int32), ("N_max", ctypes.c_int32),
+                ("num_generations", ctypes.c_int32), ("compact_interval", ctypes.c_int32)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("mutation_generations", ctypes.c_double), ("generations", ctypes.c_int64),
+                ("super_steps", ctypes.c_int64), ("replicates", ctypes.c_int32), ("active", ctypes.c_int32),
+                ("arena_slots", ctypes.c_int64)]
+
+
 class SimConfig(ctypes.Structure):
     _fields_ = [
         ("seed1", ctypes.c_int32), ("seed2", ctypes.c_int32), ("num_sites", ctypes.c_float),
@@ -94,6 +108,12 @@ SIGNATURES = {
     "gf_site_frequency_spectrum_device": (_I, [_P, _P, _I, _I, _I, _F, _P]),
     "gf_site_frequency_spectrum_noalloc": (_I, [_P, _I, _I, _I, _F, _P, _P]),
     "gf_sim_stats_read": (_I, [_P, ctypes.POINTER(SimStats)]),
+    "gf_replicate_population": (_I, [ctypes.POINTER(Replicate), _I]),
+    "gf_batch_begin": (_I, [_P, _P, _I]),
+    "gf_batch_run": (_I, [_P, _I, ctypes.POINTER(_I)]),
+    "gf_batch_read_state": (_I, [_P, _I, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "gf_batch_sfs": (_I, [_P, _I, _P]),
+    "gf_batch_stats_read": (_I, [_P, ctypes.POINTER(BatchStats)]),
     "gf_engine_set_profiling": (_I, [_P, _I]),
     "gf_engine_set_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),
     "gf_engine_get_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),

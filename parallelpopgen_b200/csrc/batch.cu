@@ -1,0 +1,707 @@
+// Batched ragged replicates: thousands of independent single-population GO_Fish simulations with
+// their own sizes, growth, selection, seeds and run lengths, advancing together.
+//
+// Layout: one arena of slots shared by all replicates; replicate r owns [base_r, base_r + cap_r) of
+// every per-slot array (frequency ping-pong, the two ID words, flags), base_r a multiple of 1024 so a
+// 1024-slot tile belongs to one replicate.  A super-step runs, for every unfinished replicate, the
+// generations up to its next compaction (its own window length) in ONE window-kernel launch over
+// all replicates' tiles, then one segmented scan (a block per replicate) and one segmented scatter.
+// The host draws the per-generation new-mutation counts (as the reference does on its host,
+// calc_new_mutations_Index, go_fish_impl.cuh:454-467) and reads the survivor counts back once per
+// super-step.  Because every per-slot operation is the plain engine's (same Philox counters relative
+// to the replicate's own slots, same compaction schedule, same MSE start code), replicate r's state
+// is bit-identical to a plain run with the same inputs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "gf_drift.cuh"
+#include "gf_internal.h"
+#include "gf_mse.cuh"
+
+namespace gf {
+
+constexpr int kBatchTile = 1024;
+
+static long long align_tiles(long long v) { return (v + kBatchTile - 1) / kBatchTile * kBatchTile; }
+
+// N(g): round(N0 * exp(rate * g)) in float (demography_exponential_growth), clamped
+static int rep_population(const gf_replicate& p, int g) {
+  const int n = static_cast<int>(std::round(p.N0 * std::exp(p.growth_rate * static_cast<float>(g))));
+  return std::min(std::max(n, p.N_min), p.N_max);
+}
+
+static int rep_nchrom(const gf_replicate& p, int g) {
+  return static_cast<int>(2 * rep_population(p, g) / (1 + p.F));
+}
+
+// ------------------------------------------------------------------------------------------------
+// batched MSE start
+// ------------------------------------------------------------------------------------------------
+struct MseRep {
+  long long area_off;   // offset of its Nc0 area / integral slices
+  long long class_off;  // offset of its Nc0 - 1 classes
+  long long slot_base;  // arena base
+  int Nc0, N0, selected;
+  float mu, L, F, h, sa, sb;
+  int seed1, seed2;
+};
+
+template <typename Off>
+__device__ __forceinline__ int find_seg(const MseRep* __restrict__ r, int n, long long idx, Off off) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off(r[mid]) <= idx) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void batch_mse_area_kernel(float* __restrict__ area, const MseRep* __restrict__ reps, int R,
+                                      long long total) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(blockDim.x) * gridDim.x) {
+    const int r = find_seg(reps, R, i, [](const MseRep& m) { return m.area_off; });
+    const MseRep m = reps[r];
+    if (!m.selected) continue;
+    const int id = static_cast<int>(i - m.area_off);
+    area[i] = mse_area(id, 1.0f / m.Nc0, m.N0, m.F, m.h, m.sa, m.sb);
+  }
+}
+
+// one block per replicate: the plain engine's integral code on its slice
+__global__ void __launch_bounds__(1024) batch_mse_integral_kernel(const float* __restrict__ area,
+                                                                  float* __restrict__ integral,
+                                                                  const MseRep* __restrict__ reps) {
+  const MseRep m = reps[blockIdx.x];
+  if (!m.selected) return;
+  mse_integral_block(area + m.area_off, integral + m.area_off, m.Nc0);
+}
+
+__global__ void batch_mse_count_kernel(unsigned* __restrict__ counts, const float* __restrict__ integral,
+                                       const MseRep* __restrict__ reps, int R, long long total) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(blockDim.x) * gridDim.x) {
+    const int r = find_seg(reps, R, i, [](const MseRep& m) { return m.class_off; });
+    const MseRep m = reps[r];
+    const int id = static_cast<int>(i - m.class_off);
+    const float* integ = integral + m.area_off;
+    const float mse_total = m.selected ? integ[0] : 0.f;
+    counts[i] = mse_class_count(id, integ, mse_total, m.mu, m.N0, m.Nc0, m.L, m.sa, m.sb, m.F, m.h, m.seed1,
+                                m.seed2, 0);
+  }
+}
+
+// one block per replicate: exclusive scan of its class counts, M0
+__global__ void __launch_bounds__(1024) batch_class_scan_kernel(const unsigned* __restrict__ counts,
+                                                                unsigned* __restrict__ starts,
+                                                                const MseRep* __restrict__ reps, int* __restrict__ M0) {
+  const MseRep m = reps[blockIdx.x];
+  const int n = max(m.Nc0 - 1, 0);
+  __shared__ unsigned s_warp[32];
+  __shared__ unsigned s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    const int i = base + threadIdx.x;
+    const unsigned v = i < n ? counts[m.class_off + i] : 0u;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned wv = s_warp[lane];
+      unsigned wi = wv;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      s_warp[lane] = wi - wv;
+    }
+    __syncthreads();
+    const unsigned excl = s_carry + s_warp[warp] + incl - v;
+    if (i < n) starts[m.class_off + i] = excl;
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) M0[blockIdx.x] = static_cast<int>(s_carry);
+}
+
+// slot k of replicate r: its class by binary search over the class starts; frequency (id + 1) / Nc0,
+// ID (0, 0, k + 1) (initialize_mse_mutation_array + mse_set_mutID, go_fish_impl.cu:45-70)
+struct FillRep {
+  long long slot_prefix;  // global fill index of the replicate's slot 0
+  long long class_off;
+  long long base;
+  int Nc0, M0;
+};
+
+__global__ void batch_mse_fill_kernel(float* __restrict__ freq, int* __restrict__ id_gp, int* __restrict__ id_tid,
+                                      const unsigned* __restrict__ starts, const FillRep* __restrict__ reps, int R,
+                                      long long total) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(blockDim.x) * gridDim.x) {
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (reps[mid].slot_prefix <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    const FillRep f = reps[lo];
+    const int k = static_cast<int>(i - f.slot_prefix);
+    if (k >= f.M0) continue;
+    int a = 0, b = f.Nc0 - 2;
+    while (a < b) {
+      const int mid = (a + b + 1) >> 1;
+      if (static_cast<int>(starts[f.class_off + mid]) <= k) a = mid;
+      else b = mid - 1;
+    }
+    freq[f.base + k] = (a + 1.f) / f.Nc0;
+    id_gp[f.base + k] = 0;
+    id_tid[f.base + k] = k + 1;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// batched SFS: one block per replicate, direct projection of its frequencies in double
+// ------------------------------------------------------------------------------------------------
+struct SfsRep {
+  long long base;
+  int M;
+  float L;
+};
+
+constexpr int kBatchSfsThreads = 128;
+
+__global__ void __launch_bounds__(kBatchSfsThreads)
+    batch_sfs_kernel(const float* __restrict__ freq, const SfsRep* __restrict__ reps, int n,
+                     const double* __restrict__ lgc, float* __restrict__ out) {
+  const SfsRep R = reps[blockIdx.x];
+  __shared__ double s_lp[kBatchSfsThreads];
+  __shared__ double s_lq[kBatchSfsThreads];
+  __shared__ unsigned s_seg[kBatchSfsThreads];
+  __shared__ double s_acc0[kBatchSfsThreads];
+  const int levels = n + 1;
+  double acc[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) acc[u] = 0.0;
+  unsigned nonseg = 0;
+  for (int c0 = 0; c0 < R.M; c0 += kBatchSfsThreads) {
+    const int i = c0 + threadIdx.x;
+    double lp = 0.0, lq = 0.0;
+    unsigned seg = 0;
+    if (i < R.M) {
+      const float p = freq[R.base + i];
+      if (p > 0.f && p < 1.f) {
+        seg = 1;
+        lp = log(static_cast<double>(p));
+        lq = log1p(-static_cast<double>(p));
+      } else {
+        ++nonseg;
+      }
+    }
+    s_lp[threadIdx.x] = lp;
+    s_lq[threadIdx.x] = lq;
+    s_seg[threadIdx.x] = seg;
+    __syncthreads();
+    const int cend = min(kBatchSfsThreads, R.M - c0);
+    for (int t = 0; t < cend; ++t) {
+      if (!s_seg[t]) continue;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = threadIdx.x + u * kBatchSfsThreads;
+        if (k < levels) acc[u] += exp(lgc[k] + k * s_lp[t] + (n - k) * s_lq[t]);
+      }
+    }
+    __syncthreads();
+  }
+  // non-segregating count of the block
+  s_acc0[threadIdx.x] = static_cast<double>(nonseg);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ns = 0;
+    for (int t = 0; t < kBatchSfsThreads; ++t) ns += s_acc0[t];
+    s_acc0[0] = ns;
+  }
+  __syncthreads();
+  const double ns = s_acc0[0];
+  __syncthreads();
+  // bin n folds into bin 0: park it in shared memory
+  double top = 0.0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int k = threadIdx.x + u * kBatchSfsThreads;
+    if (k == n) top = acc[u];
+  }
+  if (threadIdx.x == n % kBatchSfsThreads) s_acc0[1] = top;
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int k = threadIdx.x + u * kBatchSfsThreads;
+    if (k < n) {
+      double v = acc[u];
+      if (k == 0) v += s_acc0[1] + ns + static_cast<double>(R.L - R.M);
+      out[static_cast<long long>(blockIdx.x) * n + k] = static_cast<float>(v);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host
+// ------------------------------------------------------------------------------------------------
+void release_batch(Engine* e) {
+  Batch* b = e->batch;
+  if (!b) return;
+  cudaStreamSynchronize(e->stream);
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(b->freq[k]);
+    cudaFree(b->id_gp[k]);
+    cudaFree(b->id_tid[k]);
+    cudaFree(b->d_M[k]);
+  }
+  cudaFree(b->flags);
+  cudaFree(b->tile_count);
+  cudaFree(b->tile_offset);
+  cudaFree(b->d_Mend);
+  cudaFreeHost(b->h_M);
+  cudaFree(b->d_recs);
+  cudaFreeHost(b->h_recs);
+  cudaFree(b->d_reps);
+  cudaFreeHost(b->h_reps);
+  delete b;
+  e->batch = nullptr;
+}
+
+// Upper bound on a replicate's slots: neutral equilibrium of its largest population plus one window
+// of new mutations with 7-sigma margins (set_Index_Length's margin, go_fish_impl.cuh:235), with room
+// to spare; selection only lowers the count.
+static long long replicate_capacity(const gf_replicate& p, int M0) {
+  int ncmax = 0;
+  for (int g : {0, p.num_generations}) ncmax = std::max(ncmax, rep_nchrom(p, g));
+  if (p.growth_rate != 0.f) ncmax = std::max(ncmax, static_cast<int>(2 * p.N_max / (1 + p.F)));
+  const double theta = 2.0 * p.mu * p.num_sites * ncmax;
+  const double eq = theta * (std::log(std::max(ncmax, 2)) + 0.58);
+  const double lam = static_cast<double>(p.mu) * ncmax * p.num_sites;
+  const double window = p.compact_interval * (lam + 7.0 * std::sqrt(lam + 1.0));
+  const double want = std::max<double>(M0, 1.5 * eq + 10.0 * std::sqrt(eq + 1.0)) + 2.0 * window + 1024.0;
+  return align_tiles(static_cast<long long>(want));
+}
+
+template <typename T>
+static gf_status grow_pinned(Engine* e, T** d, T** h, size_t* cap, size_t need) {
+  if (*cap >= need) return GF_OK;
+  const size_t c = std::max<size_t>(need, 1024);
+  if (*d) GF_CUDA(e, cudaFree(*d));
+  if (*h) GF_CUDA(e, cudaFreeHost(*h));
+  *d = nullptr;
+  *h = nullptr;
+  *cap = 0;
+  GF_CUDA(e, cudaMalloc(d, sizeof(T) * c));
+  GF_CUDA(e, cudaMallocHost(h, sizeof(T) * c));
+  *cap = c;
+  return GF_OK;
+}
+
+static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
+  if (!in || R <= 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "no replicates");
+  for (int r = 0; r < R; ++r) {
+    const gf_replicate& p = in[r];
+    if (p.N0 < 1 || p.N_min < 1 || p.N_max < p.N_min || p.compact_interval < 1 || p.num_generations < 0 ||
+        !(p.num_sites > 0) || p.mu < 0 || p.F < 0 || p.F > 1)
+      return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: invalid parameters", r);
+    if (p.num_generations > GF_MAX_GENERATION)
+      return fail(e, GF_ERR_CAPACITY, "replicate %d: %d generations above %d", r, p.num_generations, GF_MAX_GENERATION);
+  }
+  GF_CUDA(e, cudaSetDevice(e->device));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  release_batch(e);
+  Batch* b = new Batch();
+  e->batch = b;
+  b->R = R;
+  b->reps.resize(R);
+  // ---- MSE classes ----
+  std::vector<MseRep> mr(R);
+  long long area_total = 0, class_total = 0;
+  for (int r = 0; r < R; ++r) {
+    BatchRep& br = b->reps[r];
+    br.p = in[r];
+    const gf_replicate& p = in[r];
+    MseRep& m = mr[r];
+    m.N0 = rep_population(p, 0);
+    m.Nc0 = static_cast<int>(2 * m.N0 / (1 + p.F));
+    m.selected = (p.sel_slope != 0.f || p.sel_intercept != 0.f) ? 1 : 0;
+    m.mu = p.mu;
+    m.L = p.num_sites;
+    m.F = p.F;
+    m.h = p.h;
+    m.sa = p.sel_slope;
+    m.sb = p.sel_intercept;
+    m.seed1 = p.seed1;
+    m.seed2 = p.seed2;
+    m.area_off = area_total;
+    m.class_off = class_total;
+    area_total += std::max(m.Nc0, 1);
+    class_total += std::max(m.Nc0 - 1, 0);
+    br.Nc = m.Nc0;
+  }
+  MseRep* d_mr = nullptr;
+  float *d_area = nullptr, *d_integral = nullptr;
+  unsigned *d_counts = nullptr, *d_starts = nullptr;
+  int* d_M0 = nullptr;
+  GF_CUDA(e, cudaMalloc(&d_mr, sizeof(MseRep) * R));
+  GF_CUDA(e, cudaMalloc(&d_area, sizeof(float) * area_total));
+  GF_CUDA(e, cudaMalloc(&d_integral, sizeof(float) * area_total));
+  GF_CUDA(e, cudaMalloc(&d_counts, sizeof(unsigned) * std::max<long long>(class_total, 1)));
+  GF_CUDA(e, cudaMalloc(&d_starts, sizeof(unsigned) * std::max<long long>(class_total, 1)));
+  GF_CUDA(e, cudaMalloc(&d_M0, sizeof(int) * R));
+  GF_CUDA(e, cudaMemcpyAsync(d_mr, mr.data(), sizeof(MseRep) * R, cudaMemcpyHostToDevice, e->stream));
+  const int grid = e->num_sms * 8;
+  batch_mse_area_kernel<<<grid, 256, 0, e->stream>>>(d_area, d_mr, R, area_total);
+  batch_mse_integral_kernel<<<R, 1024, 0, e->stream>>>(d_area, d_integral, d_mr);
+  if (class_total > 0) batch_mse_count_kernel<<<grid, 256, 0, e->stream>>>(d_counts, d_integral, d_mr, R, class_total);
+  batch_class_scan_kernel<<<R, 1024, 0, e->stream>>>(d_counts, d_starts, d_mr, d_M0);
+  GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 4;
+  std::vector<int> M0(R);
+  GF_CUDA(e, cudaMemcpyAsync(M0.data(), d_M0, sizeof(int) * R, cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  // ---- arena ----
+  long long arena = 0;
+  for (int r = 0; r < R; ++r) {
+    BatchRep& br = b->reps[r];
+    br.base = arena;
+    br.capacity = replicate_capacity(br.p, M0[r]);
+    br.M = M0[r];
+    br.generation = 0;
+    br.next_compact = br.p.compact_interval;
+    br.done = br.p.num_generations == 0;
+    arena += br.capacity;
+  }
+  b->arena = arena;
+  for (int k = 0; k < 2; ++k) {
+    GF_CUDA(e, cudaMalloc(&b->freq[k], sizeof(float) * arena));
+    GF_CUDA(e, cudaMalloc(&b->id_gp[k], sizeof(int) * arena));
+    GF_CUDA(e, cudaMalloc(&b->id_tid[k], sizeof(int) * arena));
+    GF_CUDA(e, cudaMalloc(&b->d_M[k], sizeof(int) * R));
+  }
+  GF_CUDA(e, cudaMalloc(&b->flags, sizeof(unsigned) * (arena / 32)));
+  GF_CUDA(e, cudaMalloc(&b->tile_count, sizeof(unsigned) * (arena / kBatchTile)));
+  GF_CUDA(e, cudaMalloc(&b->tile_offset, sizeof(unsigned) * (arena / kBatchTile)));
+  GF_CUDA(e, cudaMalloc(&b->d_Mend, sizeof(int) * R));
+  GF_CUDA(e, cudaMallocHost(&b->h_M, sizeof(int) * R));
+  GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
+  GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
+  // ---- fill ----
+  std::vector<FillRep> fr(R);
+  long long fill_total = 0;
+  for (int r = 0; r < R; ++r) {
+    fr[r].slot_prefix = fill_total;
+    fr[r].class_off = mr[r].class_off;
+    fr[r].base = b->reps[r].base;
+    fr[r].Nc0 = mr[r].Nc0;
+    fr[r].M0 = M0[r];
+    fill_total += M0[r];
+  }
+  FillRep* d_fr = nullptr;
+  GF_CUDA(e, cudaMalloc(&d_fr, sizeof(FillRep) * R));
+  GF_CUDA(e, cudaMemcpyAsync(d_fr, fr.data(), sizeof(FillRep) * R, cudaMemcpyHostToDevice, e->stream));
+  if (fill_total > 0)
+    batch_mse_fill_kernel<<<grid, 256, 0, e->stream>>>(b->freq[0], b->id_gp[0], b->id_tid[0], d_starts, d_fr, R,
+                                                        fill_total);
+  GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 1;
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  cudaFree(d_mr);
+  cudaFree(d_area);
+  cudaFree(d_integral);
+  cudaFree(d_counts);
+  cudaFree(d_starts);
+  cudaFree(d_M0);
+  cudaFree(d_fr);
+  GF_CUDA(e, cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream));
+  GF_CUDA(e, cudaMemsetAsync(e->d_count + 2, 0, sizeof(int), e->stream));
+  return GF_OK;
+}
+
+// New-mutation draws of the window records, spread over host threads for large batches.
+static void fill_records(std::vector<WinGen>& recs, const std::vector<std::pair<int, int>>& jobs,
+                         const std::vector<BatchRep>& reps, const std::vector<int>& first) {
+  auto work = [&](size_t a, size_t z) {
+    for (size_t j = a; j < z; ++j) {
+      const int r = jobs[j].first;
+      const int ngen = jobs[j].second;
+      const gf_replicate& p = reps[r].p;
+      for (int k = 0; k < ngen; ++k) {
+        const int g = reps[r].generation + 1 + k;
+        const int N = rep_population(p, g);
+        const int Nc = static_cast<int>(2 * N / (1 + p.F));
+        WinGen& w = recs[first[j] + k];
+        w.generation = g;
+        w.Nc = Nc;
+        w.new_count = (N > 0 && Nc > 0) ? host_new_mutation_count(p.seed1, p.seed2, p.mu, Nc, p.num_sites, g, 0) : 0;
+        w.new_freq = Nc > 0 ? 1.f / Nc : 0.f;
+        w.F = p.F;
+        w.h = p.h;
+        w.sel_a = p.sel_slope;
+        w.sel_b = p.sel_intercept;
+        w.alive = N > 0;
+      }
+    }
+  };
+  size_t total = 0;
+  for (auto& j : jobs) total += j.second;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = total > 20000 ? std::min<unsigned>(hw, 16) : 1;
+  if (nt <= 1) {
+    work(0, jobs.size());
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (jobs.size() + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const size_t a = t * per, z = std::min(jobs.size(), a + per);
+    if (a < z) th.emplace_back(work, a, z);
+  }
+  for (auto& x : th) x.join();
+}
+
+static gf_status batch_super_step(Engine* e, int* active_out) {
+  Batch* b = e->batch;
+  std::vector<std::pair<int, int>> jobs;
+  std::vector<int> first;
+  int nrec = 0;
+  for (int r = 0; r < b->R; ++r) {
+    BatchRep& br = b->reps[r];
+    if (br.done) continue;
+    const int end = std::min(br.next_compact, br.p.num_generations);
+    const int ngen = end - br.generation;
+    jobs.emplace_back(r, ngen);
+    first.push_back(nrec);
+    nrec += ngen;
+  }
+  if (jobs.empty()) {
+    if (active_out) *active_out = 0;
+    return GF_OK;
+  }
+  std::vector<WinGen> recs(nrec);
+  fill_records(recs, jobs, b->reps, first);
+  gf_status st = grow_pinned(e, &b->d_recs, &b->h_recs, &b->recs_cap, nrec);
+  if (st != GF_OK) return st;
+  st = grow_pinned(e, &b->d_reps, &b->h_reps, &b->reps_cap, jobs.size());
+  if (st != GF_OK) return st;
+  std::memcpy(b->h_recs, recs.data(), sizeof(WinGen) * nrec);
+  int tiles = 0;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const int r = jobs[j].first;
+    BatchRep& br = b->reps[r];
+    long long news = 0;
+    for (int k = 0; k < jobs[j].second; ++k) news += recs[first[j] + k].new_count;
+    const long long need = br.M + news;
+    if (need > br.capacity)
+      return fail(e, GF_ERR_CAPACITY, "replicate %d needs %lld slots at generation %d, its segment holds %lld", r,
+                  need, br.generation, br.capacity);
+    WinRep& w = b->h_reps[j];
+    w.base = br.base;
+    w.capacity = br.capacity;
+    w.rec = first[j];
+    w.ngen = jobs[j].second;
+    w.tile0 = tiles;
+    w.ntiles = static_cast<int>(align_tiles(std::max<long long>(need, 1)) / kBatchTile);
+    w.seed1 = br.p.seed1;
+    w.seed2 = br.p.seed2;
+    w.check_preserved = 0;
+    w.compact = 1;
+    w.preserve = 0;
+    w.rep = r;
+    tiles += w.ntiles;
+  }
+  GF_CUDA(e, cudaMemcpyAsync(b->d_recs, b->h_recs, sizeof(WinGen) * nrec, cudaMemcpyHostToDevice, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(b->d_reps, b->h_reps, sizeof(WinRep) * jobs.size(), cudaMemcpyHostToDevice, e->stream));
+  WindowLaunch w;
+  w.A = b->freq[0];
+  w.B = b->freq[1];
+  w.id_gp_cur = b->id_gp[b->id_cur];
+  w.id_tid_cur = b->id_tid[b->id_cur];
+  w.id_gp_next = b->id_gp[b->id_cur ^ 1];
+  w.id_tid_next = b->id_tid[b->id_cur ^ 1];
+  w.flags = b->flags;
+  w.tile_count = b->tile_count;
+  w.tile_offset = b->tile_offset;
+  w.M_in = b->d_M[b->mslot];
+  w.M_end = b->d_Mend;
+  w.M_next = nullptr;
+  w.M_out = b->d_M[b->mslot ^ 1];
+  w.reps = b->d_reps;
+  w.nreps = static_cast<int>(jobs.size());
+  w.recs = b->d_recs;
+  w.total_tiles = tiles;
+  w.any_compact = true;
+  w.stats = e->d_stats;
+  w.fault = e->d_count + 2;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  st = window_run(e, w, b->freq[0]);
+  if (st != GF_OK) return st;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_drift.emplace_back(ev0, ev1);
+  }
+  b->mslot ^= 1;
+  b->id_cur ^= 1;
+  b->super_steps += 1;
+  // survivor counts of every replicate (one small read-back per super-step)
+  GF_CUDA(e, cudaMemcpyAsync(b->h_M, b->d_M[b->mslot], sizeof(int) * b->R, cudaMemcpyDeviceToHost, e->stream));
+  int fault = 0;
+  GF_CUDA(e, cudaMemcpyAsync(&fault, e->d_count + 2, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  if (fault) return fail(e, GF_ERR_DEVICE, "device status word reports fault %d", fault);
+  int active = 0;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    BatchRep& br = b->reps[jobs[j].first];
+    br.M = b->h_M[jobs[j].first];
+    br.generation += jobs[j].second;
+    b->generations += jobs[j].second;
+    br.next_compact = br.generation + br.p.compact_interval;
+    br.Nc = rep_nchrom(br.p, br.generation);
+    br.id_buf = b->id_cur;
+    if (br.generation >= br.p.num_generations) br.done = true;
+    else ++active;
+  }
+  if (active_out) *active_out = active;
+  return GF_OK;
+}
+
+}  // namespace gf
+
+using namespace gf;
+
+extern "C" {
+
+int32_t gf_replicate_population(const gf_replicate* rep, int32_t generation) {
+  return rep ? rep_population(*rep, generation) : 0;
+}
+
+gf_status gf_batch_begin(gf_engine* g, const gf_replicate* reps, int32_t R) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  return batch_begin(&g->impl, reps, R);
+}
+
+gf_status gf_batch_run(gf_engine* g, int32_t max_super_steps, int32_t* out_active) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  if (!e->batch) return fail(e, GF_ERR_STATE, "gf_batch_run before gf_batch_begin");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  int active = 1;
+  for (int s = 0; (max_super_steps <= 0 || s < max_super_steps) && active > 0; ++s) {
+    gf_status st = batch_super_step(e, &active);
+    if (st != GF_OK) return st;
+  }
+  if (out_active) {
+    int a = 0;
+    for (auto& br : e->batch->reps) a += br.done ? 0 : 1;
+    *out_active = a;
+  }
+  return GF_OK;
+}
+
+gf_status gf_batch_read_state(gf_engine* g, int32_t r, float* freq_out, int32_t* ids_out, int32_t max_mutations,
+                              int32_t* out_num, int32_t* out_generation) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  Batch* b = e->batch;
+  if (!b) return fail(e, GF_ERR_STATE, "no batch");
+  if (r < 0 || r >= b->R) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d outside [0, %d)", r, b->R);
+  GF_CUDA(e, cudaSetDevice(e->device));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  const BatchRep& br = b->reps[r];
+  if (out_num) *out_num = br.M;
+  if (out_generation) *out_generation = br.generation;
+  if (br.M > max_mutations) return fail(e, GF_ERR_CAPACITY, "replicate %d holds %d mutations", r, br.M);
+  if (br.M == 0) return GF_OK;
+  if (freq_out)
+    GF_CUDA(e, cudaMemcpy(freq_out, b->freq[0] + br.base, sizeof(float) * br.M, cudaMemcpyDeviceToHost));
+  if (ids_out) {
+    std::vector<int> gp(br.M), tid(br.M);
+    GF_CUDA(e, cudaMemcpy(gp.data(), b->id_gp[br.id_buf] + br.base, sizeof(int) * br.M, cudaMemcpyDeviceToHost));
+    GF_CUDA(e, cudaMemcpy(tid.data(), b->id_tid[br.id_buf] + br.base, sizeof(int) * br.M, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < br.M; ++i) {
+      ids_out[4 * i + 0] = gp[i] & 0xFFFFFF;
+      ids_out[4 * i + 1] = gp[i] >> 24;
+      ids_out[4 * i + 2] = tid[i];
+      ids_out[4 * i + 3] = 0;
+    }
+  }
+  return GF_OK;
+}
+
+gf_status gf_batch_sfs(gf_engine* g, int32_t n, float* out) {
+  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  Batch* b = e->batch;
+  if (!b) return fail(e, GF_ERR_STATE, "no batch");
+  if (n < 1 || n + 1 > 8 * kBatchSfsThreads) return fail(e, GF_ERR_CAPACITY, "sample size %d outside [1, %d)", n, 8 * kBatchSfsThreads);
+  for (int r = 0; r < b->R; ++r)
+    if (n >= b->reps[r].Nc) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: sample size %d >= Nchrom_e %d", r, n, b->reps[r].Nc);
+  GF_CUDA(e, cudaSetDevice(e->device));
+  std::vector<SfsRep> sr(b->R);
+  for (int r = 0; r < b->R; ++r) sr[r] = {b->reps[r].base, b->reps[r].M, b->reps[r].p.num_sites};
+  std::vector<double> lgc(n + 1);
+  const double ln = std::lgamma(n + 1.0);
+  for (int k = 0; k <= n; ++k) lgc[k] = ln - std::lgamma(k + 1.0) - std::lgamma(n - k + 1.0);
+  SfsRep* d_sr = nullptr;
+  double* d_lgc = nullptr;
+  float* d_out = nullptr;
+  GF_CUDA(e, cudaMalloc(&d_sr, sizeof(SfsRep) * b->R));
+  GF_CUDA(e, cudaMalloc(&d_lgc, sizeof(double) * (n + 1)));
+  GF_CUDA(e, cudaMalloc(&d_out, sizeof(float) * b->R * n));
+  GF_CUDA(e, cudaMemcpyAsync(d_sr, sr.data(), sizeof(SfsRep) * b->R, cudaMemcpyHostToDevice, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(d_lgc, lgc.data(), sizeof(double) * (n + 1), cudaMemcpyHostToDevice, e->stream));
+  batch_sfs_kernel<<<b->R, kBatchSfsThreads, 0, e->stream>>>(b->freq[0], d_sr, n, d_lgc, d_out);
+  GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 1;
+  GF_CUDA(e, cudaMemcpyAsync(out, d_out, sizeof(float) * b->R * n, cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  cudaFree(d_sr);
+  cudaFree(d_lgc);
+  cudaFree(d_out);
+  return GF_OK;
+}
+
+gf_status gf_batch_stats_read(gf_engine* g, gf_batch_stats* out) {
+  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+  Engine* e = &g->impl;
+  Batch* b = e->batch;
+  if (!b) return fail(e, GF_ERR_STATE, "no batch");
+  GF_CUDA(e, cudaSetDevice(e->device));
+  unsigned long long st[2] = {0, 0};
+  GF_CUDA(e, cudaMemcpyAsync(st, e->d_stats, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  out->mutation_generations = static_cast<double>(st[0]);
+  out->generations = b->generations;
+  out->super_steps = b->super_steps;
+  out->replicates = b->R;
+  int a = 0;
+  for (auto& br : b->reps) a += br.done ? 0 : 1;
+  out->active = a;
+  out->arena_slots = b->arena;
+  return GF_OK;
+}
+
+}  // extern "C"

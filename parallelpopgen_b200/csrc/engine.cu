@@ -26,6 +26,7 @@
 #include "gf_internal.h"
 #include "gf_rng.cuh"
 #include "gf_drift.cuh"
+#include "gf_mse.cuh"
 
 namespace gf {
 
@@ -445,83 +446,23 @@ __global__ void mark_preserved_kernel(int* __restrict__ tid, int n) {
 // ------------------------------------------------------------------------------------------------
 // mutation-selection-equilibrium start (initialize_mse and friends, go_fish_impl.cuh:20-71, 201-332)
 // ------------------------------------------------------------------------------------------------
-__device__ __forceinline__ float mse_density(float i, int N, float F, float h, float s) {
-  return exp(2 * N * s * i * ((2 * h + (1 - 2 * h) * i) * (1 - F) + 2 * F) / (1 + F));
-}
-
-// Trapezoid slices of the MSE integrand from frequency 1 down to 0 (calculate_area + trapezoidal_upper
-// + mse_integrand, go_fish_impl.cuh:24-53).
 __global__ void mse_area_kernel(float* __restrict__ area, int num_freq, float step, int N_ind, float F, float h,
                                 float sa, float sb) {
-  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < num_freq; id += blockDim.x * gridDim.x) {
-    const float a = static_cast<float>(1.0 - id * step);
-    const float b = a - step;
-    const float s1 = fmaxf(sa * a + sb, -1.f);
-    const float s2 = fmaxf(sa * b + sb, -1.f);
-    const float f1 = mse_density(a, N_ind, F, h, -1 * s1);
-    const float f2 = mse_density(b, N_ind, F, h, -1 * s2);
-    area[id] = step * (f1 + f2) / 2;
-  }
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < num_freq; id += blockDim.x * gridDim.x)
+    area[id] = mse_area(id, step, N_ind, F, h, sa, sb);
 }
 
-// Deterministic inclusive scan of the slices in double precision, stored reversed as float:
-// integral[id] = sum_{k <= num_freq-1-id} area[k] (the reference scans in float with CUB and then
-// reverses, go_fish_impl.cuh:213-221; its float summation order is not fixed).
 __global__ void __launch_bounds__(1024) mse_integral_kernel(const float* __restrict__ area, float* __restrict__ integral,
                                                             int num_freq) {
-  __shared__ double s_warp[32];
-  __shared__ double s_carry;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_carry = 0.0;
-  __syncthreads();
-  for (int base = 0; base < num_freq; base += 1024) {
-    const int idx = base + threadIdx.x;
-    const double v = idx < num_freq ? static_cast<double>(area[idx]) : 0.0;
-    double incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const double y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      const double w = s_warp[lane];
-      double wi = w;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const double y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-        if (lane >= o) wi += y;
-      }
-      s_warp[lane] = wi - w;
-    }
-    __syncthreads();
-    const double total = s_carry + s_warp[warp] + incl;
-    if (idx < num_freq) integral[num_freq - 1 - idx] = static_cast<float>(total);
-    __syncthreads();
-    if (threadIdx.x == 1023) s_carry = total;
-    __syncthreads();
-  }
+  mse_integral_block(area, integral, num_freq);
 }
 
-// Poisson count of mutations in each frequency class (initialize_mse_frequency_array,
-// go_fish_impl.cuh:58-71); counter (0, class, pop, 0).
 __global__ void mse_count_kernel(unsigned* __restrict__ counts, const float* __restrict__ integral, int offset,
                                  float mu, int N_ind, int Nchrom, float L, float sa, float sb, float F, float h,
                                  int seed1, int seed2, int pop, int use_integral) {
   const float mse_total = use_integral ? integral[0] : 0.f;
-  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < Nchrom - 1; id += blockDim.x * gridDim.x) {
-    const float i = (id + 1.f) / Nchrom;
-    const float j = ((Nchrom - id) + 1.f) / Nchrom;
-    const float s = sa * i + sb;
-    float lambda;
-    if (s == 0) {
-      lambda = 2 * mu * L / i;
-    } else {
-      lambda = 2 * mu * L * (mse_density(i, N_ind, F, h, s) * integral[id]) / (mse_total * i * j);
-    }
-    counts[offset + id] = static_cast<unsigned>(max(pois_draw(lambda, lambda, L * Nchrom, seed1, seed2, 0, id, pop), 0));
-  }
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < Nchrom - 1; id += blockDim.x * gridDim.x)
+    counts[offset + id] = mse_class_count(id, integral, mse_total, mu, N_ind, Nchrom, L, sa, sb, F, h, seed1, seed2, pop);
 }
 
 struct MseClassRange {
@@ -1208,6 +1149,7 @@ void gf_engine_destroy(gf_engine* g) {
   cudaSetDevice(e->device);
   cudaStreamSynchronize(e->stream);
   release_sim(e);
+  release_batch(e);
   for (auto ev : e->free_events) cudaEventDestroy(ev);
   if (e->spec_scratch) cudaFree(e->spec_scratch);
   if (e->spec_in) cudaFree(e->spec_in);

@@ -98,6 +98,44 @@ struct WindowLaunch {
   int* fault;
 };
 
+// Host record of one replicate of a batch.
+struct BatchRep {
+  gf_replicate p;
+  long long base = 0;       // arena offset (multiple of 1024)
+  long long capacity = 0;   // arena slots
+  int generation = 0;       // last generation run
+  int next_compact = 0;
+  int M = 0;                // count after the last super-step (read back)
+  int Nc = 0;               // Nchrom_e at `generation`
+  int id_buf = 0;           // ID buffer holding its state
+  bool done = false;
+};
+
+struct Batch {
+  int R = 0;
+  std::vector<BatchRep> reps;
+  long long arena = 0;
+  float* freq[2] = {nullptr, nullptr};
+  int* id_gp[2] = {nullptr, nullptr};
+  int* id_tid[2] = {nullptr, nullptr};
+  unsigned* flags = nullptr;
+  unsigned* tile_count = nullptr;
+  unsigned* tile_offset = nullptr;
+  int* d_M[2] = {nullptr, nullptr};
+  int* d_Mend = nullptr;
+  int* h_M = nullptr;        // pinned read-back of the counts
+  int mslot = 0;
+  int id_cur = 0;
+  WinGen* d_recs = nullptr;
+  WinGen* h_recs = nullptr;
+  size_t recs_cap = 0;
+  WinRep* d_reps = nullptr;
+  WinRep* h_reps = nullptr;
+  size_t reps_cap = 0;
+  long long super_steps = 0;
+  long long generations = 0;
+};
+
 struct PendingCount {
   cudaEvent_t event;
   int slot;           // index into the pinned readback array
@@ -158,6 +196,9 @@ struct Engine {
   size_t wtable_cap[2] = {0, 0};
   bool use_windows = true;   // single-population runs use the window kernel
 
+  // batched replicates (gf_batch_*)
+  Batch* batch = nullptr;
+
   // measurement
   unsigned long long* d_stats = nullptr;  // [0] sum of drift slots, [1] generations
   long long compactions = 0;
@@ -189,6 +230,12 @@ gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
 
 // Window launch (+ segmented compaction into compact_dst), window.cu.
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst);
+
+// Host draw of one population's new-mutation count (engine.cu).
+int host_new_mutation_count(int seed1, int seed2, float mu, int Nchrom_e, float num_sites, int generation, int pop);
+
+// Releases the batch of an engine (batch.cu).
+void release_batch(Engine* e);
 
 }  // namespace gf
 

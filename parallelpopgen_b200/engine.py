@@ -135,6 +135,39 @@ class Engine:
         return {"drift_ms": kt.drift_ms, "drift_launches": kt.drift_launches, "compact_ms": kt.compact_ms,
                 "compactions": kt.compactions}
 
+    # ---- batched replicates ----
+    def batch_begin(self, reps) -> None:
+        arr = (_capi.Replicate * len(reps))(*reps)
+        self._batch = arr
+        self._check(self.lib.gf_batch_begin(self.h, ctypes.cast(arr, ctypes.c_void_p), len(reps)))
+
+    def batch_run(self, max_super_steps: int = 0) -> int:
+        active = ctypes.c_int32()
+        self._check(self.lib.gf_batch_run(self.h, int(max_super_steps), ctypes.byref(active)))
+        return active.value
+
+    def batch_read_state(self, r: int, with_ids: bool = True):
+        """(frequencies, IDs, generation) of replicate r."""
+        M = ctypes.c_int32()
+        gen = ctypes.c_int32()
+        self.lib.gf_batch_read_state(self.h, r, None, None, 0, ctypes.byref(M), ctypes.byref(gen))  # size query
+        n = M.value
+        freq = np.empty(max(n, 1), dtype=np.float32)
+        ids = np.empty((max(n, 1), 4), dtype=np.int32) if with_ids else None
+        self._check(self.lib.gf_batch_read_state(self.h, r, ptr(freq), ptr(ids), max(n, 1), ctypes.byref(M),
+                                                 ctypes.byref(gen)))
+        return freq[:n], (ids[:n] if with_ids else None), gen.value
+
+    def batch_sfs(self, n: int, R: int) -> np.ndarray:
+        out = np.empty((R, n), dtype=np.float32)
+        self._check(self.lib.gf_batch_sfs(self.h, int(n), ptr(out)))
+        return out
+
+    def batch_stats(self) -> dict:
+        st = _capi.BatchStats()
+        self._check(self.lib.gf_batch_stats_read(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _capi.BatchStats._fields_}
+
     def synchronize(self) -> None:
         self._check(self.lib.gf_engine_synchronize(self.h))
 
@@ -156,6 +189,56 @@ class Engine:
                                        d_out: int) -> None:
         self._check(self.lib.gf_site_frequency_spectrum_device(self.h, ctypes.c_void_p(d_freq), M, Nc, n,
                                                                float(num_sites), ctypes.c_void_p(d_out)))
+
+
+def replicate(*, seed1, seed2, num_sites, mu, F, h, s, N0, growth_rate=0.0, N_min=1, N_max=None,
+              num_generations, compact_interval=25, sel_slope=0.0):
+    """A gf_replicate record (batched engine)."""
+    return _capi.Replicate(int(np.int32(np.uint32(seed1 & 0xFFFFFFFF))), int(np.int32(np.uint32(seed2 & 0xFFFFFFFF))),
+                           float(num_sites), float(mu), float(F), float(h), float(sel_slope), float(s), int(N0),
+                           float(growth_rate), int(N_min), int(N_max if N_max is not None else N0),
+                           int(num_generations), int(compact_interval))
+
+
+def replicate_population(rep, generation: int) -> int:
+    return _capi.load().gf_replicate_population(ctypes.byref(rep), int(generation))
+
+
+def replicate_plain_generations(rep, first: int = 1) -> np.ndarray:
+    """Per-generation records of the plain engine run equivalent to a batched replicate."""
+    G = rep.num_generations
+    gens = np.zeros(G, dtype=GEN_DTYPE)
+    g = np.arange(first, first + G)
+    gens["generation"] = g
+    ci = rep.compact_interval
+    gens["compact"] = (((g % ci) == 0) | (g == first + G - 1)).astype(np.int32)
+    N = np.array([replicate_population(rep, int(x)) for x in g], dtype=np.int64)
+    Nc = (np.float32(2) * N.astype(np.float32) / np.float32(np.float32(1) + np.float32(rep.F))).astype(np.int32)
+    pops = gens["pop"]
+    pops["Nchrom_e"][:, 0] = Nc
+    pops["drift"][:, 0] = 1
+    pops["alive"][:, 0] = (N > 0).astype(np.int32)
+    pops["mutate"][:, 0] = 1
+    pops["mu"][:, 0] = rep.mu
+    pops["F"][:, 0] = rep.F
+    pops["h"][:, 0] = rep.h
+    pops["sel_slope"][:, 0] = rep.sel_slope
+    pops["sel_intercept"][:, 0] = rep.sel_intercept
+    gens["migration"][:, 0] = 1.0
+    return gens
+
+
+def replicate_mse_pops(rep) -> np.ndarray:
+    pops = np.zeros(1, dtype=MSE_DTYPE)
+    N0 = replicate_population(rep, 0)
+    pops["N_ind"] = N0
+    pops["Nchrom_e"] = int(np.float32(2 * N0) / np.float32(np.float32(1) + np.float32(rep.F)))
+    pops["mu"] = rep.mu
+    pops["F"] = rep.F
+    pops["h"] = rep.h
+    pops["sel_slope"] = rep.sel_slope
+    pops["sel_intercept"] = rep.sel_intercept
+    return pops
 
 
 def new_mutation_count(seed1, seed2, mu, Nchrom_e, num_sites, generation, pop) -> int:

@@ -1,0 +1,77 @@
+"""Batched ragged replicates: every replicate of a batch must equal, bit for bit, the plain engine
+run with the same seeds, model and compaction schedule (final frequencies and mutation IDs), and its
+SFS must match the plain engine's SFS of that state (1e-5 relative)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from parallelpopgen_b200 import (ConstantModel, Engine, replicate, replicate_mse_pops, replicate_plain_generations,
+                                 replicate_population)
+
+pytestmark = pytest.mark.gpu
+
+
+def make_replicates(count: int, seed: int, max_gens: int):
+    rng = np.random.default_rng(seed)
+    reps = []
+    for r in range(count):
+        N0 = int(np.exp(rng.uniform(np.log(300), np.log(4000))))
+        gamma = float(rng.uniform(-40, 8)) if r % 3 else 0.0
+        F = float(rng.uniform(0, 0.5))
+        s = ConstantModel.s_from_gamma(gamma, N0, F) if gamma else 0.0
+        rate = float(rng.uniform(-0.001, 0.01))
+        reps.append(replicate(seed1=0xBEEF + 2 * r, seed2=0xDECAF - 2 * r, num_sites=float(rng.choice([2e6, 1e7])),
+                              mu=1e-8, F=F, h=float(rng.uniform(0, 1)), s=s, N0=N0, growth_rate=rate,
+                              N_min=max(N0 // 4, 50), N_max=4 * N0, num_generations=int(min(4 * N0, max_gens)),
+                              compact_interval=int(rng.integers(5, 40))))
+    return reps
+
+
+def plain_run(rep):
+    with Engine() as e:
+        e.begin_mse(replicate_mse_pops(rep), seed1=rep.seed1, seed2=rep.seed2, num_sites=rep.num_sites,
+                    compact_interval=rep.compact_interval)
+        e.run(replicate_plain_generations(rep))
+        f, ids = e.read_state()
+        return f[0], ids
+
+
+def test_batched_replicates_equal_plain_runs():
+    reps = make_replicates(12, seed=3, max_gens=1500)
+    with Engine() as e:
+        e.batch_begin(reps)
+        assert e.batch_run() == 0
+        states = [e.batch_read_state(r) for r in range(len(reps))]
+        st = e.batch_stats()
+        sfs = e.batch_sfs(40, len(reps))
+    assert st["active"] == 0 and st["generations"] == sum(r.num_generations for r in reps)
+    with Engine() as plain:
+        for r, rep in enumerate(reps):
+            f_b, ids_b, gen = states[r]
+            assert gen == rep.num_generations
+            f_p, ids_p = plain_run(rep)
+            assert f_b.shape == f_p.shape, (r, f_b.shape, f_p.shape)
+            assert np.array_equal(f_b.view(np.uint32), f_p.view(np.uint32)), r
+            assert np.array_equal(ids_b, ids_p), r
+            Nc = int(np.float32(2 * replicate_population(rep, rep.num_generations)) /
+                     np.float32(np.float32(1) + np.float32(rep.F)))
+            want = plain.site_frequency_spectrum(f_p, Nc, 40, rep.num_sites)
+            np.testing.assert_allclose(sfs[r].astype(np.float64), want.astype(np.float64), rtol=1e-5, atol=1e-3)
+
+
+def test_batched_super_steps_are_resumable():
+    """Running a batch in chunks of super-steps gives the same states as running it to completion."""
+    reps = make_replicates(5, seed=11, max_gens=600)
+    out = []
+    for chunk in (0, 7):
+        with Engine() as e:
+            e.batch_begin(reps)
+            if chunk:
+                while e.batch_run(chunk) > 0:
+                    pass
+            else:
+                e.batch_run()
+            out.append([e.batch_read_state(r)[0] for r in range(len(reps))])
+    for a, b in zip(*out):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
