@@ -361,6 +361,102 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+# ------------------------------------------------------------------------------------------------
+# batched replicates: simulations/s of one batched launch sequence vs the same replicates looped
+# through the plain engine
+# ------------------------------------------------------------------------------------------------
+def batched_replicates(R: int, n_max: float, seed: int = 2024):
+    """Seeded parameter draws of the batched workload: N0 log-uniform in [1e3, n_max], gamma uniform in
+    [-100, 10], h in [0, 1], F in [0, 0.5], exponential growth r in [-0.001, 0.01] clamped to
+    [N0/10, 10 N0], mu 1e-9, L 1e7, 4 N0 generations, seeds (0xbeef + 2r, 0xdecaf - 2r)."""
+    from parallelpopgen_b200 import ConstantModel, replicate
+    rng = np.random.default_rng(seed)
+    reps = []
+    for r in range(R):
+        N0 = int(round(np.exp(rng.uniform(np.log(1e3), np.log(n_max)))))
+        gamma = float(rng.uniform(-100.0, 10.0))
+        h = float(rng.uniform(0.0, 1.0))
+        F = float(rng.uniform(0.0, 0.5))
+        rate = float(rng.uniform(-0.001, 0.01))
+        reps.append(replicate(seed1=0xBEEF + 2 * r, seed2=0xDECAF - 2 * r, num_sites=1e7, mu=1e-9, F=F, h=h,
+                              s=ConstantModel.s_from_gamma(gamma, N0, F), N0=N0, growth_rate=rate,
+                              N_min=max(N0 // 10, 1), N_max=10 * N0, num_generations=4 * N0,
+                              compact_interval=25))
+    return reps
+
+
+def run_batched(args):
+    import torch
+    from parallelpopgen_b200 import Engine, replicate_mse_pops, replicate_plain_generations, replicate_population
+    from parallelpopgen_b200.autotune import tune_batch_cadence
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    eng = Engine(device=0, stream=stream.cuda_stream)
+    reps = batched_replicates(args.replicates, args.n_max)
+    tuned = tune_batch_cadence(eng, reps, use_cache=False)
+    for r in reps:
+        r.compact_interval = tuned["compact_interval"]
+    n = 100
+
+    def batch_step():
+        eng.batch_begin(reps)
+        eng.batch_run()
+        sfs = eng.batch_sfs(n, len(reps))
+        return eng.batch_stats(), sfs
+
+    for _ in range(args.warmup):
+        batch_step()
+    times, st = [], None
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            st, sfs = batch_step()
+            ev1.record(stream)
+            ev1.synchronize()
+            times.append(ev0.elapsed_time(ev1) * 1e-3)
+    batch_s = float(np.mean(times))
+    # the same replicates, one plain engine run each (a random sample, timed engine calls only)
+    rng = np.random.default_rng(7)
+    sample = rng.choice(len(reps), size=min(args.plain_sample, len(reps)), replace=False)
+    prepared = [(reps[i], replicate_mse_pops(reps[i]), replicate_plain_generations(reps[i])) for i in sample]
+    d_sfs = torch.empty(n, dtype=torch.float32, device="cuda")
+    plain_s = 0.0
+    for rep, pops, gens in prepared:
+        Nc = int(np.float32(2 * replicate_population(rep, rep.num_generations)) /
+                 np.float32(np.float32(1) + np.float32(rep.F)))
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        eng.begin_mse(pops, seed1=rep.seed1, seed2=rep.seed2, num_sites=rep.num_sites,
+                      compact_interval=rep.compact_interval)
+        eng.run(gens)
+        d_freq, _, M = eng.device_state()
+        eng.site_frequency_spectrum_device(d_freq, M, Nc, n, rep.num_sites, d_sfs.data_ptr())
+        ev1.record(stream)
+        ev1.synchronize()
+        plain_s += ev0.elapsed_time(ev1) * 1e-3
+    plain_rate = len(prepared) / plain_s
+    value = len(reps) / batch_s
+    print(json.dumps({
+        "metric": "simulations/s (batched ragged replicates)", "value": value, "unit": "simulations/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{len(reps)} single-population replicates: N0 log-uniform [1e3, {args.n_max:g}], "
+                               "gamma U[-100, 10], h U[0, 1], F U[0, 0.5], growth r U[-0.001, 0.01] clamped to "
+                               "[N0/10, 10 N0], mu 1e-9, L 1e7, 4 N0 generations, MSE start, SFS n=100",
+                   "compact_interval": tuned["compact_interval"], "cadence_trials": tuned["trials"]},
+        "mutation_generations_per_step": st["mutation_generations"],
+        "mutation_generations_per_s": st["mutation_generations"] / batch_s,
+        "super_steps": st["super_steps"],
+        "looped_plain": {"value": plain_rate, "unit": "simulations/s", "sample": len(prepared),
+                         "speedup_batched_over_looped": value / plain_rate},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,10 +464,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+                    help="plain: the headline single-population workload; batched: batched ragged replicates")
+    ap.add_argument("--replicates", type=int, default=4096)
+    ap.add_argument("--n-max", type=float, default=1e4)
+    ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--gens", type=int, default=GENS,
                     help="generations per simulation (profiling captures use a shorter run)")
     args = ap.parse_args()
     rank, local_rank, world = dist_env()
+    if args.workload == "batched":
+        if rank == 0:
+            run_batched(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

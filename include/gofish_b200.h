@@ -179,6 +179,8 @@ typedef struct gf_replicate {
 /* Population size of replicate `rep` at `generation` (the clamped exponential above, evaluated on the
  * host in float like Sim_Model::demography_exponential_growth), for building the equivalent plain run. */
 int32_t gf_replicate_population(const gf_replicate* rep, int32_t generation);
+/* The same for generations first .. first+count-1 into out[count]. */
+void gf_replicate_population_table(const gf_replicate* rep, int32_t first, int32_t count, int32_t* out);
 
 /* Begin R replicates at mutation-selection equilibrium (initialize_mse for each). */
 gf_status gf_batch_begin(gf_engine* engine, const gf_replicate* reps, int32_t num_replicates);

@@ -109,6 +109,7 @@ SIGNATURES = {
     "gf_site_frequency_spectrum_noalloc": (_I, [_P, _I, _I, _I, _F, _P, _P]),
     "gf_sim_stats_read": (_I, [_P, ctypes.POINTER(SimStats)]),
     "gf_replicate_population": (_I, [ctypes.POINTER(Replicate), _I]),
+    "gf_replicate_population_table": (None, [ctypes.POINTER(Replicate), _I, _I, _P]),
     "gf_batch_begin": (_I, [_P, _P, _I]),
     "gf_batch_run": (_I, [_P, _I, ctypes.POINTER(_I)]),
     "gf_batch_read_state": (_I, [_P, _I, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),

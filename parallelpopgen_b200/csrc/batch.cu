@@ -598,6 +598,11 @@ int32_t gf_replicate_population(const gf_replicate* rep, int32_t generation) {
   return rep ? rep_population(*rep, generation) : 0;
 }
 
+void gf_replicate_population_table(const gf_replicate* rep, int32_t first, int32_t count, int32_t* out) {
+  if (!rep || !out) return;
+  for (int32_t k = 0; k < count; ++k) out[k] = rep_population(*rep, first + k);
+}
+
 gf_status gf_batch_begin(gf_engine* g, const gf_replicate* reps, int32_t R) {
   if (!g) return GF_ERR_INVALID_ARGUMENT;
   return batch_begin(&g->impl, reps, R);

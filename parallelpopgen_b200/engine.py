@@ -212,7 +212,9 @@ def replicate_plain_generations(rep, first: int = 1) -> np.ndarray:
     gens["generation"] = g
     ci = rep.compact_interval
     gens["compact"] = (((g % ci) == 0) | (g == first + G - 1)).astype(np.int32)
-    N = np.array([replicate_population(rep, int(x)) for x in g], dtype=np.int64)
+    N = np.empty(G, dtype=np.int32)
+    _capi.load().gf_replicate_population_table(ctypes.byref(rep), int(first), int(G), N.ctypes.data)
+    N = N.astype(np.int64)
     Nc = (np.float32(2) * N.astype(np.float32) / np.float32(np.float32(1) + np.float32(rep.F))).astype(np.int32)
     pops = gens["pop"]
     pops["Nchrom_e"][:, 0] = Nc

@@ -86,3 +86,27 @@ def test_bench_replicas_reduce_over_two_gloo_ranks():
     # every rank simulates its own replicas: no seed pair repeats across ranks or halves
     seeds = [s for r in range(world) for s in out[r][2]]
     assert len(set(seeds)) == len(seeds) == 4
+
+
+def test_autotune_helpers(tmp_path, monkeypatch):
+    """Cache location, workload buckets and replicate cloning of the autotuner (no GPU)."""
+    from parallelpopgen_b200 import replicate
+    from parallelpopgen_b200.autotune import bucket, cache_path, clone_replicate
+    monkeypatch.setenv("PARALLELPOPGEN_B200_CACHE", str(tmp_path / "x.json"))
+    assert cache_path() == tmp_path / "x.json"
+    assert bucket(1 << 20) == "M2^20:P1" and bucket(0, 3) == "M2^0:P3"
+    r = replicate(seed1=-5, seed2=6, num_sites=1e7, mu=1e-9, F=0.2, h=0.1, s=-1e-3, N0=1234, num_generations=99)
+    c = clone_replicate(r)
+    c.num_generations = 7
+    assert r.num_generations == 99 and c.N0 == 1234 and c.seed1 == -5
+
+
+def test_batched_bench_workload_draws():
+    """The batched benchmark's parameter draws stay inside their stated ranges."""
+    import bench
+    reps = bench.batched_replicates(256, 1e4)
+    N0 = np.array([r.N0 for r in reps])
+    assert N0.min() >= 1000 and N0.max() <= 10000
+    assert all(r.num_generations == 4 * r.N0 for r in reps)
+    assert all(r.N_min == r.N0 // 10 and r.N_max == 10 * r.N0 for r in reps)
+    assert all(0.0 <= r.F <= 0.5 and 0.0 <= r.h <= 1.0 for r in reps)
