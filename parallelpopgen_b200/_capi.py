@@ -82,7 +82,12 @@ class SimConfig(ctypes.Structure):
     ]
 
 
-# every symbol declared in include/gofish_b200.h, with its ctypes signature
+class MlpConfig(ctypes.Structure):
+    _fields_ = [("batch_capacity", ctypes.c_int32), ("lr", ctypes.c_float), ("beta1", ctypes.c_float),
+                ("beta2", ctypes.c_float), ("eps", ctypes.c_float), ("weight_decay", ctypes.c_float)]
+
+
+# every symbol declared in include/*.h, with its ctypes signature
 _P = ctypes.c_void_p
 _I = ctypes.c_int32
 _F = ctypes.c_float
@@ -119,6 +124,19 @@ SIGNATURES = {
     "gf_engine_set_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),
     "gf_engine_get_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),
     "gf_engine_read_profile": (_I, [_P, ctypes.POINTER(KernelTimes)]),
+    # include/gf_surrogate.h
+    "gf_mlp_create": (_I, [_I, _P, ctypes.POINTER(MlpConfig), ctypes.POINTER(_P)]),
+    "gf_mlp_destroy": (_I, [_P]),
+    "gf_mlp_last_error": (ctypes.c_char_p, [_P]),
+    "gf_mlp_param_count": (ctypes.c_int64, []),
+    "gf_mlp_set_params": (_I, [_P, _P, ctypes.c_int64]),
+    "gf_mlp_get_params": (_I, [_P, _P, ctypes.c_int64]),
+    "gf_mlp_set_learning_rate": (_I, [_P, _F]),
+    "gf_mlp_forward": (_I, [_P, _P, _I, _P]),
+    "gf_mlp_gradients": (_I, [_P, _P, _P, _I, _P, _P]),
+    "gf_mlp_train_step": (_I, [_P, _P, _P, _I, _P]),
+    "gf_mlp_check": (_I, [_P]),
+    "gf_bf16_gemm": (_I, [_P, _P, _I, _I, _I, _P, _P]),
 }
 
 _lib = None

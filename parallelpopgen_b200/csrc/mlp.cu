@@ -1,0 +1,896 @@
+// SFS surrogate network on sm_100a tensor cores: a bf16 GEMM built on TMA + tcgen05 with the
+// accumulator in tensor memory, fused epilogues (bias + GELU forward, GELU' backward with bias
+// gradients, split-K weight-gradient partials), the loss, the gradient reduction and Adam.
+//
+// Every GEMM is C[M][N] = A[M][K] * B[N][K]^T with both operands K-contiguous:
+//   forward   Z_l  = Y_{l-1} W_l^T          A = Y_{l-1} [batch][in]      B = W_l   [out][in]
+//   input     dY_{l-1} = dZ_l W_l           A = dZ_l    [batch][out]     B = W_l^T [in][out]
+//   weights   dW_l = dZ_l^T Y_{l-1}         A = dZ_l^T  [out][batch]     B = Y_{l-1}^T [in][batch]
+// so the forward epilogue writes each activation twice (row-major and transposed), the backward
+// epilogue does the same for dZ, and Adam keeps bf16 copies of W and W^T.  Layer 1's six inputs are
+// zero-padded to 64 columns and layer 5's 99 outputs to 128 rows; padding stays exactly zero.
+//
+// The reference has no network (3P answers every SFS query by simulation, go_fish.cuh:280 and
+// spectrum.h:90); this file serves the surrogate that stands in for those calls.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gf_surrogate.h"
+#include "gf_umma.cuh"
+
+namespace gfm {
+
+constexpr int BM = 128;       // tile rows = tensor-memory lanes
+constexpr int BK = 64;        // K per pipeline stage: one 128-byte swizzle row of bf16
+constexpr int STAGES = 4;
+constexpr long long WAIT_LIMIT = 1ll << 31;   // SM cycles (about a second) before a wait gives up
+constexpr int HID = GF_MLP_HIDDEN;
+constexpr int IN_PAD = 64;
+constexpr int OUT_PAD = 128;
+constexpr int MAX_SPLITS = 16;
+
+enum Epi : int { EPI_STORE_F32 = 0, EPI_FWD_GELU = 1, EPI_FWD_LINEAR = 2, EPI_BWD_GELU = 3, EPI_PARTIAL = 4 };
+
+struct EpiArgs {
+  float* c;                  // fp32 output (C, pre-activation Z, linear output, or split-K partials)
+  long long ldc;
+  long long split_stride;    // elements between split-K partial slices of c
+  __nv_bfloat16* y;          // bf16 row-major output
+  long long ldy;
+  __nv_bfloat16* yt;         // bf16 transposed output
+  long long ldyt;
+  const float* bias;         // [N]
+  const float* z;            // forward pre-activation read by the backward epilogue
+  long long ldz;
+  float* bias_part;          // [M / 128][ld_bias_part] column sums of the backward output
+  long long ld_bias_part;
+  int* fault;                // set when a bounded wait ran out
+};
+
+template <int BN>
+struct Smem {
+  static constexpr int A_BYTES = BM * BK * 2;
+  static constexpr int B_BYTES = BN * BK * 2;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int BAR_OFFSET = STAGES * STAGE_BYTES;
+  static constexpr int BYTES = BAR_OFFSET + 256 + 4 * 32 * 4 + 1024;   // + barriers, reduction, alignment
+};
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.7071067811865476f)); }
+
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float cdf = 0.5f * (1.f + erff(z * 0.7071067811865476f));
+  const float pdf = 0.3989422804014327f * expf(-0.5f * z * z);
+  return cdf + z * pdf;
+}
+
+__device__ __forceinline__ void store_bf16_row32(__nv_bfloat16* dst, const float* v) {
+  uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t w[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      __nv_bfloat162 p = __floats2bfloat162_rn(v[q * 8 + 2 * t], v[q * 8 + 2 * t + 1]);
+      w[t] = *reinterpret_cast<uint32_t*>(&p);
+    }
+    d[q] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__device__ __forceinline__ void store_f32_row32(float* dst, const float* v) {
+  float4* d = reinterpret_cast<float4*>(dst);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// One 128 x BN output tile per CTA, K range split over gridDim.z.  Thread 0 drives TMA, thread 32
+// issues the MMAs, all four warps run the epilogue from tensor memory.
+template <int BN, int EPI>
+__global__ void __launch_bounds__(128, 1)
+umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
+                 int k_blocks, EpiArgs ep) {
+  using L = Smem<BN>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFFSET);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  int* timed_out = reinterpret_cast<int*>(tmem_slot + 1);
+  float* red = reinterpret_cast<float*>(smem + L::BAR_OFFSET + 256);   // [4][32]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+  const int kb0 = blockIdx.z * k_blocks;
+
+  if (threadIdx.x == 0) {
+    tma_prefetch_desc(&tma_a);
+    tma_prefetch_desc(&tma_b);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *timed_out = 0;
+    mbar_fence_init();
+  }
+  __syncwarp();
+  if (warp == 0) tmem_alloc(tmem_slot, BN);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool late = false;
+
+  if (threadIdx.x == 0) {
+    for (int kb = 0; kb < k_blocks; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (kb / STAGES) & 1;
+      if (!mbar_wait(&empty[s], ph ^ 1, WAIT_LIMIT)) late = true;
+      uint8_t* a = smem + s * L::STAGE_BYTES;
+      mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
+      tma_load_2d(a, &tma_a, (kb0 + kb) * BK, m0, &full[s]);
+      tma_load_2d(a + L::A_BYTES, &tma_b, (kb0 + kb) * BK, n0, &full[s]);
+    }
+  } else if (threadIdx.x == 32) {
+    constexpr uint32_t idesc = bf16_idesc(BM, BN);
+    for (int kb = 0; kb < k_blocks; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (kb / STAGES) & 1;
+      if (!mbar_wait(&full[s], ph, WAIT_LIMIT)) late = true;
+      tc_fence_after();
+      const uint32_t a_addr = smem_u32(smem + s * L::STAGE_BYTES);
+      const uint32_t b_addr = a_addr + L::A_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk)
+        umma_bf16(tmem, sw128_kmajor_desc(a_addr + kk * 32), sw128_kmajor_desc(b_addr + kk * 32), idesc,
+                  (kb | kk) != 0);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  if (!mbar_wait(done, 0, WAIT_LIMIT)) late = true;
+  __syncwarp();
+  tc_fence_after();
+
+  const int row = m0 + warp * 32 + lane;
+  const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+#pragma unroll 1
+  for (int c0 = 0; c0 < BN; c0 += 32) {
+    float v[32];
+    tmem_ld_32cols(tbase + c0, v);
+    const int n = n0 + c0;
+    if constexpr (EPI == EPI_STORE_F32) {
+      store_f32_row32(ep.c + row * ep.ldc + n, v);
+    } else if constexpr (EPI == EPI_PARTIAL) {
+      store_f32_row32(ep.c + blockIdx.z * ep.split_stride + row * ep.ldc + n, v);
+    } else if constexpr (EPI == EPI_FWD_LINEAR) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
+      store_f32_row32(ep.c + row * ep.ldc + n, v);
+    } else if constexpr (EPI == EPI_FWD_GELU) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
+      store_f32_row32(ep.c + row * ep.ldc + n, v);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+      store_bf16_row32(ep.y + row * ep.ldy + n, v);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) ep.yt[(n + j) * ep.ldyt + row] = __float2bfloat16_rn(v[j]);
+    } else if constexpr (EPI == EPI_BWD_GELU) {
+      const float4* zp = reinterpret_cast<const float4*>(ep.z + row * ep.ldz + n);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float4 z = zp[q];
+        v[4 * q] *= gelu_grad(z.x);
+        v[4 * q + 1] *= gelu_grad(z.y);
+        v[4 * q + 2] *= gelu_grad(z.z);
+        v[4 * q + 3] *= gelu_grad(z.w);
+      }
+      store_bf16_row32(ep.y + row * ep.ldy + n, v);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) ep.yt[(n + j) * ep.ldyt + row] = __float2bfloat16_rn(v[j]);
+      // column sums over the tile's 128 rows (fixed order: lanes, then warps)
+      float mine = 0.f;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        float s = v[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == j) mine = s;
+      }
+      red[warp * 32 + lane] = mine;
+      __syncthreads();
+      if (warp == 0) {
+        const float t = ((red[lane] + red[32 + lane]) + red[64 + lane]) + red[96 + lane];
+        ep.bias_part[blockIdx.y * ep.ld_bias_part + n + lane] = t;
+      }
+      __syncthreads();
+    }
+  }
+  tc_fence_before();
+  if (late) atomicOr(timed_out, 1);
+  __syncthreads();
+  if (*timed_out) {
+    // a wait ran out: let every copy this CTA issued land before its shared memory is released
+    if (threadIdx.x == 0) {
+      for (int kb = k_blocks - STAGES < 0 ? 0 : k_blocks - STAGES; kb < k_blocks; ++kb)
+        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, WAIT_LIMIT);
+      if (ep.fault) atomicOr(ep.fault, 1);
+    }
+    __syncthreads();
+  }
+  if (warp == 0) tmem_dealloc(tmem, BN);
+}
+
+// ---------------------------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------------------------
+
+// Inputs [batch][6] fp32 -> X0 [cap][64] and X0^T [64][cap] bf16 (padding columns stay zero).
+__global__ void encode_inputs_kernel(const float* __restrict__ x, int batch, __nv_bfloat16* __restrict__ x0,
+                                     __nv_bfloat16* __restrict__ x0t, long long cap) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+#pragma unroll
+  for (int j = 0; j < GF_MLP_INPUTS; ++j) {
+    const __nv_bfloat16 v = __float2bfloat16_rn(x[b * GF_MLP_INPUTS + j]);
+    x0[b * IN_PAD + j] = v;
+    x0t[j * cap + b] = v;
+  }
+}
+
+// Squared-error loss of one 128-row tile and its gradient: dOut = 2 (out - target) / (batch * 99),
+// written row-major and transposed in bf16, with the tile's column sums (bias gradient of layer 5)
+// and loss sum.  One block of 128 threads per tile; thread = row for the gradient, thread = column
+// for the column sums (recomputed, same expression, fixed row order).
+__global__ void __launch_bounds__(128)
+loss_kernel(const float* __restrict__ out, const float* __restrict__ target, int batch,
+            __nv_bfloat16* __restrict__ dout, __nv_bfloat16* __restrict__ doutt, long long cap,
+            float* __restrict__ bias_part, float* __restrict__ loss_part) {
+  __shared__ float rl[BM];
+  const int r = threadIdx.x;
+  const int row0 = blockIdx.x * BM;
+  const int row = row0 + r;
+  const float scale = 2.f / (static_cast<float>(batch) * GF_MLP_OUTPUTS);
+  float l = 0.f;
+  for (int j = 0; j < GF_MLP_OUTPUTS; ++j) {
+    const float d = out[row * OUT_PAD + j] - target[row * GF_MLP_OUTPUTS + j];
+    l += d * d;
+    const __nv_bfloat16 b = __float2bfloat16_rn(scale * d);
+    dout[row * OUT_PAD + j] = b;
+    doutt[j * cap + row] = b;
+  }
+  rl[r] = l;
+  if (r < GF_MLP_OUTPUTS) {
+    float s = 0.f;
+    for (int i = 0; i < BM; ++i) s += scale * (out[(row0 + i) * OUT_PAD + r] - target[(row0 + i) * GF_MLP_OUTPUTS + r]);
+    bias_part[blockIdx.x * OUT_PAD + r] = s;
+  }
+  __syncthreads();
+  if (r == 0) {
+    float s = 0.f;
+    for (int i = 0; i < BM; ++i) s += rl[i];
+    loss_part[blockIdx.x] = s / (static_cast<float>(batch) * GF_MLP_OUTPUTS);
+  }
+}
+
+__global__ void loss_finish_kernel(const float* __restrict__ loss_part, int tiles, float* __restrict__ loss) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    float s = 0.f;
+    for (int i = 0; i < tiles; ++i) s += loss_part[i];
+    *loss = s;
+  }
+}
+
+// One parameter tensor (padded shape rows x cols) and where its gradient partials are.
+struct ParamSlot {
+  float* w;
+  float* m;
+  float* v;
+  float* g;
+  __nv_bfloat16* wb;     // bf16 copy [rows][cols] (weights only)
+  __nv_bfloat16* wt;     // bf16 transposed copy [cols][rows] (weights only)
+  const float* part;     // gradient partials
+  long long part_stride;
+  int nparts;
+  int rows, cols, rows_true, cols_true;
+  long long offset;      // first element in the concatenated index space
+};
+
+struct ParamTable {
+  ParamSlot s[2 * GF_MLP_LAYERS];
+  long long total;
+};
+
+__device__ __forceinline__ int find_slot(const ParamTable& t, long long i) {
+  int k = 0;
+#pragma unroll 1
+  while (k + 1 < 2 * GF_MLP_LAYERS && t.s[k + 1].offset <= i) ++k;
+  return k;
+}
+
+// g = sum of the partials in a fixed order.
+__global__ void reduce_grads_kernel(const __grid_constant__ ParamTable t) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < t.total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const ParamSlot& p = t.s[find_slot(t, i)];
+    const long long e = i - p.offset;
+    float acc = 0.f;
+    for (int k = 0; k < p.nparts; ++k) acc += p.part[k * p.part_stride + e];
+    p.g[e] = acc;
+  }
+}
+
+// Adam (with optional decoupled weight decay) on the master weights, then the bf16 copies.
+__global__ void adam_kernel(const __grid_constant__ ParamTable t, float lr, float beta1, float beta2, float eps,
+                            float bc1, float bc2, float decay) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < t.total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const ParamSlot& p = t.s[find_slot(t, i)];
+    const long long e = i - p.offset;
+    const int r = static_cast<int>(e / p.cols), c = static_cast<int>(e % p.cols);
+    if (r >= p.rows_true || c >= p.cols_true) continue;
+    const float g = p.g[e];
+    const float m = beta1 * p.m[e] + (1.f - beta1) * g;
+    const float v = beta2 * p.v[e] + (1.f - beta2) * g * g;
+    p.m[e] = m;
+    p.v[e] = v;
+    float w = p.w[e];
+    w -= lr * decay * w;
+    w -= lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+    p.w[e] = w;
+    if (p.wb) {
+      const __nv_bfloat16 b = __float2bfloat16_rn(w);
+      p.wb[e] = b;
+      p.wt[static_cast<long long>(c) * p.rows + r] = b;
+    }
+  }
+}
+
+// bf16 copies of the master weights (after set_params).
+__global__ void refresh_bf16_kernel(const __grid_constant__ ParamTable t) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < t.total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const ParamSlot& p = t.s[find_slot(t, i)];
+    if (!p.wb) continue;
+    const long long e = i - p.offset;
+    const int r = static_cast<int>(e / p.cols), c = static_cast<int>(e % p.cols);
+    const __nv_bfloat16 b = __float2bfloat16_rn(p.w[e]);
+    p.wb[e] = b;
+    p.wt[static_cast<long long>(c) * p.rows + r] = b;
+  }
+}
+
+__global__ void copy_output_kernel(const float* __restrict__ out, int batch, float* __restrict__ dst) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= static_cast<long long>(batch) * GF_MLP_OUTPUTS) return;
+  const long long b = i / GF_MLP_OUTPUTS, j = i % GF_MLP_OUTPUTS;
+  dst[i] = out[b * OUT_PAD + j];
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor map of a row-major bf16 matrix [rows][cols] (cols contiguous), tile box_rows x 64.
+bool make_map(CUtensorMap* m, const void* base, long long rows, long long cols, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 2};
+  cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int EPI>
+cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, int M, int N, int K, int splits,
+                        const EpiArgs& ep, cudaStream_t stream) {
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    cudaError_t err = cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           Smem<BN>::BYTES);
+    if (err != cudaSuccess) return err;
+    attr_set[dev] = true;
+  }
+  dim3 grid(N / BN, M / BM, splits);
+  umma_gemm_kernel<BN, EPI><<<grid, 128, Smem<BN>::BYTES, stream>>>(a, b, K / BK / splits, ep);
+  return cudaGetLastError();
+}
+
+// Split count for a weight-gradient GEMM: enough CTAs to cover the SMs, each split a whole number
+// of 64-wide K blocks.
+int choose_splits(int tiles, int K) {
+  const int kblocks = K / BK;
+  int s = 1;
+  while (s < MAX_SPLITS && tiles * s < 148 && kblocks % (2 * s) == 0 && kblocks / (2 * s) >= 2) s *= 2;
+  return s;
+}
+
+}  // namespace gfm
+
+using namespace gfm;
+
+struct gf_mlp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  gf_mlp_config cfg{};
+  long long cap = 0;
+  long long step = 0;
+  std::string error;
+
+  // layer geometry (padded): out x in
+  int rows[GF_MLP_LAYERS] = {HID, HID, HID, HID, OUT_PAD};
+  int cols[GF_MLP_LAYERS] = {IN_PAD, HID, HID, HID, HID};
+  int rows_true[GF_MLP_LAYERS] = {HID, HID, HID, HID, GF_MLP_OUTPUTS};
+  int cols_true[GF_MLP_LAYERS] = {GF_MLP_INPUTS, HID, HID, HID, HID};
+
+  // parameters (fp32 master, Adam moments, gradient) -- one allocation each, weights then biases
+  float* w[GF_MLP_LAYERS] = {};
+  float* b[GF_MLP_LAYERS] = {};
+  float* m_all = nullptr;
+  float* v_all = nullptr;
+  float* g_all = nullptr;
+  float* w_all = nullptr;
+  __nv_bfloat16* wb[GF_MLP_LAYERS] = {};
+  __nv_bfloat16* wt[GF_MLP_LAYERS] = {};
+  long long off_w[GF_MLP_LAYERS] = {}, off_b[GF_MLP_LAYERS] = {};
+  long long n_params_padded = 0;
+
+  // activations
+  __nv_bfloat16 *x0 = nullptr, *x0t = nullptr;
+  float* z[4] = {};
+  __nv_bfloat16 *y[4] = {}, *yt[4] = {};
+  float* out = nullptr;
+  __nv_bfloat16 *dout = nullptr, *doutt = nullptr;
+  __nv_bfloat16 *dz[4] = {}, *dzt[4] = {};
+  float* wpart[GF_MLP_LAYERS] = {};
+  float* bpart[GF_MLP_LAYERS] = {};
+  int wsplits[GF_MLP_LAYERS] = {};
+  float* loss_part = nullptr;
+  float* loss = nullptr;
+  int* fault = nullptr;
+
+  // tensor maps
+  CUtensorMap fwd_a[GF_MLP_LAYERS], fwd_b[GF_MLP_LAYERS];     // A = input activations, B = W
+  CUtensorMap bwd_a[GF_MLP_LAYERS], bwd_b[GF_MLP_LAYERS];     // A = dZ_l (dOut), B = W_l^T  (l >= 2)
+  CUtensorMap dw_a[GF_MLP_LAYERS], dw_b[GF_MLP_LAYERS];       // A = dZ_l^T, B = Y_{l-1}^T
+
+  std::vector<void*> allocations;
+};
+
+namespace {
+
+gf_status mlp_fail(gf_mlp* m, gf_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (m) m->error = buf;
+  return st;
+}
+
+#define MLP_CUDA(m, call)                                                                         \
+  do {                                                                                            \
+    cudaError_t _e = (call);                                                                      \
+    if (_e != cudaSuccess) return mlp_fail((m), GF_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e)); \
+  } while (0)
+
+template <class T>
+gf_status alloc(gf_mlp* m, T** p, long long count) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, static_cast<size_t>(count) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return mlp_fail(m, GF_ERR_OUT_OF_MEMORY, "device allocation of %lld bytes failed",
+                    static_cast<long long>(count * sizeof(T)));
+  }
+  m->allocations.push_back(q);
+  *p = static_cast<T*>(q);
+  if (cudaMemsetAsync(q, 0, static_cast<size_t>(count) * sizeof(T), m->stream) != cudaSuccess)
+    return mlp_fail(m, GF_ERR_CUDA, "memset failed");
+  return GF_OK;
+}
+
+ParamTable param_table(gf_mlp* m, int batch) {
+  ParamTable t{};
+  long long off = 0;
+  for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+    ParamSlot& s = t.s[l];
+    s.w = m->w[l];
+    s.m = m->m_all + m->off_w[l];
+    s.v = m->v_all + m->off_w[l];
+    s.g = m->g_all + m->off_w[l];
+    s.wb = m->wb[l];
+    s.wt = m->wt[l];
+    s.part = m->wpart[l];
+    s.part_stride = static_cast<long long>(m->rows[l]) * m->cols[l];
+    s.nparts = m->wsplits[l];
+    s.rows = m->rows[l];
+    s.cols = m->cols[l];
+    s.rows_true = m->rows_true[l];
+    s.cols_true = m->cols_true[l];
+    s.offset = off;
+    off += s.part_stride;
+  }
+  for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+    ParamSlot& s = t.s[GF_MLP_LAYERS + l];
+    s.w = m->b[l];
+    s.m = m->m_all + m->off_b[l];
+    s.v = m->v_all + m->off_b[l];
+    s.g = m->g_all + m->off_b[l];
+    s.wb = nullptr;
+    s.wt = nullptr;
+    s.part = m->bpart[l];
+    s.part_stride = m->rows[l];
+    s.nparts = batch / BM;
+    s.rows = 1;
+    s.cols = m->rows[l];
+    s.rows_true = 1;
+    s.cols_true = m->rows_true[l];
+    s.offset = off;
+    off += m->rows[l];
+  }
+  t.total = off;
+  return t;
+}
+
+gf_status check_batch(gf_mlp* m, int batch) {
+  if (batch <= 0 || batch % BM != 0 || batch > m->cap)
+    return mlp_fail(m, GF_ERR_INVALID_ARGUMENT, "batch %d must be a positive multiple of %d and at most %lld",
+                    batch, BM, m->cap);
+  return GF_OK;
+}
+
+gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch) {
+  encode_inputs_kernel<<<(batch + 255) / 256, 256, 0, m->stream>>>(d_inputs, batch, m->x0, m->x0t, m->cap);
+  MLP_CUDA(m, cudaGetLastError());
+  for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+    EpiArgs ep{};
+    ep.bias = m->b[l];
+    ep.fault = m->fault;
+    cudaError_t err;
+    if (l < 4) {
+      ep.c = m->z[l];
+      ep.ldc = HID;
+      ep.y = m->y[l];
+      ep.ldy = HID;
+      ep.yt = m->yt[l];
+      ep.ldyt = m->cap;
+      err = launch_gemm<128, EPI_FWD_GELU>(m->fwd_a[l], m->fwd_b[l], batch, HID, m->cols[l], 1, ep, m->stream);
+    } else {
+      ep.c = m->out;
+      ep.ldc = OUT_PAD;
+      err = launch_gemm<128, EPI_FWD_LINEAR>(m->fwd_a[l], m->fwd_b[l], batch, OUT_PAD, HID, 1, ep, m->stream);
+    }
+    if (err != cudaSuccess) return mlp_fail(m, GF_ERR_CUDA, "forward GEMM %d: %s", l + 1, cudaGetErrorString(err));
+  }
+  return GF_OK;
+}
+
+gf_status run_backward(gf_mlp* m, const float* d_targets, int batch) {
+  const int tiles = batch / BM;
+  loss_kernel<<<tiles, BM, 0, m->stream>>>(m->out, d_targets, batch, m->dout, m->doutt, m->cap, m->bpart[4],
+                                          m->loss_part);
+  MLP_CUDA(m, cudaGetLastError());
+  loss_finish_kernel<<<1, 32, 0, m->stream>>>(m->loss_part, tiles, m->loss);
+  MLP_CUDA(m, cudaGetLastError());
+  for (int l = GF_MLP_LAYERS - 1; l >= 0; --l) {
+    // weight gradient partials of layer l+1
+    {
+      EpiArgs ep{};
+      ep.c = m->wpart[l];
+      ep.ldc = m->cols[l];
+      ep.split_stride = static_cast<long long>(m->rows[l]) * m->cols[l];
+      ep.fault = m->fault;
+      const int M = m->rows[l], N = m->cols[l];
+      const int bn = (N % 128 == 0) ? 128 : 64;
+      const int splits = choose_splits((M / BM) * (N / bn), batch);
+      m->wsplits[l] = splits;
+      cudaError_t err = bn == 128
+          ? launch_gemm<128, EPI_PARTIAL>(m->dw_a[l], m->dw_b[l], M, N, batch, splits, ep, m->stream)
+          : launch_gemm<64, EPI_PARTIAL>(m->dw_a[l], m->dw_b[l], M, N, batch, splits, ep, m->stream);
+      if (err != cudaSuccess)
+        return mlp_fail(m, GF_ERR_CUDA, "weight-gradient GEMM %d: %s", l + 1, cudaGetErrorString(err));
+    }
+    if (l == 0) break;
+    // input gradient of layer l+1 = output gradient of layer l, times GELU'(Z_l)
+    EpiArgs ep{};
+    ep.z = m->z[l - 1];
+    ep.ldz = HID;
+    ep.y = m->dz[l - 1];
+    ep.ldy = HID;
+    ep.yt = m->dzt[l - 1];
+    ep.ldyt = m->cap;
+    ep.bias_part = m->bpart[l - 1];
+    ep.ld_bias_part = HID;
+    ep.fault = m->fault;
+    cudaError_t err = launch_gemm<128, EPI_BWD_GELU>(m->bwd_a[l], m->bwd_b[l], batch, HID, m->rows[l], 1, ep,
+                                                    m->stream);
+    if (err != cudaSuccess)
+      return mlp_fail(m, GF_ERR_CUDA, "input-gradient GEMM %d: %s", l + 1, cudaGetErrorString(err));
+  }
+  ParamTable t = param_table(m, batch);
+  reduce_grads_kernel<<<2 * 148, 256, 0, m->stream>>>(t);
+  MLP_CUDA(m, cudaGetLastError());
+  return GF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t gf_mlp_param_count(void) {
+  int64_t n = 0;
+  const int r[GF_MLP_LAYERS] = {HID, HID, HID, HID, GF_MLP_OUTPUTS};
+  const int c[GF_MLP_LAYERS] = {GF_MLP_INPUTS, HID, HID, HID, HID};
+  for (int l = 0; l < GF_MLP_LAYERS; ++l) n += static_cast<int64_t>(r[l]) * c[l] + r[l];
+  return n;
+}
+
+const char* gf_mlp_last_error(const gf_mlp* mlp) { return mlp ? mlp->error.c_str() : "null network"; }
+
+gf_status gf_mlp_create(int32_t device, void* stream, const gf_mlp_config* config, gf_mlp** out) {
+  if (!out || !config) return GF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return GF_ERR_NO_DEVICE;
+  }
+  if (config->batch_capacity <= 0 || config->batch_capacity % BM != 0) return GF_ERR_INVALID_ARGUMENT;
+  if (!encode_fn()) return GF_ERR_CUDA;
+  auto* m = new gf_mlp();
+  m->device = device;
+  m->cfg = *config;
+  m->cap = config->batch_capacity;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete m;
+    return GF_ERR_CUDA;
+  }
+  m->stream = static_cast<cudaStream_t>(stream);
+  gf_status st = GF_OK;
+#define MLP_TRY(x)            \
+  do {                        \
+    st = (x);                 \
+    if (st != GF_OK) goto bad; \
+  } while (0)
+  {
+    long long off = 0;
+    for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+      m->off_w[l] = off;
+      off += static_cast<long long>(m->rows[l]) * m->cols[l];
+    }
+    for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+      m->off_b[l] = off;
+      off += m->rows[l];
+    }
+    m->n_params_padded = off;
+    MLP_TRY(alloc(m, &m->w_all, off));
+    MLP_TRY(alloc(m, &m->m_all, off));
+    MLP_TRY(alloc(m, &m->v_all, off));
+    MLP_TRY(alloc(m, &m->g_all, off));
+    for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+      m->w[l] = m->w_all + m->off_w[l];
+      m->b[l] = m->w_all + m->off_b[l];
+      const long long n = static_cast<long long>(m->rows[l]) * m->cols[l];
+      MLP_TRY(alloc(m, &m->wb[l], n));
+      MLP_TRY(alloc(m, &m->wt[l], n));
+      MLP_TRY(alloc(m, &m->wpart[l], n * MAX_SPLITS));
+      MLP_TRY(alloc(m, &m->bpart[l], (m->cap / BM) * m->rows[l]));
+    }
+    const long long cap = m->cap;
+    MLP_TRY(alloc(m, &m->x0, cap * IN_PAD));
+    MLP_TRY(alloc(m, &m->x0t, cap * IN_PAD));
+    for (int l = 0; l < 4; ++l) {
+      MLP_TRY(alloc(m, &m->z[l], cap * HID));
+      MLP_TRY(alloc(m, &m->y[l], cap * HID));
+      MLP_TRY(alloc(m, &m->yt[l], cap * HID));
+      MLP_TRY(alloc(m, &m->dz[l], cap * HID));
+      MLP_TRY(alloc(m, &m->dzt[l], cap * HID));
+    }
+    MLP_TRY(alloc(m, &m->out, cap * OUT_PAD));
+    MLP_TRY(alloc(m, &m->dout, cap * OUT_PAD));
+    MLP_TRY(alloc(m, &m->doutt, cap * OUT_PAD));
+    MLP_TRY(alloc(m, &m->loss_part, cap / BM));
+    MLP_TRY(alloc(m, &m->loss, 1));
+    MLP_TRY(alloc(m, &m->fault, 1));
+
+    bool ok = true;
+    for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+      const void* in = l == 0 ? static_cast<const void*>(m->x0) : m->y[l - 1];
+      const void* in_t = l == 0 ? static_cast<const void*>(m->x0t) : m->yt[l - 1];
+      const void* g = l == 4 ? static_cast<const void*>(m->dout) : m->dz[l];
+      const void* g_t = l == 4 ? static_cast<const void*>(m->doutt) : m->dzt[l];
+      ok = ok && make_map(&m->fwd_a[l], in, cap, m->cols[l], BM);
+      ok = ok && make_map(&m->fwd_b[l], m->wb[l], m->rows[l], m->cols[l], 128);
+      if (l > 0) {   // layer 1's input gradient is never formed
+        ok = ok && make_map(&m->bwd_a[l], g, cap, m->rows[l], BM);
+        ok = ok && make_map(&m->bwd_b[l], m->wt[l], m->cols[l], m->rows[l], 128);
+      }
+      ok = ok && make_map(&m->dw_a[l], g_t, m->rows[l], cap, BM);
+      ok = ok && make_map(&m->dw_b[l], in_t, m->cols[l], cap, m->cols[l] % 128 == 0 ? 128 : 64);
+    }
+    if (!ok) {
+      st = mlp_fail(m, GF_ERR_CUDA, "tensor map encoding failed");
+      goto bad;
+    }
+    if (cudaStreamSynchronize(m->stream) != cudaSuccess) {
+      st = GF_ERR_CUDA;
+      goto bad;
+    }
+  }
+#undef MLP_TRY
+  *out = m;
+  return GF_OK;
+bad:
+  for (void* p : m->allocations) cudaFree(p);
+  delete m;
+  return st == GF_OK ? GF_ERR_CUDA : st;
+}
+
+gf_status gf_mlp_destroy(gf_mlp* mlp) {
+  if (!mlp) return GF_OK;
+  cudaSetDevice(mlp->device);
+  cudaStreamSynchronize(mlp->stream);
+  for (void* p : mlp->allocations) cudaFree(p);
+  delete mlp;
+  return GF_OK;
+}
+
+gf_status gf_mlp_set_params(gf_mlp* m, const float* params, int64_t count) {
+  if (!m || !params) return GF_ERR_INVALID_ARGUMENT;
+  if (count != gf_mlp_param_count())
+    return mlp_fail(m, GF_ERR_INVALID_ARGUMENT, "expected %lld parameters, got %lld",
+                    static_cast<long long>(gf_mlp_param_count()), static_cast<long long>(count));
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  std::vector<float> h(m->n_params_padded, 0.f);
+  const float* p = params;
+  for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+    for (int r = 0; r < m->rows_true[l]; ++r)
+      for (int c = 0; c < m->cols_true[l]; ++c) h[m->off_w[l] + static_cast<long long>(r) * m->cols[l] + c] = *p++;
+    for (int r = 0; r < m->rows_true[l]; ++r) h[m->off_b[l] + r] = *p++;
+  }
+  MLP_CUDA(m, cudaMemcpyAsync(m->w_all, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+  MLP_CUDA(m, cudaMemsetAsync(m->m_all, 0, h.size() * sizeof(float), m->stream));
+  MLP_CUDA(m, cudaMemsetAsync(m->v_all, 0, h.size() * sizeof(float), m->stream));
+  ParamTable t = param_table(m, BM);
+  refresh_bf16_kernel<<<2 * 148, 256, 0, m->stream>>>(t);
+  MLP_CUDA(m, cudaGetLastError());
+  MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+  m->step = 0;
+  return GF_OK;
+}
+
+static gf_status unpad_to_host(gf_mlp* m, const float* d_all, float* out) {
+  std::vector<float> h(m->n_params_padded);
+  MLP_CUDA(m, cudaMemcpyAsync(h.data(), d_all, h.size() * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+  MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+  float* p = out;
+  for (int l = 0; l < GF_MLP_LAYERS; ++l) {
+    for (int r = 0; r < m->rows_true[l]; ++r)
+      for (int c = 0; c < m->cols_true[l]; ++c) *p++ = h[m->off_w[l] + static_cast<long long>(r) * m->cols[l] + c];
+    for (int r = 0; r < m->rows_true[l]; ++r) *p++ = h[m->off_b[l] + r];
+  }
+  return GF_OK;
+}
+
+gf_status gf_mlp_get_params(gf_mlp* m, float* params, int64_t count) {
+  if (!m || !params) return GF_ERR_INVALID_ARGUMENT;
+  if (count != gf_mlp_param_count()) return mlp_fail(m, GF_ERR_INVALID_ARGUMENT, "parameter count mismatch");
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  return unpad_to_host(m, m->w_all, params);
+}
+
+gf_status gf_mlp_set_learning_rate(gf_mlp* m, float lr) {
+  if (!m || !(lr >= 0.f)) return GF_ERR_INVALID_ARGUMENT;
+  m->cfg.lr = lr;
+  return GF_OK;
+}
+
+gf_status gf_mlp_forward(gf_mlp* m, const float* d_inputs, int32_t batch, float* d_outputs) {
+  if (!m || !d_inputs || !d_outputs) return GF_ERR_INVALID_ARGUMENT;
+  gf_status st = check_batch(m, batch);
+  if (st != GF_OK) return st;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  if ((st = run_forward(m, d_inputs, batch)) != GF_OK) return st;
+  const long long n = static_cast<long long>(batch) * GF_MLP_OUTPUTS;
+  copy_output_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, m->stream>>>(m->out, batch, d_outputs);
+  MLP_CUDA(m, cudaGetLastError());
+  return GF_OK;
+}
+
+gf_status gf_mlp_gradients(gf_mlp* m, const float* d_inputs, const float* d_targets, int32_t batch, float* grads,
+                           float* loss) {
+  if (!m || !d_inputs || !d_targets) return GF_ERR_INVALID_ARGUMENT;
+  gf_status st = check_batch(m, batch);
+  if (st != GF_OK) return st;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  if ((st = run_forward(m, d_inputs, batch)) != GF_OK) return st;
+  if ((st = run_backward(m, d_targets, batch)) != GF_OK) return st;
+  if (loss) {
+    MLP_CUDA(m, cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+  }
+  if (grads) {
+    if ((st = unpad_to_host(m, m->g_all, grads)) != GF_OK) return st;
+  }
+  MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+  return gf_mlp_check(m);
+}
+
+gf_status gf_mlp_train_step(gf_mlp* m, const float* d_inputs, const float* d_targets, int32_t batch,
+                            float* d_loss) {
+  if (!m || !d_inputs || !d_targets) return GF_ERR_INVALID_ARGUMENT;
+  gf_status st = check_batch(m, batch);
+  if (st != GF_OK) return st;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  if ((st = run_forward(m, d_inputs, batch)) != GF_OK) return st;
+  if ((st = run_backward(m, d_targets, batch)) != GF_OK) return st;
+  m->step += 1;
+  const double bc1 = 1.0 - std::pow(static_cast<double>(m->cfg.beta1), static_cast<double>(m->step));
+  const double bc2 = 1.0 - std::pow(static_cast<double>(m->cfg.beta2), static_cast<double>(m->step));
+  ParamTable t = param_table(m, batch);
+  adam_kernel<<<2 * 148, 256, 0, m->stream>>>(t, m->cfg.lr, m->cfg.beta1, m->cfg.beta2, m->cfg.eps,
+                                             static_cast<float>(bc1), static_cast<float>(bc2), m->cfg.weight_decay);
+  MLP_CUDA(m, cudaGetLastError());
+  if (d_loss) MLP_CUDA(m, cudaMemcpyAsync(d_loss, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, m->stream));
+  return GF_OK;
+}
+
+gf_status gf_mlp_check(gf_mlp* m) {
+  if (!m) return GF_ERR_INVALID_ARGUMENT;
+  MLP_CUDA(m, cudaSetDevice(m->device));
+  int f = 0;
+  MLP_CUDA(m, cudaMemcpyAsync(&f, m->fault, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+  if (f) return mlp_fail(m, GF_ERR_DEVICE, "a tensor-core GEMM wait ran out of time");
+  return GF_OK;
+}
+
+gf_status gf_bf16_gemm(const void* d_a, const void* d_b, int32_t M, int32_t N, int32_t K, float* d_c,
+                       void* stream) {
+  if (!d_a || !d_b || !d_c || M <= 0 || N <= 0 || K <= 0 || M % BM || N % 64 || K % BK)
+    return GF_ERR_INVALID_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(d_a) | reinterpret_cast<uintptr_t>(d_b) | reinterpret_cast<uintptr_t>(d_c)) & 15)
+    return GF_ERR_INVALID_ARGUMENT;
+  const int bn = N % 128 == 0 ? 128 : 64;
+  CUtensorMap a, b;
+  if (!make_map(&a, d_a, M, K, BM) || !make_map(&b, d_b, N, K, bn)) return GF_ERR_CUDA;
+  EpiArgs ep{};
+  ep.c = d_c;
+  ep.ldc = N;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t err = bn == 128 ? launch_gemm<128, EPI_STORE_F32>(a, b, M, N, K, 1, ep, s)
+                              : launch_gemm<64, EPI_STORE_F32>(a, b, M, N, K, 1, ep, s);
+  return err == cudaSuccess ? GF_OK : GF_ERR_CUDA;
+}
+
+}  // extern "C"

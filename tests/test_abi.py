@@ -15,12 +15,15 @@ from parallelpopgen_b200 import _capi
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "gofish_b200.h"
+HEADERS = sorted((ROOT / "include").glob("*.h"))
 
 
 def declared_functions() -> list[str]:
-    text = HEADER.read_text()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(gf_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(gf_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol():
