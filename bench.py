@@ -457,6 +457,160 @@ def run_batched(args):
     }), flush=True)
 
 
+# ------------------------------------------------------------------------------------------------
+# surrogate: train on batched-simulator spectra, evaluate against held-out simulator means, and compare
+# SFS queries/s with the simulator at matched error
+# ------------------------------------------------------------------------------------------------
+def run_surrogate(args):
+    import torch
+    from parallelpopgen_b200 import Engine
+    from parallelpopgen_b200 import surrogate as sg
+
+    torch.cuda.set_device(0)
+    if args.infer_only:
+        return surrogate_inference_only(args)
+    eng = Engine(device=0)
+    cached = None
+    if args.data_cache and os.path.exists(args.data_cache):
+        cached = np.load(args.data_cache)
+        if len(cached["ptrain"]) != args.train_draws or len(cached["peval"]) != args.eval_draws:
+            cached = None
+    if cached is not None:
+        ptrain, train_sfs, peval, ref = cached["ptrain"], cached["train_sfs"], cached["peval"], cached["ref"]
+        t_data = float(cached["t_data"]) if "t_data" in cached else None
+    else:
+        t0 = time.perf_counter()
+        ptrain = sg.draw_parameters(args.train_draws, seed=101)
+        train_sfs = sg.simulate_spectra(eng, ptrain, reps=16, seed=1 << 20)
+        eng.synchronize()
+        t_data = time.perf_counter() - t0
+        peval = sg.draw_parameters(args.eval_draws, seed=202)
+        ref = sg.simulate_spectra(eng, peval, reps=64, seed=1 << 28)        # the judge: 64-replicate means
+        if args.data_cache:
+            np.savez(args.data_cache, ptrain=ptrain, train_sfs=train_sfs, peval=peval, ref=ref, t_data=t_data)
+    # simulator throughput on the training distribution: 512 draws x 16 replicates, timed on its own
+    eng.synchronize()
+    t0 = time.perf_counter()
+    sg.simulate_spectra(eng, ptrain[:512], reps=16, seed=(1 << 29) + 7)
+    eng.synchronize()
+    sims_per_s = 512 * 16 / (time.perf_counter() - t0)
+    indep = sg.simulate_spectra(eng, peval, reps=16, seed=(1 << 28) + (1 << 26))   # independent replicates
+
+    X = torch.from_numpy(sg.encode(ptrain)).cuda()
+    T = torch.from_numpy(sg.spectra_to_targets(train_sfs)).cuda()
+    mlp = sg.Mlp(capacity=max(32768, args.batch), lr=args.lr, weight_decay=args.weight_decay)
+    mlp.set_params(sg.init_params(0))
+    tr = sg.train(mlp, X, T, steps=args.train_steps, batch=args.batch, lr=args.lr, log_every=5000)
+
+    surr = sg.Surrogate(mlp, eng)
+    pred = surr.predict(peval)
+    err, used = sg.median_relative_error(pred, ref)
+    # the simulator's own error with k replicates per query (k = 16 from independent seeds; fewer from
+    # subsets of them are not available without rerunning, so k < 16 are simulated separately)
+    sim_err = {16: sg.median_relative_error(indep / indep.sum(axis=1, keepdims=True), ref)[0]}
+    for k in (1, 4):
+        sk = sg.simulate_spectra(eng, peval, reps=k, seed=(1 << 28) + (1 << 27) + k)
+        sim_err[k] = sg.median_relative_error(sk / sk.sum(axis=1, keepdims=True), ref)[0]
+    ks = sorted(sim_err)
+    match = [k for k in ks if sim_err[k] <= err]
+    if match:
+        k_match = float(match[0])
+    else:  # noise-limited: error falls as 1/sqrt(k)
+        k_match = 16.0 * (sim_err[16] / err) ** 2
+    sim_queries_per_s = sims_per_s / k_match
+
+    # inference throughput: device-resident batches of B queries
+    def time_forward(B, iters):
+        xq = torch.from_numpy(sg.encode(sg.draw_parameters(B, seed=303))).cuda()
+        yq = torch.empty((B, 99), dtype=torch.float32, device="cuda")
+        for _ in range(10):
+            mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(iters):
+            mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
+        ev1.record()
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) * 1e-3 / iters
+
+    fwd_small = time_forward(4096, 200)
+    B = 32768
+    fwd_s = time_forward(B, 100)
+    q_per_s = B / fwd_s
+    flops = 2.0 * B * (6 * 512 + 3 * 512 * 512 + 512 * 99)
+    # end to end through the query API (host parameters in, host spectra out)
+    hostq = sg.draw_parameters(4096, seed=404)
+    surr.query(hostq)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(5):
+        surr.query(hostq)
+    e2e_q_per_s = 5 * len(hostq) / (time.perf_counter() - t1)
+    peak, peak_kind = tensor_peak()
+    tf = flops / fwd_s / 1e12
+    print(json.dumps({
+        "metric": "SFS queries/s (surrogate)", "value": q_per_s, "unit": "queries/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (batched simulator)",
+        "config": {"workload": "6->512x4->99 GELU MLP; train " f"{args.train_draws} draws x 16 replicates, "
+                               f"eval {args.eval_draws} draws x 64 replicates; support: logN [log 500, log 2000], "
+                               "gamma [-100, 10], h [0, 1], F [0, 0.5], r [-0.001, 0.01], T [0.05, 1]; "
+                               f"theta {sg.THETA:g}, L {sg.NUM_SITES:g}, n 100",
+                   "train_steps": args.train_steps, "batch": args.batch, "lr": args.lr,
+                   "weight_decay": args.weight_decay, "inference_batch": B},
+        "median_rel_error": err, "bins_used": used,
+        "simulator_median_rel_error": {str(k): v for k, v in sim_err.items()},
+        "matched_replicates": k_match,
+        "simulator_sims_per_s": sims_per_s,
+        "simulator_queries_per_s_at_matched_error": sim_queries_per_s,
+        "speedup_at_matched_error": q_per_s / sim_queries_per_s,
+        "e2e": {"value": e2e_q_per_s, "unit": "queries/s", "path": "Surrogate.query (host in, host out)"},
+        "train": {"seconds": tr.seconds, "steps": tr.steps, "ms_per_step": tr.seconds / tr.steps * 1e3,
+                  "losses": tr.losses, "data_seconds": t_data},
+        "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "peak_kind": peak_kind,
+                     "unit": "TFLOP/s", "frac": tf / peak, "forward_us": fwd_s * 1e6,
+                     "forward_us_4096": fwd_small * 1e6, "queries_per_s_4096": 4096 / fwd_small},
+    }), flush=True)
+
+
+def surrogate_inference_only(args):
+    """Forward passes of the surrogate network with initial weights (throughput does not depend on them):
+    the tensor-core kernels alone, for profiling."""
+    import torch
+    from parallelpopgen_b200 import surrogate as sg
+    B = 32768
+    mlp = sg.Mlp(capacity=B)
+    mlp.set_params(sg.init_params(0))
+    xq = torch.from_numpy(sg.encode(sg.draw_parameters(B, seed=303))).cuda()
+    yq = torch.empty((B, 99), dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
+    ev1.record()
+    ev1.synchronize()
+    mlp.check()
+    fwd_s = ev0.elapsed_time(ev1) * 1e-3 / args.steps
+    flops = 2.0 * B * (6 * 512 + 3 * 512 * 512 + 512 * 99)
+    peak, kind = tensor_peak()
+    tf = flops / fwd_s / 1e12
+    print(json.dumps({"metric": "SFS queries/s (surrogate forward)", "value": B / fwd_s, "unit": "queries/s",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "batch": B,
+                      "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "peak_kind": kind,
+                                   "unit": "TFLOP/s", "frac": tf / peak, "forward_us": fwd_s * 1e6}}), flush=True)
+
+
+def tensor_peak():
+    """(bf16 dense TFLOP/s, "measured" | "fallback") for a kernel timed on its own (burst figure)."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,8 +618,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
-                    help="plain: the headline single-population workload; batched: batched ragged replicates")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "surrogate"],
+                    help="plain: the headline single-population workload; batched: batched ragged replicates; "
+                         "surrogate: the SFS surrogate network against the simulator")
+    ap.add_argument("--train-draws", type=int, default=16384)
+    ap.add_argument("--eval-draws", type=int, default=1024)
+    ap.add_argument("--train-steps", type=int, default=60000)
+    ap.add_argument("--infer-only", action="store_true",
+                    help="surrogate workload: time forward passes of batches of 32768 queries only")
+    ap.add_argument("--weight-decay", type=float, default=0.1)
+    ap.add_argument("--data-cache", default="",
+                    help="npz file holding (or receiving) the simulated training / evaluation spectra")
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--replicates", type=int, default=4096)
     ap.add_argument("--n-max", type=float, default=1e4)
     ap.add_argument("--plain-sample", type=int, default=32)
@@ -476,6 +641,10 @@ def main():
     if args.workload == "batched":
         if rank == 0:
             run_batched(args)
+        return
+    if args.workload == "surrogate":
+        if rank == 0:
+            run_surrogate(args)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -30,7 +30,8 @@ N_SAMPLE = 100
 OUTPUTS = 99
 THETA = 2000.0
 NUM_SITES = 1e7
-LOG_FLOOR = 1e-7          # targets are log(max(p, LOG_FLOOR))
+LOG_FLOOR = 1e-4          # targets are log(max(p, LOG_FLOOR)): bins below hold well under one site
+GAMMA_SCALE = 5.0         # gamma enters the network as asinh(gamma / GAMMA_SCALE), rescaled to [-1, 1]
 
 # name, low, high (inputs are scaled to [-1, 1] over these ranges)
 SUPPORT = (
@@ -153,7 +154,14 @@ def in_support(params: np.ndarray) -> np.ndarray:
 
 
 def encode(params: np.ndarray) -> np.ndarray:
-    return (2.0 * (params - LOW) / (HIGH - LOW) - 1.0).astype(np.float32)
+    """Network inputs: every parameter scaled linearly to [-1, 1] over the support, except gamma, which
+    is scaled through asinh(gamma / 5) (the spectrum's dependence on strong selection is close to
+    logarithmic in |gamma|)."""
+    params = np.asarray(params, dtype=np.float64)
+    x = 2.0 * (params - LOW) / (HIGH - LOW) - 1.0
+    g_lo, g_hi = np.arcsinh(LOW[1] / GAMMA_SCALE), np.arcsinh(HIGH[1] / GAMMA_SCALE)
+    x[:, 1] = 2.0 * (np.arcsinh(params[:, 1] / GAMMA_SCALE) - g_lo) / (g_hi - g_lo) - 1.0
+    return x.astype(np.float32)
 
 
 def replicate_for(p: np.ndarray, seed1: int, seed2: int, compact_interval: int = 25):
