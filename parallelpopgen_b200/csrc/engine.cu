@@ -48,6 +48,17 @@ gf_status cuda_fail(Engine* e, cudaError_t err, const char* what) {
   return fail(e, st, "CUDA error %d (%s) in %s", static_cast<int>(err), cudaGetErrorString(err), what);
 }
 
+gf_status pool_alloc(Engine* e, void** ptr, size_t bytes) {
+  const cudaError_t err = e->pool ? cudaMallocFromPoolAsync(ptr, bytes, e->pool, e->stream)
+                                  : cudaMallocAsync(ptr, bytes, e->stream);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return cuda_fail(e, err, "stream-ordered allocation");
+  }
+  return GF_OK;
+}
+
 gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need) {
   if (*have >= need && *ptr) return GF_OK;
   if (*ptr) {
@@ -499,17 +510,18 @@ __global__ void mse_fill_kernel(float* __restrict__ freq, int* __restrict__ id_g
 static long long align_up(long long v, long long a) { return (v + a - 1) / a * a; }
 
 static void release_sim(Engine* e) {
+  // stream-ordered frees: the memory returns to the engine's pool for the next simulation
   for (int b = 0; b < 2; ++b) {
-    if (e->freq[b]) cudaFree(e->freq[b]);
-    if (e->id_gp[b]) cudaFree(e->id_gp[b]);
-    if (e->id_tid[b]) cudaFree(e->id_tid[b]);
+    if (e->freq[b]) cudaFreeAsync(e->freq[b], e->stream);
+    if (e->id_gp[b]) cudaFreeAsync(e->id_gp[b], e->stream);
+    if (e->id_tid[b]) cudaFreeAsync(e->id_tid[b], e->stream);
     e->freq[b] = nullptr;
     e->id_gp[b] = nullptr;
     e->id_tid[b] = nullptr;
   }
-  if (e->flags) cudaFree(e->flags);
-  if (e->tile_count) cudaFree(e->tile_count);
-  if (e->tile_offset) cudaFree(e->tile_offset);
+  if (e->flags) cudaFreeAsync(e->flags, e->stream);
+  if (e->tile_count) cudaFreeAsync(e->tile_count, e->stream);
+  if (e->tile_offset) cudaFreeAsync(e->tile_offset, e->stream);
   e->flags = nullptr;
   e->tile_count = nullptr;
   e->tile_offset = nullptr;
@@ -531,14 +543,17 @@ static gf_status set_capacity(Engine* e, long long cap, long long keep) {
   unsigned *nflags = nullptr, *ncount = nullptr, *noffset = nullptr;
   const long long ntiles = cap / kTileSlots;
   cudaError_t err = cudaSuccess;
+  auto palloc = [e](void** p, size_t bytes) {
+    return e->pool ? cudaMallocFromPoolAsync(p, bytes, e->pool, e->stream) : cudaMallocAsync(p, bytes, e->stream);
+  };
   for (int b = 0; b < 2 && err == cudaSuccess; ++b) {
-    err = cudaMallocAsync(&nf[b], sizeof(float) * P * cap, e->stream);
-    if (err == cudaSuccess) err = cudaMallocAsync(&ngp[b], sizeof(int) * cap, e->stream);
-    if (err == cudaSuccess) err = cudaMallocAsync(&ntid[b], sizeof(int) * cap, e->stream);
+    err = palloc(reinterpret_cast<void**>(&nf[b]), sizeof(float) * P * cap);
+    if (err == cudaSuccess) err = palloc(reinterpret_cast<void**>(&ngp[b]), sizeof(int) * cap);
+    if (err == cudaSuccess) err = palloc(reinterpret_cast<void**>(&ntid[b]), sizeof(int) * cap);
   }
-  if (err == cudaSuccess) err = cudaMallocAsync(&nflags, sizeof(unsigned) * (cap / 32), e->stream);
-  if (err == cudaSuccess) err = cudaMallocAsync(&ncount, sizeof(unsigned) * ntiles, e->stream);
-  if (err == cudaSuccess) err = cudaMallocAsync(&noffset, sizeof(unsigned) * ntiles, e->stream);
+  if (err == cudaSuccess) err = palloc(reinterpret_cast<void**>(&nflags), sizeof(unsigned) * (cap / 32));
+  if (err == cudaSuccess) err = palloc(reinterpret_cast<void**>(&ncount), sizeof(unsigned) * ntiles);
+  if (err == cudaSuccess) err = palloc(reinterpret_cast<void**>(&noffset), sizeof(unsigned) * ntiles);
   if (err != cudaSuccess) {
     for (int b = 0; b < 2; ++b) {
       if (nf[b]) cudaFreeAsync(nf[b], e->stream);
@@ -1139,6 +1154,20 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
   }
   cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream);
   cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream);
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&e->pool, &props) == cudaSuccess) {
+      uint64_t keep_all = UINT64_MAX;
+      cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+    } else {
+      cudaGetLastError();
+      e->pool = nullptr;   // fall back to the device's default pool
+    }
+  }
   *out = g;
   return GF_OK;
 }
@@ -1150,6 +1179,8 @@ void gf_engine_destroy(gf_engine* g) {
   cudaStreamSynchronize(e->stream);
   release_sim(e);
   release_batch(e);
+  cudaStreamSynchronize(e->stream);
+  if (e->pool) cudaMemPoolDestroy(e->pool);
   for (auto ev : e->free_events) cudaEventDestroy(ev);
   if (e->spec_scratch) cudaFree(e->spec_scratch);
   if (e->spec_in) cudaFree(e->spec_in);
@@ -1257,11 +1288,19 @@ gf_status gf_sim_begin_mse(gf_engine* g, const gf_sim_config* c, const gf_mse_po
   const long long ncls = std::max<long long>(num_classes, 1);
   long long max_nc = 1;
   for (int p = 0; p < P; ++p) max_nc = std::max<long long>(max_nc, pops[p].Nchrom_e);
-  GF_CUDA(e, cudaMalloc(&d_counts, sizeof(unsigned) * ncls));
-  GF_CUDA(e, cudaMalloc(&d_starts, sizeof(unsigned) * ncls));
-  GF_CUDA(e, cudaMalloc(&d_area, sizeof(float) * max_nc));
-  GF_CUDA(e, cudaMalloc(&d_integral, sizeof(float) * max_nc));
-  GF_CUDA(e, cudaMalloc(&d_total, sizeof(int)));
+  {
+    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_counts), sizeof(unsigned) * ncls);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_starts), sizeof(unsigned) * ncls);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_area), sizeof(float) * max_nc);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_integral), sizeof(float) * max_nc);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_total), sizeof(int));
+    if (ast != GF_OK) {
+      for (void* q : {static_cast<void*>(d_counts), static_cast<void*>(d_starts), static_cast<void*>(d_area),
+                      static_cast<void*>(d_integral), static_cast<void*>(d_total)})
+        if (q) cudaFreeAsync(q, e->stream);
+      return ast;
+    }
+  }
   GF_CUDA(e, cudaMemsetAsync(d_counts, 0, sizeof(unsigned) * ncls, e->stream));
   for (int p = 0; p < P; ++p) {
     const gf_mse_population& mp = pops[p];
@@ -1299,12 +1338,11 @@ gf_status gf_sim_begin_mse(gf_engine* g, const gf_sim_config* c, const gf_mse_po
     }
     e->any_preserved = preserve != 0;
   }
-  cudaStreamSynchronize(e->stream);
-  cudaFree(d_counts);
-  cudaFree(d_starts);
-  cudaFree(d_area);
-  cudaFree(d_integral);
-  cudaFree(d_total);
+  cudaFreeAsync(d_counts, e->stream);
+  cudaFreeAsync(d_starts, e->stream);
+  cudaFreeAsync(d_area, e->stream);
+  cudaFreeAsync(d_integral, e->stream);
+  cudaFreeAsync(d_total, e->stream);
   return st;
 }
 

@@ -149,6 +149,9 @@ struct Engine {
   int blocks_per_sm = 0;   // drift grid limit per SM (0: occupancy maximum)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // stream-ordered pool for the mutation arrays and per-run scratch; it keeps freed memory, so a new
+  // simulation on the same engine reuses the previous one's buffers without driver allocations
+  cudaMemPool_t pool = nullptr;
   std::string last_error;
 
   // simulation constants
@@ -226,6 +229,7 @@ gf_status cuda_fail(Engine* e, cudaError_t err, const char* what);
     if (_err != cudaSuccess) return ::gf::cuda_fail((e), _err, #call); \
   } while (0)
 
+gf_status pool_alloc(Engine* e, void** ptr, size_t bytes);
 gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
 
 // Window launch (+ segmented compaction into compact_dst), window.cu.
