@@ -39,30 +39,43 @@ constexpr int IN_PAD = 64;
 constexpr int OUT_PAD = 128;
 constexpr int MAX_SPLITS = 16;
 
-enum Epi : int { EPI_STORE_F32 = 0, EPI_FWD_GELU = 1, EPI_FWD_LINEAR = 2, EPI_BWD_GELU = 3, EPI_PARTIAL = 4 };
+enum Epi : int {
+  EPI_STORE_F32 = 0,     // C (fp32)
+  EPI_FWD_GELU = 1,      // Z = acc + bias (fp32), Y = GELU(Z) (bf16) and Y^T (bf16)
+  EPI_FWD_LINEAR = 2,    // out = acc + bias (fp32)
+  EPI_BWD_GELU = 3,      // dZ = acc * GELU'(Z) (bf16) and dZ^T (bf16), bias partials
+  EPI_PARTIAL = 4,       // split-K partial slice of C (fp32)
+  EPI_FWD_GELU_INFER = 5 // Y = GELU(acc + bias) (bf16) only
+};
 
 struct EpiArgs {
-  float* c;                  // fp32 output (C, pre-activation Z, linear output, or split-K partials)
-  long long ldc;
-  long long split_stride;    // elements between split-K partial slices of c
-  __nv_bfloat16* y;          // bf16 row-major output
-  long long ldy;
-  __nv_bfloat16* yt;         // bf16 transposed output
-  long long ldyt;
   const float* bias;         // [N]
   const float* z;            // forward pre-activation read by the backward epilogue
   long long ldz;
   float* bias_part;          // [M / 128][ld_bias_part] column sums of the backward output
   long long ld_bias_part;
+  int rows_per_split;        // row offset of split s in the partial-slice map (EPI_PARTIAL)
   int* fault;                // set when a bounded wait ran out
 };
+
+constexpr int EPI_WARPS = 4;
+constexpr int GEMM_THREADS = 64 + 32 * EPI_WARPS;   // TMA warp, MMA warp, 4 epilogue warps
+
+// Per-epilogue-warp staging of one 32 x 32 output chunk, double-buffered: fp32 rows with the 128-byte
+// swizzle, bf16 rows with the 64-byte swizzle, bf16 transposed rows unswizzled -- the layouts the
+// output tensor maps expect, and conflict-free for the row-per-lane writes.
+constexpr int STG_F32 = 32 * 32 * 4;
+constexpr int STG_BF16 = 32 * 32 * 2;
+constexpr int STG_BUF = STG_F32 + 2 * STG_BF16;           // 8 KB
+constexpr int STG_WARP = 2 * STG_BUF;
 
 template <int BN>
 struct Smem {
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int BAR_OFFSET = STAGES * STAGE_BYTES;
+  static constexpr int STG_OFFSET = STAGES * STAGE_BYTES;
+  static constexpr int BAR_OFFSET = STG_OFFSET + EPI_WARPS * STG_WARP;
   static constexpr int BYTES = BAR_OFFSET + 256 + 4 * 32 * 4 + 1024;   // + barriers, reduction, alignment
 };
 
@@ -74,8 +87,16 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return cdf + z * pdf;
 }
 
-__device__ __forceinline__ void store_bf16_row32(__nv_bfloat16* dst, const float* v) {
-  uint4* d = reinterpret_cast<uint4*>(dst);
+// row `r` of a 32 x 32 fp32 chunk, 128-byte swizzle (16-byte unit q of row r sits at q ^ (r % 8))
+__device__ __forceinline__ void stage_f32_row(uint8_t* buf, int r, const float* v) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    *reinterpret_cast<float4*>(buf + r * 128 + ((q ^ (r & 7)) << 4)) =
+        make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// row `r` of a 32 x 32 bf16 chunk, 64-byte swizzle (16-byte unit q of row r sits at q ^ ((r / 2) % 4))
+__device__ __forceinline__ void stage_bf16_row(uint8_t* buf, int r, const float* v) {
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     uint32_t w[4];
@@ -84,35 +105,57 @@ __device__ __forceinline__ void store_bf16_row32(__nv_bfloat16* dst, const float
       __nv_bfloat162 p = __floats2bfloat162_rn(v[q * 8 + 2 * t], v[q * 8 + 2 * t + 1]);
       w[t] = *reinterpret_cast<uint32_t*>(&p);
     }
-    d[q] = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(buf + r * 64 + ((q ^ ((r >> 1) & 3)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
-__device__ __forceinline__ void store_f32_row32(float* dst, const float* v) {
-  float4* d = reinterpret_cast<float4*>(dst);
+// column `r` of the transposed chunk: element (j, r) at j * 64 + 2 r
+__device__ __forceinline__ void stage_bf16_col(uint8_t* buf, int r, const float* v) {
 #pragma unroll
-  for (int q = 0; q < 8; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  for (int j = 0; j < 32; ++j) *reinterpret_cast<__nv_bfloat16*>(buf + j * 64 + 2 * r) = __float2bfloat16_rn(v[j]);
 }
 
-// One 128 x BN output tile per CTA, K range split over gridDim.z.  Thread 0 drives TMA, thread 32
-// issues the MMAs, all four warps run the epilogue from tensor memory.
+// Persistent tensor-core GEMM: CTAs stride over 128 x BN output tiles (N fastest, then M, then the
+// K split).  Warp 0 streams A/B K-blocks with TMA into a 4-stage ring, warp 1 issues tcgen05 MMAs
+// into one of two tensor-memory accumulators, warps 2-5 drain the other accumulator through the
+// epilogue (tcgen05.ld -> registers -> swizzled shared staging -> TMA store), so a tile's epilogue
+// overlaps the next tile's MMAs.
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
 umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
-                 int k_blocks, EpiArgs ep) {
+                 const __grid_constant__ CUtensorMap tma_c, const __grid_constant__ CUtensorMap tma_y,
+                 const __grid_constant__ CUtensorMap tma_yt, int m_tiles, int n_tiles, int splits, int k_blocks,
+                 EpiArgs ep) {
   using L = Smem<BN>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFFSET);
   uint64_t* empty = full + STAGES;
-  uint64_t* done = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* tfull = empty + STAGES;      // accumulator ready (MMA -> epilogue)
+  uint64_t* tempty = tfull + 2;          // accumulator drained (epilogue -> MMA)
+  uint64_t* drain = tempty + 2;           // MMA completion before tensor memory is released (abort path)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   int* timed_out = reinterpret_cast<int*>(tmem_slot + 1);
   float* red = reinterpret_cast<float*>(smem + L::BAR_OFFSET + 256);   // [4][32]
+  volatile int* abort_flag = timed_out;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
-  const int kb0 = blockIdx.z * k_blocks;
+  const int tiles = m_tiles * n_tiles * splits;
+  // Bounded wait: once any wait of this CTA has run out, every later wait returns at once, so a
+  // broken pipeline ends the CTA after one time limit rather than one per stage.
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (*abort_flag) return false;
+    const uint32_t addr = smem_u32(bar);
+    const long long t0 = clock64();
+    while (!mbar_try_wait(addr, parity)) {
+      if (*abort_flag) return false;
+      if (clock64() - t0 > WAIT_LIMIT) {
+        *abort_flag = 1;
+        return false;
+      }
+    }
+    return true;
+  };
 
   if (threadIdx.x == 0) {
     tma_prefetch_desc(&tma_a);
@@ -121,117 +164,182 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], EPI_WARPS);
+    }
+    mbar_init(drain, 1);
     *timed_out = 0;
     mbar_fence_init();
   }
   __syncwarp();
-  if (warp == 0) tmem_alloc(tmem_slot, BN);
+  if (warp == 1) tmem_alloc(tmem_slot, 2 * BN);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   bool late = false;
+  int issued = 0;   // K-blocks the producer issued (for the drain after a timeout)
 
-  if (threadIdx.x == 0) {
-    for (int kb = 0; kb < k_blocks; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t ph = (kb / STAGES) & 1;
-      if (!mbar_wait(&empty[s], ph ^ 1, WAIT_LIMIT)) late = true;
-      uint8_t* a = smem + s * L::STAGE_BYTES;
-      mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
-      tma_load_2d(a, &tma_a, (kb0 + kb) * BK, m0, &full[s]);
-      tma_load_2d(a + L::A_BYTES, &tma_b, (kb0 + kb) * BK, n0, &full[s]);
+  if (warp == 0) {
+    if (lane == 0) {
+      int it = 0;
+      for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int nt = tile % n_tiles;
+        const int rest = tile / n_tiles;
+        const int mt = rest % m_tiles;
+        const int sp = rest / m_tiles;
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int s = it % STAGES;
+          const uint32_t ph = (it / STAGES) & 1;
+          if (!wait(&empty[s], ph ^ 1)) late = true;
+          uint8_t* a = smem + s * L::STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
+          const int kx = (sp * k_blocks + kb) * BK;
+          tma_load_2d(a, &tma_a, kx, mt * BM, &full[s]);
+          tma_load_2d(a + L::A_BYTES, &tma_b, kx, nt * BN, &full[s]);
+        }
+      }
+      issued = it;
     }
-  } else if (threadIdx.x == 32) {
-    constexpr uint32_t idesc = bf16_idesc(BM, BN);
-    for (int kb = 0; kb < k_blocks; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t ph = (kb / STAGES) & 1;
-      if (!mbar_wait(&full[s], ph, WAIT_LIMIT)) late = true;
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = bf16_idesc(BM, BN);
+      int it = 0, local = 0;
+      for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++local) {
+        const int acc = local & 1;
+        const uint32_t use = static_cast<uint32_t>(local >> 1);
+        if (!wait(&tempty[acc], (use & 1) ^ 1)) late = true;
+        tc_fence_after();
+        const uint32_t d = tmem + static_cast<uint32_t>(acc * BN);
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int s = it % STAGES;
+          const uint32_t ph = (it / STAGES) & 1;
+          if (!wait(&full[s], ph)) late = true;
+          tc_fence_after();
+          const uint32_t a_addr = smem_u32(smem + s * L::STAGE_BYTES);
+          const uint32_t b_addr = a_addr + L::A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk)
+            umma_bf16(d, sw128_kmajor_desc(a_addr + kk * 32), sw128_kmajor_desc(b_addr + kk * 32), idesc,
+                      (kb | kk) != 0);
+          umma_commit(&empty[s]);
+        }
+        umma_commit(&tfull[acc]);
+      }
+    }
+    __syncwarp();
+  } else {
+    // epilogue warps: TMEM lane quarter = warp % 4
+    const int qd = warp & 3;
+    const int ew = warp - 2;
+    uint8_t* stg = smem + L::STG_OFFSET + ew * STG_WARP;
+    int chunk = 0, local = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++local) {
+      const int nt = tile % n_tiles;
+      const int rest = tile / n_tiles;
+      const int mt = rest % m_tiles;
+      const int sp = rest / m_tiles;
+      const int acc = local & 1;
+      const uint32_t use = static_cast<uint32_t>(local >> 1);
+      if (!wait(&tfull[acc], use & 1)) late = true;
+      __syncwarp();
       tc_fence_after();
-      const uint32_t a_addr = smem_u32(smem + s * L::STAGE_BYTES);
-      const uint32_t b_addr = a_addr + L::A_BYTES;
-#pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk)
-        umma_bf16(tmem, sw128_kmajor_desc(a_addr + kk * 32), sw128_kmajor_desc(b_addr + kk * 32), idesc,
-                  (kb | kk) != 0);
-      umma_commit(&empty[s]);
-    }
-    umma_commit(done);
-  }
-  if (!mbar_wait(done, 0, WAIT_LIMIT)) late = true;
-  __syncwarp();
-  tc_fence_after();
-
-  const int row = m0 + warp * 32 + lane;
-  const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+      const int row0 = mt * BM + qd * 32;        // first output row of this warp
+      const int row = row0 + lane;
+      const uint32_t tbase = tmem + (static_cast<uint32_t>(qd * 32) << 16) + static_cast<uint32_t>(acc * BN);
 #pragma unroll 1
-  for (int c0 = 0; c0 < BN; c0 += 32) {
-    float v[32];
-    tmem_ld_32cols(tbase + c0, v);
-    const int n = n0 + c0;
-    if constexpr (EPI == EPI_STORE_F32) {
-      store_f32_row32(ep.c + row * ep.ldc + n, v);
-    } else if constexpr (EPI == EPI_PARTIAL) {
-      store_f32_row32(ep.c + blockIdx.z * ep.split_stride + row * ep.ldc + n, v);
-    } else if constexpr (EPI == EPI_FWD_LINEAR) {
+      for (int c0 = 0; c0 < BN; c0 += 32, ++chunk) {
+        const int n = nt * BN + c0;
+        uint8_t* buf = stg + (chunk & 1) * STG_BUF;
+        if (lane == 0) bulk_wait_read<1>();     // the store that last used this buffer has read it
+        __syncwarp();
+        float v[32];
+        tmem_ld_32cols(tbase + c0, v);
+        if constexpr (EPI == EPI_STORE_F32 || EPI == EPI_PARTIAL) {
+          stage_f32_row(buf, lane, v);
+        } else if constexpr (EPI == EPI_FWD_LINEAR) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
-      store_f32_row32(ep.c + row * ep.ldc + n, v);
-    } else if constexpr (EPI == EPI_FWD_GELU) {
+          for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
+          stage_f32_row(buf, lane, v);
+        } else if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
-      store_f32_row32(ep.c + row * ep.ldc + n, v);
+          for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
+          if constexpr (EPI == EPI_FWD_GELU) stage_f32_row(buf, lane, v);
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
-      store_bf16_row32(ep.y + row * ep.ldy + n, v);
+          for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+          stage_bf16_row(buf + STG_F32, lane, v);
+          if constexpr (EPI == EPI_FWD_GELU) stage_bf16_col(buf + STG_F32 + STG_BF16, lane, v);
+        } else if constexpr (EPI == EPI_BWD_GELU) {
+          const float4* zp = reinterpret_cast<const float4*>(ep.z + static_cast<long long>(row) * ep.ldz + n);
 #pragma unroll
-      for (int j = 0; j < 32; ++j) ep.yt[(n + j) * ep.ldyt + row] = __float2bfloat16_rn(v[j]);
-    } else if constexpr (EPI == EPI_BWD_GELU) {
-      const float4* zp = reinterpret_cast<const float4*>(ep.z + row * ep.ldz + n);
+          for (int q = 0; q < 8; ++q) {
+            const float4 z = __ldg(zp + q);
+            v[4 * q] *= gelu_grad(z.x);
+            v[4 * q + 1] *= gelu_grad(z.y);
+            v[4 * q + 2] *= gelu_grad(z.z);
+            v[4 * q + 3] *= gelu_grad(z.w);
+          }
+          stage_bf16_row(buf + STG_F32, lane, v);
+          stage_bf16_col(buf + STG_F32 + STG_BF16, lane, v);
+          // column sums over the tile's 128 rows (fixed order: lanes, then quarters 0..3)
+          float mine = 0.f;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const float4 z = zp[q];
-        v[4 * q] *= gelu_grad(z.x);
-        v[4 * q + 1] *= gelu_grad(z.y);
-        v[4 * q + 2] *= gelu_grad(z.z);
-        v[4 * q + 3] *= gelu_grad(z.w);
+          for (int j = 0; j < 32; ++j) {
+            float t = v[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == j) mine = t;
+          }
+          red[qd * 32 + lane] = mine;
+          named_barrier_sync(1, 32 * EPI_WARPS);
+          if (qd == 0) {
+            const float t = ((red[lane] + red[32 + lane]) + red[64 + lane]) + red[96 + lane];
+            ep.bias_part[mt * ep.ld_bias_part + n + lane] = t;
+          }
+          named_barrier_sync(1, 32 * EPI_WARPS);
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          if constexpr (EPI == EPI_STORE_F32 || EPI == EPI_FWD_LINEAR || EPI == EPI_FWD_GELU) {
+            tma_store_2d(&tma_c, n, row0, buf);
+          } else if constexpr (EPI == EPI_PARTIAL) {
+            tma_store_2d(&tma_c, n, sp * ep.rows_per_split + row0, buf);
+          }
+          if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER || EPI == EPI_BWD_GELU)
+            tma_store_2d(&tma_y, n, row0, buf + STG_F32);
+          if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_BWD_GELU)
+            tma_store_2d(&tma_yt, row0, n, buf + STG_F32 + STG_BF16);
+          bulk_commit();
+        }
       }
-      store_bf16_row32(ep.y + row * ep.ldy + n, v);
-#pragma unroll
-      for (int j = 0; j < 32; ++j) ep.yt[(n + j) * ep.ldyt + row] = __float2bfloat16_rn(v[j]);
-      // column sums over the tile's 128 rows (fixed order: lanes, then warps)
-      float mine = 0.f;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        float s = v[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == j) mine = s;
-      }
-      red[warp * 32 + lane] = mine;
-      __syncthreads();
-      if (warp == 0) {
-        const float t = ((red[lane] + red[32 + lane]) + red[64 + lane]) + red[96 + lane];
-        ep.bias_part[blockIdx.y * ep.ld_bias_part + n + lane] = t;
-      }
-      __syncthreads();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[acc]);
     }
+    if (lane == 0) bulk_wait_all();
+    __syncwarp();
   }
+
   tc_fence_before();
-  if (late) atomicOr(timed_out, 1);
+  if (late) *abort_flag = 1;
   __syncthreads();
-  if (*timed_out) {
-    // a wait ran out: let every copy this CTA issued land before its shared memory is released
+  if (*abort_flag) {
+    // a wait ran out: let every load and MMA this CTA issued finish before its shared and tensor
+    // memory are released (each wait again bounded)
     if (threadIdx.x == 0) {
-      for (int kb = k_blocks - STAGES < 0 ? 0 : k_blocks - STAGES; kb < k_blocks; ++kb)
-        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, WAIT_LIMIT);
+      for (int it = issued - STAGES < 0 ? 0 : issued - STAGES; it < issued; ++it)
+        mbar_wait(&full[it % STAGES], (it / STAGES) & 1, WAIT_LIMIT);
       if (ep.fault) atomicOr(ep.fault, 1);
+    } else if (threadIdx.x == 32) {
+      umma_commit(drain);
+      mbar_wait(drain, 0, WAIT_LIMIT);
     }
     __syncthreads();
   }
-  if (warp == 0) tmem_dealloc(tmem, BN);
+  if (warp == 1) tmem_dealloc(tmem, 2 * BN);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -396,7 +504,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Tensor map of a row-major bf16 matrix [rows][cols] (cols contiguous), tile box_rows x 64.
+// Operand map: row-major bf16 [rows][cols] (cols contiguous), box box_rows x 64, 128-byte swizzle
+// (the layout the UMMA matrix descriptors name).
 bool make_map(CUtensorMap* m, const void* base, long long rows, long long cols, int box_rows) {
   auto fn = encode_fn();
   if (!fn) return false;
@@ -409,9 +518,44 @@ bool make_map(CUtensorMap* m, const void* base, long long rows, long long cols, 
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Output map of a row-major [rows][cols] matrix with 32 x 32 boxes, in the staging layout of the
+// epilogue: fp32 with the 128-byte swizzle, bf16 with the 64-byte swizzle, or (transposed outputs) bf16
+// unswizzled.
+enum OutKind { OUT_F32 = 0, OUT_BF16 = 1, OUT_BF16_T = 2 };
+bool make_out_map(CUtensorMap* m, const void* base, long long rows, long long cols, OutKind kind) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const int esize = kind == OUT_F32 ? 4 : 2;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * esize};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapSwizzle sw = kind == OUT_F32    ? CU_TENSOR_MAP_SWIZZLE_128B
+                                : kind == OUT_BF16 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                   : CU_TENSOR_MAP_SWIZZLE_NONE;
+  return fn(m, kind == OUT_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+            const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      n = 148;
+    }
+  }
+  return n;
+}
+
+// Outputs the epilogue does not write get the A map in their slot (never used).
 template <int BN, int EPI>
-cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, int M, int N, int K, int splits,
-                        const EpiArgs& ep, cudaStream_t stream) {
+cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap* c, const CUtensorMap* y,
+                        const CUtensorMap* yt, int M, int N, int K, int splits, const EpiArgs& ep,
+                        cudaStream_t stream) {
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -421,8 +565,11 @@ cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, int M, int N
     if (err != cudaSuccess) return err;
     attr_set[dev] = true;
   }
-  dim3 grid(N / BN, M / BM, splits);
-  umma_gemm_kernel<BN, EPI><<<grid, 128, Smem<BN>::BYTES, stream>>>(a, b, K / BK / splits, ep);
+  const int m_tiles = M / BM, n_tiles = N / BN;
+  const int tiles = m_tiles * n_tiles * splits;
+  const int grid = tiles < sm_count() ? tiles : sm_count();
+  umma_gemm_kernel<BN, EPI><<<grid, GEMM_THREADS, Smem<BN>::BYTES, stream>>>(
+      a, b, c ? *c : a, y ? *y : a, yt ? *yt : a, m_tiles, n_tiles, splits, K / BK / splits, ep);
   return cudaGetLastError();
 }
 
@@ -483,6 +630,10 @@ struct gf_mlp {
   CUtensorMap fwd_a[GF_MLP_LAYERS], fwd_b[GF_MLP_LAYERS];     // A = input activations, B = W
   CUtensorMap bwd_a[GF_MLP_LAYERS], bwd_b[GF_MLP_LAYERS];     // A = dZ_l (dOut), B = W_l^T  (l >= 2)
   CUtensorMap dw_a[GF_MLP_LAYERS], dw_b[GF_MLP_LAYERS];       // A = dZ_l^T, B = Y_{l-1}^T
+  CUtensorMap out_z[4], out_y[4], out_yt[4];                  // forward outputs of the hidden layers
+  CUtensorMap out_final;                                      // layer-5 output (fp32)
+  CUtensorMap out_dz[4], out_dzt[4];                          // backward outputs dZ, dZ^T
+  CUtensorMap out_wpart[GF_MLP_LAYERS];                       // split-K weight-gradient slices
 
   std::vector<void*> allocations;
 };
@@ -570,7 +721,7 @@ gf_status check_batch(gf_mlp* m, int batch) {
   return GF_OK;
 }
 
-gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch) {
+gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch, bool train) {
   encode_inputs_kernel<<<(batch + 255) / 256, 256, 0, m->stream>>>(d_inputs, batch, m->x0, m->x0t, m->cap);
   MLP_CUDA(m, cudaGetLastError());
   for (int l = 0; l < GF_MLP_LAYERS; ++l) {
@@ -579,17 +730,13 @@ gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch) {
     ep.fault = m->fault;
     cudaError_t err;
     if (l < 4) {
-      ep.c = m->z[l];
-      ep.ldc = HID;
-      ep.y = m->y[l];
-      ep.ldy = HID;
-      ep.yt = m->yt[l];
-      ep.ldyt = m->cap;
-      err = launch_gemm<128, EPI_FWD_GELU>(m->fwd_a[l], m->fwd_b[l], batch, HID, m->cols[l], 1, ep, m->stream);
+      err = train ? launch_gemm<128, EPI_FWD_GELU>(m->fwd_a[l], m->fwd_b[l], &m->out_z[l], &m->out_y[l],
+                                                   &m->out_yt[l], batch, HID, m->cols[l], 1, ep, m->stream)
+                  : launch_gemm<128, EPI_FWD_GELU_INFER>(m->fwd_a[l], m->fwd_b[l], nullptr, &m->out_y[l], nullptr,
+                                                         batch, HID, m->cols[l], 1, ep, m->stream);
     } else {
-      ep.c = m->out;
-      ep.ldc = OUT_PAD;
-      err = launch_gemm<128, EPI_FWD_LINEAR>(m->fwd_a[l], m->fwd_b[l], batch, OUT_PAD, HID, 1, ep, m->stream);
+      err = launch_gemm<128, EPI_FWD_LINEAR>(m->fwd_a[l], m->fwd_b[l], &m->out_final, nullptr, nullptr, batch,
+                                             OUT_PAD, HID, 1, ep, m->stream);
     }
     if (err != cudaSuccess) return mlp_fail(m, GF_ERR_CUDA, "forward GEMM %d: %s", l + 1, cudaGetErrorString(err));
   }
@@ -607,17 +754,17 @@ gf_status run_backward(gf_mlp* m, const float* d_targets, int batch) {
     // weight gradient partials of layer l+1
     {
       EpiArgs ep{};
-      ep.c = m->wpart[l];
-      ep.ldc = m->cols[l];
-      ep.split_stride = static_cast<long long>(m->rows[l]) * m->cols[l];
+      ep.rows_per_split = m->rows[l];
       ep.fault = m->fault;
       const int M = m->rows[l], N = m->cols[l];
       const int bn = (N % 128 == 0) ? 128 : 64;
       const int splits = choose_splits((M / BM) * (N / bn), batch);
       m->wsplits[l] = splits;
       cudaError_t err = bn == 128
-          ? launch_gemm<128, EPI_PARTIAL>(m->dw_a[l], m->dw_b[l], M, N, batch, splits, ep, m->stream)
-          : launch_gemm<64, EPI_PARTIAL>(m->dw_a[l], m->dw_b[l], M, N, batch, splits, ep, m->stream);
+          ? launch_gemm<128, EPI_PARTIAL>(m->dw_a[l], m->dw_b[l], &m->out_wpart[l], nullptr, nullptr, M, N, batch,
+                                          splits, ep, m->stream)
+          : launch_gemm<64, EPI_PARTIAL>(m->dw_a[l], m->dw_b[l], &m->out_wpart[l], nullptr, nullptr, M, N, batch,
+                                         splits, ep, m->stream);
       if (err != cudaSuccess)
         return mlp_fail(m, GF_ERR_CUDA, "weight-gradient GEMM %d: %s", l + 1, cudaGetErrorString(err));
     }
@@ -626,15 +773,11 @@ gf_status run_backward(gf_mlp* m, const float* d_targets, int batch) {
     EpiArgs ep{};
     ep.z = m->z[l - 1];
     ep.ldz = HID;
-    ep.y = m->dz[l - 1];
-    ep.ldy = HID;
-    ep.yt = m->dzt[l - 1];
-    ep.ldyt = m->cap;
     ep.bias_part = m->bpart[l - 1];
     ep.ld_bias_part = HID;
     ep.fault = m->fault;
-    cudaError_t err = launch_gemm<128, EPI_BWD_GELU>(m->bwd_a[l], m->bwd_b[l], batch, HID, m->rows[l], 1, ep,
-                                                    m->stream);
+    cudaError_t err = launch_gemm<128, EPI_BWD_GELU>(m->bwd_a[l], m->bwd_b[l], nullptr, &m->out_dz[l - 1],
+                                                    &m->out_dzt[l - 1], batch, HID, m->rows[l], 1, ep, m->stream);
     if (err != cudaSuccess)
       return mlp_fail(m, GF_ERR_CUDA, "input-gradient GEMM %d: %s", l + 1, cudaGetErrorString(err));
   }
@@ -738,7 +881,17 @@ gf_status gf_mlp_create(int32_t device, void* stream, const gf_mlp_config* confi
       }
       ok = ok && make_map(&m->dw_a[l], g_t, m->rows[l], cap, BM);
       ok = ok && make_map(&m->dw_b[l], in_t, m->cols[l], cap, m->cols[l] % 128 == 0 ? 128 : 64);
+      ok = ok && make_out_map(&m->out_wpart[l], m->wpart[l], static_cast<long long>(MAX_SPLITS) * m->rows[l],
+                              m->cols[l], OUT_F32);
     }
+    for (int l = 0; l < 4; ++l) {
+      ok = ok && make_out_map(&m->out_z[l], m->z[l], cap, HID, OUT_F32);
+      ok = ok && make_out_map(&m->out_y[l], m->y[l], cap, HID, OUT_BF16);
+      ok = ok && make_out_map(&m->out_yt[l], m->yt[l], HID, cap, OUT_BF16_T);
+      ok = ok && make_out_map(&m->out_dz[l], m->dz[l], cap, HID, OUT_BF16);
+      ok = ok && make_out_map(&m->out_dzt[l], m->dzt[l], HID, cap, OUT_BF16_T);
+    }
+    ok = ok && make_out_map(&m->out_final, m->out, cap, OUT_PAD, OUT_F32);
     if (!ok) {
       st = mlp_fail(m, GF_ERR_CUDA, "tensor map encoding failed");
       goto bad;
@@ -821,7 +974,7 @@ gf_status gf_mlp_forward(gf_mlp* m, const float* d_inputs, int32_t batch, float*
   gf_status st = check_batch(m, batch);
   if (st != GF_OK) return st;
   MLP_CUDA(m, cudaSetDevice(m->device));
-  if ((st = run_forward(m, d_inputs, batch)) != GF_OK) return st;
+  if ((st = run_forward(m, d_inputs, batch, false)) != GF_OK) return st;
   const long long n = static_cast<long long>(batch) * GF_MLP_OUTPUTS;
   copy_output_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, m->stream>>>(m->out, batch, d_outputs);
   MLP_CUDA(m, cudaGetLastError());
@@ -834,7 +987,7 @@ gf_status gf_mlp_gradients(gf_mlp* m, const float* d_inputs, const float* d_targ
   gf_status st = check_batch(m, batch);
   if (st != GF_OK) return st;
   MLP_CUDA(m, cudaSetDevice(m->device));
-  if ((st = run_forward(m, d_inputs, batch)) != GF_OK) return st;
+  if ((st = run_forward(m, d_inputs, batch, true)) != GF_OK) return st;
   if ((st = run_backward(m, d_targets, batch)) != GF_OK) return st;
   if (loss) {
     MLP_CUDA(m, cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
@@ -852,7 +1005,7 @@ gf_status gf_mlp_train_step(gf_mlp* m, const float* d_inputs, const float* d_tar
   gf_status st = check_batch(m, batch);
   if (st != GF_OK) return st;
   MLP_CUDA(m, cudaSetDevice(m->device));
-  if ((st = run_forward(m, d_inputs, batch)) != GF_OK) return st;
+  if ((st = run_forward(m, d_inputs, batch, true)) != GF_OK) return st;
   if ((st = run_backward(m, d_targets, batch)) != GF_OK) return st;
   m->step += 1;
   const double bc1 = 1.0 - std::pow(static_cast<double>(m->cfg.beta1), static_cast<double>(m->step));
@@ -882,14 +1035,13 @@ gf_status gf_bf16_gemm(const void* d_a, const void* d_b, int32_t M, int32_t N, i
   if ((reinterpret_cast<uintptr_t>(d_a) | reinterpret_cast<uintptr_t>(d_b) | reinterpret_cast<uintptr_t>(d_c)) & 15)
     return GF_ERR_INVALID_ARGUMENT;
   const int bn = N % 128 == 0 ? 128 : 64;
-  CUtensorMap a, b;
-  if (!make_map(&a, d_a, M, K, BM) || !make_map(&b, d_b, N, K, bn)) return GF_ERR_CUDA;
+  CUtensorMap a, b, c;
+  if (!make_map(&a, d_a, M, K, BM) || !make_map(&b, d_b, N, K, bn) || !make_out_map(&c, d_c, M, N, OUT_F32))
+    return GF_ERR_CUDA;
   EpiArgs ep{};
-  ep.c = d_c;
-  ep.ldc = N;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaError_t err = bn == 128 ? launch_gemm<128, EPI_STORE_F32>(a, b, M, N, K, 1, ep, s)
-                              : launch_gemm<64, EPI_STORE_F32>(a, b, M, N, K, 1, ep, s);
+  cudaError_t err = bn == 128 ? launch_gemm<128, EPI_STORE_F32>(a, b, &c, nullptr, nullptr, M, N, K, 1, ep, s)
+                              : launch_gemm<64, EPI_STORE_F32>(a, b, &c, nullptr, nullptr, M, N, K, 1, ep, s);
   return err == cudaSuccess ? GF_OK : GF_ERR_CUDA;
 }
 
