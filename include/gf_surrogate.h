@@ -1,5 +1,5 @@
 /* C ABI of the SFS surrogate network: a 6 -> 512 -> 512 -> 512 -> 512 -> 99 multilayer perceptron
- * with GELU activations, bf16 weights and activations, fp32 accumulation (tcgen05 tensor cores, sm_100a),
+ * with GELU activations (tanh form), bf16 weights and activations, fp32 accumulation (tcgen05 tensor cores, sm_100a),
  * fp32 master weights and Adam.
  *
  * The reference has no counterpart: 3P answers every SFS query with a forward simulation

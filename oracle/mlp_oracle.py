@@ -7,7 +7,8 @@ go_fish.cuh:280, then Spectrum::site_frequency_spectrum, spectrum.h:90), so ther
 to follow; this module states the network the surrogate is defined as:
 
     a_0 = x                                   x: 6 scaled parameters
-    z_l = a_{l-1} W_l^T + b_l,  a_l = GELU(z_l)   l = 1..4, width 512, GELU(z) = z Phi(z) (erf form)
+    z_l = a_{l-1} W_l^T + b_l,  a_l = GELU(z_l)   l = 1..4, width 512,
+                                               GELU(z) = z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))
     out = a_4 W_5^T + b_5                      99 outputs
     loss = mean over rows and outputs of (out - target)^2
 
@@ -20,7 +21,6 @@ central finite differences and against torch autograd in the CPU tests.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 INPUTS, HIDDEN, OUTPUTS, LAYERS = 6, 512, 99, 5
 SHAPES = [(HIDDEN, INPUTS), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (OUTPUTS, HIDDEN)]
@@ -54,12 +54,17 @@ def bf16(x: np.ndarray) -> np.ndarray:
     return ((u + r) & np.uint32(0xFFFF0000)).view(np.float32)
 
 
+GELU_C = np.sqrt(2.0 / np.pi)
+GELU_A = 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def forward(vec: np.ndarray, x: np.ndarray, emulate_bf16: bool = True, dtype=np.float32):

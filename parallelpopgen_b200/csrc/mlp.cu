@@ -32,7 +32,6 @@ namespace gfm {
 
 constexpr int BM = 128;       // tile rows = tensor-memory lanes
 constexpr int BK = 64;        // K per pipeline stage: one 128-byte swizzle row of bf16
-constexpr int STAGES = 4;
 constexpr long long WAIT_LIMIT = 1ll << 31;   // SM cycles (about a second) before a wait gives up
 constexpr int HID = GF_MLP_HIDDEN;
 constexpr int IN_PAD = 64;
@@ -45,7 +44,8 @@ enum Epi : int {
   EPI_FWD_LINEAR = 2,    // out = acc + bias (fp32)
   EPI_BWD_GELU = 3,      // dZ = acc * GELU'(Z) (bf16) and dZ^T (bf16), bias partials
   EPI_PARTIAL = 4,       // split-K partial slice of C (fp32)
-  EPI_FWD_GELU_INFER = 5 // Y = GELU(acc + bias) (bf16) only
+  EPI_FWD_GELU_INFER = 5,// Y = GELU(acc + bias) (bf16) only
+  EPI_FWD_OUT = 6        // out = acc + bias written straight to the caller's [rows][99] array
 };
 
 struct EpiArgs {
@@ -55,36 +55,67 @@ struct EpiArgs {
   float* bias_part;          // [M / 128][ld_bias_part] column sums of the backward output
   long long ld_bias_part;
   int rows_per_split;        // row offset of split s in the partial-slice map (EPI_PARTIAL)
+  float* out;                // caller's output [rows][out_cols] (EPI_FWD_OUT)
+  int out_cols;
   int* fault;                // set when a bounded wait ran out
 };
 
-constexpr int EPI_WARPS = 4;
-constexpr int GEMM_THREADS = 64 + 32 * EPI_WARPS;   // TMA warp, MMA warp, 4 epilogue warps
+constexpr int EPI_WARPS = 8;                        // two per tensor-memory lane quarter
+constexpr int GEMM_THREADS = 64 + 32 * EPI_WARPS;   // TMA warp, MMA warp, 8 epilogue warps
+constexpr int SMEM_LIMIT = 232448;                  // dynamic shared memory per CTA on sm_100
 
 // Per-epilogue-warp staging of one 32 x 32 output chunk, double-buffered: fp32 rows with the 128-byte
 // swizzle, bf16 rows with the 64-byte swizzle, bf16 transposed rows unswizzled -- the layouts the
-// output tensor maps expect, and conflict-free for the row-per-lane writes.
-constexpr int STG_F32 = 32 * 32 * 4;
-constexpr int STG_BF16 = 32 * 32 * 2;
-constexpr int STG_BUF = STG_F32 + 2 * STG_BF16;           // 8 KB
-constexpr int STG_WARP = 2 * STG_BUF;
+// output tensor maps expect, and conflict-free for the row-per-lane writes.  Only the outputs the
+// epilogue writes get space.
+template <int EPI>
+struct Stage {
+  static constexpr bool F32 = EPI == EPI_STORE_F32 || EPI == EPI_PARTIAL || EPI == EPI_FWD_LINEAR || EPI == EPI_FWD_GELU;
+  static constexpr bool BF16 = EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER || EPI == EPI_BWD_GELU;
+  static constexpr bool T = EPI == EPI_FWD_GELU || EPI == EPI_BWD_GELU;
+  static constexpr int F32_OFF = 0;
+  static constexpr int BF16_OFF = F32 ? 4096 : 0;
+  static constexpr int T_OFF = BF16_OFF + (BF16 ? 2048 : 0);
+  static constexpr int BUF = ((T_OFF + (T ? 2048 : 0)) + 1023) / 1024 * 1024;
+  static constexpr int WARP = 2 * BUF;
+};
 
-template <int BN>
+template <int BN, int EPI>
 struct Smem {
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int BIAS_FLOATS = 512;   // the bias vector of the whole output width
+  static constexpr int EXTRA = EPI_WARPS * Stage<EPI>::WARP + 256 + 2 * 4 * 32 * 4 + 4 * BIAS_FLOATS + 1024;
+  static constexpr int STAGES = (4 * STAGE_BYTES + EXTRA <= SMEM_LIMIT)   ? 4
+                                : (3 * STAGE_BYTES + EXTRA <= SMEM_LIMIT) ? 3
+                                                                          : 2;
   static constexpr int STG_OFFSET = STAGES * STAGE_BYTES;
-  static constexpr int BAR_OFFSET = STG_OFFSET + EPI_WARPS * STG_WARP;
-  static constexpr int BYTES = BAR_OFFSET + 256 + 4 * 32 * 4 + 1024;   // + barriers, reduction, alignment
+  static constexpr int BAR_OFFSET = STG_OFFSET + EPI_WARPS * Stage<EPI>::WARP;
+  static constexpr int BIAS_OFFSET = BAR_OFFSET + 256 + 2 * 4 * 32 * 4;
+  static constexpr int BYTES = BIAS_OFFSET + 4 * BIAS_FLOATS + 1024;   // + barriers, reductions, bias, alignment
+  static_assert(BYTES <= SMEM_LIMIT, "shared memory");
 };
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.7071067811865476f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), on the hardware tanh.
+constexpr float GELU_C = 0.7978845608028654f;
+constexpr float GELU_A = 0.044715f;
+
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_hw(GELU_C * fmaf(GELU_A * z, z * z, z));
+  return 0.5f * z * (1.f + t);
+}
 
 __device__ __forceinline__ float gelu_grad(float z) {
-  const float cdf = 0.5f * (1.f + erff(z * 0.7071067811865476f));
-  const float pdf = 0.3989422804014327f * expf(-0.5f * z * z);
-  return cdf + z * pdf;
+  const float z2 = z * z;
+  const float t = tanh_hw(GELU_C * fmaf(GELU_A * z, z2, z));
+  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * GELU_C * fmaf(3.f * GELU_A, z2, 1.f);
 }
 
 // row `r` of a 32 x 32 fp32 chunk, 128-byte swizzle (16-byte unit q of row r sits at q ^ (r % 8))
@@ -126,7 +157,9 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
                  const __grid_constant__ CUtensorMap tma_c, const __grid_constant__ CUtensorMap tma_y,
                  const __grid_constant__ CUtensorMap tma_yt, int m_tiles, int n_tiles, int splits, int k_blocks,
                  EpiArgs ep) {
-  using L = Smem<BN>;
+  using L = Smem<BN, EPI>;
+  using SG = Stage<EPI>;
+  constexpr int STAGES = L::STAGES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFFSET);
@@ -136,8 +169,11 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
   uint64_t* drain = tempty + 2;           // MMA completion before tensor memory is released (abort path)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   int* timed_out = reinterpret_cast<int*>(tmem_slot + 1);
-  float* red = reinterpret_cast<float*>(smem + L::BAR_OFFSET + 256);   // [4][32]
+  float* red = reinterpret_cast<float*>(smem + L::BAR_OFFSET + 256);   // [2 halves][4 quarters][32]
+  float* s_bias = reinterpret_cast<float*>(smem + L::BIAS_OFFSET);
   volatile int* abort_flag = timed_out;
+  constexpr bool HAS_BIAS = EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER || EPI == EPI_FWD_LINEAR ||
+                            EPI == EPI_FWD_OUT;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles = m_tiles * n_tiles * splits;
@@ -171,6 +207,9 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
     mbar_init(drain, 1);
     *timed_out = 0;
     mbar_fence_init();
+  }
+  if constexpr (HAS_BIAS) {
+    for (int i = threadIdx.x; i < n_tiles * BN && i < L::BIAS_FLOATS; i += blockDim.x) s_bias[i] = ep.bias[i];
   }
   __syncwarp();
   if (warp == 1) tmem_alloc(tmem_slot, 2 * BN);
@@ -231,10 +270,12 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
     }
     __syncwarp();
   } else {
-    // epilogue warps: TMEM lane quarter = warp % 4
+    // epilogue warps: TMEM lane quarter = warp % 4; the two warps of a quarter take alternate
+    // 32-column chunks
     const int qd = warp & 3;
     const int ew = warp - 2;
-    uint8_t* stg = smem + L::STG_OFFSET + ew * STG_WARP;
+    const int half = ew >> 2;
+    uint8_t* stg = smem + L::STG_OFFSET + ew * SG::WARP;
     int chunk = 0, local = 0;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++local) {
       const int nt = tile % n_tiles;
@@ -250,27 +291,32 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
       const int row = row0 + lane;
       const uint32_t tbase = tmem + (static_cast<uint32_t>(qd * 32) << 16) + static_cast<uint32_t>(acc * BN);
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 32, ++chunk) {
+      for (int c0 = 32 * half; c0 < BN; c0 += 64, ++chunk) {
         const int n = nt * BN + c0;
-        uint8_t* buf = stg + (chunk & 1) * STG_BUF;
+        uint8_t* buf = stg + (chunk & 1) * SG::BUF;
         if (lane == 0) bulk_wait_read<1>();     // the store that last used this buffer has read it
         __syncwarp();
         float v[32];
         tmem_ld_32cols(tbase + c0, v);
         if constexpr (EPI == EPI_STORE_F32 || EPI == EPI_PARTIAL) {
-          stage_f32_row(buf, lane, v);
+          stage_f32_row(buf + SG::F32_OFF, lane, v);
         } else if constexpr (EPI == EPI_FWD_LINEAR) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
-          stage_f32_row(buf, lane, v);
+          for (int j = 0; j < 32; ++j) v[j] += s_bias[n + j];
+          stage_f32_row(buf + SG::F32_OFF, lane, v);
+        } else if constexpr (EPI == EPI_FWD_OUT) {
+          float* o = ep.out + static_cast<long long>(row) * ep.out_cols;
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (n + j < ep.out_cols) o[n + j] = v[j] + s_bias[n + j];
         } else if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] += ep.bias[n + j];
-          if constexpr (EPI == EPI_FWD_GELU) stage_f32_row(buf, lane, v);
+          for (int j = 0; j < 32; ++j) v[j] += s_bias[n + j];
+          if constexpr (EPI == EPI_FWD_GELU) stage_f32_row(buf + SG::F32_OFF, lane, v);
 #pragma unroll
           for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
-          stage_bf16_row(buf + STG_F32, lane, v);
-          if constexpr (EPI == EPI_FWD_GELU) stage_bf16_col(buf + STG_F32 + STG_BF16, lane, v);
+          stage_bf16_row(buf + SG::BF16_OFF, lane, v);
+          if constexpr (EPI == EPI_FWD_GELU) stage_bf16_col(buf + SG::T_OFF, lane, v);
         } else if constexpr (EPI == EPI_BWD_GELU) {
           const float4* zp = reinterpret_cast<const float4*>(ep.z + static_cast<long long>(row) * ep.ldz + n);
 #pragma unroll
@@ -281,9 +327,10 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
             v[4 * q + 2] *= gelu_grad(z.z);
             v[4 * q + 3] *= gelu_grad(z.w);
           }
-          stage_bf16_row(buf + STG_F32, lane, v);
-          stage_bf16_col(buf + STG_F32 + STG_BF16, lane, v);
-          // column sums over the tile's 128 rows (fixed order: lanes, then quarters 0..3)
+          stage_bf16_row(buf + SG::BF16_OFF, lane, v);
+          stage_bf16_col(buf + SG::T_OFF, lane, v);
+          // column sums over the tile's 128 rows (fixed order: lanes, then quarters 0..3); the four
+          // warps of a half work on the same chunk and meet at their own named barrier
           float mine = 0.f;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
@@ -292,26 +339,26 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
             for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
             if (lane == j) mine = t;
           }
-          red[qd * 32 + lane] = mine;
-          named_barrier_sync(1, 32 * EPI_WARPS);
+          float* rh = red + half * 128;
+          rh[qd * 32 + lane] = mine;
+          named_barrier_sync(1 + half, 128);
           if (qd == 0) {
-            const float t = ((red[lane] + red[32 + lane]) + red[64 + lane]) + red[96 + lane];
+            const float t = ((rh[lane] + rh[32 + lane]) + rh[64 + lane]) + rh[96 + lane];
             ep.bias_part[mt * ep.ld_bias_part + n + lane] = t;
           }
-          named_barrier_sync(1, 32 * EPI_WARPS);
+          named_barrier_sync(1 + half, 128);
         }
+        if constexpr (EPI == EPI_FWD_OUT) continue;   // written directly
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
           if constexpr (EPI == EPI_STORE_F32 || EPI == EPI_FWD_LINEAR || EPI == EPI_FWD_GELU) {
-            tma_store_2d(&tma_c, n, row0, buf);
+            tma_store_2d(&tma_c, n, row0, buf + SG::F32_OFF);
           } else if constexpr (EPI == EPI_PARTIAL) {
-            tma_store_2d(&tma_c, n, sp * ep.rows_per_split + row0, buf);
+            tma_store_2d(&tma_c, n, sp * ep.rows_per_split + row0, buf + SG::F32_OFF);
           }
-          if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER || EPI == EPI_BWD_GELU)
-            tma_store_2d(&tma_y, n, row0, buf + STG_F32);
-          if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_BWD_GELU)
-            tma_store_2d(&tma_yt, row0, n, buf + STG_F32 + STG_BF16);
+          if constexpr (SG::BF16) tma_store_2d(&tma_y, n, row0, buf + SG::BF16_OFF);
+          if constexpr (SG::T) tma_store_2d(&tma_yt, row0, n, buf + SG::T_OFF);
           bulk_commit();
         }
       }
@@ -346,16 +393,27 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
 // small kernels
 // ---------------------------------------------------------------------------------------------
 
-// Inputs [batch][6] fp32 -> X0 [cap][64] and X0^T [64][cap] bf16 (padding columns stay zero).
+// Inputs [batch][6] fp32 -> X0 [cap][64] bf16 (one 16-byte store of columns 0..7 per row; columns
+// 8..63 stay zero) and, for training, X0^T [64][cap].
 __global__ void encode_inputs_kernel(const float* __restrict__ x, int batch, __nv_bfloat16* __restrict__ x0,
-                                     __nv_bfloat16* __restrict__ x0t, long long cap) {
+                                     __nv_bfloat16* __restrict__ x0t, long long cap, int transposed) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
+  float v[8];
 #pragma unroll
-  for (int j = 0; j < GF_MLP_INPUTS; ++j) {
-    const __nv_bfloat16 v = __float2bfloat16_rn(x[b * GF_MLP_INPUTS + j]);
-    x0[b * IN_PAD + j] = v;
-    x0t[j * cap + b] = v;
+  for (int j = 0; j < GF_MLP_INPUTS; ++j) v[j] = x[b * GF_MLP_INPUTS + j];
+  v[6] = 0.f;
+  v[7] = 0.f;
+  uint32_t w[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * t], v[2 * t + 1]);
+    w[t] = *reinterpret_cast<uint32_t*>(&p);
+  }
+  *reinterpret_cast<uint4*>(x0 + static_cast<long long>(b) * IN_PAD) = make_uint4(w[0], w[1], w[2], w[3]);
+  if (transposed) {
+#pragma unroll
+    for (int j = 0; j < GF_MLP_INPUTS; ++j) x0t[j * cap + b] = __float2bfloat16_rn(v[j]);
   }
 }
 
@@ -481,12 +539,6 @@ __global__ void refresh_bf16_kernel(const __grid_constant__ ParamTable t) {
   }
 }
 
-__global__ void copy_output_kernel(const float* __restrict__ out, int batch, float* __restrict__ dst) {
-  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (i >= static_cast<long long>(batch) * GF_MLP_OUTPUTS) return;
-  const long long b = i / GF_MLP_OUTPUTS, j = i % GF_MLP_OUTPUTS;
-  dst[i] = out[b * OUT_PAD + j];
-}
 
 // ---------------------------------------------------------------------------------------------
 // host side
@@ -561,14 +613,14 @@ cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtens
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
     cudaError_t err = cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           Smem<BN>::BYTES);
+                                           Smem<BN, EPI>::BYTES);
     if (err != cudaSuccess) return err;
     attr_set[dev] = true;
   }
   const int m_tiles = M / BM, n_tiles = N / BN;
   const int tiles = m_tiles * n_tiles * splits;
   const int grid = tiles < sm_count() ? tiles : sm_count();
-  umma_gemm_kernel<BN, EPI><<<grid, GEMM_THREADS, Smem<BN>::BYTES, stream>>>(
+  umma_gemm_kernel<BN, EPI><<<grid, GEMM_THREADS, Smem<BN, EPI>::BYTES, stream>>>(
       a, b, c ? *c : a, y ? *y : a, yt ? *yt : a, m_tiles, n_tiles, splits, K / BK / splits, ep);
   return cudaGetLastError();
 }
@@ -628,6 +680,7 @@ struct gf_mlp {
 
   // tensor maps
   CUtensorMap fwd_a[GF_MLP_LAYERS], fwd_b[GF_MLP_LAYERS];     // A = input activations, B = W
+  CUtensorMap fwd_b256[4];                                    // B = W in 256-row boxes (inference tiles)
   CUtensorMap bwd_a[GF_MLP_LAYERS], bwd_b[GF_MLP_LAYERS];     // A = dZ_l (dOut), B = W_l^T  (l >= 2)
   CUtensorMap dw_a[GF_MLP_LAYERS], dw_b[GF_MLP_LAYERS];       // A = dZ_l^T, B = Y_{l-1}^T
   CUtensorMap out_z[4], out_y[4], out_yt[4];                  // forward outputs of the hidden layers
@@ -721,8 +774,11 @@ gf_status check_batch(gf_mlp* m, int batch) {
   return GF_OK;
 }
 
-gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch, bool train) {
-  encode_inputs_kernel<<<(batch + 255) / 256, 256, 0, m->stream>>>(d_inputs, batch, m->x0, m->x0t, m->cap);
+// Forward pass.  Training writes Z, Y, Y^T and the padded fp32 output; inference (d_out != nullptr)
+// writes Y only, on 128 x 256 tiles, and the last layer writes the caller's [batch][99] array.
+gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch, bool train, float* d_out = nullptr) {
+  encode_inputs_kernel<<<(batch + 255) / 256, 256, 0, m->stream>>>(d_inputs, batch, m->x0, m->x0t, m->cap,
+                                                                  train ? 1 : 0);
   MLP_CUDA(m, cudaGetLastError());
   for (int l = 0; l < GF_MLP_LAYERS; ++l) {
     EpiArgs ep{};
@@ -732,11 +788,16 @@ gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch, bool train) {
     if (l < 4) {
       err = train ? launch_gemm<128, EPI_FWD_GELU>(m->fwd_a[l], m->fwd_b[l], &m->out_z[l], &m->out_y[l],
                                                    &m->out_yt[l], batch, HID, m->cols[l], 1, ep, m->stream)
-                  : launch_gemm<128, EPI_FWD_GELU_INFER>(m->fwd_a[l], m->fwd_b[l], nullptr, &m->out_y[l], nullptr,
-                                                         batch, HID, m->cols[l], 1, ep, m->stream);
-    } else {
+                  : launch_gemm<256, EPI_FWD_GELU_INFER>(m->fwd_a[l], m->fwd_b256[l], nullptr, &m->out_y[l],
+                                                         nullptr, batch, HID, m->cols[l], 1, ep, m->stream);
+    } else if (train) {
       err = launch_gemm<128, EPI_FWD_LINEAR>(m->fwd_a[l], m->fwd_b[l], &m->out_final, nullptr, nullptr, batch,
                                              OUT_PAD, HID, 1, ep, m->stream);
+    } else {
+      ep.out = d_out;
+      ep.out_cols = GF_MLP_OUTPUTS;
+      err = launch_gemm<128, EPI_FWD_OUT>(m->fwd_a[l], m->fwd_b[l], nullptr, nullptr, nullptr, batch, OUT_PAD, HID,
+                                          1, ep, m->stream);
     }
     if (err != cudaSuccess) return mlp_fail(m, GF_ERR_CUDA, "forward GEMM %d: %s", l + 1, cudaGetErrorString(err));
   }
@@ -875,6 +936,7 @@ gf_status gf_mlp_create(int32_t device, void* stream, const gf_mlp_config* confi
       const void* g_t = l == 4 ? static_cast<const void*>(m->doutt) : m->dzt[l];
       ok = ok && make_map(&m->fwd_a[l], in, cap, m->cols[l], BM);
       ok = ok && make_map(&m->fwd_b[l], m->wb[l], m->rows[l], m->cols[l], 128);
+      if (l < 4) ok = ok && make_map(&m->fwd_b256[l], m->wb[l], m->rows[l], m->cols[l], 256);
       if (l > 0) {   // layer 1's input gradient is never formed
         ok = ok && make_map(&m->bwd_a[l], g, cap, m->rows[l], BM);
         ok = ok && make_map(&m->bwd_b[l], m->wt[l], m->cols[l], m->rows[l], 128);
@@ -974,11 +1036,7 @@ gf_status gf_mlp_forward(gf_mlp* m, const float* d_inputs, int32_t batch, float*
   gf_status st = check_batch(m, batch);
   if (st != GF_OK) return st;
   MLP_CUDA(m, cudaSetDevice(m->device));
-  if ((st = run_forward(m, d_inputs, batch, false)) != GF_OK) return st;
-  const long long n = static_cast<long long>(batch) * GF_MLP_OUTPUTS;
-  copy_output_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, m->stream>>>(m->out, batch, d_outputs);
-  MLP_CUDA(m, cudaGetLastError());
-  return GF_OK;
+  return run_forward(m, d_inputs, batch, false, d_outputs);
 }
 
 gf_status gf_mlp_gradients(gf_mlp* m, const float* d_inputs, const float* d_targets, int32_t batch, float* grads,
