@@ -54,7 +54,8 @@ gf_status gf_mlp_set_params(gf_mlp* mlp, const float* params, int64_t count);
 gf_status gf_mlp_get_params(gf_mlp* mlp, float* params, int64_t count);
 gf_status gf_mlp_set_learning_rate(gf_mlp* mlp, float lr);
 
-/* Inference: d_inputs [batch][6] fp32 -> d_outputs [batch][99] fp32 (device pointers). */
+/* Inference: d_inputs [batch][6] fp32 -> d_outputs [batch][99] fp32 (device pointers; d_outputs
+ * 16-byte aligned). */
 gf_status gf_mlp_forward(gf_mlp* mlp, const float* d_inputs, int32_t batch, float* d_outputs);
 
 /* Mean-squared-error gradients of the loss (1 / (batch * 99)) sum (out - target)^2 with respect to

@@ -83,6 +83,12 @@ __device__ __forceinline__ void tma_store_2d(const void* tmap, int x, int y, con
                "r"(x), "r"(y), "r"(smem_u32(smem_src))
                : "memory");
 }
+// untiled bulk store shared -> global: both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_store_1d(void* gdst, const void* smem_src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(reinterpret_cast<uint64_t>(gdst)),
+               "r"(smem_u32(smem_src)), "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // at most N committed store groups may still be reading shared memory
 template <int N>

@@ -86,12 +86,15 @@ struct Smem {
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
   static constexpr int BIAS_FLOATS = 512;   // the bias vector of the whole output width
-  static constexpr int EXTRA = EPI_WARPS * Stage<EPI>::WARP + 256 + 2 * 4 * 32 * 4 + 4 * BIAS_FLOATS + 1024;
+  // EPI_FWD_OUT stages a whole 128-row tile of the caller's [rows][99] output (one contiguous span)
+  static constexpr int OUT_TILE = EPI == EPI_FWD_OUT ? (BM * GF_MLP_OUTPUTS * 4 + 1023) / 1024 * 1024 : 0;
+  static constexpr int EXTRA = EPI_WARPS * Stage<EPI>::WARP + OUT_TILE + 256 + 2 * 4 * 32 * 4 + 4 * BIAS_FLOATS + 1024;
   static constexpr int STAGES = (4 * STAGE_BYTES + EXTRA <= SMEM_LIMIT)   ? 4
                                 : (3 * STAGE_BYTES + EXTRA <= SMEM_LIMIT) ? 3
                                                                           : 2;
   static constexpr int STG_OFFSET = STAGES * STAGE_BYTES;
-  static constexpr int BAR_OFFSET = STG_OFFSET + EPI_WARPS * Stage<EPI>::WARP;
+  static constexpr int BAR_OFFSET = STG_OFFSET + EPI_WARPS * Stage<EPI>::WARP + OUT_TILE;
+  static constexpr int OUT_OFFSET = BAR_OFFSET - OUT_TILE;
   static constexpr int BIAS_OFFSET = BAR_OFFSET + 256 + 2 * 4 * 32 * 4;
   static constexpr int BYTES = BIAS_OFFSET + 4 * BIAS_FLOATS + 1024;   // + barriers, reductions, bias, alignment
   static_assert(BYTES <= SMEM_LIMIT, "shared memory");
@@ -289,6 +292,12 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
       tc_fence_after();
       const int row0 = mt * BM + qd * 32;        // first output row of this warp
       const int row = row0 + lane;
+      float* s_out = reinterpret_cast<float*>(smem + L::OUT_OFFSET);
+      if constexpr (EPI == EPI_FWD_OUT) {
+        // the previous tile's bulk store has read the staging tile
+        if (ew == 0 && lane == 0) bulk_wait_read<0>();
+        named_barrier_sync(3, 32 * EPI_WARPS);
+      }
       const uint32_t tbase = tmem + (static_cast<uint32_t>(qd * 32) << 16) + static_cast<uint32_t>(acc * BN);
 #pragma unroll 1
       for (int c0 = 32 * half; c0 < BN; c0 += 64, ++chunk) {
@@ -305,10 +314,11 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
           for (int j = 0; j < 32; ++j) v[j] += s_bias[n + j];
           stage_f32_row(buf + SG::F32_OFF, lane, v);
         } else if constexpr (EPI == EPI_FWD_OUT) {
-          float* o = ep.out + static_cast<long long>(row) * ep.out_cols;
+          // row stride 99 words: lanes (rows) hit distinct banks
+          float* o = s_out + (qd * 32 + lane) * GF_MLP_OUTPUTS;
 #pragma unroll
           for (int j = 0; j < 32; ++j)
-            if (n + j < ep.out_cols) o[n + j] = v[j] + s_bias[n + j];
+            if (n + j < GF_MLP_OUTPUTS) o[n + j] = v[j] + s_bias[n + j];
         } else if constexpr (EPI == EPI_FWD_GELU || EPI == EPI_FWD_GELU_INFER) {
 #pragma unroll
           for (int j = 0; j < 32; ++j) v[j] += s_bias[n + j];
@@ -359,6 +369,15 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
           }
           if constexpr (SG::BF16) tma_store_2d(&tma_y, n, row0, buf + SG::BF16_OFF);
           if constexpr (SG::T) tma_store_2d(&tma_yt, row0, n, buf + SG::T_OFF);
+          bulk_commit();
+        }
+      }
+      if constexpr (EPI == EPI_FWD_OUT) {
+        // rows [mt*128, mt*128 + 128) of a [rows][99] array are one contiguous span
+        fence_proxy_async_smem();
+        named_barrier_sync(3, 32 * EPI_WARPS);
+        if (ew == 0 && lane == 0) {
+          bulk_store_1d(ep.out + static_cast<long long>(mt) * BM * GF_MLP_OUTPUTS, s_out, BM * GF_MLP_OUTPUTS * 4);
           bulk_commit();
         }
       }
@@ -1036,6 +1055,8 @@ gf_status gf_mlp_forward(gf_mlp* m, const float* d_inputs, int32_t batch, float*
   gf_status st = check_batch(m, batch);
   if (st != GF_OK) return st;
   MLP_CUDA(m, cudaSetDevice(m->device));
+  if (reinterpret_cast<uintptr_t>(d_outputs) & 15)
+    return mlp_fail(m, GF_ERR_INVALID_ARGUMENT, "d_outputs must be 16-byte aligned");
   return run_forward(m, d_inputs, batch, false, d_outputs);
 }
 
