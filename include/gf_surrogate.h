@@ -69,8 +69,15 @@ gf_status gf_mlp_gradients(gf_mlp* mlp, const float* d_inputs, const float* d_ta
 gf_status gf_mlp_train_step(gf_mlp* mlp, const float* d_inputs, const float* d_targets, int32_t batch,
                             float* d_loss);
 
-/* Kernel-fault word of the network's kernels (bounded waits that ran out); synchronous. */
+/* Kernel-fault word of the network's kernels (bounded waits that ran out); synchronous.  Returns
+ * GF_ERR_DEVICE once per fault and clears the word; the network stays usable. */
 gf_status gf_mlp_check(gf_mlp* mlp);
+
+/* Failure-path testing: kind 1 arms the next inference pass so that its first GEMM withholds the
+ * hand-off of one accumulator; the epilogue's bounded wait (about 2 ms under injection) runs out, the
+ * kernel stops, drains what it issued, releases tensor memory and sets the fault word.  Outputs of
+ * that pass are undefined.  kind 0 disarms. */
+gf_status gf_mlp_inject_fault(gf_mlp* mlp, int32_t kind);
 
 /* Plain tensor-core GEMM C[M][N] = A[M][K] * B[N][K]^T (bf16 operands, both K-contiguous, fp32 out),
  * the kernel the network is built on.  M a multiple of 128, N of 64, K of 64; 16-byte aligned device

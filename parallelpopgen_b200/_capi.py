@@ -136,6 +136,7 @@ SIGNATURES = {
     "gf_mlp_gradients": (_I, [_P, _P, _P, _I, _P, _P]),
     "gf_mlp_train_step": (_I, [_P, _P, _P, _I, _P]),
     "gf_mlp_check": (_I, [_P]),
+    "gf_mlp_inject_fault": (_I, [_P, _I]),
     "gf_bf16_gemm": (_I, [_P, _P, _I, _I, _I, _P, _P]),
 }
 

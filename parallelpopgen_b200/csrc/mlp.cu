@@ -33,6 +33,7 @@ namespace gfm {
 constexpr int BM = 128;       // tile rows = tensor-memory lanes
 constexpr int BK = 64;        // K per pipeline stage: one 128-byte swizzle row of bf16
 constexpr long long WAIT_LIMIT = 1ll << 31;   // SM cycles (about a second) before a wait gives up
+constexpr long long INJECT_WAIT_LIMIT = 1ll << 22;   // the same under fault injection (about 2 ms)
 constexpr int HID = GF_MLP_HIDDEN;
 constexpr int IN_PAD = 64;
 constexpr int OUT_PAD = 128;
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constant__ CUtensorMap tma_b,
                  const __grid_constant__ CUtensorMap tma_c, const __grid_constant__ CUtensorMap tma_y,
                  const __grid_constant__ CUtensorMap tma_yt, int m_tiles, int n_tiles, int splits, int k_blocks,
-                 EpiArgs ep) {
+                 EpiArgs ep, long long wait_limit, int inject) {
   using L = Smem<BN, EPI>;
   using SG = Stage<EPI>;
   constexpr int STAGES = L::STAGES;
@@ -172,6 +173,8 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
   uint64_t* drain = tempty + 2;           // MMA completion before tensor memory is released (abort path)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   int* timed_out = reinterpret_cast<int*>(tmem_slot + 1);
+  int* epi_fail = timed_out + 1;         // the epilogue warps' joint verdict (sticky)
+  int* consumed_s = timed_out + 2;       // K-blocks the MMA thread received (for the drain)
   float* red = reinterpret_cast<float*>(smem + L::BAR_OFFSET + 256);   // [2 halves][4 quarters][32]
   float* s_bias = reinterpret_cast<float*>(smem + L::BIAS_OFFSET);
   volatile int* abort_flag = timed_out;
@@ -180,15 +183,17 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles = m_tiles * n_tiles * splits;
-  // Bounded wait: once any wait of this CTA has run out, every later wait returns at once, so a
-  // broken pipeline ends the CTA after one time limit rather than one per stage.
+  // Bounded waits.  The producer and MMA threads stop issuing work as soon as any wait of the CTA has
+  // run out (`wait`); the epilogue warps wait on the barrier alone and then agree on the outcome, so
+  // all of them leave the tile loop together.  An aborted CTA never touches unsynchronised data: it
+  // drains what it issued and releases tensor memory.
   auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
     if (*abort_flag) return false;
     const uint32_t addr = smem_u32(bar);
     const long long t0 = clock64();
     while (!mbar_try_wait(addr, parity)) {
       if (*abort_flag) return false;
-      if (clock64() - t0 > WAIT_LIMIT) {
+      if (clock64() - t0 > wait_limit) {
         *abort_flag = 1;
         return false;
       }
@@ -209,6 +214,8 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
     }
     mbar_init(drain, 1);
     *timed_out = 0;
+    *epi_fail = 0;
+    *consumed_s = 0;
     mbar_fence_init();
   }
   if constexpr (HAS_BIAS) {
@@ -234,7 +241,10 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
         for (int kb = 0; kb < k_blocks; ++kb, ++it) {
           const int s = it % STAGES;
           const uint32_t ph = (it / STAGES) & 1;
-          if (!wait(&empty[s], ph ^ 1)) late = true;
+          if (!wait(&empty[s], ph ^ 1)) {
+            late = true;
+            goto producer_done;
+          }
           uint8_t* a = smem + s * L::STAGE_BYTES;
           mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
           const int kx = (sp * k_blocks + kb) * BK;
@@ -242,6 +252,7 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
           tma_load_2d(a + L::A_BYTES, &tma_b, kx, nt * BN, &full[s]);
         }
       }
+    producer_done:
       issued = it;
     }
     __syncwarp();
@@ -252,13 +263,21 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
       for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++local) {
         const int acc = local & 1;
         const uint32_t use = static_cast<uint32_t>(local >> 1);
-        if (!wait(&tempty[acc], (use & 1) ^ 1)) late = true;
+        if (!wait(&tempty[acc], (use & 1) ^ 1)) {
+          late = true;
+          break;
+        }
         tc_fence_after();
         const uint32_t d = tmem + static_cast<uint32_t>(acc * BN);
+        bool stop = false;
         for (int kb = 0; kb < k_blocks; ++kb, ++it) {
           const int s = it % STAGES;
           const uint32_t ph = (it / STAGES) & 1;
-          if (!wait(&full[s], ph)) late = true;
+          if (!wait(&full[s], ph)) {
+            late = true;
+            stop = true;
+            break;
+          }
           tc_fence_after();
           const uint32_t a_addr = smem_u32(smem + s * L::STAGE_BYTES);
           const uint32_t b_addr = a_addr + L::A_BYTES;
@@ -268,8 +287,11 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
                       (kb | kk) != 0);
           umma_commit(&empty[s]);
         }
-        umma_commit(&tfull[acc]);
+        if (stop) break;
+        // fault injection for tests: withhold the first accumulator hand-off
+        if (!((inject & 1) && local == 0)) umma_commit(&tfull[acc]);
       }
+      *consumed_s = it;
     }
     __syncwarp();
   } else {
@@ -287,7 +309,12 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
       const int sp = rest / m_tiles;
       const int acc = local & 1;
       const uint32_t use = static_cast<uint32_t>(local >> 1);
-      if (!wait(&tfull[acc], use & 1)) late = true;
+      if (lane == 0 && !mbar_wait(&tfull[acc], use & 1, wait_limit)) atomicOr(epi_fail, 1);
+      named_barrier_sync(4, 32 * EPI_WARPS);     // every epilogue warp has its verdict in epi_fail
+      if (*reinterpret_cast<volatile int*>(epi_fail)) {
+        late = true;
+        break;
+      }
       __syncwarp();
       tc_fence_after();
       const int row0 = mt * BM + qd * 32;        // first output row of this warp
@@ -396,12 +423,12 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
     // a wait ran out: let every load and MMA this CTA issued finish before its shared and tensor
     // memory are released (each wait again bounded)
     if (threadIdx.x == 0) {
-      for (int it = issued - STAGES < 0 ? 0 : issued - STAGES; it < issued; ++it)
-        mbar_wait(&full[it % STAGES], (it / STAGES) & 1, WAIT_LIMIT);
+      // loads issued but never received by the MMA thread are still landing
+      for (int it = *consumed_s; it < issued; ++it) mbar_wait(&full[it % STAGES], (it / STAGES) & 1, wait_limit);
       if (ep.fault) atomicOr(ep.fault, 1);
     } else if (threadIdx.x == 32) {
-      umma_commit(drain);
-      mbar_wait(drain, 0, WAIT_LIMIT);
+      umma_commit(drain);   // arrives once every MMA this thread issued has completed
+      mbar_wait(drain, 0, wait_limit);
     }
     __syncthreads();
   }
@@ -626,7 +653,7 @@ int sm_count() {
 template <int BN, int EPI>
 cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap* c, const CUtensorMap* y,
                         const CUtensorMap* yt, int M, int N, int K, int splits, const EpiArgs& ep,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int inject = 0) {
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -640,7 +667,8 @@ cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtens
   const int tiles = m_tiles * n_tiles * splits;
   const int grid = tiles < sm_count() ? tiles : sm_count();
   umma_gemm_kernel<BN, EPI><<<grid, GEMM_THREADS, Smem<BN, EPI>::BYTES, stream>>>(
-      a, b, c ? *c : a, y ? *y : a, yt ? *yt : a, m_tiles, n_tiles, splits, K / BK / splits, ep);
+      a, b, c ? *c : a, y ? *y : a, yt ? *yt : a, m_tiles, n_tiles, splits, K / BK / splits, ep,
+      inject ? INJECT_WAIT_LIMIT : WAIT_LIMIT, inject);
   return cudaGetLastError();
 }
 
@@ -708,6 +736,7 @@ struct gf_mlp {
   CUtensorMap out_wpart[GF_MLP_LAYERS];                       // split-K weight-gradient slices
 
   std::vector<void*> allocations;
+  int inject = 0;   // fault injection armed for the next forward pass (tests)
 };
 
 namespace {
@@ -808,7 +837,9 @@ gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch, bool train, f
       err = train ? launch_gemm<128, EPI_FWD_GELU>(m->fwd_a[l], m->fwd_b[l], &m->out_z[l], &m->out_y[l],
                                                    &m->out_yt[l], batch, HID, m->cols[l], 1, ep, m->stream)
                   : launch_gemm<256, EPI_FWD_GELU_INFER>(m->fwd_a[l], m->fwd_b256[l], nullptr, &m->out_y[l],
-                                                         nullptr, batch, HID, m->cols[l], 1, ep, m->stream);
+                                                         nullptr, batch, HID, m->cols[l], 1, ep, m->stream,
+                                                         l == 0 ? m->inject : 0);
+      if (l == 0) m->inject = 0;
     } else if (train) {
       err = launch_gemm<128, EPI_FWD_LINEAR>(m->fwd_a[l], m->fwd_b[l], &m->out_final, nullptr, nullptr, batch,
                                              OUT_PAD, HID, 1, ep, m->stream);
@@ -1103,7 +1134,17 @@ gf_status gf_mlp_check(gf_mlp* m) {
   int f = 0;
   MLP_CUDA(m, cudaMemcpyAsync(&f, m->fault, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
   MLP_CUDA(m, cudaStreamSynchronize(m->stream));
-  if (f) return mlp_fail(m, GF_ERR_DEVICE, "a tensor-core GEMM wait ran out of time");
+  if (f) {
+    MLP_CUDA(m, cudaMemsetAsync(m->fault, 0, sizeof(int), m->stream));
+    MLP_CUDA(m, cudaStreamSynchronize(m->stream));
+    return mlp_fail(m, GF_ERR_DEVICE, "a tensor-core GEMM wait ran out of time");
+  }
+  return GF_OK;
+}
+
+gf_status gf_mlp_inject_fault(gf_mlp* m, int32_t kind) {
+  if (!m || kind < 0 || kind > 1) return GF_ERR_INVALID_ARGUMENT;
+  m->inject = kind;
   return GF_OK;
 }
 

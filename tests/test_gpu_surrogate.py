@@ -127,3 +127,22 @@ def test_surrogate_on_simulator_spectra():
         assert list(routed) == [False, False, True]
         assert np.allclose(p.sum(axis=1), 1.0)
         mlp.check()
+
+
+def test_bounded_wait_reports_and_recovers():
+    """Failure path without a GPU fault: an injected missing accumulator hand-off makes the GEMM's
+    bounded wait run out; the kernel ends, the fault word reports it once, and the next pass is exact."""
+    from parallelpopgen_b200 import _capi
+    mlp, vec, x, _ = _net(6, 512)
+    xs = torch.from_numpy(x).cuda()
+    want = mlp.forward(xs).cpu().numpy()
+    mlp.check()
+    lib = _capi.load()
+    assert lib.gf_mlp_inject_fault(mlp.h, 1) == 0
+    mlp.forward(xs)
+    assert lib.gf_mlp_check(mlp.h) == 6            # GF_ERR_DEVICE
+    assert b"ran out" in lib.gf_mlp_last_error(mlp.h)
+    assert lib.gf_mlp_check(mlp.h) == 0            # reported once, cleared
+    again = mlp.forward(xs).cpu().numpy()
+    mlp.check()
+    assert np.array_equal(again.view(np.uint32), want.view(np.uint32))
