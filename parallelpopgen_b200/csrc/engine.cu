@@ -509,6 +509,15 @@ __global__ void mse_fill_kernel(float* __restrict__ freq, int* __restrict__ id_g
 // ------------------------------------------------------------------------------------------------
 static long long align_up(long long v, long long a) { return (v + a - 1) / a * a; }
 
+// Packed IDs (generation | population << 24, threadID) -> the reference's int4 layout.
+__global__ void expand_ids_kernel(const int* __restrict__ gp, const int* __restrict__ tid, int M,
+                                  int4* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+    const int w = gp[i];
+    out[i] = make_int4(w & 0xFFFFFF, w >> 24, tid[i], 0);
+  }
+}
+
 static void release_sim(Engine* e) {
   // stream-ordered frees: the memory returns to the engine's pool for the next simulation
   for (int b = 0; b < 2; ++b) {
@@ -1385,16 +1394,18 @@ gf_status gf_sim_read_state(gf_engine* g, float* freq_out, int32_t* ids_out, int
                                  sizeof(float) * M, e->P, cudaMemcpyDeviceToHost, e->stream));
   }
   if (ids_out) {
-    std::vector<int> gp(M), tid(M);
-    GF_CUDA(e, cudaMemcpyAsync(gp.data(), e->id_gp[e->id_cur], sizeof(int) * M, cudaMemcpyDeviceToHost, e->stream));
-    GF_CUDA(e, cudaMemcpyAsync(tid.data(), e->id_tid[e->id_cur], sizeof(int) * M, cudaMemcpyDeviceToHost, e->stream));
-    GF_CUDA(e, cudaStreamSynchronize(e->stream));
-    for (int i = 0; i < M; ++i) {
-      ids_out[4 * i + 0] = gp[i] & 0xFFFFFF;
-      ids_out[4 * i + 1] = gp[i] >> 24;
-      ids_out[4 * i + 2] = tid[i];
-      ids_out[4 * i + 3] = 0;
-    }
+    // the reference's int4 IDs (generation, population, threadID, 0) are assembled on the device from
+    // the packed words and copied out in one transfer
+    int4* d_ids = nullptr;
+    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_ids), sizeof(int4) * static_cast<size_t>(M));
+    if (ast != GF_OK) return ast;
+    expand_ids_kernel<<<std::min(148 * 8, (M + 255) / 256), 256, 0, e->stream>>>(e->id_gp[e->id_cur],
+                                                                               e->id_tid[e->id_cur], M, d_ids);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(ids_out, d_ids, sizeof(int4) * static_cast<size_t>(M), cudaMemcpyDeviceToHost, e->stream);
+    cudaFreeAsync(d_ids, e->stream);
+    if (err != cudaSuccess) return cuda_fail(e, err, "reading mutation IDs");
   }
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
   return GF_OK;

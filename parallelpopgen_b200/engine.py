@@ -104,6 +104,17 @@ class Engine:
         M = got.value
         return freq[:, :M], (ids[:M] if with_ids else None)
 
+    def read_state_into(self, freq_out: np.ndarray, ids_out: np.ndarray | None = None) -> int:
+        """Copy the current state into caller-owned arrays and return M: `freq_out` (fp32, at least
+        P * capacity values) receives the rows packed as [P][M], `ids_out` ([>= M][4] int32) the
+        reference's mutation IDs.  Page-locked arrays make both copies direct DMA transfers."""
+        got = ctypes.c_int32()
+        cap = freq_out.size // max(self.P, 1)
+        if ids_out is not None and ids_out.shape[0] < cap:
+            cap = ids_out.shape[0]
+        self._check(self.lib.gf_sim_read_state(self.h, ptr(freq_out), ptr(ids_out), int(cap), ctypes.byref(got)))
+        return got.value
+
     def device_state(self):
         p = ctypes.c_void_p()
         stride = ctypes.c_int32()
