@@ -158,6 +158,47 @@ inline void site_frequency_spectrum(SFS& mySFS, const GO_Fish::allele_trajectori
   mySFS.sampled_generation = generation;
 }
 
+/* Joint SFS of populations a and b at one time sample (an extension; the reference computes
+ * single-population marginals only): frequency_spectrum[i * (n_b + 1) + j] = expected number of sites
+ * with i derived copies in a sample of n_a from population a and j in a sample of n_b from b, plus the
+ * monomorphic sites at (0, 0).  Requires 1 <= n_a < Nchrom_e(a), 1 <= n_b < Nchrom_e(b), n <= 1023. */
+inline void joint_site_frequency_spectrum(SFS& mySFS, const GO_Fish::allele_trajectories& all_results,
+                                          const int sample_index, const int population_a, const int population_b,
+                                          const int sample_size_a, const int sample_size_b, int cuda_device = -1) {
+  GO_Fish::allele_trajectories& a = const_cast<GO_Fish::allele_trajectories&>(all_results);
+  const float *fa, *fb;
+  int M, Nca, Ncb, generation;
+  float L;
+  gofish_detail::spectrum_access::row(a, sample_index, population_a, &fa, &M, &Nca, &generation, &L);
+  gofish_detail::spectrum_access::row(a, sample_index, population_b, &fb, &M, &Ncb, &generation, &L);
+  if (sample_size_a <= 0 || sample_size_a >= Nca || sample_size_b <= 0 || sample_size_b >= Ncb) {
+    std::fprintf(stderr,
+                 "joint_site_frequency_spectrum error: requested sample sizes out of range: %d [1,%d), %d [1,%d)\n",
+                 sample_size_a, Nca, sample_size_b, Ncb);
+    std::exit(1);
+  }
+  gf_engine* e = gofish_detail::spectrum_engine(cuda_device);
+  const size_t bins = static_cast<size_t>(sample_size_a + 1) * (sample_size_b + 1);
+  float* h = new float[bins];
+  const gf_status st = gf_joint_site_frequency_spectrum(e, fa, fb, M, sample_size_a, sample_size_b, L, h);
+  if (st != GF_OK) {
+    std::fprintf(stderr, "joint_site_frequency_spectrum error: %s\n", gf_engine_last_error(e));
+    std::exit(1);
+  }
+  mySFS.clear();
+  mySFS.frequency_spectrum = h;
+  mySFS.num_populations = 2;
+  mySFS.sample_size = new int[2];
+  mySFS.sample_size[0] = sample_size_a;
+  mySFS.sample_size[1] = sample_size_b;
+  mySFS.num_sites = L;
+  mySFS.num_mutations = mySFS.num_sites - mySFS.frequency_spectrum[0];
+  mySFS.populations = new int[2];
+  mySFS.populations[0] = population_a;
+  mySFS.populations[1] = population_b;
+  mySFS.sampled_generation = generation;
+}
+
 }  // namespace Spectrum
 
 #endif  // GOFISH_B200_SPECTRUM_H_

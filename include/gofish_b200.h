@@ -266,6 +266,21 @@ typedef struct gf_sim_stats {
 /* Counters of the current simulation.  Synchronizes the stream. */
 gf_status gf_sim_stats_read(gf_engine* engine, gf_sim_stats* out);
 
+/* Joint SFS of two populations (an extension: the reference computes single-population marginals,
+ * Spectrum::site_frequency_spectrum, spectrum.cu:213-294).  out[i * (n_b + 1) + j] = expected number of
+ * sites whose sample of n_a chromosomes from population a holds i derived copies and whose sample of
+ * n_b from population b holds j: every one of the M mutations contributes the product of its two
+ * binomial projections (spectrum.cu:90-139), and the num_sites - M monomorphic sites go to (0, 0).
+ * For 1 <= i <= n_a - 1 the row sums equal population a's single-population SFS.  1 <= n_a, n_b <= 1023.
+ * freq_a / freq_b are the two populations' rows of the same M mutations.  Computed in double,
+ * deterministic.  The _device variant takes device pointers and runs asynchronously. */
+gf_status gf_joint_site_frequency_spectrum(gf_engine* engine, const float* freq_a, const float* freq_b,
+                                           int32_t num_mutations, int32_t n_a, int32_t n_b, float num_sites,
+                                           float* out);
+gf_status gf_joint_site_frequency_spectrum_device(gf_engine* engine, const float* d_freq_a, const float* d_freq_b,
+                                                  int32_t num_mutations, int32_t n_a, int32_t n_b,
+                                                  float num_sites, float* d_out);
+
 /* Launch choices of the drift pass (results do not depend on them). */
 typedef struct gf_tuning {
   int32_t draw_strategy; /* 0: each thread draws its own four lanes; 1: warp-cooperative draws, grouped by

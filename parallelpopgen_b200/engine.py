@@ -196,6 +196,24 @@ class Engine:
                                                         ptr(out)))
         return out
 
+    def joint_site_frequency_spectrum(self, freq_a: np.ndarray, freq_b: np.ndarray, n_a: int, n_b: int,
+                                      num_sites: float) -> np.ndarray:
+        """Expected joint SFS [n_a + 1][n_b + 1] of two populations' rows of the same mutations."""
+        fa = np.ascontiguousarray(freq_a, dtype=np.float32)
+        fb = np.ascontiguousarray(freq_b, dtype=np.float32)
+        if fa.shape != fb.shape:
+            raise ValueError("the two rows must hold the same mutations")
+        out = np.empty((n_a + 1, n_b + 1), dtype=np.float32)
+        self._check(self.lib.gf_joint_site_frequency_spectrum(self.h, ptr(fa), ptr(fb), len(fa), int(n_a), int(n_b),
+                                                              float(num_sites), ptr(out)))
+        return out
+
+    def joint_site_frequency_spectrum_device(self, d_freq_a: int, d_freq_b: int, M: int, n_a: int, n_b: int,
+                                             num_sites: float, d_out: int) -> None:
+        self._check(self.lib.gf_joint_site_frequency_spectrum_device(
+            self.h, ctypes.c_void_p(d_freq_a), ctypes.c_void_p(d_freq_b), int(M), int(n_a), int(n_b),
+            float(num_sites), ctypes.c_void_p(d_out)))
+
     def site_frequency_spectrum_device(self, d_freq: int, M: int, Nc: int, n: int, num_sites: float,
                                        d_out: int) -> None:
         self._check(self.lib.gf_site_frequency_spectrum_device(self.h, ctypes.c_void_p(d_freq), M, Nc, n,

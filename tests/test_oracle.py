@@ -158,3 +158,24 @@ def test_single_population_run_is_neutral_equilibrium_like():
     expected = 2 * mu * L * Nc * np.sum(1.0 / i)
     assert abs(len(f) - expected) < 5 * math.sqrt(expected) + 0.05 * expected
     assert mg > 200 * 0.8 * expected
+
+
+def test_joint_oracle_matches_brute_force():
+    """The joint-SFS restatement against an explicit loop over mutations and sample counts."""
+    import math
+    from oracle.joint_oracle import joint_sfs
+    rng = np.random.default_rng(8)
+    Nc = 50
+    fa = (rng.integers(0, Nc + 1, 40) / Nc).astype(np.float32)
+    fb = (rng.integers(0, Nc + 1, 40) / Nc).astype(np.float32)
+    na, nb, L = 5, 4, 1000.0
+    want = np.zeros((na + 1, nb + 1))
+    want[0, 0] = L - 40
+    for pa, pb in zip(fa.astype(np.float64), fb.astype(np.float64)):
+        for i in range(na + 1):
+            for j in range(nb + 1):
+                want[i, j] += (math.comb(na, i) * pa ** i * (1 - pa) ** (na - i) *
+                               math.comb(nb, j) * pb ** j * (1 - pb) ** (nb - j))
+    got = joint_sfs(fa, fb, na, nb, L)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+    assert abs(got.sum() - L) < 1e-9
