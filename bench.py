@@ -422,11 +422,18 @@ def run_batched(args):
             ev1.synchronize()
             times.append(ev0.elapsed_time(ev1) * 1e-3)
     batch_s = float(np.mean(times))
+    # one more batch with the window launches bracketed by CUDA events: device time of the drift work
+    eng.set_profiling(True)
+    eng.read_profile()
+    batch_step()
+    prof = eng.read_profile()
+    eng.set_profiling(False)
     # the same replicates, one plain engine run each (a random sample, timed engine calls only)
     rng = np.random.default_rng(7)
     sample = rng.choice(len(reps), size=min(args.plain_sample, len(reps)), replace=False)
     prepared = [(reps[i], replicate_mse_pops(reps[i]), replicate_plain_generations(reps[i])) for i in sample]
     d_sfs = torch.empty(n, dtype=torch.float32, device="cuda")
+    eng = Engine(device=0, stream=stream.cuda_stream)     # a fresh engine: no batch state alongside
     plain_s = 0.0
     for rep, pops, gens in prepared:
         Nc = int(np.float32(2 * replicate_population(rep, rep.num_generations)) /
@@ -455,6 +462,7 @@ def run_batched(args):
         "mutation_generations_per_step": st["mutation_generations"],
         "mutation_generations_per_s": st["mutation_generations"] / batch_s,
         "super_steps": st["super_steps"],
+        "window_ms_per_step": prof["drift_ms"], "window_launches_per_step": prof["drift_launches"],
         "looped_plain": {"value": plain_rate, "unit": "simulations/s", "sample": len(prepared),
                          "speedup_batched_over_looped": value / plain_rate},
         "clocks": clk.summary(),

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -22,6 +23,28 @@
 #include "gf_drift.cuh"
 #include "gf_internal.h"
 #include "gf_mse.cuh"
+
+#ifdef GF_TRACE
+#include <chrono>
+#include <cstdio>
+// phase timings of batch_begin on stderr (build with -DGF_TRACE): time since the previous point
+static double gf_trace_elapsed_ms() {
+  static auto last = std::chrono::steady_clock::now();
+  const auto now = std::chrono::steady_clock::now();
+  const double ms = std::chrono::duration<double, std::milli>(now - last).count();
+  last = now;
+  return ms;
+}
+#define GF_TRACE_POINT(e, label)                                                     \
+  do {                                                                               \
+    cudaStreamSynchronize((e)->stream);                                              \
+    std::fprintf(stderr, "[batch] %-28s %9.2f ms\n", label, gf_trace_elapsed_ms()); \
+  } while (0)
+#else
+#define GF_TRACE_POINT(e, label) \
+  do {                           \
+  } while (0)
+#endif
 
 namespace gf {
 
@@ -265,21 +288,32 @@ void release_batch(Engine* e) {
   Batch* b = e->batch;
   if (!b) return;
   cudaStreamSynchronize(e->stream);
+  auto release = [e](void* p) {
+    if (p) cudaFreeAsync(p, e->stream);
+  };
   for (int k = 0; k < 2; ++k) {
-    cudaFree(b->freq[k]);
-    cudaFree(b->id_gp[k]);
-    cudaFree(b->id_tid[k]);
-    cudaFree(b->d_M[k]);
+    release(b->freq[k]);
+    release(b->id_gp[k]);
+    release(b->id_tid[k]);
+    release(b->d_M[k]);
   }
-  cudaFree(b->flags);
-  cudaFree(b->tile_count);
-  cudaFree(b->tile_offset);
-  cudaFree(b->d_Mend);
-  cudaFreeHost(b->h_M);
-  cudaFree(b->d_recs);
-  cudaFreeHost(b->h_recs);
-  cudaFree(b->d_reps);
-  cudaFreeHost(b->h_reps);
+  release(b->flags);
+  release(b->tile_count);
+  release(b->tile_offset);
+  release(b->d_Mend);
+  release(b->d_all_recs);
+  release(b->d_total_tiles);
+  cudaStreamSynchronize(e->stream);
+  if (b->h_M) cudaFreeHost(b->h_M);
+  if (b->d_recs) cudaFree(b->d_recs);
+  if (b->h_recs) cudaFreeHost(b->h_recs);
+  if (b->d_reps) cudaFree(b->d_reps);
+  if (b->h_reps) cudaFreeHost(b->h_reps);
+  for (int k = 0; k < Batch::kRing; ++k) {
+    if (b->d_ring[k]) cudaFree(b->d_ring[k]);
+    if (b->h_ring[k]) cudaFreeHost(b->h_ring[k]);
+    if (b->ring_done[k]) cudaEventDestroy(b->ring_done[k]);
+  }
   delete b;
   e->batch = nullptr;
 }
@@ -314,6 +348,71 @@ static gf_status grow_pinned(Engine* e, T** d, T** h, size_t* cap, size_t need) 
   return GF_OK;
 }
 
+// Generation record of replicate `p` at generation g (what the reference's run_sim evaluates per
+// generation: population size, Nchrom_e, the host-drawn new-mutation count, calc_new_mutations_Index
+// go_fish_impl.cuh:454-467, and the model scalars).
+static void make_record(const gf_replicate& p, int g, WinGen& w) {
+  const int N = rep_population(p, g);
+  const int Nc = static_cast<int>(2 * N / (1 + p.F));
+  w.generation = g;
+  w.Nc = Nc;
+  w.new_count = (N > 0 && Nc > 0) ? host_new_mutation_count(p.seed1, p.seed2, p.mu, Nc, p.num_sites, g, 0) : 0;
+  w.new_freq = Nc > 0 ? 1.f / Nc : 0.f;
+  w.F = p.F;
+  w.h = p.h;
+  w.sel_a = p.sel_slope;
+  w.sel_b = p.sel_intercept;
+  w.alive = N > 0;
+}
+
+// Records depend only on each replicate's seeds and size trajectory, so when they fit (64 M records)
+// they are computed once, in parallel over replicates, into the engine's page-locked staging buffer
+// (kept across batches: no zero fill, no page faults after the first batch) and uploaded with one
+// asynchronous copy; super-steps then need neither host record work nor a read-back.
+constexpr long long kPrecomputeRecords = 64ll << 20;
+
+static gf_status precompute_records(Engine* e, Batch* b) {
+  long long total = 0;
+  for (auto& br : b->reps) total += br.p.num_generations;
+  b->precomputed = false;
+  if (total > kPrecomputeRecords || total == 0) return GF_OK;
+  long long off = 0;
+  for (auto& br : b->reps) {
+    br.rec0 = off;
+    off += br.p.num_generations;
+  }
+  if (e->h_rec_stage_cap < static_cast<size_t>(total)) {
+    if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
+    e->h_rec_stage = nullptr;
+    e->h_rec_stage_cap = 0;
+    const size_t cap = static_cast<size_t>(total) + static_cast<size_t>(total) / 4;
+    GF_CUDA(e, cudaMallocHost(&e->h_rec_stage, sizeof(WinGen) * cap));
+    e->h_rec_stage_cap = cap;
+  }
+  GF_TRACE_POINT(e, "record buffers");
+  WinGen* recs = e->h_rec_stage;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = total > 50000 ? std::min<unsigned>(hw, 32) : 1;
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    for (int r; (r = next.fetch_add(1)) < b->R;) {
+      const BatchRep& br = b->reps[r];
+      for (int g = 1; g <= br.p.num_generations; ++g) make_record(br.p, g, recs[br.rec0 + g - 1]);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  GF_TRACE_POINT(e, "record draws");
+  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * total);
+  if (st != GF_OK) return st;
+  // the staging buffer is rewritten only by the next batch_begin, which first synchronizes the stream
+  GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs, recs, sizeof(WinGen) * total, cudaMemcpyHostToDevice, e->stream));
+  b->precomputed = true;
+  return GF_OK;
+}
+
 static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
   if (!in || R <= 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "no replicates");
   for (int r = 0; r < R; ++r) {
@@ -326,7 +425,9 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
   }
   GF_CUDA(e, cudaSetDevice(e->device));
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  GF_TRACE_POINT(e, "begin");
   release_batch(e);
+  GF_TRACE_POINT(e, "release previous batch");
   Batch* b = new Batch();
   e->batch = b;
   b->R = R;
@@ -360,12 +461,17 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
   float *d_area = nullptr, *d_integral = nullptr;
   unsigned *d_counts = nullptr, *d_starts = nullptr;
   int* d_M0 = nullptr;
-  GF_CUDA(e, cudaMalloc(&d_mr, sizeof(MseRep) * R));
-  GF_CUDA(e, cudaMalloc(&d_area, sizeof(float) * area_total));
-  GF_CUDA(e, cudaMalloc(&d_integral, sizeof(float) * area_total));
-  GF_CUDA(e, cudaMalloc(&d_counts, sizeof(unsigned) * std::max<long long>(class_total, 1)));
-  GF_CUDA(e, cudaMalloc(&d_starts, sizeof(unsigned) * std::max<long long>(class_total, 1)));
-  GF_CUDA(e, cudaMalloc(&d_M0, sizeof(int) * R));
+  {
+    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_mr), sizeof(MseRep) * R);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_area), sizeof(float) * area_total);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_integral), sizeof(float) * area_total);
+    if (ast == GF_OK)
+      ast = pool_alloc(e, reinterpret_cast<void**>(&d_counts), sizeof(unsigned) * std::max<long long>(class_total, 1));
+    if (ast == GF_OK)
+      ast = pool_alloc(e, reinterpret_cast<void**>(&d_starts), sizeof(unsigned) * std::max<long long>(class_total, 1));
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_M0), sizeof(int) * R);
+    if (ast != GF_OK) return ast;
+  }
   GF_CUDA(e, cudaMemcpyAsync(d_mr, mr.data(), sizeof(MseRep) * R, cudaMemcpyHostToDevice, e->stream));
   const int grid = e->num_sms * 8;
   batch_mse_area_kernel<<<grid, 256, 0, e->stream>>>(d_area, d_mr, R, area_total);
@@ -377,6 +483,7 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
   std::vector<int> M0(R);
   GF_CUDA(e, cudaMemcpyAsync(M0.data(), d_M0, sizeof(int) * R, cudaMemcpyDeviceToHost, e->stream));
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  GF_TRACE_POINT(e, "MSE classes and counts");
   // ---- arena ----
   long long arena = 0;
   for (int r = 0; r < R; ++r) {
@@ -390,17 +497,30 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     arena += br.capacity;
   }
   b->arena = arena;
-  for (int k = 0; k < 2; ++k) {
-    GF_CUDA(e, cudaMalloc(&b->freq[k], sizeof(float) * arena));
-    GF_CUDA(e, cudaMalloc(&b->id_gp[k], sizeof(int) * arena));
-    GF_CUDA(e, cudaMalloc(&b->id_tid[k], sizeof(int) * arena));
-    GF_CUDA(e, cudaMalloc(&b->d_M[k], sizeof(int) * R));
+  {
+    gf_status ast = GF_OK;
+    auto pa = [&](void** p, size_t bytes) {
+      if (ast == GF_OK) ast = pool_alloc(e, p, bytes);
+    };
+    for (int k = 0; k < 2; ++k) {
+      pa(reinterpret_cast<void**>(&b->freq[k]), sizeof(float) * arena);
+      pa(reinterpret_cast<void**>(&b->id_gp[k]), sizeof(int) * arena);
+      pa(reinterpret_cast<void**>(&b->id_tid[k]), sizeof(int) * arena);
+      pa(reinterpret_cast<void**>(&b->d_M[k]), sizeof(int) * R);
+    }
+    pa(reinterpret_cast<void**>(&b->flags), sizeof(unsigned) * (arena / 32));
+    pa(reinterpret_cast<void**>(&b->tile_count), sizeof(unsigned) * (arena / kBatchTile));
+    pa(reinterpret_cast<void**>(&b->tile_offset), sizeof(unsigned) * (arena / kBatchTile));
+    pa(reinterpret_cast<void**>(&b->d_Mend), sizeof(int) * R);
+    pa(reinterpret_cast<void**>(&b->d_total_tiles), sizeof(int));
+    if (ast != GF_OK) return ast;
   }
-  GF_CUDA(e, cudaMalloc(&b->flags, sizeof(unsigned) * (arena / 32)));
-  GF_CUDA(e, cudaMalloc(&b->tile_count, sizeof(unsigned) * (arena / kBatchTile)));
-  GF_CUDA(e, cudaMalloc(&b->tile_offset, sizeof(unsigned) * (arena / kBatchTile)));
-  GF_CUDA(e, cudaMalloc(&b->d_Mend, sizeof(int) * R));
-  GF_CUDA(e, cudaMallocHost(&b->h_M, sizeof(int) * R));
+  GF_CUDA(e, cudaMallocHost(&b->h_M, sizeof(int) * 2 * R));
+  for (int k = 0; k < Batch::kRing; ++k) {
+    GF_CUDA(e, cudaMalloc(&b->d_ring[k], sizeof(WinRep) * R));
+    GF_CUDA(e, cudaMallocHost(&b->h_ring[k], sizeof(WinRep) * R));
+    GF_CUDA(e, cudaEventCreateWithFlags(&b->ring_done[k], cudaEventDisableTiming));
+  }
   GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
@@ -416,24 +536,26 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     fill_total += M0[r];
   }
   FillRep* d_fr = nullptr;
-  GF_CUDA(e, cudaMalloc(&d_fr, sizeof(FillRep) * R));
+  {
+    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_fr), sizeof(FillRep) * R);
+    if (ast != GF_OK) return ast;
+  }
   GF_CUDA(e, cudaMemcpyAsync(d_fr, fr.data(), sizeof(FillRep) * R, cudaMemcpyHostToDevice, e->stream));
   if (fill_total > 0)
     batch_mse_fill_kernel<<<grid, 256, 0, e->stream>>>(b->freq[0], b->id_gp[0], b->id_tid[0], d_starts, d_fr, R,
                                                         fill_total);
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  cudaFree(d_mr);
-  cudaFree(d_area);
-  cudaFree(d_integral);
-  cudaFree(d_counts);
-  cudaFree(d_starts);
-  cudaFree(d_M0);
-  cudaFree(d_fr);
+  for (void* q : {static_cast<void*>(d_mr), static_cast<void*>(d_area), static_cast<void*>(d_integral),
+                  static_cast<void*>(d_counts), static_cast<void*>(d_starts), static_cast<void*>(d_M0),
+                  static_cast<void*>(d_fr)})
+    cudaFreeAsync(q, e->stream);
   GF_CUDA(e, cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream));
   GF_CUDA(e, cudaMemsetAsync(e->d_count + 2, 0, sizeof(int), e->stream));
-  return GF_OK;
+  GF_TRACE_POINT(e, "arena and MSE fill");
+  const gf_status pst = precompute_records(e, b);
+  GF_TRACE_POINT(e, "records");
+  return pst;
 }
 
 // New-mutation draws of the window records, spread over host threads for large batches.
@@ -478,7 +600,123 @@ static void fill_records(std::vector<WinGen>& recs, const std::vector<std::pair<
   for (auto& x : th) x.join();
 }
 
+static gf_status batch_super_step_fallback(Engine* e, int* active_out);
+
+// Survivor counts of every replicate back to the host (one transfer of both count arrays), and the
+// device status word.
+static gf_status sync_counts(Engine* e) {
+  Batch* b = e->batch;
+  if (!b->counts_stale) return GF_OK;
+  GF_CUDA(e, cudaMemcpyAsync(b->h_M, b->d_M[0], sizeof(int) * b->R, cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(b->h_M + b->R, b->d_M[1], sizeof(int) * b->R, cudaMemcpyDeviceToHost, e->stream));
+  int fault = 0;
+  GF_CUDA(e, cudaMemcpyAsync(&fault, e->d_count + 2, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  GF_CUDA(e, cudaStreamSynchronize(e->stream));
+  for (int r = 0; r < b->R; ++r) b->reps[r].M = b->h_M[b->reps[r].m_slot * b->R + r];
+  b->counts_stale = false;
+  if (fault) return fail(e, GF_ERR_DEVICE, "device status word reports fault %d (replicate capacity exceeded)", fault);
+  return GF_OK;
+}
+
+// One window of every active replicate from the precomputed records: no host record work and no
+// read-back (a one-block kernel assigns each replicate's tiles from its device-side count; tiles past
+// a replicate's end-of-window count return at once).  The replicate table goes through a ring of
+// pinned/device slots, each reused only after the launch that read it has finished.
 static gf_status batch_super_step(Engine* e, int* active_out) {
+  Batch* b = e->batch;
+  if (!b->precomputed) return batch_super_step_fallback(e, active_out);
+  const int slot = b->ring;
+  GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
+  WinRep* hr = b->h_ring[slot];
+  int nj = 0, tiles = 0;
+  for (int r = 0; r < b->R; ++r) {
+    BatchRep& br = b->reps[r];
+    if (br.done) continue;
+    const int end = std::min(br.next_compact, br.p.num_generations);
+    const int ngen = end - br.generation;
+    WinRep& w = hr[nj++];
+    w.base = br.base;
+    w.capacity = br.capacity;
+    w.rec = static_cast<int>(br.rec0 + br.generation);
+    w.ngen = ngen;
+    w.tile0 = tiles;
+    w.ntiles = static_cast<int>(br.capacity / kBatchTile);
+    w.seed1 = br.p.seed1;
+    w.seed2 = br.p.seed2;
+    w.check_preserved = 0;
+    w.compact = 1;
+    w.preserve = 0;
+    w.rep = r;
+    w.births = 0;   // summed on the device from the records (batch_tiles_kernel)
+    tiles += w.ntiles;
+  }
+  if (nj == 0) {
+    if (active_out) *active_out = 0;
+    return GF_OK;
+  }
+  GF_CUDA(e, cudaMemcpyAsync(b->d_ring[slot], hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));
+  // each replicate's tiles from its device-side count: only its live slots are visited
+  assign_batch_tiles(e, b->d_ring[slot], nj, b->d_M[b->mslot], b->d_all_recs, b->d_total_tiles);
+  GF_CUDA(e, cudaGetLastError());
+  WindowLaunch w;
+  w.A = b->freq[0];
+  w.B = b->freq[1];
+  w.id_gp_cur = b->id_gp[b->id_cur];
+  w.id_tid_cur = b->id_tid[b->id_cur];
+  w.id_gp_next = b->id_gp[b->id_cur ^ 1];
+  w.id_tid_next = b->id_tid[b->id_cur ^ 1];
+  w.flags = b->flags;
+  w.tile_count = b->tile_count;
+  w.tile_offset = b->tile_offset;
+  w.M_in = b->d_M[b->mslot];
+  w.M_end = b->d_Mend;
+  w.M_next = nullptr;
+  w.M_out = b->d_M[b->mslot ^ 1];
+  w.reps = b->d_ring[slot];
+  w.nreps = nj;
+  w.recs = b->d_all_recs;
+  w.total_tiles = tiles;                 // segment tiles: an upper bound, sizes the grid
+  w.total_tiles_dev = b->d_total_tiles;
+  w.any_compact = true;
+  w.stats = e->d_stats;
+  w.fault = e->d_count + 2;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  gf_status st = window_run(e, w, b->freq[0]);
+  if (st != GF_OK) return st;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_drift.emplace_back(ev0, ev1);
+  }
+  GF_CUDA(e, cudaEventRecord(b->ring_done[slot], e->stream));
+  b->ring = (slot + 1) % Batch::kRing;
+  b->mslot ^= 1;
+  b->id_cur ^= 1;
+  b->super_steps += 1;
+  b->counts_stale = true;
+  int active = 0;
+  for (int j = 0; j < nj; ++j) {
+    BatchRep& br = b->reps[hr[j].rep];
+    br.generation += hr[j].ngen;
+    b->generations += hr[j].ngen;
+    br.next_compact = br.generation + br.p.compact_interval;
+    br.Nc = rep_nchrom(br.p, br.generation);
+    br.id_buf = b->id_cur;
+    br.m_slot = b->mslot;
+    if (br.generation >= br.p.num_generations) br.done = true;
+    else ++active;
+  }
+  if (active_out) *active_out = active;
+  return GF_OK;
+}
+
+// Super-step for batches whose records do not fit the precomputation budget: records built per
+// super-step and the counts read back every time.
+static gf_status batch_super_step_fallback(Engine* e, int* active_out) {
   Batch* b = e->batch;
   std::vector<std::pair<int, int>> jobs;
   std::vector<int> first;
@@ -526,6 +764,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     w.compact = 1;
     w.preserve = 0;
     w.rep = r;
+    w.births = news;
     tiles += w.ntiles;
   }
   GF_CUDA(e, cudaMemcpyAsync(b->d_recs, b->h_recs, sizeof(WinGen) * nrec, cudaMemcpyHostToDevice, e->stream));
@@ -581,6 +820,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     br.next_compact = br.generation + br.p.compact_interval;
     br.Nc = rep_nchrom(br.p, br.generation);
     br.id_buf = b->id_cur;
+    br.m_slot = b->mslot;
     if (br.generation >= br.p.num_generations) br.done = true;
     else ++active;
   }
@@ -618,6 +858,8 @@ gf_status gf_batch_run(gf_engine* g, int32_t max_super_steps, int32_t* out_activ
     gf_status st = batch_super_step(e, &active);
     if (st != GF_OK) return st;
   }
+  gf_status st = sync_counts(e);
+  if (st != GF_OK) return st;
   if (out_active) {
     int a = 0;
     for (auto& br : e->batch->reps) a += br.done ? 0 : 1;
@@ -634,6 +876,10 @@ gf_status gf_batch_read_state(gf_engine* g, int32_t r, float* freq_out, int32_t*
   if (!b) return fail(e, GF_ERR_STATE, "no batch");
   if (r < 0 || r >= b->R) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d outside [0, %d)", r, b->R);
   GF_CUDA(e, cudaSetDevice(e->device));
+  {
+    gf_status st = sync_counts(e);
+    if (st != GF_OK) return st;
+  }
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
   const BatchRep& br = b->reps[r];
   if (out_num) *out_num = br.M;
@@ -665,6 +911,10 @@ gf_status gf_batch_sfs(gf_engine* g, int32_t n, float* out) {
   for (int r = 0; r < b->R; ++r)
     if (n >= b->reps[r].Nc) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: sample size %d >= Nchrom_e %d", r, n, b->reps[r].Nc);
   GF_CUDA(e, cudaSetDevice(e->device));
+  {
+    gf_status st = sync_counts(e);
+    if (st != GF_OK) return st;
+  }
   std::vector<SfsRep> sr(b->R);
   for (int r = 0; r < b->R; ++r) sr[r] = {b->reps[r].base, b->reps[r].M, b->reps[r].p.num_sites};
   std::vector<double> lgc(n + 1);
@@ -673,19 +923,22 @@ gf_status gf_batch_sfs(gf_engine* g, int32_t n, float* out) {
   SfsRep* d_sr = nullptr;
   double* d_lgc = nullptr;
   float* d_out = nullptr;
-  GF_CUDA(e, cudaMalloc(&d_sr, sizeof(SfsRep) * b->R));
-  GF_CUDA(e, cudaMalloc(&d_lgc, sizeof(double) * (n + 1)));
-  GF_CUDA(e, cudaMalloc(&d_out, sizeof(float) * b->R * n));
+  {
+    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_sr), sizeof(SfsRep) * b->R);
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_lgc), sizeof(double) * (n + 1));
+    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_out), sizeof(float) * b->R * n);
+    if (ast != GF_OK) return ast;
+  }
   GF_CUDA(e, cudaMemcpyAsync(d_sr, sr.data(), sizeof(SfsRep) * b->R, cudaMemcpyHostToDevice, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(d_lgc, lgc.data(), sizeof(double) * (n + 1), cudaMemcpyHostToDevice, e->stream));
   batch_sfs_kernel<<<b->R, kBatchSfsThreads, 0, e->stream>>>(b->freq[0], d_sr, n, d_lgc, d_out);
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;
   GF_CUDA(e, cudaMemcpyAsync(out, d_out, sizeof(float) * b->R * n, cudaMemcpyDeviceToHost, e->stream));
+  cudaFreeAsync(d_sr, e->stream);
+  cudaFreeAsync(d_lgc, e->stream);
+  cudaFreeAsync(d_out, e->stream);
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  cudaFree(d_sr);
-  cudaFree(d_lgc);
-  cudaFree(d_out);
   return GF_OK;
 }
 

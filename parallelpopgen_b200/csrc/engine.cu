@@ -958,6 +958,7 @@ static gf_status launch_window(Engine* e, int b, int first, int count, const Gen
   R.compact = last.flag ? 1 : 0;
   R.preserve = (last.flag && gh[first + count - 1].preserve) ? 1 : 0;
   R.rep = 0;
+  R.births = news;
   GF_CUDA(e, cudaMemcpyAsync(e->d_wrep[b] + first, &R, sizeof(WinRep), cudaMemcpyHostToDevice, e->stream));
   const int slot = e->count_slot;
   WindowLaunch w;
@@ -1189,6 +1190,7 @@ void gf_engine_destroy(gf_engine* g) {
   release_sim(e);
   release_batch(e);
   cudaStreamSynchronize(e->stream);
+  if (e->h_rec_stage) cudaFreeHost(e->h_rec_stage);
   if (e->pool) cudaMemPoolDestroy(e->pool);
   for (auto ev : e->free_events) cudaEventDestroy(ev);
   if (e->spec_scratch) cudaFree(e->spec_scratch);

@@ -72,6 +72,7 @@ struct WinRep {
   int compact;          // flags after the last generation; compaction follows
   int preserve;         // the compaction marks survivors preserved
   int rep;              // index into the per-replicate count arrays
+  long long births;     // new mutations over the window: tiles at or beyond M0 + births hold nothing
 };
 
 // Pointers and sizes of one window launch plus its optional compaction.
@@ -92,7 +93,8 @@ struct WindowLaunch {
   const WinRep* reps;      // device
   int nreps;
   const WinGen* recs;      // device
-  int total_tiles;
+  int total_tiles;         // launch tiles (an upper bound when total_tiles_dev is set)
+  const int* total_tiles_dev = nullptr;   // device-side tile count (tiles assigned on the device)
   bool any_compact;
   unsigned long long* stats;
   int* fault;
@@ -105,9 +107,11 @@ struct BatchRep {
   long long capacity = 0;   // arena slots
   int generation = 0;       // last generation run
   int next_compact = 0;
-  int M = 0;                // count after the last super-step (read back)
+  int M = 0;                // count after the last read-back
   int Nc = 0;               // Nchrom_e at `generation`
   int id_buf = 0;           // ID buffer holding its state
+  int m_slot = 0;           // count array (d_M[m_slot]) holding its latest count
+  long long rec0 = -1;      // first precomputed record (generation 1), or -1
   bool done = false;
 };
 
@@ -134,6 +138,17 @@ struct Batch {
   size_t reps_cap = 0;
   long long super_steps = 0;
   long long generations = 0;
+  // generation records of every replicate, computed once at begin (when they fit the budget)
+  bool precomputed = false;
+  WinGen* d_all_recs = nullptr;
+  // ring of per-super-step replicate tables: a slot is rewritten only after the launch that read it
+  static constexpr int kRing = 4;
+  WinRep* d_ring[kRing] = {};
+  WinRep* h_ring[kRing] = {};
+  cudaEvent_t ring_done[kRing] = {};
+  int ring = 0;
+  bool counts_stale = false;          // counts on the device are newer than reps[].M
+  int* d_total_tiles = nullptr;       // tiles of the current super-step, assigned on the device
 };
 
 struct PendingCount {
@@ -211,6 +226,9 @@ struct Engine {
   std::vector<cudaEvent_t> prof_pool;
 
   // spectrum scratch
+  // page-locked staging of batched generation records, kept across batches (grown on demand)
+  WinGen* h_rec_stage = nullptr;
+  size_t h_rec_stage_cap = 0;
   void* spec_scratch = nullptr;
   size_t spec_scratch_bytes = 0;
   float* spec_in = nullptr;
@@ -233,6 +251,8 @@ gf_status pool_alloc(Engine* e, void** ptr, size_t bytes);
 gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
 
 // Window launch (+ segmented compaction into compact_dst), window.cu.
+void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
+                        int* total_out);
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst);
 
 // Host draw of one population's new-mutation count (engine.cu).

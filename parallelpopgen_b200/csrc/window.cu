@@ -34,17 +34,96 @@ __device__ __forceinline__ int find_rep(const WinRep* __restrict__ reps, int nre
   return lo;
 }
 
+// Shared-memory copy of the replicates' first tiles (batches of up to kRepCache replicates), so the
+// per-tile owner search does not chase global memory.
+constexpr int kRepCache = 4096;
+
+__device__ __forceinline__ int find_rep_cached(const int* s_tile0, const WinRep* __restrict__ reps, int nreps,
+                                               int gt) {
+  if (nreps > kRepCache) return find_rep(reps, nreps, gt);
+  int lo = 0, hi = nreps - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s_tile0[mid] <= gt) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void load_tile0(int* s_tile0, const WinRep* __restrict__ reps, int nreps) {
+  if (nreps <= kRepCache)
+    for (int j = threadIdx.x; j < nreps; j += blockDim.x) s_tile0[j] = reps[j].tile0;
+  __syncthreads();
+}
+
+// Tiles of one super-step, assigned on the device: replicate j's births over its window are summed
+// from its generation records, and it gets ceil((M_in + births) / 1024) tiles (at least one, at most
+// its segment), laid out in replicate order.  One block.
+__global__ void __launch_bounds__(1024) batch_tiles_kernel(WinRep* __restrict__ reps, int nreps,
+                                                           const int* __restrict__ M_in,
+                                                           const WinGen* __restrict__ recs, int* __restrict__ total) {
+  __shared__ int s_warp[32];
+  __shared__ int s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nreps; base += 1024) {
+    const int j = base + threadIdx.x;
+    int need = 0;
+    if (j < nreps) {
+      WinRep& R = reps[j];
+      long long births = 0;
+      for (int k = 0; k < R.ngen; ++k) births += recs[R.rec + k].new_count;
+      R.births = births;
+      const long long end = static_cast<long long>(M_in[R.rep]) + births;
+      const long long cap_tiles = R.capacity / kWinTile;
+      need = static_cast<int>(max(1ll, min(cap_tiles, (end + kWinTile - 1) / kWinTile)));
+    }
+    int incl = need;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      int w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const int before = s_carry + (warp > 0 ? s_warp[warp - 1] : 0) + incl - need;
+    if (j < nreps) {
+      reps[j].tile0 = before;
+      reps[j].ntiles = need;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += s_warp[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = s_carry;
+}
+
 __global__ void __launch_bounds__(kWinThreads, GF_DRIFT_MIN_BLOCKS)
     window_kernel(const float* __restrict__ A, float* __restrict__ B, int* __restrict__ id_gp,
                   int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
                   const WinRep* __restrict__ reps, int nreps, const WinGen* __restrict__ recs, int total_tiles,
-                  unsigned long long* __restrict__ stats, int* __restrict__ fault) {
+                  const int* __restrict__ total_dev, unsigned long long* __restrict__ stats,
+                  int* __restrict__ fault) {
   __shared__ int s_rep;
   __shared__ unsigned s_warp[kWinThreads / 32];
+  __shared__ int s_tile0[kRepCache];
   const int lane = threadIdx.x & 31;
-  for (int gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
-    if (threadIdx.x == 0) s_rep = find_rep(reps, nreps, gt);
+  const int ntiles_all = total_dev ? *total_dev : total_tiles;
+  load_tile0(s_tile0, reps, nreps);
+  for (int gt = blockIdx.x; gt < ntiles_all; gt += gridDim.x) {
+    if (threadIdx.x == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
     __syncthreads();
     const WinRep R = reps[s_rep];
     __syncthreads();
@@ -53,6 +132,8 @@ __global__ void __launch_bounds__(kWinThreads, GF_DRIFT_MIN_BLOCKS)
     const int s0 = 4 * q;
     const int cap = static_cast<int>(R.capacity);
     const int M0 = M_in[R.rep];
+    // a tile past the replicate's end-of-window count has nothing to do (tile 0 keeps the bookkeeping)
+    if (t > 0 && static_cast<long long>(t) * kWinTile >= M0 + R.births) continue;   // block-uniform
     float* const rowB = B + R.base;
     const float* const rowA = A + R.base;
     int* const gp = id_gp + R.base;
@@ -245,14 +326,18 @@ __global__ void __launch_bounds__(kWinThreads)
     seg_scatter_kernel(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ gp_src,
                        const int* __restrict__ tid_src, int* __restrict__ gp_dst, int* __restrict__ tid_dst,
                        const unsigned* __restrict__ flags, const unsigned* __restrict__ tile_offset,
-                       const WinRep* __restrict__ reps, int nreps, const int* __restrict__ M_end, int total_tiles) {
+                       const WinRep* __restrict__ reps, int nreps, const int* __restrict__ M_end, int total_tiles,
+                       const int* __restrict__ total_dev) {
   __shared__ int s_rep;
+  __shared__ int s_tile0[kRepCache];
+  const int ntiles_all = total_dev ? *total_dev : total_tiles;
+  load_tile0(s_tile0, reps, nreps);
   __shared__ unsigned s_words[32];
   __shared__ unsigned s_prefix[32];
   __shared__ float s_stage[kWinTile];
   const int t = threadIdx.x;
-  for (int gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
-    if (t == 0) s_rep = find_rep(reps, nreps, gt);
+  for (int gt = blockIdx.x; gt < ntiles_all; gt += gridDim.x) {
+    if (t == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
     __syncthreads();
     const WinRep R = reps[s_rep];
     __syncthreads();
@@ -313,6 +398,12 @@ __global__ void __launch_bounds__(kWinThreads)
 
 // Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
 // and scatter into `compact_dst` (the other state buffer).
+void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
+                        int* total_out) {
+  batch_tiles_kernel<<<1, 1024, 0, e->stream>>>(d_reps, nreps, M_in, recs, total_out);
+  e->kernel_launches += 1;
+}
+
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
   static int occupancy = 0;
   if (occupancy == 0) {
@@ -326,7 +417,7 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
   const int blocks = std::max(1, std::min(w.total_tiles, e->num_sms * per_sm));
   window_kernel<<<blocks, kWinThreads, 0, e->stream>>>(w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count,
                                                        w.M_in, w.M_end, w.M_next, w.reps, w.nreps, w.recs,
-                                                       w.total_tiles, w.stats, w.fault);
+                                                       w.total_tiles, w.total_tiles_dev, w.stats, w.fault);
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;
   if (w.any_compact) {
@@ -337,7 +428,7 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
     seg_scatter_kernel<<<sblocks, kWinThreads, 0, e->stream>>>(w.B, compact_dst, w.id_gp_cur, w.id_tid_cur,
                                                                w.id_gp_next, w.id_tid_next, w.flags,
                                                                w.tile_offset, w.reps, w.nreps, w.M_end,
-                                                               w.total_tiles);
+                                                               w.total_tiles, w.total_tiles_dev);
     GF_CUDA(e, cudaGetLastError());
     e->kernel_launches += 2;
   }
