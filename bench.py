@@ -329,11 +329,15 @@ def cpu_sample(threads: int, gens: int, seed: int = 1):
     return mg, dt
 
 
-def cpu_baseline_sample(threads: int, gens: int = 40):
+def cpu_baseline_sample(threads: int, gens: int = 40, serial_gens: int = 4):
+    """The CPU restatement on all host threads (the baseline) and, on a shorter sample, on one thread."""
     mg, dt = cpu_sample(threads, gens)
+    smg, sdt = cpu_sample(1, serial_gens)
     return {"value": mg / dt, "unit": "mutation-generations/s", "cores": threads, "kind": "port",
             "sample": f"{gens} generations of the neutral half (Nchrom_e 400,000, L 2.5e8, ~2.7M mutations) "
-                      f"from a synthetic equilibrium state; {dt:.1f} s of CPU time"}
+                      f"from a synthetic equilibrium state; {dt:.1f} s of CPU time",
+            "serial": {"value": smg / sdt, "cores": 1,
+                       "sample": f"{serial_gens} generations of the same state on one thread; {sdt:.1f} s"}}
 
 
 def run_reference(args, rank, world):
