@@ -199,6 +199,26 @@ def spectra_to_targets(mean_sfs: np.ndarray) -> np.ndarray:
     return np.log(np.maximum(p, LOG_FLOOR)).astype(np.float32)
 
 
+@dataclass
+class TargetScale:
+    """Per-bin standardisation of the log-spectrum targets: the network learns (t - mean) / std, so its
+    outputs are O(1) and the bf16 rounding of its activations and weights costs a fraction of a
+    standard deviation instead of a fixed fraction of |log p| (up to ~9)."""
+    mean: np.ndarray
+    std: np.ndarray
+
+    @staticmethod
+    def fit(targets: np.ndarray) -> "TargetScale":
+        t = np.asarray(targets, dtype=np.float64)
+        return TargetScale(t.mean(axis=0), np.maximum(t.std(axis=0), 1e-3))
+
+    def apply(self, targets: np.ndarray) -> np.ndarray:
+        return ((np.asarray(targets, dtype=np.float64) - self.mean) / self.std).astype(np.float32)
+
+    def invert(self, outputs: np.ndarray) -> np.ndarray:
+        return np.asarray(outputs, dtype=np.float64) * self.std + self.mean
+
+
 def median_relative_error(pred_p: np.ndarray, sim_mean: np.ndarray, min_count: float = 1.0):
     """Median over (query, bin) of |pred - sim| / sim on normalised spectra, over bins whose simulated
     mean count is at least `min_count` sites per replicate.  Returns (median, fraction of bins used)."""
@@ -247,8 +267,10 @@ def train(mlp: Mlp, x, t, steps: int, batch: int = 1024, lr: float = 1e-3, lr_mi
 class Surrogate:
     """SFS queries answered by the network inside its support and by the simulator outside it."""
 
-    def __init__(self, mlp: Mlp, engine: Engine, fallback_reps: int = 64, seed: int = 0x5EED):
+    def __init__(self, mlp: Mlp, engine: Engine, fallback_reps: int = 64, seed: int = 0x5EED,
+                 scale: TargetScale | None = None):
         self.mlp = mlp
+        self.scale = scale
         self.engine = engine
         self.fallback_reps = fallback_reps
         self.seed = seed
@@ -267,7 +289,8 @@ class Surrogate:
             n = min(len(y), B - c0)
             if n > 0:
                 out[c0:c0 + n] = y[:n]
-        p = np.exp(out.astype(np.float64))
+        logp = self.scale.invert(out) if self.scale is not None else out.astype(np.float64)
+        p = np.exp(logp)
         return p / p.sum(axis=1, keepdims=True)
 
     def query(self, params: np.ndarray) -> tuple[np.ndarray, np.ndarray]:

@@ -96,3 +96,15 @@ def test_parameter_mapping():
     assert abs(rep.mu * 4 * 1000 * sg.NUM_SITES - sg.THETA) < 1e-3 * sg.THETA
     t = sg.spectra_to_targets(np.array([[1.0] * 98 + [0.0]]))
     assert t.shape == (1, 99) and abs(t[0, 0] - math.log(1 / 98)) < 1e-6 and abs(t[0, -1] - math.log(sg.LOG_FLOOR)) < 1e-5
+
+
+def test_target_scale_round_trip():
+    from parallelpopgen_b200 import surrogate as sg
+    rng = np.random.default_rng(2)
+    t = rng.normal(-5, 2, (300, 99)).astype(np.float32)
+    t[:, 7] = -9.2      # a constant bin keeps a floor on its scale
+    sc = sg.TargetScale.fit(t)
+    z = sc.apply(t)
+    assert abs(z[:, :7].mean()) < 1e-5 and abs(z[:, :7].std() - 1) < 1e-3
+    assert np.all(np.isfinite(z)) and np.allclose(z[:, 7], 0.0)
+    np.testing.assert_allclose(sc.invert(z), t, rtol=1e-5, atol=1e-5)
