@@ -122,6 +122,7 @@ SIGNATURES = {
     "gf_batch_read_state": (_I, [_P, _I, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "gf_batch_sfs": (_I, [_P, _I, _P]),
     "gf_batch_stats_read": (_I, [_P, ctypes.POINTER(BatchStats)]),
+    "gf_batch_set_record_budget": (_I, [_P, ctypes.c_int64]),
     "gf_engine_set_profiling": (_I, [_P, _I]),
     "gf_engine_set_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),
     "gf_engine_get_tuning": (_I, [_P, ctypes.POINTER(Tuning)]),

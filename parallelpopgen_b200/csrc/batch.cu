@@ -365,17 +365,16 @@ static void make_record(const gf_replicate& p, int g, WinGen& w) {
   w.alive = N > 0;
 }
 
-// Records depend only on each replicate's seeds and size trajectory, so when they fit (64 M records)
+// Records depend only on each replicate's seeds and size trajectory, so when they fit the engine's
+// budget (64 M records by default)
 // they are computed once, in parallel over replicates, into the engine's page-locked staging buffer
 // (kept across batches: no zero fill, no page faults after the first batch) and uploaded with one
 // asynchronous copy; super-steps then need neither host record work nor a read-back.
-constexpr long long kPrecomputeRecords = 64ll << 20;
-
 static gf_status precompute_records(Engine* e, Batch* b) {
   long long total = 0;
   for (auto& br : b->reps) total += br.p.num_generations;
   b->precomputed = false;
-  if (total > kPrecomputeRecords || total == 0) return GF_OK;
+  if (total > e->batch_record_budget || total == 0) return GF_OK;
   long long off = 0;
   for (auto& br : b->reps) {
     br.rec0 = off;
@@ -846,6 +845,13 @@ void gf_replicate_population_table(const gf_replicate* rep, int32_t first, int32
 gf_status gf_batch_begin(gf_engine* g, const gf_replicate* reps, int32_t R) {
   if (!g) return GF_ERR_INVALID_ARGUMENT;
   return batch_begin(&g->impl, reps, R);
+}
+
+gf_status gf_batch_set_record_budget(gf_engine* g, int64_t records) {
+  if (!g) return GF_ERR_INVALID_ARGUMENT;
+  if (records < 0) return fail(&g->impl, GF_ERR_INVALID_ARGUMENT, "negative record budget");
+  g->impl.batch_record_budget = records;
+  return GF_OK;
 }
 
 gf_status gf_batch_run(gf_engine* g, int32_t max_super_steps, int32_t* out_active) {

@@ -162,6 +162,7 @@ struct Engine {
   int num_sms = 148;
   int draw_coop = 0;       // 1: warp-cooperative draws
   int blocks_per_sm = 0;   // drift grid limit per SM (0: occupancy maximum)
+  long long batch_record_budget = 64ll << 20;   // batches up to this many records are precomputed
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   // stream-ordered pool for the mutation arrays and per-run scratch; it keeps freed memory, so a new

@@ -152,6 +152,9 @@ class Engine:
         self._batch = arr
         self._check(self.lib.gf_batch_begin(self.h, ctypes.cast(arr, ctypes.c_void_p), len(reps)))
 
+    def batch_set_record_budget(self, records: int) -> None:
+        self._check(self.lib.gf_batch_set_record_budget(self.h, int(records)))
+
     def batch_run(self, max_super_steps: int = 0) -> int:
         active = ctypes.c_int32()
         self._check(self.lib.gf_batch_run(self.h, int(max_super_steps), ctypes.byref(active)))

@@ -75,3 +75,23 @@ def test_batched_super_steps_are_resumable():
             out.append([e.batch_read_state(r)[0] for r in range(len(reps))])
     for a, b in zip(*out):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_precomputed_and_per_super_step_records_agree():
+    """Batches whose records exceed the precomputation budget build them per super-step and read the
+    counts back each time; both paths must give the same states, also when run in chunks."""
+    reps = make_replicates(6, seed=17, max_gens=700)
+    out = []
+    for budget in (1 << 26, 0):
+        with Engine() as e:
+            e.batch_set_record_budget(budget)
+            e.batch_begin(reps)
+            while e.batch_run(5) > 0:
+                pass
+            out.append([e.batch_read_state(r) for r in range(len(reps))])
+            st = e.batch_stats()
+            assert st["active"] == 0 and st["generations"] == sum(r.num_generations for r in reps)
+    for (fa, ia, ga), (fb, ib, gb) in zip(*out):
+        assert ga == gb
+        assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
+        assert np.array_equal(ia, ib)
