@@ -622,6 +622,145 @@ def surrogate_inference_only(args):
                                    "unit": "TFLOP/s", "frac": tf / peak, "forward_us": fwd_s * 1e6}}), flush=True)
 
 
+# ------------------------------------------------------------------------------------------------
+# multi-population demography (per-generation drift kernel, P = 3)
+# ------------------------------------------------------------------------------------------------
+MP_GENS, MP_L, MP_MU, MP_M, MP_H = 5000, 2e8, 1e-9, 1e-4, 0.3
+MP_N0, MP_R, MP_CAPS, MP_FOUND = 10_000, 0.005, (100_000, 250_000, 500_000), (0, 1, 2000)
+MP_SHIFT, MP_GAMMA = 3000, (-5.0, 2.0)
+
+
+def multipop_size(pop: int, g: int) -> int:
+    """Population `pop` exists from generation MP_FOUND[pop] (the ancestral population 0 from the start),
+    starts at N = 1e4 and grows exponentially at r = 0.005 to its cap (1e5, 2.5e5, 5e5)."""
+    f = MP_FOUND[pop]
+    if pop > 0 and g < max(f, 1):
+        return 0
+    t = g - f
+    return int(min(MP_CAPS[pop], round(MP_N0 * np.exp(MP_R * t))))
+
+
+def multipop_generations(first: int, last: int, sample_every: int = 500, compact_interval: int = 35,
+                         last_generation: int = MP_GENS):
+    """gf_generation records of generations first..last, packed the way GO_Fish::run_sim packs them:
+    population 1 founded from population 0 at generation 1, population 2 from population 1 at 2000
+    (migration proportion 1 from the parent in the founding generation), symmetric migration 1e-4 among
+    existing populations otherwise, selection gamma -5 then +2 from generation 3000 (s = gamma / 2e4,
+    selection_constant of the ancestral size), h 0.3, inbreeding F 0.1 in population 2, mu 1e-9, L 2e8,
+    a time sample (preserve + compaction) every 500 generations."""
+    from parallelpopgen_b200._capi import GEN_DTYPE, MAX_POPULATIONS as MP
+    gens = np.zeros(last - first + 1, dtype=GEN_DTYPE)
+    # the reference's schedule: every compact_interval generations from the start, restarted at each
+    # compaction, plus the final generation and every time sample
+    next_compact = compact_interval
+    for g in range(1, first):
+        if g == next_compact or g % sample_every == 0:
+            next_compact = g + compact_interval
+    for i, g in enumerate(range(first, last + 1)):
+        G = gens[i]
+        G["generation"] = g
+        exists = [multipop_size(p, g) > 0 for p in range(3)]
+        gamma = MP_GAMMA[0] if g < MP_SHIFT else MP_GAMMA[1]
+        for p in range(3):
+            N = multipop_size(p, g)
+            F = 0.1 if p == 2 else 0.0
+            pp = G["pop"][p]
+            pp["drift"] = 1 if N > 0 else 0
+            pp["Nchrom_e"] = int(np.float32(2 * N) / np.float32(1 + np.float32(F))) if N > 0 else 0
+            pp["alive"] = pp["mutate"] = 1 if N > 0 else 0
+            pp["mu"], pp["F"], pp["h"] = MP_MU, F, MP_H
+            pp["sel_slope"], pp["sel_intercept"] = 0.0, np.float32(gamma) / np.float32(2 * MP_N0)
+        mig = G["migration"]
+        n_exist = sum(exists)
+        for to in range(3):
+            if not exists[to]:
+                continue
+            founder = {1: 0, 2: 1}.get(to)
+            if to > 0 and g == max(MP_FOUND[to], 1):
+                mig[founder * MP + to] = 1.0               # the founding generation copies the parent
+                continue
+            for frm in range(3):
+                if exists[frm]:
+                    mig[frm * MP + to] = (1.0 - (n_exist - 1) * MP_M) if frm == to else MP_M
+        preserve = g % sample_every == 0
+        compact = g == next_compact or g == last_generation or preserve
+        G["compact"] = 1 if compact else 0
+        G["preserve"] = 1 if (compact and preserve) else 0
+        if compact:
+            next_compact = g + compact_interval
+    return gens
+
+
+def run_multipop(args):
+    import torch
+    from parallelpopgen_b200 import Engine
+    from parallelpopgen_b200._capi import MSE_DTYPE
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    eng = Engine(device=0, stream=stream.cuda_stream)
+    total = args.mp_gens
+    segments = [multipop_generations(a, min(a + 499, total), last_generation=total) for a in range(1, total + 1, 500)]
+    pops = np.zeros(3, dtype=MSE_DTYPE)
+    pops[0] = (MP_N0, 2 * MP_N0, MP_MU, 0.0, MP_H, 0.0, np.float32(MP_GAMMA[0]) / np.float32(2 * MP_N0))
+    reserve = 48_000_000     # time samples preserve their survivors: the state grows past 25 M slots
+    h_freq = torch.empty(3 * reserve, dtype=torch.float32, pin_memory=True).numpy()
+    h_ids = torch.empty((reserve, 4), dtype=torch.int32, pin_memory=True).numpy()
+    n = 200
+
+    def step(samples: bool):
+        eng.begin_mse(pops, seed1=SEED1, seed2=SEED2, num_sites=MP_L, compact_interval=35, reserve=reserve)
+        d2h, M = 0, 0
+        for seg in segments:
+            eng.run(seg)
+            if samples:     # the time sample taken at the segment's last generation (rows packed [3][M])
+                M = eng.read_state_into(h_freq, h_ids)
+                d2h += 3 * 4 * M + 16 * M
+        return eng.stats()["mutation_generations"], d2h, M
+
+    for _ in range(args.warmup):
+        step(False)
+    times, mg = [], 0.0
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            m, _, _ = step(False)
+            ev1.record(stream)
+            ev1.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+            mg += m
+    e2e_t, e2e_mg, d2h = [], 0.0, 0
+    for _ in range(args.steps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        m, d2h, M = step(True)
+        # the final sample's SFS of a sample of 200 in each population
+        for p in range(3):
+            Nc = int(np.float32(2 * multipop_size(p, total)) / np.float32(1 + np.float32(0.1 if p == 2 else 0.0)))
+            if Nc > n:          # populations founded later than a shortened run's end are skipped
+                eng.site_frequency_spectrum(h_freq[p * M:(p + 1) * M], Nc, n, MP_L)
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_t.append(ev0.elapsed_time(ev1))
+        e2e_mg += m
+    value = mg / (sum(times) * 1e-3)
+    print(json.dumps({
+        "metric": "mutation-generations/s (multi-population)", "value": value, "unit": "mutation-generations/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "3 populations: ancestral N=1e4 (MSE start), population 1 founded at generation 1, "
+                               "population 2 at 2000, exponential growth r=0.005 to 1e5 / 2.5e5 / 5e5, symmetric "
+                               "migration 1e-4, gamma -5 -> +2 at 3000, h 0.3, F 0.1 in population 2, mu 1e-9, "
+                               "L 2e8, 5000 generations, compaction every 35 and at every time sample (500)",
+                   "kernel": "per-generation drift kernel (P = 3)"},
+        "mutation_generations_per_step": mg / args.steps,
+        "e2e": {"value": e2e_mg / (sum(e2e_t) * 1e-3), "unit": "mutation-generations/s",
+                "path": "10 time samples read into page-locked buffers, SFS n=200 of each population",
+                "d2h_bytes_per_step": d2h},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
 def tensor_peak():
     """(bf16 dense TFLOP/s, "measured" | "fallback") for a kernel timed on its own (burst figure)."""
     p = ROOT / "MEASURED_PEAKS.json"
@@ -639,9 +778,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "surrogate"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "surrogate", "multipop"],
                     help="plain: the headline single-population workload; batched: batched ragged replicates; "
                          "surrogate: the SFS surrogate network against the simulator")
+    ap.add_argument("--mp-gens", type=int, default=MP_GENS, help="multipop workload: generations per run")
     ap.add_argument("--train-draws", type=int, default=65536)
     ap.add_argument("--eval-draws", type=int, default=1024)
     ap.add_argument("--train-steps", type=int, default=120000)
@@ -666,6 +806,10 @@ def main():
     if args.workload == "surrogate":
         if rank == 0:
             run_surrogate(args)
+        return
+    if args.workload == "multipop":
+        if rank == 0:
+            run_multipop(args)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)
