@@ -110,3 +110,24 @@ def test_batched_bench_workload_draws():
     assert all(r.num_generations == 4 * r.N0 for r in reps)
     assert all(r.N_min == r.N0 // 10 and r.N_max == 10 * r.N0 for r in reps)
     assert all(0.0 <= r.F <= 0.5 and 0.0 <= r.h <= 1.0 for r in reps)
+
+
+def test_multipop_bench_schedule():
+    """The three-population benchmark's records: founding generations copy the parent, migration columns
+    of existing populations sum to 1, segmented tables reproduce the continuous compaction schedule."""
+    import bench
+    from parallelpopgen_b200._capi import MAX_POPULATIONS as MP
+    whole = bench.multipop_generations(1, 3000, last_generation=3000)
+    parts = np.concatenate([bench.multipop_generations(a, min(a + 499, 3000), last_generation=3000)
+                            for a in range(1, 3001, 500)])
+    assert np.array_equal(whole["compact"], parts["compact"]) and np.array_equal(whole["preserve"], parts["preserve"])
+    assert whole["preserve"][499] == 1 and whole["compact"][2999] == 1
+    g1, g2000 = whole[0], whole[1999]
+    assert g1["migration"][0 * MP + 1] == 1.0 and g2000["migration"][1 * MP + 2] == 1.0
+    for G in (whole[10], whole[2500]):
+        for to in range(3):
+            if G["pop"]["drift"][to]:
+                col = sum(float(G["migration"][f * MP + to]) for f in range(3))
+                assert abs(col - 1.0) < 1e-6
+    assert whole[0]["pop"]["drift"][2] == 0 and whole[2500]["pop"]["drift"][2] == 1
+    assert whole[2500]["pop"]["F"][2] == np.float32(0.1)
