@@ -636,17 +636,21 @@ bool make_out_map(CUtensorMap* m, const void* base, long long rows, long long co
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// SM count of the current device (cached per device)
 int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
+  static int counts[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (counts[dev] == 0) {
+    int n = 0;
     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
       cudaGetLastError();
       n = 148;
     }
+    counts[dev] = n;
   }
-  return n;
+  return counts[dev];
 }
 
 // Outputs the epilogue does not write get the A map in their slot (never used).
