@@ -309,11 +309,11 @@ void release_batch(Engine* e) {
   if (b->h_recs) cudaFreeHost(b->h_recs);
   if (b->d_reps) cudaFree(b->d_reps);
   if (b->h_reps) cudaFreeHost(b->h_reps);
-  for (int k = 0; k < Batch::kRing; ++k) {
-    if (b->d_ring[k]) cudaFree(b->d_ring[k]);
-    if (b->h_ring[k]) cudaFreeHost(b->h_ring[k]);
+  if (b->d_ring_all) cudaFree(b->d_ring_all);
+  if (b->h_ring_all) cudaFreeHost(b->h_ring_all);
+  for (int k = 0; k < Batch::kRing; ++k)
     if (b->ring_done[k]) cudaEventDestroy(b->ring_done[k]);
-  }
+  if (b->stage_done) cudaEventDestroy(b->stage_done);
   delete b;
   e->batch = nullptr;
 }
@@ -365,49 +365,105 @@ static void make_record(const gf_replicate& p, int g, WinGen& w) {
   w.alive = N > 0;
 }
 
-// Records depend only on each replicate's seeds and size trajectory, so when they fit the engine's
-// budget (64 M records by default)
-// they are computed once, in parallel over replicates, into the engine's page-locked staging buffer
-// (kept across batches: no zero fill, no page faults after the first batch) and uploaded with one
-// asynchronous copy; super-steps then need neither host record work nor a read-back.
-static gf_status precompute_records(Engine* e, Batch* b) {
-  long long total = 0;
-  for (auto& br : b->reps) total += br.p.num_generations;
-  b->precomputed = false;
-  if (total > e->batch_record_budget || total == 0) return GF_OK;
-  long long off = 0;
-  for (auto& br : b->reps) {
-    br.rec0 = off;
-    off += br.p.num_generations;
-  }
-  if (e->h_rec_stage_cap < static_cast<size_t>(total)) {
-    if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
-    e->h_rec_stage = nullptr;
-    e->h_rec_stage_cap = 0;
-    const size_t cap = static_cast<size_t>(total) + static_cast<size_t>(total) / 4;
-    GF_CUDA(e, cudaMallocHost(&e->h_rec_stage, sizeof(WinGen) * cap));
-    e->h_rec_stage_cap = cap;
-  }
-  GF_TRACE_POINT(e, "record buffers");
-  WinGen* recs = e->h_rec_stage;
+// Records depend only on each replicate's seeds and size trajectory, so they are computed ahead of
+// the GPU (host threads over replicates, into the engine's page-locked staging buffer, kept across
+// batches) and uploaded in bulk; super-steps then need neither host record work nor a read-back.
+// A batch within the engine's record budget has all its records resident; a larger one keeps two
+// regions per replicate of `chunk` generations (a multiple of its cadence, so no window straddles
+// two chunks), and chunk j + 1 is computed and uploaded when a replicate enters chunk j -- into the
+// region chunk j - 1 used, after (in stream order) the super-steps that read it.
+
+// Compute chunk j of every listed replicate into the staging buffer at its device offsets, then
+// upload each run of consecutive replicates with one copy.
+static gf_status fill_chunks(Engine* e, Batch* b, const std::vector<std::pair<int, int>>& todo) {
+  if (todo.empty()) return GF_OK;
+  GF_CUDA(e, cudaEventSynchronize(b->stage_done));   // the previous upload has read the staging buffer
+  WinGen* stage = e->h_rec_stage;
+  long long recs = 0;
+  for (auto& t : todo) recs += b->reps[t.first].chunk;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned nt = total > 50000 ? std::min<unsigned>(hw, 32) : 1;
-  std::atomic<int> next(0);
+  const unsigned nt = recs > 50000 ? std::min<unsigned>(hw, 32) : 1;
+  std::atomic<size_t> next(0);
   auto work = [&]() {
-    for (int r; (r = next.fetch_add(1)) < b->R;) {
-      const BatchRep& br = b->reps[r];
-      for (int g = 1; g <= br.p.num_generations; ++g) make_record(br.p, g, recs[br.rec0 + g - 1]);
+    for (size_t i; (i = next.fetch_add(1)) < todo.size();) {
+      const BatchRep& br = b->reps[todo[i].first];
+      const int j = todo[i].second;
+      const long long base = (j % br.regions) * b->region_stride + br.rec0;
+      const int g0 = j * br.chunk;
+      const int g1 = std::min(br.p.num_generations, g0 + br.chunk);
+      for (int g = g0 + 1; g <= g1; ++g) make_record(br.p, g, stage[base + (g - g0 - 1)]);
     }
   };
   std::vector<std::thread> pool;
   for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
   work();
   for (auto& t : pool) t.join();
-  GF_TRACE_POINT(e, "record draws");
-  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * total);
+  // copies: runs of replicates whose regions are adjacent in the layout
+  size_t i = 0;
+  while (i < todo.size()) {
+    const BatchRep& a = b->reps[todo[i].first];
+    const long long start = (todo[i].second % a.regions) * b->region_stride + a.rec0;
+    long long end = start + a.chunk;
+    size_t k = i + 1;
+    while (k < todo.size()) {
+      const BatchRep& c = b->reps[todo[k].first];
+      const long long cs = (todo[k].second % c.regions) * b->region_stride + c.rec0;
+      if (cs != end) break;
+      end = cs + c.chunk;
+      ++k;
+    }
+    GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs + start, stage + start, sizeof(WinGen) * (end - start),
+                               cudaMemcpyHostToDevice, e->stream));
+    i = k;
+  }
+  GF_CUDA(e, cudaEventRecord(b->stage_done, e->stream));
+  for (auto& t : todo) b->reps[t.first].filled = std::max(b->reps[t.first].filled, t.second);
+  return GF_OK;
+}
+
+static gf_status precompute_records(Engine* e, Batch* b) {
+  long long total = 0;
+  for (auto& br : b->reps) total += br.p.num_generations;
+  b->precomputed = false;
+  if (e->batch_record_budget <= 0 || total == 0) return GF_OK;
+  const bool resident = total <= e->batch_record_budget;
+  const long long target = std::max<long long>(64, e->batch_record_budget / (2ll * b->R));
+  long long off = 0;
+  for (auto& br : b->reps) {
+    const int G = std::max(br.p.num_generations, 1);
+    const int c = std::max(br.p.compact_interval, 1);
+    long long chunk = resident ? G : std::max<long long>(c, (target / c) * c);
+    if (chunk >= G) {
+      chunk = G;
+      br.regions = 1;
+    } else {
+      br.regions = 2;
+    }
+    br.chunk = static_cast<int>(chunk);
+    br.rec0 = off;
+    br.filled = -1;
+    off += chunk;
+  }
+  b->region_stride = off;
+  const long long slots = 2 * off;   // region 1 is used only by replicates with two regions
+  if (e->h_rec_stage_cap < static_cast<size_t>(slots)) {
+    if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
+    e->h_rec_stage = nullptr;
+    e->h_rec_stage_cap = 0;
+    const size_t cap = static_cast<size_t>(slots) + static_cast<size_t>(slots) / 4;
+    GF_CUDA(e, cudaMallocHost(&e->h_rec_stage, sizeof(WinGen) * cap));
+    e->h_rec_stage_cap = cap;
+  }
+  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * slots);
   if (st != GF_OK) return st;
-  // the staging buffer is rewritten only by the next batch_begin, which first synchronizes the stream
-  GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs, recs, sizeof(WinGen) * total, cudaMemcpyHostToDevice, e->stream));
+  GF_TRACE_POINT(e, "record buffers");
+  std::vector<std::pair<int, int>> todo;
+  for (int r = 0; r < b->R; ++r) todo.emplace_back(r, 0);
+  for (int r = 0; r < b->R; ++r)
+    if (b->reps[r].regions == 2) todo.emplace_back(r, 1);
+  st = fill_chunks(e, b, todo);
+  if (st != GF_OK) return st;
+  GF_TRACE_POINT(e, "record draws and upload");
   b->precomputed = true;
   return GF_OK;
 }
@@ -515,11 +571,11 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     if (ast != GF_OK) return ast;
   }
   GF_CUDA(e, cudaMallocHost(&b->h_M, sizeof(int) * 2 * R));
-  for (int k = 0; k < Batch::kRing; ++k) {
-    GF_CUDA(e, cudaMalloc(&b->d_ring[k], sizeof(WinRep) * R));
-    GF_CUDA(e, cudaMallocHost(&b->h_ring[k], sizeof(WinRep) * R));
+  GF_CUDA(e, cudaMalloc(&b->d_ring_all, sizeof(WinRep) * R * Batch::kRing));
+  GF_CUDA(e, cudaMallocHost(&b->h_ring_all, sizeof(WinRep) * R * Batch::kRing));
+  for (int k = 0; k < Batch::kRing; ++k)
     GF_CUDA(e, cudaEventCreateWithFlags(&b->ring_done[k], cudaEventDisableTiming));
-  }
+  GF_CUDA(e, cudaEventCreateWithFlags(&b->stage_done, cudaEventDisableTiming));
   GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
@@ -624,19 +680,34 @@ static gf_status sync_counts(Engine* e) {
 static gf_status batch_super_step(Engine* e, int* active_out) {
   Batch* b = e->batch;
   if (!b->precomputed) return batch_super_step_fallback(e, active_out);
+  // a replicate entering chunk j gets chunk j + 1 computed and uploaded now (into the region chunk
+  // j - 1 used, after the super-steps that read it in stream order)
+  std::vector<std::pair<int, int>> refill;
+  for (int r = 0; r < b->R; ++r) {
+    const BatchRep& br = b->reps[r];
+    if (br.done || br.regions != 2) continue;
+    const int j = br.generation / br.chunk;
+    if (br.filled == j && (j + 1) * static_cast<long long>(br.chunk) < br.p.num_generations) refill.emplace_back(r, j + 1);
+  }
+  gf_status rst = fill_chunks(e, b, refill);
+  if (rst != GF_OK) return rst;
   const int slot = b->ring;
   GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
-  WinRep* hr = b->h_ring[slot];
+  WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->R;
+  WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->R;
   int nj = 0, tiles = 0;
   for (int r = 0; r < b->R; ++r) {
     BatchRep& br = b->reps[r];
     if (br.done) continue;
     const int end = std::min(br.next_compact, br.p.num_generations);
     const int ngen = end - br.generation;
+    const int j = br.generation / br.chunk;
+    if (br.filled < j) return fail(e, GF_ERR_STATE, "replicate %d: record chunk %d not resident", r, j);
     WinRep& w = hr[nj++];
     w.base = br.base;
     w.capacity = br.capacity;
-    w.rec = static_cast<int>(br.rec0 + br.generation);
+    w.rec = static_cast<int>((j % br.regions) * b->region_stride + br.rec0 +
+                             (br.generation - static_cast<long long>(j) * br.chunk));
     w.ngen = ngen;
     w.tile0 = tiles;
     w.ntiles = static_cast<int>(br.capacity / kBatchTile);
@@ -653,9 +724,9 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     if (active_out) *active_out = 0;
     return GF_OK;
   }
-  GF_CUDA(e, cudaMemcpyAsync(b->d_ring[slot], hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));
+  GF_CUDA(e, cudaMemcpyAsync(dr, hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));
   // each replicate's tiles from its device-side count: only its live slots are visited
-  assign_batch_tiles(e, b->d_ring[slot], nj, b->d_M[b->mslot], b->d_all_recs, b->d_total_tiles);
+  assign_batch_tiles(e, dr, nj, b->d_M[b->mslot], b->d_all_recs, b->d_total_tiles);
   GF_CUDA(e, cudaGetLastError());
   WindowLaunch w;
   w.A = b->freq[0];
@@ -671,7 +742,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   w.M_end = b->d_Mend;
   w.M_next = nullptr;
   w.M_out = b->d_M[b->mslot ^ 1];
-  w.reps = b->d_ring[slot];
+  w.reps = dr;
   w.nreps = nj;
   w.recs = b->d_all_recs;
   w.total_tiles = tiles;                 // segment tiles: an upper bound, sizes the grid

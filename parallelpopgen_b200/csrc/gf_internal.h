@@ -111,7 +111,10 @@ struct BatchRep {
   int Nc = 0;               // Nchrom_e at `generation`
   int id_buf = 0;           // ID buffer holding its state
   int m_slot = 0;           // count array (d_M[m_slot]) holding its latest count
-  long long rec0 = -1;      // first precomputed record (generation 1), or -1
+  long long rec0 = -1;      // its offset inside each record region, or -1 (records not precomputed)
+  int chunk = 0;            // generations per record chunk (a multiple of its compaction cadence)
+  int regions = 1;          // 1: all its records resident; 2: chunks alternate between two regions
+  int filled = -1;          // highest chunk uploaded
   bool done = false;
 };
 
@@ -142,10 +145,13 @@ struct Batch {
   bool precomputed = false;
   WinGen* d_all_recs = nullptr;
   // ring of per-super-step replicate tables: a slot is rewritten only after the launch that read it
-  static constexpr int kRing = 4;
-  WinRep* d_ring[kRing] = {};
-  WinRep* h_ring[kRing] = {};
+  // (64 slots: the host may run that many super-steps ahead of the GPU)
+  static constexpr int kRing = 64;
+  WinRep* d_ring_all = nullptr;       // kRing tables of R entries, one allocation each side
+  WinRep* h_ring_all = nullptr;
   cudaEvent_t ring_done[kRing] = {};
+  long long region_stride = 0;        // records per region (region k of replicate r: k * stride + rec0)
+  cudaEvent_t stage_done = nullptr;   // the last upload from the page-locked staging buffer
   int ring = 0;
   bool counts_stale = false;          // counts on the device are newer than reps[].M
   int* d_total_tiles = nullptr;       // tiles of the current super-step, assigned on the device

@@ -77,12 +77,13 @@ def test_batched_super_steps_are_resumable():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
-def test_precomputed_and_per_super_step_records_agree():
-    """Batches whose records exceed the precomputation budget build them per super-step and read the
-    counts back each time; both paths must give the same states, also when run in chunks."""
+def test_record_paths_agree():
+    """All records resident, records in alternating chunks (a budget far below the batch's total), and
+    records built per super-step with a count read-back (budget 0) must give the same states, also
+    when the batch runs in chunks of super-steps."""
     reps = make_replicates(6, seed=17, max_gens=700)
     out = []
-    for budget in (1 << 26, 0):
+    for budget in (1 << 26, 600, 0):
         with Engine() as e:
             e.batch_set_record_budget(budget)
             e.batch_begin(reps)
@@ -91,7 +92,8 @@ def test_precomputed_and_per_super_step_records_agree():
             out.append([e.batch_read_state(r) for r in range(len(reps))])
             st = e.batch_stats()
             assert st["active"] == 0 and st["generations"] == sum(r.num_generations for r in reps)
-    for (fa, ia, ga), (fb, ib, gb) in zip(*out):
-        assert ga == gb
-        assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
-        assert np.array_equal(ia, ib)
+    for other in out[1:]:
+        for (fa, ia, ga), (fb, ib, gb) in zip(out[0], other):
+            assert ga == gb
+            assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
+            assert np.array_equal(ia, ib)
