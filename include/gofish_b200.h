@@ -201,11 +201,11 @@ typedef struct gf_batch_stats {
   int64_t arena_slots;         /* device slots reserved for all replicates */
 } gf_batch_stats;
 gf_status gf_batch_stats_read(gf_engine* engine, gf_batch_stats* out);
-/* Largest batch (in generation records, one per replicate per generation) whose records
- * gf_batch_begin computes up front so that super-steps run without host work or read-backs
- * (default 67,108,864 records, 36 bytes each, held page-locked on the host and on the device);
- * larger batches build each super-step's records on the host and read the counts back per
- * super-step.  Results are identical either way.  Takes effect at the next gf_batch_begin. */
+/* Generation records (one per replicate per generation, 36 bytes, page-locked on the host and on
+ * the device) the batched engine keeps resident: a batch within the budget (default 67,108,864) has
+ * all its records computed at gf_batch_begin; a larger one keeps two chunks per replicate, refilled
+ * ahead of the GPU; 0 builds each super-step's records on the host and reads the counts back per
+ * super-step.  Results are identical in every case.  Takes effect at the next gf_batch_begin. */
 gf_status gf_batch_set_record_budget(gf_engine* engine, int64_t records);
 
 /* ---------------------------------------------------------------------------------------------
