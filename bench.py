@@ -7,7 +7,8 @@ gamma = 2Ns = -10 on half of the sites and the other half neutral, mutation-sele
 start, 10,000 generations with compaction every 25, then the site frequency spectrum of a sample of
 n = 1,000.  Selection acts per (population, generation, frequency) in GO_Fish, so "gamma on 50% of
 new mutations" is run exactly as two independent simulations of L = 2.5e8 sites each (neutral and
-gamma = -10), which is the same model under the Poisson-random-field independence of sites.
+gamma = -10), which is the same model under the Poisson-random-field independence of sites.  The two
+simulations run concurrently, each on its own engine, stream and host thread.
 
 Metric: mutation-generations/s = sum over generations of the mutation slots the drift pass updated,
 divided by device time.  `value` times the whole step on the device (MSE initialization, every
@@ -133,51 +134,80 @@ def build_halves(rank: int, gens_per_sim: int = GENS):
 
 
 def run_b200(args, rank, local_rank, world):
+    """The headline step: the two halves are independent simulations, run concurrently on two engines
+    (one stream and one host thread each), so one simulation's compaction kernels and launch tails
+    overlap the other's window kernels.  Time = CUDA events on a third stream that waits for both."""
+    import threading
+
     import torch
     from parallelpopgen_b200 import Engine
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    stream = torch.cuda.Stream(device=dev)
-    eng = Engine(device=local_rank, stream=stream.cuda_stream)
+    main = torch.cuda.Stream(device=dev)
+    streams = [torch.cuda.Stream(device=dev) for _ in range(2)]
+    engines = [Engine(device=local_rank, stream=st.cuda_stream) for st in streams]
     halves = build_halves(rank, args.gens)
     Nc = halves[0]["model"].Nchrom_e
-    d_sfs = torch.empty(SFS_N, dtype=torch.float32, device=dev)
+    d_sfs = [torch.empty(SFS_N, dtype=torch.float32, device=dev) for _ in range(2)]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     reserve = 12_000_000
 
-    def device_step():
-        """The step on device-resident state; returns mutation-generations."""
-        mg = 0.0
-        for hv in halves:
-            eng.begin_mse(hv["model"].mse_pops(), seed1=hv["seed1"], seed2=hv["seed2"], num_sites=L_HALF,
-                          compact_interval=COMPACT, reserve=reserve)
-            eng.run(hv["gens"])
-            d_freq, stride, M = eng.device_state()
-            eng.site_frequency_spectrum_device(d_freq, M, Nc, SFS_N, L_HALF, d_sfs.data_ptr())
-            mg += eng.stats()["mutation_generations"]
-        return mg
+    def device_half(k, eng):
+        """One half on device-resident state; returns its mutation-generations."""
+        hv = halves[k]
+        eng.begin_mse(hv["model"].mse_pops(), seed1=hv["seed1"], seed2=hv["seed2"], num_sites=L_HALF,
+                      compact_interval=COMPACT, reserve=reserve)
+        eng.run(hv["gens"])
+        d_freq, stride, M = eng.device_state()
+        eng.site_frequency_spectrum_device(d_freq, M, Nc, SFS_N, L_HALF, d_sfs[k].data_ptr())
+        return eng.stats()["mutation_generations"]
 
     # page-locked host buffers for the e2e step's outputs (allocated once, outside the timed region)
-    h_freq = torch.empty(reserve, dtype=torch.float32, pin_memory=True).numpy()
-    h_ids = torch.empty((reserve, 4), dtype=torch.int32, pin_memory=True).numpy()
+    h_freq = [torch.empty(reserve, dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    h_ids = [torch.empty((reserve, 4), dtype=torch.int32, pin_memory=True).numpy() for _ in range(2)]
 
-    def e2e_step():
-        """The step through the C ABI with host buffers: final frequencies, IDs and SFS to host."""
-        mg = 0.0
-        h2d = d2h = 0
-        for hv in halves:
-            eng.begin_mse(hv["model"].mse_pops(), seed1=hv["seed1"], seed2=hv["seed2"], num_sites=L_HALF,
-                          compact_interval=COMPACT, reserve=reserve)
-            eng.run(hv["gens"])
-            h2d += hv["gens"].nbytes
-            M = eng.read_state_into(h_freq, h_ids)
-            d2h += 4 * M + 16 * M
-            sfs = eng.site_frequency_spectrum(h_freq[:M], Nc, SFS_N, L_HALF)
-            h2d += 4 * M
-            d2h += sfs.nbytes
-            mg += eng.stats()["mutation_generations"]
-        return mg, h2d, d2h
+    def e2e_half(k, eng):
+        """One half through the C ABI with host buffers: final frequencies, IDs and SFS to host."""
+        hv = halves[k]
+        eng.begin_mse(hv["model"].mse_pops(), seed1=hv["seed1"], seed2=hv["seed2"], num_sites=L_HALF,
+                      compact_interval=COMPACT, reserve=reserve)
+        eng.run(hv["gens"])
+        M = eng.read_state_into(h_freq[k], h_ids[k])
+        sfs = eng.site_frequency_spectrum(h_freq[k][:M], Nc, SFS_N, L_HALF)
+        return (eng.stats()["mutation_generations"], hv["gens"].nbytes + 4 * M, 4 * M + 16 * M + sfs.nbytes)
+
+    def concurrent(fn):
+        """Both halves at once; returns (their results, elapsed ms by CUDA events)."""
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(main)
+        for st in streams:
+            st.wait_event(ev0)
+        out = [None, None]
+
+        def work(k):
+            out[k] = fn(k, engines[k])
+
+        threads = [threading.Thread(target=work, args=(k,)) for k in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            main.wait_event(e)
+        ev1.record(main)
+        ev1.synchronize()
+        if any(o is None for o in out):
+            raise RuntimeError("a half failed")
+        return out, ev0.elapsed_time(ev1)
+
+    def flush_l2():
+        with torch.cuda.stream(main):
+            flush.fill_(1.0)
+        main.synchronize()
 
     def barrier():
         if world > 1:
@@ -185,37 +215,31 @@ def run_b200(args, rank, local_rank, world):
         torch.cuda.synchronize(dev)
 
     for _ in range(args.warmup):
-        device_step()
-        e2e_step()
+        concurrent(device_half)
+        concurrent(e2e_half)
     barrier()
 
     # ---- value: device time of the whole step ----
-    launches0 = eng.stats()["kernel_launches"]
+    launches0 = sum(e.stats()["kernel_launches"] for e in engines)
     times = []
     mg_total = 0.0
     with ClockSampler(local_rank) as clk:
         for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            stream.synchronize()
-            ev0 = torch.cuda.Event(enable_timing=True)
-            ev1 = torch.cuda.Event(enable_timing=True)
-            ev0.record(stream)
-            mg_total += device_step()
-            ev1.record(stream)
-            ev1.synchronize()
-            times.append(ev0.elapsed_time(ev1))
-    launches = (eng.stats()["kernel_launches"] - launches0) // max(args.steps, 1) * args.steps
+            flush_l2()
+            out, ms = concurrent(device_half)
+            times.append(ms)
+            mg_total += sum(out)
+    launches = (sum(e.stats()["kernel_launches"] for e in engines) - launches0) // max(args.steps, 1) * args.steps
     barrier()
     ms_total = float(sum(times))
 
-    # ---- roofline: one more step with every drift launch bracketed by CUDA events ----
-    with torch.cuda.stream(stream):
-        flush.fill_(1.0)
-    stream.synchronize()
+    # ---- roofline: one more step, the halves one after the other on one engine, with every drift
+    # launch bracketed by CUDA events (uncontended kernel times) ----
+    flush_l2()
+    eng = engines[0]
     eng.set_profiling(True)
     eng.read_profile()
-    prof_mg = device_step()
+    prof_mg = device_half(0, eng) + device_half(1, eng)
     prof = eng.read_profile()
     eng.set_profiling(False)
     barrier()
@@ -223,18 +247,11 @@ def run_b200(args, rank, local_rank, world):
     # ---- e2e: host buffers, copies inside the timed region ----
     e2e_times, e2e_mg, h2d_b, d2h_b = [], 0.0, 0, 0
     for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        stream.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        mg, h2d, d2h = e2e_step()
-        ev1.record(stream)
-        ev1.synchronize()
-        e2e_times.append(ev0.elapsed_time(ev1))
-        e2e_mg += mg
-        h2d_b, d2h_b = h2d, d2h
+        flush_l2()
+        out, ms = concurrent(e2e_half)
+        e2e_times.append(ms)
+        e2e_mg += sum(o[0] for o in out)
+        h2d_b, d2h_b = sum(o[1] for o in out), sum(o[2] for o in out)
     barrier()
 
     # max time over ranks, total work over ranks
@@ -277,7 +294,8 @@ def run_b200(args, rank, local_rank, world):
             "mutation_generations_per_step": mg_total / args.steps,
             "l2": "256 MB buffer written between steps (L2 is 126 MB); the 10-40 MB working set of one "
                   "simulation is L2-resident inside a step",
-            "parallelism": f"replicas x{world} (independent seeds per rank, no collective)",
+            "parallelism": f"replicas x{world} (independent seeds per rank, no collective); the two halves "
+                           "run concurrently on two engines and streams",
         },
         "e2e": {
             "value": e2e_mg_all / (e2e_ms * 1e-3),
