@@ -687,15 +687,16 @@ int host_new_mutation_count(int seed1, int seed2, float mu, int Nchrom_e, float 
 
 template <int PT, bool NEUTRAL, bool FLAG, bool COOP>
 static void launch_drift_t(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a) {
-  static int occupancy = 0;
   auto kernel = drift_kernel<PT, NEUTRAL, FLAG, COOP>;
-  if (occupancy == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kernel, kDriftThreads, 0) != cudaSuccess ||
-        occupancy < 1) {
+  // resident blocks per SM, queried once (thread-safe initialisation; the same on every B200)
+  static const int occupancy = [kernel] {
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, kDriftThreads, 0) != cudaSuccess || o < 1) {
       cudaGetLastError();
-      occupancy = 1;
+      o = 1;
     }
-  }
+    return o;
+  }();
   const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
   const int blocks = std::max(1, std::min(tiles_bound, e->num_sms * per_sm));
   kernel<<<blocks, kDriftThreads, 0, e->stream>>>(e->freq[e->cur], e->freq[e->cur ^ 1], e->id_gp[e->id_cur],

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -638,7 +639,7 @@ bool make_out_map(CUtensorMap* m, const void* base, long long rows, long long co
 
 // SM count of the current device (cached per device)
 int sm_count() {
-  static int counts[64] = {};
+  static std::atomic<int> counts[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return 148;
@@ -658,7 +659,7 @@ template <int BN, int EPI>
 cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap* c, const CUtensorMap* y,
                         const CUtensorMap* yt, int M, int N, int K, int splits, const EpiArgs& ep,
                         cudaStream_t stream, int inject = 0) {
-  static bool attr_set[64] = {};
+  static std::atomic<bool> attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {

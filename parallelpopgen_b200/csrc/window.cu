@@ -405,14 +405,15 @@ void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, c
 }
 
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
-  static int occupancy = 0;
-  if (occupancy == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, window_kernel, kWinThreads, 0) != cudaSuccess ||
-        occupancy < 1) {
+  // resident blocks per SM, queried once (thread-safe initialisation; the same on every B200)
+  static const int occupancy = [] {
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel, kWinThreads, 0) != cudaSuccess || o < 1) {
       cudaGetLastError();
-      occupancy = 1;
+      o = 1;
     }
-  }
+    return o;
+  }();
   const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
   const int blocks = std::max(1, std::min(w.total_tiles, e->num_sms * per_sm));
   window_kernel<<<blocks, kWinThreads, 0, e->stream>>>(w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count,
