@@ -641,7 +641,7 @@ def surrogate_inference_only(args):
 
 
 # ------------------------------------------------------------------------------------------------
-# multi-population demography (per-generation drift kernel, P = 3)
+# multi-population demography (multi-population window kernel, P = 3)
 # ------------------------------------------------------------------------------------------------
 MP_GENS, MP_L, MP_MU, MP_M, MP_H = 5000, 2e8, 1e-9, 1e-4, 0.3
 MP_N0, MP_R, MP_CAPS, MP_FOUND = 10_000, 0.005, (100_000, 250_000, 500_000), (0, 1, 2000)
@@ -770,7 +770,7 @@ def run_multipop(args):
                                "population 2 at 2000, exponential growth r=0.005 to 1e5 / 2.5e5 / 5e5, symmetric "
                                "migration 1e-4, gamma -5 -> +2 at 3000, h 0.3, F 0.1 in population 2, mu 1e-9, "
                                "L 2e8, 5000 generations, compaction every 35 and at every time sample (500)",
-                   "kernel": "per-generation drift kernel (P = 3)"},
+                   "kernel": "window_mp_kernel (P = 3: all generations of a compaction window per launch)"},
         "mutation_generations_per_step": mg / args.steps,
         "e2e": {"value": e2e_mg / (sum(e2e_t) * 1e-3), "unit": "mutation-generations/s",
                 "path": "10 time samples read into page-locked buffers, SFS n=200 of each population",

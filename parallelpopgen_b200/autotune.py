@@ -1,7 +1,7 @@
 """Autotuner for the engine's launch choices and the batched engine's compaction cadence.
 
-Launch choices (`gf_tuning`: per-thread vs warp-cooperative draws, resident drift blocks per SM,
-window launches on/off) never change results; the tuner times a short calibration run per candidate
+Launch choices (`gf_tuning`: per-thread draws in lane order, warp-pooled draws or per-thread draws
+grouped by sampler branch; resident drift blocks per SM; window launches on/off) never change results; the tuner times a short calibration run per candidate
 and keeps the fastest.  The compaction cadence of batched replicates does change results (the
 Philox counter of a mutation is its slot, and compaction moves slots), so it is tuned only when the
 caller asks for it -- batched statistics, where any cadence gives a valid, differently-seeded
@@ -26,7 +26,9 @@ LAUNCH_CANDIDATES = [
     {"draw_strategy": 0, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 0, "blocks_per_sm": 4, "windows": 1},
     {"draw_strategy": 1, "blocks_per_sm": 0, "windows": 1},
+    {"draw_strategy": 2, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 0, "blocks_per_sm": 0, "windows": 0},
+    {"draw_strategy": 2, "blocks_per_sm": 0, "windows": 0},
 ]
 CADENCE_CANDIDATES = (10, 25, 50, 100)
 

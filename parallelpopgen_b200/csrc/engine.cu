@@ -76,87 +76,22 @@ gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need) {
 // ------------------------------------------------------------------------------------------------
 // the fused generation kernel
 // ------------------------------------------------------------------------------------------------
-// Work items of one warp: the draws of its 128 slots that need the sampler, compacted so that every
-// round of 32 lanes runs the same branch of the sampler.  Normal-approximation items fill the
-// arrays from the front, sequential-search items from the back.
-struct WarpDraws {
-  uint32_t bits[128];
-  float mean[128];
-  float var[128];
-  int res[128];
-  unsigned char slot[128];
-};
-
-// Draws of the four lanes of one quad.  COOP = false: each thread draws its own lanes.  COOP = true:
-// the warp pools its work items and draws them branch by branch (all 32 lanes of the warp must call
-// this together).  Both give identical results: the same function of the same (bits, mean, var, N).
 constexpr int kDriftMinBlocks = GF_DRIFT_MIN_BLOCKS;
-
-template <bool COOP>
-__device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsigned need, int N, int lane,
-                                          WarpDraws* w, int res[4]) {
-  const float Nf = static_cast<float>(N);
-  const uint32_t rb[4] = {r.x, r.y, r.z, r.w};
-  if (!COOP) {
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
-    return;
-  }
-  const unsigned lt = (1u << lane) - 1u;
-  int nN = 0, nS = 0;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const bool has = (need >> j) & 1u;
-    const float mean = xs[j] * N;
-    const float var = (1.0f - xs[j]) * mean;
-    const bool search = has && (mean <= kMeanBoundary || mean >= Nf - kMeanBoundary);
-    const bool normal = has && !search;
-    const unsigned bN = __ballot_sync(0xFFFFFFFFu, normal);
-    const unsigned bS = __ballot_sync(0xFFFFFFFFu, search);
-    int k = -1;
-    if (normal) k = nN + __popc(bN & lt);
-    if (search) k = 127 - (nS + __popc(bS & lt));
-    if (k >= 0) {
-      w->bits[k] = rb[j];
-      w->mean[k] = mean;
-      w->var[k] = var;
-      w->slot[k] = static_cast<unsigned char>(4 * lane + j);
-    }
-    nN += __popc(bN);
-    nS += __popc(bS);
-  }
-  __syncwarp();
-  for (int k = lane; k < nN; k += 32) w->res[w->slot[k]] = binom_draw_lane(w->bits[k], w->mean[k], w->var[k], Nf);
-  for (int k = lane; k < nS; k += 32) {
-    const int kk = 127 - k;
-    w->res[w->slot[kk]] = binom_draw_lane(w->bits[kk], w->mean[kk], w->var[kk], Nf);
-  }
-  __syncwarp();
-  if (need) {
-    const int4 rr = reinterpret_cast<const int4*>(w->res)[lane];
-    if (need & 1u) res[0] = rr.x;
-    if (need & 2u) res[1] = rr.y;
-    if (need & 4u) res[2] = rr.z;
-    if (need & 8u) res[3] = rr.w;
-  }
-  __syncwarp();
-}
 
 // PT: 1 = single-population specialization, 0 = any P <= kMaxPops.
 // NEUTRAL: every drifted population has s(x) == 0.
 // FLAG: compaction generation -- also write the survival bitmask and tile counts.
-// COOP: warp-cooperative draws (see draw_quad).
+// DRAW: how a warp schedules its sampler draws (DrawStrategy, see draw_quad).
 // The grid is sized by occupancy and strides over the 1024-slot tiles of the current generation,
 // whose number the kernel derives from the device-side mutation count.
-template <int PT, bool NEUTRAL, bool FLAG, bool COOP>
+template <int PT, bool NEUTRAL, bool FLAG, int DRAW>
 __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
     drift_kernel(const float* __restrict__ prev, float* __restrict__ next, int* __restrict__ id_gp,
                  int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                  int* __restrict__ d_count, unsigned long long* __restrict__ stats, long long stride, int slot_in,
                  int slot_out, long long capacity, const GenArgs* __restrict__ table) {
   __shared__ GenArgs a;
-  __shared__ WarpDraws s_draws[COOP ? kDriftThreads / 32 : 1];
+  __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kDriftThreads / 32 : 1];
   __shared__ unsigned s_warp[kDriftThreads / 32];
   {
     const int* src = reinterpret_cast<const int*>(table);
@@ -172,7 +107,7 @@ __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
   const int P = (PT > 0) ? PT : a.num_pops;
   const int g = a.generation;
   const int lane = threadIdx.x & 31;
-  WarpDraws* w = &s_draws[COOP ? (threadIdx.x >> 5) : 0];
+  WarpDraws* w = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
 
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     d_count[slot_out] = total;
@@ -223,7 +158,7 @@ __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
         }
         uint4 r = make_uint4(0u, 0u, 0u, 0u);
         if (need) r = philox(a.seed1, a.seed2, q + 2, g, p, 0);
-        draw_quad<COOP>(xs, r, need, N, lane, w, res);
+        draw_quad<DRAW>(xs, r, need, N, lane, w, res);
         const float Nf = static_cast<float>(N);
         o.x = static_cast<float>(clampi(res[0], 0, N)) / Nf;
         o.y = static_cast<float>(clampi(res[1], 0, N)) / Nf;
@@ -631,6 +566,7 @@ static gf_status begin_common(Engine* e, const gf_sim_config* c, long long initi
   e->num_sites = c->num_sites;
   e->compact_interval = c->compact_interval;
   e->any_preserved = false;
+  e->live_rows = 0;
   e->step_index = 0;
   e->count_slot = 0;
   e->cur = 0;
@@ -685,9 +621,9 @@ int host_new_mutation_count(int seed1, int seed2, float mu, int Nchrom_e, float 
   return std::max(pois_draw(lambda, lambda, Nchrom_e * num_sites, seed1, seed2, 1, generation, pop), 0);
 }
 
-template <int PT, bool NEUTRAL, bool FLAG, bool COOP>
+template <int PT, bool NEUTRAL, bool FLAG, int DRAW>
 static void launch_drift_t(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a) {
-  auto kernel = drift_kernel<PT, NEUTRAL, FLAG, COOP>;
+  auto kernel = drift_kernel<PT, NEUTRAL, FLAG, DRAW>;
   // resident blocks per SM, queried once (thread-safe initialisation; the same on every B200)
   static const int occupancy = [kernel] {
     int o = 0;
@@ -706,8 +642,11 @@ static void launch_drift_t(Engine* e, int tiles_bound, int slot_in, int slot_out
 
 template <int PT, bool NEUTRAL, bool FLAG>
 static void launch_drift_c(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a) {
-  if (e->draw_coop) launch_drift_t<PT, NEUTRAL, FLAG, true>(e, tiles_bound, slot_in, slot_out, a);
-  else launch_drift_t<PT, NEUTRAL, FLAG, false>(e, tiles_bound, slot_in, slot_out, a);
+  switch (e->draw_strategy) {
+    case kDrawWarp: launch_drift_t<PT, NEUTRAL, FLAG, kDrawWarp>(e, tiles_bound, slot_in, slot_out, a); break;
+    case kDrawGrouped: launch_drift_t<PT, NEUTRAL, FLAG, kDrawGrouped>(e, tiles_bound, slot_in, slot_out, a); break;
+    default: launch_drift_t<PT, NEUTRAL, FLAG, kDrawLanes>(e, tiles_bound, slot_in, slot_out, a); break;
+  }
 }
 
 static void launch_drift(Engine* e, int tiles_bound, int slot_in, int slot_out, const GenArgs* a, bool single,
@@ -792,6 +731,43 @@ static gf_status build_args(Engine* e, const gf_generation& gen, GenArgs& a, Gen
   return GF_OK;
 }
 
+// Compaction of the state a drift or window launch just wrote into freq[cur ^ 1] with its flags and
+// tile counts (d_count[3] = slots): exclusive scan of the tile counts (the survivor total lands in
+// d_count[slot_out]), then the stable scatter of all P rows and the IDs back into freq[cur]
+// (compact, go_fish_impl.cuh:370-429).
+static gf_status launch_compaction(Engine* e, int tiles_bound, int slot_out, bool preserve) {
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    ev0 = prof_event(e);
+    ev1 = prof_event(e);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(e->tile_count, e->tile_offset, 0, e->d_count + slot_out,
+                                                            e->d_count + 3);
+  const int sblocks = std::max(1, std::min(tiles_bound, e->num_sms * 8));
+  GF_CUDA(e, cudaGetLastError());
+  const int src = e->cur ^ 1;
+  if (preserve) {
+    scatter_kernel<true><<<sblocks, kDriftThreads, 0, e->stream>>>(
+        e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
+        e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, e->P, e->d_count + 3);
+    e->any_preserved = true;
+  } else {
+    scatter_kernel<false><<<sblocks, kDriftThreads, 0, e->stream>>>(
+        e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
+        e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, e->P, e->d_count + 3);
+  }
+  GF_CUDA(e, cudaGetLastError());
+  e->kernel_launches += 2;
+  e->compactions += 1;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_compact.emplace_back(ev0, ev1);
+  }
+  e->id_cur ^= 1;
+  return GF_OK;
+}
+
 // Launch one generation whose arguments are `h` on the host and `d` in the device table.
 static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int index, const GenHost& gh) {
   const int P = e->P;
@@ -832,6 +808,7 @@ static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int 
   launch_drift(e, tiles_bound, slot_in, slot_out, d_table + index, P == 1, gh.neutral, h.flag != 0);
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;
+  e->live_rows |= h.drift_mask;
   if (e->profiling) {
     GF_CUDA(e, cudaEventRecord(ev1, e->stream));
     e->prof_drift.emplace_back(ev0, ev1);
@@ -840,34 +817,8 @@ static gf_status launch_generation(Engine* e, GenArgs& h, GenArgs* d_table, int 
   for (auto& pc : e->pending) pc.added += new_total;
 
   if (h.flag) {
-    if (e->profiling) {
-      ev0 = prof_event(e);
-      ev1 = prof_event(e);
-      GF_CUDA(e, cudaEventRecord(ev0, e->stream));
-    }
-    scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(e->tile_count, e->tile_offset, 0,
-                                                              e->d_count + slot_out, e->d_count + 3);
-    const int sblocks = std::max(1, std::min(tiles_bound, e->num_sms * 8));
-    GF_CUDA(e, cudaGetLastError());
-    const int src = e->cur ^ 1;
-    if (gh.preserve) {
-      scatter_kernel<true><<<sblocks, kDriftThreads, 0, e->stream>>>(
-          e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
-          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P, e->d_count + 3);
-      e->any_preserved = true;
-    } else {
-      scatter_kernel<false><<<sblocks, kDriftThreads, 0, e->stream>>>(
-          e->freq[src], e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], e->id_gp[e->id_cur ^ 1],
-          e->id_tid[e->id_cur ^ 1], e->flags, e->tile_offset, e->capacity, P, e->d_count + 3);
-    }
-    GF_CUDA(e, cudaGetLastError());
-    e->kernel_launches += 2;
-    e->compactions += 1;
-    if (e->profiling) {
-      GF_CUDA(e, cudaEventRecord(ev1, e->stream));
-      e->prof_compact.emplace_back(ev0, ev1);
-    }
-    e->id_cur ^= 1;
+    gf_status cst = launch_compaction(e, tiles_bound, slot_out, gh.preserve);
+    if (cst != GF_OK) return cst;
     // asynchronous read-back of the survivor count
     poll_pending(e, false);
     PendingCount pc;
@@ -936,7 +887,31 @@ static bool window_eligible(const Engine* e, const gf_generation& g) {
   return e->use_windows && e->P == 1 && g.pop[0].drift == 1 && g.migration[0] == 1.0f;
 }
 
-constexpr int kMaxWindow = 128;
+constexpr int kMaxWindow = kMaxWindowGenerations;
+
+// Generations a multi-population window may hold (2 <= P <= 4): every population is either drifted
+// with Nc > 0, or not drifted and its rows are zero in both state buffers (`live`: the populations
+// whose rows may hold a nonzero value, given the generations before this one).  Extinction
+// generations and every generation after an extinction run one launch each.
+static bool window_mp_eligible(const Engine* e, const gf_generation& g, int live) {
+  if (!e->use_windows || e->P < 2 || e->P > kMaxWindowPops) return false;
+  for (int p = 0; p < e->P; ++p) {
+    const gf_population_params& pp = g.pop[p];
+    if (pp.drift) {
+      if (pp.Nchrom_e <= 0) return false;
+    } else if ((live >> p) & 1) {
+      return false;
+    }
+  }
+  return true;
+}
+
+static int drift_bits(const gf_generation& g, int P) {
+  int m = 0;
+  for (int p = 0; p < P; ++p)
+    if (g.pop[p].drift) m |= 1 << p;
+  return m;
+}
 
 // Run generations [first, first + count) of the batch as one window launch.
 static gf_status launch_window(Engine* e, int b, int first, int count, const GenHost* gh) {
@@ -1011,6 +986,72 @@ static gf_status launch_window(Engine* e, int b, int first, int count, const Gen
   return GF_OK;
 }
 
+// Run generations [first, first + count) of a multi-population batch as one window launch; the
+// kernel reads their records from the device table d_table[b].
+static gf_status launch_window_mp(Engine* e, int b, int first, int count, const GenHost* gh) {
+  long long news = 0;
+  int drifted = 0;
+  for (int k = 0; k < count; ++k) {
+    news += e->h_table[b][first + k].new_total;
+    drifted |= e->h_table[b][first + k].drift_mask;
+  }
+  long long need = 0;
+  gf_status st = ensure_capacity(e, news, &need);
+  if (st != GF_OK) return st;
+  const GenArgs& last = e->h_table[b][first + count - 1];
+  const bool compact = last.flag != 0;
+  const bool preserve = compact && gh[first + count - 1].preserve;
+  const int tiles_bound = static_cast<int>(align_up(std::max<long long>(need, 1), kTileSlots) / kTileSlots);
+  const int slot_in = e->count_slot;
+  const int slot_out = slot_in ^ 1;
+  WindowMpLaunch w;
+  w.P = e->P;
+  w.A = e->freq[e->cur];
+  w.B = e->freq[e->cur ^ 1];
+  w.stride = e->capacity;
+  w.id_gp = e->id_gp[e->id_cur];
+  w.id_tid = e->id_tid[e->id_cur];
+  w.flags = e->flags;
+  w.tile_count = e->tile_count;
+  w.d_count = e->d_count;
+  w.slot_in = slot_in;
+  w.slot_out = slot_out;
+  w.table = e->d_table[b] + first;
+  w.ngen = count;
+  w.births = news;
+  w.compact = compact ? 1 : 0;
+  w.check_preserved = e->any_preserved ? 1 : 0;
+  w.seed1 = e->seed1;
+  w.seed2 = e->seed2;
+  w.stats = e->d_stats;
+  w.tiles_bound = tiles_bound;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    ev0 = prof_event(e);
+    ev1 = prof_event(e);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  st = window_mp_run(e, w);
+  if (st != GF_OK) return st;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_drift.emplace_back(ev0, ev1);
+  }
+  e->live_rows |= drifted;
+  e->M_upper = need;
+  for (auto& pc : e->pending) pc.added += news;
+  e->step_index += count;
+  if (compact) {
+    st = launch_compaction(e, tiles_bound, slot_out, preserve);
+    if (st != GF_OK) return st;
+    e->count_slot ^= 1;
+    return push_readback(e, e->count_slot);
+  }
+  e->cur ^= 1;
+  e->count_slot ^= 1;
+  return GF_OK;
+}
+
 // Run a batch of generations: evaluate all records on the host, upload them as one table, launch.
 static gf_status run_batch(Engine* e, const gf_generation* gens, int n) {
   const int b = e->table_next;
@@ -1068,9 +1109,22 @@ static gf_status run_batch(Engine* e, const gf_generation* gens, int n) {
   GF_CUDA(e, cudaMemcpyAsync(e->d_table[b], e->h_table[b], sizeof(GenArgs) * n, cudaMemcpyHostToDevice, e->stream));
   if (windows)
     GF_CUDA(e, cudaMemcpyAsync(e->d_wgen[b], e->h_wgen[b], sizeof(WinGen) * n, cudaMemcpyHostToDevice, e->stream));
+  const bool windows_mp = e->use_windows && e->P >= 2 && e->P <= kMaxWindowPops;
   int i = 0;
   while (i < n) {
-    if (windows && window_eligible(e, gens[i])) {
+    if (windows_mp && window_mp_eligible(e, gens[i], e->live_rows)) {
+      int j = i;
+      int live = e->live_rows;
+      while (j < n && j - i < kMaxWindow && window_mp_eligible(e, gens[j], live)) {
+        live |= drift_bits(gens[j], e->P);
+        const bool ends = e->h_table[b][j].flag != 0;
+        ++j;
+        if (ends) break;
+      }
+      gf_status st = launch_window_mp(e, b, i, j - i, gh.data());
+      if (st != GF_OK) return st;
+      i = j;
+    } else if (windows && window_eligible(e, gens[i])) {
       int j = i;
       while (j < n && j - i < kMaxWindow && window_eligible(e, gens[j])) {
         const bool ends = e->h_table[b][j].flag != 0;
@@ -1254,6 +1308,14 @@ gf_status gf_sim_begin_from_state(gf_engine* g, const gf_sim_config* c, int32_t 
   const int P = e->P;
   GF_CUDA(e, cudaMemcpy2DAsync(e->freq[e->cur], sizeof(float) * e->capacity, freq, sizeof(float) * num_mutations,
                                sizeof(float) * num_mutations, P, cudaMemcpyHostToDevice, e->stream));
+  for (int p = 0; p < P; ++p) {  // rows holding anything but +0.0 (bit pattern 0)
+    const uint32_t* row = reinterpret_cast<const uint32_t*>(freq + static_cast<size_t>(p) * num_mutations);
+    for (int i = 0; i < num_mutations; ++i)
+      if (row[i] != 0u) {
+        e->live_rows |= 1 << p;
+        break;
+      }
+  }
   std::vector<int> gp(num_mutations), tid(num_mutations);
   bool any_neg = false;
   for (int i = 0; i < num_mutations; ++i) {
@@ -1349,6 +1411,8 @@ gf_status gf_sim_begin_mse(gf_engine* g, const gf_sim_config* c, const gf_mse_po
       if (err != cudaSuccess) st = cuda_fail(e, err, "cudaMemcpyAsync");
     }
     e->any_preserved = preserve != 0;
+    for (int p = 0; p < P; ++p)  // populations with equilibrium mutations (the others' rows stay zero)
+      if (pops[p].Nchrom_e > 1) e->live_rows |= 1 << p;
   }
   cudaFreeAsync(d_counts, e->stream);
   cudaFreeAsync(d_starts, e->stream);
@@ -1431,9 +1495,10 @@ gf_status gf_sim_stats_read(gf_engine* g, gf_sim_stats* out) {
 gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
   if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
   Engine* e = &g->impl;
-  if (t->draw_strategy < 0 || t->draw_strategy > 1 || t->blocks_per_sm < 0 || t->windows < 0 || t->windows > 1)
-    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1}, blocks_per_sm >= 0, windows in {0, 1}");
-  e->draw_coop = t->draw_strategy;
+  if (t->draw_strategy < 0 || t->draw_strategy >= kDrawStrategies || t->blocks_per_sm < 0 || t->windows < 0 ||
+      t->windows > 1)
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2}, blocks_per_sm >= 0, windows in {0, 1}");
+  e->draw_strategy = t->draw_strategy;
   e->blocks_per_sm = t->blocks_per_sm;
   e->use_windows = t->windows != 0;
   return GF_OK;
@@ -1441,7 +1506,7 @@ gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
 
 gf_status gf_engine_get_tuning(const gf_engine* g, gf_tuning* t) {
   if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
-  t->draw_strategy = g->impl.draw_coop;
+  t->draw_strategy = g->impl.draw_strategy;
   t->blocks_per_sm = g->impl.blocks_per_sm;
   t->windows = g->impl.use_windows ? 1 : 0;
   return GF_OK;

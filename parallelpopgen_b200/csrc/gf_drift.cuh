@@ -10,6 +10,10 @@
 #ifndef GF_DRIFT_MIN_BLOCKS
 #define GF_DRIFT_MIN_BLOCKS 6
 #endif
+// The same bound for the window kernel (its state lives in registers across a whole window).
+#ifndef GF_WINDOW_MIN_BLOCKS
+#define GF_WINDOW_MIN_BLOCKS GF_DRIFT_MIN_BLOCKS
+#endif
 
 namespace gf {
 
@@ -57,5 +61,110 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return max(lo, mi
 #define GF_LANE_DRAW binom_draw_body
 #endif
 
+
+// How the draws of a warp's quads are scheduled.  All three give identical results: every lane
+// calls the same sampler on the same (bits, mean, var, N); only the order of the calls differs.
+enum DrawStrategy : int {
+  kDrawLanes = 0,    // each thread draws its needed lanes in lane order
+  kDrawWarp = 1,     // the warp pools its draws in shared memory and runs them branch by branch
+  kDrawGrouped = 2,  // each thread draws its normal-branch lanes first, then its search-branch lanes
+};
+constexpr int kDrawStrategies = 3;
+
+// Sampler branch of a lane (binom_draw_body): the sequential searches for mean <= 6 or
+// mean >= N - 6, the normal approximation otherwise.
+__device__ __forceinline__ bool search_branch(float mean, float Nf) {
+  return mean <= kMeanBoundary || mean >= Nf - kMeanBoundary;
+}
+
+// Work items of one warp for kDrawWarp: the draws of its 128 slots that need the sampler, compacted
+// so that every round of 32 lanes runs the same branch of the sampler.  Normal-approximation items
+// fill the arrays from the front, sequential-search items from the back.  The results are read
+// back four at a time (int4), so the struct is 16-byte aligned wherever it is declared.
+struct __align__(16) WarpDraws {
+  uint32_t bits[128];
+  float mean[128];
+  float var[128];
+  int res[128];
+  unsigned char slot[128];
+};
+static_assert(alignof(WarpDraws) == 16 && sizeof(WarpDraws) % 16 == 0, "int4 reads of WarpDraws::res");
+
+// Draws of the lanes of one quad whose bit is set in `need` (res[j] keeps its value elsewhere).
+// kDrawWarp must be called by all 32 lanes of the warp together; `w` is only used by it.
+template <int DRAW>
+__device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsigned need, int N, int lane,
+                                          WarpDraws* w, int res[4]) {
+  const float Nf = static_cast<float>(N);
+  const uint32_t rb[4] = {r.x, r.y, r.z, r.w};
+  if (DRAW == kDrawLanes) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
+    return;
+  }
+  if (DRAW == kDrawGrouped) {
+    // A warp's lanes mix both branches at almost every lane position, so drawing lane j of every
+    // thread at once runs both branches four times; grouping a thread's lanes by branch runs the
+    // normal branch (at most) four times and the search branch only as often as the thread with
+    // the most search lanes needs.  The lane is picked by selects, keeping the quad in registers.
+    unsigned search = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (((need >> j) & 1u) && search_branch(xs[j] * N, Nf)) search |= 1u << j;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      for (unsigned m = pass ? search : (need & ~search); m; m &= m - 1u) {
+        const int j = __ffs(m) - 1;
+        const float x = j == 0 ? xs[0] : j == 1 ? xs[1] : j == 2 ? xs[2] : xs[3];
+        const uint32_t b = j == 0 ? rb[0] : j == 1 ? rb[1] : j == 2 ? rb[2] : rb[3];
+        const int d = GF_LANE_DRAW(b, x * N, (1.0f - x) * (x * N), Nf);
+        res[0] = j == 0 ? d : res[0];
+        res[1] = j == 1 ? d : res[1];
+        res[2] = j == 2 ? d : res[2];
+        res[3] = j == 3 ? d : res[3];
+      }
+    }
+    return;
+  }
+  const unsigned lt = (1u << lane) - 1u;
+  int nN = 0, nS = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const bool has = (need >> j) & 1u;
+    const float mean = xs[j] * N;
+    const float var = (1.0f - xs[j]) * mean;
+    const bool search = has && search_branch(mean, Nf);
+    const bool normal = has && !search;
+    const unsigned bN = __ballot_sync(0xFFFFFFFFu, normal);
+    const unsigned bS = __ballot_sync(0xFFFFFFFFu, search);
+    int k = -1;
+    if (normal) k = nN + __popc(bN & lt);
+    if (search) k = 127 - (nS + __popc(bS & lt));
+    if (k >= 0) {
+      w->bits[k] = rb[j];
+      w->mean[k] = mean;
+      w->var[k] = var;
+      w->slot[k] = static_cast<unsigned char>(4 * lane + j);
+    }
+    nN += __popc(bN);
+    nS += __popc(bS);
+  }
+  __syncwarp();
+  for (int k = lane; k < nN; k += 32) w->res[w->slot[k]] = GF_LANE_DRAW(w->bits[k], w->mean[k], w->var[k], Nf);
+  for (int k = lane; k < nS; k += 32) {
+    const int kk = 127 - k;
+    w->res[w->slot[kk]] = GF_LANE_DRAW(w->bits[kk], w->mean[kk], w->var[kk], Nf);
+  }
+  __syncwarp();
+  if (need) {
+    const int4 rr = reinterpret_cast<const int4*>(w->res)[lane];
+    if (need & 1u) res[0] = rr.x;
+    if (need & 2u) res[1] = rr.y;
+    if (need & 4u) res[2] = rr.z;
+    if (need & 8u) res[3] = rr.w;
+  }
+  __syncwarp();
+}
 
 }  // namespace gf

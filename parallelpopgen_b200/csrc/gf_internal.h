@@ -100,6 +100,33 @@ struct WindowLaunch {
   int* fault;
 };
 
+// Longest window (generations per window launch).
+constexpr int kMaxWindowGenerations = 128;
+
+// One multi-population window launch of the plain engine (window_mp.cu): generations
+// table[0 .. ngen) from state A into state B, counts in d_count[slot_in] -> d_count[slot_out] (and
+// d_count[3]), compaction flags and tile counts after the last generation when `compact`.
+struct WindowMpLaunch {
+  int P;
+  const float* A;
+  float* B;
+  long long stride;          // row stride of A and B in slots (= the capacity)
+  int* id_gp;
+  int* id_tid;
+  unsigned* flags;
+  unsigned* tile_count;
+  int* d_count;
+  int slot_in, slot_out;
+  const GenArgs* table;      // device
+  int ngen;
+  long long births;          // new mutations over the window (host draws)
+  int compact;
+  int check_preserved;
+  int seed1, seed2;
+  unsigned long long* stats;
+  int tiles_bound;           // launch tiles (an upper bound of the end-of-window tiles)
+};
+
 // Host record of one replicate of a batch.
 struct BatchRep {
   gf_replicate p;
@@ -166,7 +193,7 @@ struct PendingCount {
 struct Engine {
   int device = 0;
   int num_sms = 148;
-  int draw_coop = 0;       // 1: warp-cooperative draws
+  int draw_strategy = 0;   // DrawStrategy of the drift and window kernels
   int blocks_per_sm = 0;   // drift grid limit per SM (0: occupancy maximum)
   long long batch_record_budget = 64ll << 20;   // batches up to this many records are precomputed
   cudaStream_t stream = nullptr;
@@ -183,6 +210,7 @@ struct Engine {
   float num_sites = 0.f;
   int compact_interval = 0;
   bool any_preserved = false;
+  int live_rows = 0;         // bit p: row p may hold a nonzero value in either state buffer
   long long step_index = 0;  // generations run since begin
   int count_slot = 0;        // d_count slot holding the current mutation count
 
@@ -261,6 +289,9 @@ gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
 void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
                         int* total_out);
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst);
+// Multi-population window launch (window_mp.cu); P in [2, 4].
+gf_status window_mp_run(Engine* e, const WindowMpLaunch& w);
+constexpr int kMaxWindowPops = 4;
 
 // Host draw of one population's new-mutation count (engine.cu).
 int host_new_mutation_count(int seed1, int seed2, float mu, int Nchrom_e, float num_sites, int generation, int pop);

@@ -109,7 +109,9 @@ __global__ void __launch_bounds__(1024) batch_tiles_kernel(WinRep* __restrict__ 
   if (threadIdx.x == 0) *total = s_carry;
 }
 
-__global__ void __launch_bounds__(kWinThreads, GF_DRIFT_MIN_BLOCKS)
+// DRAW: how a warp schedules its sampler draws (DrawStrategy).
+template <int DRAW>
+__global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     window_kernel(const float* __restrict__ A, float* __restrict__ B, int* __restrict__ id_gp,
                   int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
@@ -119,7 +121,9 @@ __global__ void __launch_bounds__(kWinThreads, GF_DRIFT_MIN_BLOCKS)
   __shared__ int s_rep;
   __shared__ unsigned s_warp[kWinThreads / 32];
   __shared__ int s_tile0[kRepCache];
+  __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinThreads / 32 : 1];
   const int lane = threadIdx.x & 31;
+  WarpDraws* wd = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
   load_tile0(s_tile0, reps, nreps);
   for (int gt = blockIdx.x; gt < ntiles_all; gt += gridDim.x) {
@@ -156,48 +160,50 @@ __global__ void __launch_bounds__(kWinThreads, GF_DRIFT_MIN_BLOCKS)
       const int N = G.Nc;
       const int g = G.generation;
       alive = G.alive;
-      if (s0 < M) {
-        if (N <= 0) {
-          // extinction generation: the population's row is cleared
+      if (N <= 0) {
+        // extinction generation: the population's row is cleared
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (s0 + j < M) x[j] = 0.f;
-        } else if (q < (M >> 2)) {
-          // whole quad: Philox (q + 2, g, 0, 0), lanes x, y, z, w
-          const bool neutral = (G.sel_a == 0.f && G.sel_b == 0.f);
-          float xs[4];
+        for (int j = 0; j < 4; ++j)
+          if (s0 + j < M) x[j] = 0.f;
+      } else {
+        // whole quad: Philox (q + 2, g, 0, 0), lanes x, y, z, w.  Every lane of the warp reaches the
+        // draw (N and the loop are uniform over the block), as the warp-pooled strategy requires.
+        const bool quad = q < (M >> 2);
+        const bool neutral = (G.sel_a == 0.f && G.sel_b == 0.f);
+        float xs[4] = {0.f, 0.f, 0.f, 0.f};
+        int res[4] = {0, 0, 0, 0};
+        unsigned need = 0;
+        if (quad) {
 #pragma unroll
           for (int j = 0; j < 4; ++j)
             xs[j] = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
                             : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
-          int res[4];
-          unsigned need = 0;
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             res[j] = (xs[j] == 1.f && N > 6) ? N : 0;
             if (!(xs[j] == 0.f || (xs[j] == 1.f && N > 6))) need |= 1u << j;
           }
-          if (need) {
-            const uint4 r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
-            const uint32_t rb[4] = {r.x, r.y, r.z, r.w};
-            const float Nf = static_cast<float>(N);
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-              if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
-          }
+        }
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);
+        if (need) r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
+        if (DRAW == kDrawWarp) {
+          draw_quad<kDrawWarp>(xs, r, need, N, lane, wd, res);
+        } else if (need) {
+          draw_quad<DRAW>(xs, r, need, N, lane, wd, res);
+        }
+        if (quad) {
           const float Nf = static_cast<float>(N);
 #pragma unroll
           for (int j = 0; j < 4; ++j) x[j] = static_cast<float>(clampi(res[j], 0, N)) / Nf;
-        } else {
+        } else if (s0 < M) {
           // scalar tail: Philox (slot + 2, g, 0, 0) lane x, variance in double
-          const bool neutral = (G.sel_a == 0.f && G.sel_b == 0.f);
 #pragma unroll 1
           for (int j = 0; j < 4; ++j) {
             const int e = s0 + j;
             if (e >= M) break;
-            const float xs = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
-                                     : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
-            x[j] = static_cast<float>(clampi(drift_tail(R.seed1, R.seed2, e, g, 0, xs, N), 0, N)) /
+            const float xs1 = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
+                                      : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
+            x[j] = static_cast<float>(clampi(drift_tail(R.seed1, R.seed2, e, g, 0, xs1, N), 0, N)) /
                    static_cast<float>(N);
           }
         }
@@ -396,19 +402,20 @@ __global__ void __launch_bounds__(kWinThreads)
   }
 }
 
-// Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
-// and scatter into `compact_dst` (the other state buffer).
+// Tile assignment of a batched super-step (batch_tiles_kernel), on the engine stream.
 void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
                         int* total_out) {
   batch_tiles_kernel<<<1, 1024, 0, e->stream>>>(d_reps, nreps, M_in, recs, total_out);
   e->kernel_launches += 1;
 }
 
-gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
-  // resident blocks per SM, queried once (thread-safe initialisation; the same on every B200)
+template <int DRAW>
+static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
+  // resident blocks per SM, queried once per strategy (thread-safe initialisation; the same on every B200)
   static const int occupancy = [] {
     int o = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel, kWinThreads, 0) != cudaSuccess || o < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel<DRAW>, kWinThreads, 0) != cudaSuccess ||
+        o < 1) {
       cudaGetLastError();
       o = 1;
     }
@@ -416,9 +423,19 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
   }();
   const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
   const int blocks = std::max(1, std::min(w.total_tiles, e->num_sms * per_sm));
-  window_kernel<<<blocks, kWinThreads, 0, e->stream>>>(w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count,
-                                                       w.M_in, w.M_end, w.M_next, w.reps, w.nreps, w.recs,
-                                                       w.total_tiles, w.total_tiles_dev, w.stats, w.fault);
+  window_kernel<DRAW><<<blocks, kWinThreads, 0, e->stream>>>(
+      w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count, w.M_in, w.M_end, w.M_next, w.reps, w.nreps,
+      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault);
+}
+
+// Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
+// and scatter into `compact_dst` (the other state buffer).
+gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
+  switch (e->draw_strategy) {
+    case kDrawWarp: launch_window_kernel<kDrawWarp>(e, w); break;
+    case kDrawGrouped: launch_window_kernel<kDrawGrouped>(e, w); break;
+    default: launch_window_kernel<kDrawLanes>(e, w); break;
+  }
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;
   if (w.any_compact) {

@@ -262,3 +262,29 @@ def test_window_path_equals_per_generation_path(gamma, ci, mse):
     assert np.array_equal(f1.view(np.uint32), f0.view(np.uint32))
     assert np.array_equal(i1, i0)
     assert m1 == m0
+
+
+@pytest.mark.parametrize("pops", [1, 3])
+def test_draw_strategies_agree(pops):
+    """The three draw schedules (lane order, warp-pooled, grouped by sampler branch) call the same
+    sampler on the same inputs, so window and per-generation runs, single- and multi-population,
+    give the same state bit for bit under every one of them."""
+    N = 4000
+    if pops == 1:
+        model = ConstantModel(N=N, s=ConstantModel.s_from_gamma(-4.0, N, 0.0), mu=2e-8, h=0.3)
+    else:
+        model = ConstantModel(N=N, s=ConstantModel.s_from_gamma(-4.0, N, 0.0), mu=2e-8, h=0.3, P=3, m=0.01)
+    gens = constant_generations(model, 1, 200, 25)
+    out = []
+    for strategy in (0, 1, 2):
+        for windows in ((1, 0) if pops == 1 else (1,)):
+            with Engine() as e:
+                e.set_tuning(draw_strategy=strategy, windows=windows)
+                e.begin_mse(model.mse_pops(), seed1=11, seed2=13, num_sites=4e6, compact_interval=25)
+                e.run(gens)
+                out.append(((strategy, windows),) + e.read_state())
+    (_, f0, i0) = out[0]
+    assert f0.shape[1] > 1000
+    for key, f, ids in out[1:]:
+        assert np.array_equal(f.view(np.uint32), f0.view(np.uint32)), key
+        assert np.array_equal(ids, i0), key
