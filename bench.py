@@ -47,6 +47,11 @@ GAMMA_SEL = -10.0
 H = 0.5
 SEED1, SEED2 = 0xBEEF, 0xDECAF
 ALG_BYTES_PER_MUTGEN = 8  # P = 1: read one fp32 frequency, write one fp32 frequency
+# Thread instructions per mutation-generation of the window kernel on this workload (ncu
+# smsp__inst_executed x threads per instruction / mutation-generations of one launch: 72, neutral half),
+# the figure behind the instruction-issue ceiling reported beside the HBM roofline.
+THREAD_INSTR_PER_MUTGEN = 72
+B200_SMS, SCHEDULERS_PER_SM = 148, 4
 
 
 def dist_env():
@@ -307,7 +312,8 @@ def run_b200(args, rank, local_rank, world):
         "gpu_launches": int(launches),
         "roofline": {
             "bound": "hbm",
-            "kernel": "drift_kernel (fused migration/selection/drift + new mutations + compaction flags)",
+            "kernel": "window_kernel (every generation of a compaction window per launch: selection, drift, "
+                      "births, compaction flags) with its segmented scan and scatter",
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
@@ -323,6 +329,15 @@ def run_b200(args, rank, local_rank, world):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
+    # the kernel is issue-bound: its rate against the instruction-issue ceiling at full warps
+    mhz = line["clocks"].get("sm_mhz") or 1965.0
+    issue_ceiling = B200_SMS * SCHEDULERS_PER_SM * mhz * 1e6 * 32 / THREAD_INSTR_PER_MUTGEN
+    if achieved:
+        line["roofline"]["issue"] = {
+            "thread_instructions_per_mutation_generation": THREAD_INSTR_PER_MUTGEN,
+            "ceiling": issue_ceiling, "unit": "mutation-generations/s",
+            "frac": achieved * 1e9 / ALG_BYTES_PER_MUTGEN / issue_ceiling,
+        }
     print(json.dumps(line), flush=True)
 
 
@@ -347,13 +362,14 @@ def cpu_sample(threads: int, gens: int, seed: int = 1):
     return mg, dt
 
 
-def cpu_baseline_sample(threads: int, gens: int = 40, serial_gens: int = 4):
-    """The CPU restatement on all host threads (the baseline) and, on a shorter sample, on one thread."""
+def cpu_baseline_sample(threads: int, gens: int = 80, serial_gens: int = 8):
+    """The CPU restatement on all host threads (the baseline) and, on a shorter sample, on one thread
+    (about 20 core-seconds of work in all)."""
     mg, dt = cpu_sample(threads, gens)
     smg, sdt = cpu_sample(1, serial_gens)
     return {"value": mg / dt, "unit": "mutation-generations/s", "cores": threads, "kind": "port",
             "sample": f"{gens} generations of the neutral half (Nchrom_e 400,000, L 2.5e8, ~2.7M mutations) "
-                      f"from a synthetic equilibrium state; {dt:.1f} s of CPU time",
+                      f"from a synthetic equilibrium state; {dt:.1f} s wall on {threads} threads",
             "serial": {"value": smg / sdt, "cores": 1,
                        "sample": f"{serial_gens} generations of the same state on one thread; {sdt:.1f} s"}}
 
