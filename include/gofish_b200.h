@@ -203,9 +203,11 @@ typedef struct gf_batch_stats {
 gf_status gf_batch_stats_read(gf_engine* engine, gf_batch_stats* out);
 /* Generation records (one per replicate per generation, 36 bytes, page-locked on the host and on
  * the device) the batched engine keeps resident: a batch within the budget (default 67,108,864) has
- * all its records computed at gf_batch_begin; a larger one keeps two chunks per replicate, refilled
- * ahead of the GPU; 0 builds each super-step's records on the host and reads the counts back per
- * super-step.  Results are identical in every case.  Takes effect at the next gf_batch_begin. */
+ * all its records resident -- drawn by host threads region by region (about 512 generations of every
+ * replicate per region) while the first super-steps run, or at gf_batch_begin below 131,072 records;
+ * a larger one keeps two chunks per replicate, refilled ahead of the GPU; 0 builds each super-step's
+ * records on the host and reads the counts back per super-step.  Results are identical in every
+ * case.  Takes effect at the next gf_batch_begin. */
 gf_status gf_batch_set_record_budget(gf_engine* engine, int64_t records);
 
 /* ---------------------------------------------------------------------------------------------

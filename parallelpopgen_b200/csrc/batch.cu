@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -287,6 +288,9 @@ __global__ void __launch_bounds__(kBatchSfsThreads)
 void release_batch(Engine* e) {
   Batch* b = e->batch;
   if (!b) return;
+  b->cancel.store(true);
+  for (auto& t : b->producers) t.join();
+  b->producers.clear();
   cudaStreamSynchronize(e->stream);
   auto release = [e](void* p) {
     if (p) cudaFreeAsync(p, e->stream);
@@ -368,8 +372,9 @@ static void make_record(const gf_replicate& p, int g, WinGen& w) {
 // Records depend only on each replicate's seeds and size trajectory, so they are computed ahead of
 // the GPU (host threads over replicates, into the engine's page-locked staging buffer, kept across
 // batches) and uploaded in bulk; super-steps then need neither host record work nor a read-back.
-// A batch within the engine's record budget has all its records resident; a larger one keeps two
-// regions per replicate of `chunk` generations (a multiple of its cadence, so no window straddles
+// A batch within the engine's record budget has all its records resident (streamed by host threads
+// while the super-steps run, see start_streamed_records, or drawn at begin when it is small); a
+// larger one keeps two regions per replicate of `chunk` generations (a multiple of its cadence, so no window straddles
 // two chunks), and chunk j + 1 is computed and uploaded when a replicate enters chunk j -- into the
 // region chunk j - 1 used, after (in stream order) the super-steps that read it.
 
@@ -421,12 +426,127 @@ static gf_status fill_chunks(Engine* e, Batch* b, const std::vector<std::pair<in
   return GF_OK;
 }
 
+// Streamed records (a resident batch of at least kStreamMinRecords records): the slabs of region 0
+// are drawn first, and the GPU starts as soon as region 0 is uploaded, while host threads draw the
+// later regions.  A replicate's slab is kStreamSlab generations rounded up to a multiple of its
+// cadence, so no window straddles two regions, and every replicate reaches region j after about the
+// same number of generations -- the regions are drawn in the order the super-steps need them.
+constexpr long long kStreamMinRecords = 1 << 17;
+constexpr int kStreamSlab = 512;
+
+static void produce_records(Batch* b, WinGen* stage) {
+  const long long R = b->R;
+  const long long jobs = R * b->nregions;
+  for (;;) {
+    if (b->cancel.load(std::memory_order_relaxed)) return;
+    const long long i = b->next_job.fetch_add(1, std::memory_order_relaxed);
+    if (i >= jobs) return;
+    const int j = static_cast<int>(i / R), r = static_cast<int>(i % R);
+    const int off = b->region_off[static_cast<size_t>(r) * b->nregions + j];
+    if (off < 0) continue;
+    const BatchRep& br = b->reps[r];
+    const int g0 = j * br.chunk;
+    const int g1 = std::min(br.p.num_generations, g0 + br.chunk);
+    WinGen* out = stage + b->region_base[j] + off;
+    for (int g = g0 + 1; g <= g1; ++g) make_record(br.p, g, out[g - g0 - 1]);
+    b->region_done[j].fetch_add(1, std::memory_order_release);
+  }
+}
+
+static gf_status start_streamed_records(Engine* e, Batch* b, long long total) {
+  int nreg = 0;
+  for (auto& br : b->reps) {
+    const int G = br.p.num_generations;
+    const int c = std::max(br.p.compact_interval, 1);
+    br.chunk = c * ((kStreamSlab + c - 1) / c);
+    br.regions = 1;
+    br.rec0 = 0;
+    br.filled = 0;
+    nreg = std::max(nreg, (G + br.chunk - 1) / br.chunk);
+  }
+  b->nregions = nreg;
+  b->region_off.assign(static_cast<size_t>(b->R) * nreg, -1);
+  b->region_base.assign(nreg + 1, 0);
+  b->region_jobs.assign(nreg, 0);
+  long long off = 0;
+  for (int j = 0; j < nreg; ++j) {
+    b->region_base[j] = off;
+    for (int r = 0; r < b->R; ++r) {
+      const BatchRep& br = b->reps[r];
+      const int g0 = j * br.chunk;
+      if (g0 >= br.p.num_generations) continue;
+      b->region_off[static_cast<size_t>(r) * nreg + j] = static_cast<int>(off - b->region_base[j]);
+      off += std::min(br.p.num_generations, g0 + br.chunk) - g0;
+      b->region_jobs[j] += 1;
+    }
+  }
+  b->region_base[nreg] = off;
+  if (off != total) return fail(e, GF_ERR_STATE, "streamed record layout holds %lld of %lld records", off, total);
+  if (e->h_rec_stage_cap < static_cast<size_t>(total)) {
+    if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
+    e->h_rec_stage = nullptr;
+    e->h_rec_stage_cap = 0;
+    const size_t cap = static_cast<size_t>(total) + static_cast<size_t>(total) / 4;
+    GF_CUDA(e, cudaMallocHost(&e->h_rec_stage, sizeof(WinGen) * cap));
+    e->h_rec_stage_cap = cap;
+  }
+  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * total);
+  if (st != GF_OK) return st;
+  b->region_done.reset(new std::atomic<long long>[nreg]);
+  for (int j = 0; j < nreg; ++j) b->region_done[j].store(0);
+  b->next_job.store(0);
+  b->cancel.store(false);
+  b->uploaded = 0;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const long long want = std::max<long long>(1, total / 65536);
+  const int workers = static_cast<int>(std::min<long long>(want, std::max(1u, std::min(hw - 1, 31u))));
+  WinGen* stage = e->h_rec_stage;
+  for (int t = 0; t < workers; ++t) b->producers.emplace_back(produce_records, b, stage);
+  b->streamed = true;
+  b->precomputed = true;
+  return GF_OK;
+}
+
+// Upload every region whose slabs are all drawn, in order; regions below `need` are waited for
+// (bounded: producers that make no progress for two minutes are reported as a state error).
+static gf_status stream_upload(Engine* e, Batch* b, int need) {
+  while (b->uploaded < b->nregions) {
+    const int j = b->uploaded;
+    if (b->region_done[j].load(std::memory_order_acquire) != b->region_jobs[j]) {
+      if (j >= need) break;
+      const auto t0 = std::chrono::steady_clock::now();
+      long long last = -1;
+      auto progress = t0;
+      for (;;) {
+        const long long d = b->region_done[j].load(std::memory_order_acquire);
+        if (d == b->region_jobs[j]) break;
+        const auto now = std::chrono::steady_clock::now();
+        if (d != last) {
+          last = d;
+          progress = now;
+        } else if (now - progress > std::chrono::seconds(120)) {
+          return fail(e, GF_ERR_STATE, "record producers made no progress on region %d for 120 s", j);
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+      }
+    }
+    const long long a = b->region_base[j], n = b->region_base[j + 1] - a;
+    if (n > 0)
+      GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs + a, e->h_rec_stage + a, sizeof(WinGen) * n, cudaMemcpyHostToDevice,
+                                 e->stream));
+    b->uploaded += 1;
+  }
+  return GF_OK;
+}
+
 static gf_status precompute_records(Engine* e, Batch* b) {
   long long total = 0;
   for (auto& br : b->reps) total += br.p.num_generations;
   b->precomputed = false;
+  b->streamed = false;
   if (e->batch_record_budget <= 0 || total == 0) return GF_OK;
   const bool resident = total <= e->batch_record_budget;
+  if (resident && total >= kStreamMinRecords) return start_streamed_records(e, b, total);
   const long long target = std::max<long long>(64, e->batch_record_budget / (2ll * b->R));
   long long off = 0;
   for (auto& br : b->reps) {
@@ -683,7 +803,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   // a replicate entering chunk j gets chunk j + 1 computed and uploaded now (into the region chunk
   // j - 1 used, after the super-steps that read it in stream order)
   std::vector<std::pair<int, int>> refill;
-  for (int r = 0; r < b->R; ++r) {
+  for (int r = 0; r < b->R && !b->streamed; ++r) {
     const BatchRep& br = b->reps[r];
     if (br.done || br.regions != 2) continue;
     const int j = br.generation / br.chunk;
@@ -695,19 +815,26 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
   WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->R;
   WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->R;
-  int nj = 0, tiles = 0;
+  int nj = 0, tiles = 0, need_regions = 0;
   for (int r = 0; r < b->R; ++r) {
     BatchRep& br = b->reps[r];
     if (br.done) continue;
     const int end = std::min(br.next_compact, br.p.num_generations);
     const int ngen = end - br.generation;
     const int j = br.generation / br.chunk;
-    if (br.filled < j) return fail(e, GF_ERR_STATE, "replicate %d: record chunk %d not resident", r, j);
     WinRep& w = hr[nj++];
+    if (b->streamed) {
+      const int off = (j < b->nregions) ? b->region_off[static_cast<size_t>(r) * b->nregions + j] : -1;
+      if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
+      w.rec = static_cast<int>(b->region_base[j] + off + (br.generation - static_cast<long long>(j) * br.chunk));
+      need_regions = std::max(need_regions, j + 1);
+    } else {
+      if (br.filled < j) return fail(e, GF_ERR_STATE, "replicate %d: record chunk %d not resident", r, j);
+      w.rec = static_cast<int>((j % br.regions) * b->region_stride + br.rec0 +
+                               (br.generation - static_cast<long long>(j) * br.chunk));
+    }
     w.base = br.base;
     w.capacity = br.capacity;
-    w.rec = static_cast<int>((j % br.regions) * b->region_stride + br.rec0 +
-                             (br.generation - static_cast<long long>(j) * br.chunk));
     w.ngen = ngen;
     w.tile0 = tiles;
     w.ntiles = static_cast<int>(br.capacity / kBatchTile);
@@ -723,6 +850,10 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   if (nj == 0) {
     if (active_out) *active_out = 0;
     return GF_OK;
+  }
+  if (b->streamed) {
+    gf_status ust = stream_upload(e, b, need_regions);   // the records of this super-step, in stream order
+    if (ust != GF_OK) return ust;
   }
   GF_CUDA(e, cudaMemcpyAsync(dr, hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));
   // each replicate's tiles from its device-side count: only its live slots are visited

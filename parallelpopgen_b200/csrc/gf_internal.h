@@ -3,10 +3,13 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <deque>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gofish_b200.h"
@@ -182,6 +185,19 @@ struct Batch {
   int ring = 0;
   bool counts_stale = false;          // counts on the device are newer than reps[].M
   int* d_total_tiles = nullptr;       // tiles of the current super-step, assigned on the device
+  // streamed records: host threads draw the records region by region (region j holds slab j -- the
+  // generations (j * chunk, (j + 1) * chunk] -- of every replicate that runs that long) while the GPU
+  // runs the super-steps; each region is uploaded once all of its slabs are drawn
+  bool streamed = false;
+  int nregions = 0;
+  int uploaded = 0;                           // regions uploaded so far
+  std::vector<long long> region_base;         // first record of region j (nregions + 1 entries)
+  std::vector<long long> region_jobs;         // slabs in region j
+  std::vector<int> region_off;                // [r * nregions + j]: offset of replicate r's slab in region j
+  std::unique_ptr<std::atomic<long long>[]> region_done;   // slabs drawn per region
+  std::atomic<long long> next_job{0};         // producers' job counter (region-major over replicates)
+  std::atomic<bool> cancel{false};
+  std::vector<std::thread> producers;
 };
 
 struct PendingCount {

@@ -77,6 +77,32 @@ def test_batched_super_steps_are_resumable():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+def test_streamed_records_agree():
+    """A resident batch of at least 2**17 generation records has its records drawn by host threads
+    region by region while the super-steps run; it must give the same states as the chunked path
+    (a small budget) and the per-super-step path (budget 0), also when run in chunks of super-steps."""
+    reps = make_replicates(64, seed=29, max_gens=4000)
+    total = sum(r.num_generations for r in reps)
+    assert total >= 1 << 17, total
+    out = []
+    for budget, steps in ((1 << 26, 0), (1 << 26, 9), (600, 0), (0, 0)):
+        with Engine() as e:
+            e.batch_set_record_budget(budget)
+            e.batch_begin(reps)
+            if steps:
+                while e.batch_run(steps) > 0:
+                    pass
+            else:
+                assert e.batch_run() == 0
+            out.append([e.batch_read_state(r) for r in range(len(reps))])
+            assert e.batch_stats()["generations"] == total
+    for other in out[1:]:
+        for (fa, ia, ga), (fb, ib, gb) in zip(out[0], other):
+            assert ga == gb
+            assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
+            assert np.array_equal(ia, ib)
+
+
 def test_record_paths_agree():
     """All records resident, records in alternating chunks (a budget far below the batch's total), and
     records built per super-step with a count read-back (budget 0) must give the same states, also
