@@ -496,7 +496,8 @@ def run_batched(args):
         "config": {"workload": f"{len(reps)} single-population replicates: N0 log-uniform [1e3, {args.n_max:g}], "
                                "gamma U[-100, 10], h U[0, 1], F U[0, 0.5], growth r U[-0.001, 0.01] clamped to "
                                "[N0/10, 10 N0], mu 1e-9, L 1e7, 4 N0 generations, MSE start, SFS n=100",
-                   "compact_interval": tuned["compact_interval"], "cadence_trials": tuned["trials"]},
+                   "compact_interval": tuned["compact_interval"], "cadence_trials": tuned["trials"],
+                   "host_threads": os.cpu_count()},
         "mutation_generations_per_step": st["mutation_generations"],
         "mutation_generations_per_s": st["mutation_generations"] / batch_s,
         "super_steps": st["super_steps"],

@@ -202,12 +202,12 @@ typedef struct gf_batch_stats {
 } gf_batch_stats;
 gf_status gf_batch_stats_read(gf_engine* engine, gf_batch_stats* out);
 /* Generation records (one per replicate per generation, 36 bytes, page-locked on the host and on
- * the device) the batched engine keeps resident: a batch within the budget (default 67,108,864) has
- * all its records resident -- drawn by host threads region by region (about 512 generations of every
- * replicate per region) while the first super-steps run, or at gf_batch_begin below 131,072 records;
- * a larger one keeps two chunks per replicate, refilled ahead of the GPU; 0 builds each super-step's
- * records on the host and reads the counts back per super-step.  Results are identical in every
- * case.  Takes effect at the next gf_batch_begin. */
+ * the device) the batched engine keeps resident.  Host threads draw them region by region (about 512
+ * generations of every replicate per region) while the super-steps run: a batch within the budget
+ * (default 67,108,864) keeps every region resident; a larger one cycles its regions through as many
+ * slots as fit the budget (at least two); 0 builds each super-step's records on the host and reads
+ * the counts back per super-step.  Results are identical in every case.  Takes effect at the next
+ * gf_batch_begin. */
 gf_status gf_batch_set_record_budget(gf_engine* engine, int64_t records);
 
 /* ---------------------------------------------------------------------------------------------

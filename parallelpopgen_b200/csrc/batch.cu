@@ -7,8 +7,8 @@
 // generations up to its next compaction (its own window length) in ONE window-kernel launch over
 // all replicates' tiles, then one segmented scan (a block per replicate) and one segmented scatter.
 // The host draws the per-generation new-mutation counts (as the reference does on its host,
-// calc_new_mutations_Index, go_fish_impl.cuh:454-467) and reads the survivor counts back once per
-// super-step.  Because every per-slot operation is the plain engine's (same Philox counters relative
+// calc_new_mutations_Index, go_fish_impl.cuh:454-467) ahead of the GPU, and the survivor counts stay
+// on the device until the run returns.  Because every per-slot operation is the plain engine's (same Philox counters relative
 // to the replicate's own slots, same compaction schedule, same MSE start code), replicate r's state
 // is bit-identical to a plain run with the same inputs.
 #include <cuda_runtime.h>
@@ -317,7 +317,8 @@ void release_batch(Engine* e) {
   if (b->h_ring_all) cudaFreeHost(b->h_ring_all);
   for (int k = 0; k < Batch::kRing; ++k)
     if (b->ring_done[k]) cudaEventDestroy(b->ring_done[k]);
-  if (b->stage_done) cudaEventDestroy(b->stage_done);
+  for (cudaEvent_t ev : b->slot_upload)
+    if (ev) cudaEventDestroy(ev);
   delete b;
   e->batch = nullptr;
 }
@@ -369,70 +370,25 @@ static void make_record(const gf_replicate& p, int g, WinGen& w) {
   w.alive = N > 0;
 }
 
-// Records depend only on each replicate's seeds and size trajectory, so they are computed ahead of
-// the GPU (host threads over replicates, into the engine's page-locked staging buffer, kept across
-// batches) and uploaded in bulk; super-steps then need neither host record work nor a read-back.
-// A batch within the engine's record budget has all its records resident (streamed by host threads
-// while the super-steps run, see start_streamed_records, or drawn at begin when it is small); a
-// larger one keeps two regions per replicate of `chunk` generations (a multiple of its cadence, so no window straddles
-// two chunks), and chunk j + 1 is computed and uploaded when a replicate enters chunk j -- into the
-// region chunk j - 1 used, after (in stream order) the super-steps that read it.
-
-// Compute chunk j of every listed replicate into the staging buffer at its device offsets, then
-// upload each run of consecutive replicates with one copy.
-static gf_status fill_chunks(Engine* e, Batch* b, const std::vector<std::pair<int, int>>& todo) {
-  if (todo.empty()) return GF_OK;
-  GF_CUDA(e, cudaEventSynchronize(b->stage_done));   // the previous upload has read the staging buffer
-  WinGen* stage = e->h_rec_stage;
-  long long recs = 0;
-  for (auto& t : todo) recs += b->reps[t.first].chunk;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned nt = recs > 50000 ? std::min<unsigned>(hw, 32) : 1;
-  std::atomic<size_t> next(0);
-  auto work = [&]() {
-    for (size_t i; (i = next.fetch_add(1)) < todo.size();) {
-      const BatchRep& br = b->reps[todo[i].first];
-      const int j = todo[i].second;
-      const long long base = (j % br.regions) * b->region_stride + br.rec0;
-      const int g0 = j * br.chunk;
-      const int g1 = std::min(br.p.num_generations, g0 + br.chunk);
-      for (int g = g0 + 1; g <= g1; ++g) make_record(br.p, g, stage[base + (g - g0 - 1)]);
-    }
-  };
-  std::vector<std::thread> pool;
-  for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
-  work();
-  for (auto& t : pool) t.join();
-  // copies: runs of replicates whose regions are adjacent in the layout
-  size_t i = 0;
-  while (i < todo.size()) {
-    const BatchRep& a = b->reps[todo[i].first];
-    const long long start = (todo[i].second % a.regions) * b->region_stride + a.rec0;
-    long long end = start + a.chunk;
-    size_t k = i + 1;
-    while (k < todo.size()) {
-      const BatchRep& c = b->reps[todo[k].first];
-      const long long cs = (todo[k].second % c.regions) * b->region_stride + c.rec0;
-      if (cs != end) break;
-      end = cs + c.chunk;
-      ++k;
-    }
-    GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs + start, stage + start, sizeof(WinGen) * (end - start),
-                               cudaMemcpyHostToDevice, e->stream));
-    i = k;
-  }
-  GF_CUDA(e, cudaEventRecord(b->stage_done, e->stream));
-  for (auto& t : todo) b->reps[t.first].filled = std::max(b->reps[t.first].filled, t.second);
-  return GF_OK;
-}
-
-// Streamed records (a resident batch of at least kStreamMinRecords records): the slabs of region 0
-// are drawn first, and the GPU starts as soon as region 0 is uploaded, while host threads draw the
-// later regions.  A replicate's slab is kStreamSlab generations rounded up to a multiple of its
-// cadence, so no window straddles two regions, and every replicate reaches region j after about the
-// same number of generations -- the regions are drawn in the order the super-steps need them.
-constexpr long long kStreamMinRecords = 1 << 17;
+// Records depend only on each replicate's seeds and size trajectory, so host threads draw them ahead
+// of the GPU into the engine's page-locked staging buffer and they are uploaded in bulk; super-steps
+// then need neither host record work nor a count read-back.
+//
+// Slab j of replicate r is its generations (j * S_r, (j + 1) * S_r] with S_r = W * c_r: W windows
+// of its cadence c_r, W chosen so that S is about kStreamSlab generations.  Every replicate advances
+// one window per super-step, so all of them enter slab j at super-step j * W, and no window straddles
+// two slabs.  Region j holds slab j of every replicate that runs that long; producers draw the
+// slabs region-major, the order in which the super-steps need them, and a super-step uploads every
+// completed region before its launches (waiting, bounded, only for a region it needs).  A batch within
+// the engine's record budget keeps all regions resident, one after another; a larger one cycles
+// through a ring of K equal slots (K regions fit the budget, at least two): region j goes into slot
+// j % K once the super-steps that read region j - K are enqueued (the upload follows them in stream
+// order), and its slabs are drawn once the upload of region j - K has read the staging slot.
 constexpr int kStreamSlab = 512;
+
+static long long region_slot_base(const Batch* b, int j) {
+  return b->ring_slots > 0 ? static_cast<long long>(j % b->ring_slots) * b->slot_records : b->region_base[j];
+}
 
 static void produce_records(Batch* b, WinGen* stage) {
   const long long R = b->R;
@@ -444,31 +400,39 @@ static void produce_records(Batch* b, WinGen* stage) {
     const int j = static_cast<int>(i / R), r = static_cast<int>(i % R);
     const int off = b->region_off[static_cast<size_t>(r) * b->nregions + j];
     if (off < 0) continue;
+    while (j >= b->producible.load(std::memory_order_acquire)) {   // its staging slot is still being read
+      if (b->cancel.load(std::memory_order_relaxed)) return;
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
     const BatchRep& br = b->reps[r];
     const int g0 = j * br.chunk;
     const int g1 = std::min(br.p.num_generations, g0 + br.chunk);
-    WinGen* out = stage + b->region_base[j] + off;
+    WinGen* out = stage + region_slot_base(b, j) + off;
     for (int g = g0 + 1; g <= g1; ++g) make_record(br.p, g, out[g - g0 - 1]);
     b->region_done[j].fetch_add(1, std::memory_order_release);
   }
 }
 
-static gf_status start_streamed_records(Engine* e, Batch* b, long long total) {
+static gf_status precompute_records(Engine* e, Batch* b) {
+  long long total = 0;
+  int cmax = 1;
+  for (auto& br : b->reps) {
+    total += br.p.num_generations;
+    cmax = std::max(cmax, br.p.compact_interval);
+  }
+  b->precomputed = false;
+  if (e->batch_record_budget <= 0 || total == 0) return GF_OK;
+  const int W = std::max(1, (kStreamSlab + cmax - 1) / cmax);
   int nreg = 0;
   for (auto& br : b->reps) {
-    const int G = br.p.num_generations;
-    const int c = std::max(br.p.compact_interval, 1);
-    br.chunk = c * ((kStreamSlab + c - 1) / c);
-    br.regions = 1;
-    br.rec0 = 0;
-    br.filled = 0;
-    nreg = std::max(nreg, (G + br.chunk - 1) / br.chunk);
+    br.chunk = W * std::max(br.p.compact_interval, 1);
+    nreg = std::max(nreg, (br.p.num_generations + br.chunk - 1) / br.chunk);
   }
   b->nregions = nreg;
   b->region_off.assign(static_cast<size_t>(b->R) * nreg, -1);
   b->region_base.assign(nreg + 1, 0);
   b->region_jobs.assign(nreg, 0);
-  long long off = 0;
+  long long off = 0, largest = 0;
   for (int j = 0; j < nreg; ++j) {
     b->region_base[j] = off;
     for (int r = 0; r < b->R; ++r) {
@@ -479,93 +443,20 @@ static gf_status start_streamed_records(Engine* e, Batch* b, long long total) {
       off += std::min(br.p.num_generations, g0 + br.chunk) - g0;
       b->region_jobs[j] += 1;
     }
+    largest = std::max(largest, off - b->region_base[j]);
   }
   b->region_base[nreg] = off;
-  if (off != total) return fail(e, GF_ERR_STATE, "streamed record layout holds %lld of %lld records", off, total);
-  if (e->h_rec_stage_cap < static_cast<size_t>(total)) {
-    if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
-    e->h_rec_stage = nullptr;
-    e->h_rec_stage_cap = 0;
-    const size_t cap = static_cast<size_t>(total) + static_cast<size_t>(total) / 4;
-    GF_CUDA(e, cudaMallocHost(&e->h_rec_stage, sizeof(WinGen) * cap));
-    e->h_rec_stage_cap = cap;
-  }
-  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * total);
-  if (st != GF_OK) return st;
-  b->region_done.reset(new std::atomic<long long>[nreg]);
-  for (int j = 0; j < nreg; ++j) b->region_done[j].store(0);
-  b->next_job.store(0);
-  b->cancel.store(false);
-  b->uploaded = 0;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const long long want = std::max<long long>(1, total / 65536);
-  const int workers = static_cast<int>(std::min<long long>(want, std::max(1u, std::min(hw - 1, 31u))));
-  WinGen* stage = e->h_rec_stage;
-  for (int t = 0; t < workers; ++t) b->producers.emplace_back(produce_records, b, stage);
-  b->streamed = true;
-  b->precomputed = true;
-  return GF_OK;
-}
-
-// Upload every region whose slabs are all drawn, in order; regions below `need` are waited for
-// (bounded: producers that make no progress for two minutes are reported as a state error).
-static gf_status stream_upload(Engine* e, Batch* b, int need) {
-  while (b->uploaded < b->nregions) {
-    const int j = b->uploaded;
-    if (b->region_done[j].load(std::memory_order_acquire) != b->region_jobs[j]) {
-      if (j >= need) break;
-      const auto t0 = std::chrono::steady_clock::now();
-      long long last = -1;
-      auto progress = t0;
-      for (;;) {
-        const long long d = b->region_done[j].load(std::memory_order_acquire);
-        if (d == b->region_jobs[j]) break;
-        const auto now = std::chrono::steady_clock::now();
-        if (d != last) {
-          last = d;
-          progress = now;
-        } else if (now - progress > std::chrono::seconds(120)) {
-          return fail(e, GF_ERR_STATE, "record producers made no progress on region %d for 120 s", j);
-        }
-        std::this_thread::sleep_for(std::chrono::microseconds(20));
-      }
+  if (off != total) return fail(e, GF_ERR_STATE, "record layout holds %lld of %lld records", off, total);
+  long long slots = total;
+  b->ring_slots = 0;
+  if ((total > e->batch_record_budget || total >= (1ll << 31)) && nreg > 2) {   // record indices are int
+    const int K = static_cast<int>(std::min<long long>(nreg, std::max<long long>(2, e->batch_record_budget / largest)));
+    if (K < nreg) {
+      b->ring_slots = K;
+      b->slot_records = largest;
+      slots = K * largest;
     }
-    const long long a = b->region_base[j], n = b->region_base[j + 1] - a;
-    if (n > 0)
-      GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs + a, e->h_rec_stage + a, sizeof(WinGen) * n, cudaMemcpyHostToDevice,
-                                 e->stream));
-    b->uploaded += 1;
   }
-  return GF_OK;
-}
-
-static gf_status precompute_records(Engine* e, Batch* b) {
-  long long total = 0;
-  for (auto& br : b->reps) total += br.p.num_generations;
-  b->precomputed = false;
-  b->streamed = false;
-  if (e->batch_record_budget <= 0 || total == 0) return GF_OK;
-  const bool resident = total <= e->batch_record_budget;
-  if (resident && total >= kStreamMinRecords) return start_streamed_records(e, b, total);
-  const long long target = std::max<long long>(64, e->batch_record_budget / (2ll * b->R));
-  long long off = 0;
-  for (auto& br : b->reps) {
-    const int G = std::max(br.p.num_generations, 1);
-    const int c = std::max(br.p.compact_interval, 1);
-    long long chunk = resident ? G : std::max<long long>(c, (target / c) * c);
-    if (chunk >= G) {
-      chunk = G;
-      br.regions = 1;
-    } else {
-      br.regions = 2;
-    }
-    br.chunk = static_cast<int>(chunk);
-    br.rec0 = off;
-    br.filled = -1;
-    off += chunk;
-  }
-  b->region_stride = off;
-  const long long slots = 2 * off;   // region 1 is used only by replicates with two regions
   if (e->h_rec_stage_cap < static_cast<size_t>(slots)) {
     if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
     e->h_rec_stage = nullptr;
@@ -576,15 +467,70 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   }
   gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * slots);
   if (st != GF_OK) return st;
-  GF_TRACE_POINT(e, "record buffers");
-  std::vector<std::pair<int, int>> todo;
-  for (int r = 0; r < b->R; ++r) todo.emplace_back(r, 0);
-  for (int r = 0; r < b->R; ++r)
-    if (b->reps[r].regions == 2) todo.emplace_back(r, 1);
-  st = fill_chunks(e, b, todo);
-  if (st != GF_OK) return st;
-  GF_TRACE_POINT(e, "record draws and upload");
+  const int K = b->ring_slots > 0 ? b->ring_slots : nreg;
+  b->slot_upload.assign(K, nullptr);
+  for (int k = 0; k < K && b->ring_slots > 0; ++k)
+    GF_CUDA(e, cudaEventCreateWithFlags(&b->slot_upload[k], cudaEventDisableTiming));
+  b->region_done.reset(new std::atomic<long long>[nreg]);
+  for (int j = 0; j < nreg; ++j) b->region_done[j].store(0);
+  b->next_job.store(0);
+  b->cancel.store(false);
+  b->uploaded = 0;
+  b->upload_done = 0;
+  b->producible.store(b->ring_slots > 0 ? b->ring_slots : nreg);
+  // A producer draws ~25 M records/s and the super-steps consume ~50 M/s at most, so a few producers
+  // stay ahead of the GPU; more would take cores from the thread that enqueues the super-steps.
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const long long want = std::max<long long>(1, total / 65536);
+  const int workers = static_cast<int>(std::min<long long>(want, std::max(1u, std::min(hw / 2, 6u))));
+  WinGen* stage = e->h_rec_stage;
+  for (int t = 0; t < workers; ++t) b->producers.emplace_back(produce_records, b, stage);
   b->precomputed = true;
+  GF_TRACE_POINT(e, "record producers started");
+  return GF_OK;
+}
+
+// Upload the drawn regions a super-step in region `need` may see: every completed region up to
+// need + K - 1 in order (K ring slots; all regions when resident), waiting for the producers only for
+// regions up to `need`.  Finished uploads free their staging slots for the producers.  A wait that
+// sees no progress for 120 s is reported as a state error.
+static gf_status stream_upload(Engine* e, Batch* b, int need) {
+  const int K = b->ring_slots > 0 ? b->ring_slots : b->nregions;
+  auto poll = [&]() {
+    if (b->ring_slots <= 0) return;
+    while (b->upload_done < b->uploaded) {
+      if (cudaEventQuery(b->slot_upload[b->upload_done % K]) != cudaSuccess) break;
+      b->upload_done += 1;
+    }
+    b->producible.store(std::min(b->nregions, b->upload_done + K), std::memory_order_release);
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+  auto progress = t0;
+  long long last = -1;
+  for (;;) {
+    poll();
+    const int j = b->uploaded;
+    if (j >= b->nregions || j >= need + K) break;
+    const long long done = b->region_done[j].load(std::memory_order_acquire);
+    if (done == b->region_jobs[j]) {
+      const long long a = region_slot_base(b, j), n = b->region_base[j + 1] - b->region_base[j];
+      if (n > 0)
+        GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs + a, e->h_rec_stage + a, sizeof(WinGen) * n, cudaMemcpyHostToDevice,
+                                   e->stream));
+      if (b->ring_slots > 0) GF_CUDA(e, cudaEventRecord(b->slot_upload[j % K], e->stream));
+      b->uploaded += 1;
+      continue;
+    }
+    if (j > need) break;   // not needed by this super-step
+    const auto now = std::chrono::steady_clock::now();
+    if (done != last) {
+      last = done;
+      progress = now;
+    } else if (now - progress > std::chrono::seconds(120)) {
+      return fail(e, GF_ERR_STATE, "record producers made no progress on region %d for 120 s", j);
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
   return GF_OK;
 }
 
@@ -695,7 +641,6 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
   GF_CUDA(e, cudaMallocHost(&b->h_ring_all, sizeof(WinRep) * R * Batch::kRing));
   for (int k = 0; k < Batch::kRing; ++k)
     GF_CUDA(e, cudaEventCreateWithFlags(&b->ring_done[k], cudaEventDisableTiming));
-  GF_CUDA(e, cudaEventCreateWithFlags(&b->stage_done, cudaEventDisableTiming));
   GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
@@ -800,22 +745,11 @@ static gf_status sync_counts(Engine* e) {
 static gf_status batch_super_step(Engine* e, int* active_out) {
   Batch* b = e->batch;
   if (!b->precomputed) return batch_super_step_fallback(e, active_out);
-  // a replicate entering chunk j gets chunk j + 1 computed and uploaded now (into the region chunk
-  // j - 1 used, after the super-steps that read it in stream order)
-  std::vector<std::pair<int, int>> refill;
-  for (int r = 0; r < b->R && !b->streamed; ++r) {
-    const BatchRep& br = b->reps[r];
-    if (br.done || br.regions != 2) continue;
-    const int j = br.generation / br.chunk;
-    if (br.filled == j && (j + 1) * static_cast<long long>(br.chunk) < br.p.num_generations) refill.emplace_back(r, j + 1);
-  }
-  gf_status rst = fill_chunks(e, b, refill);
-  if (rst != GF_OK) return rst;
   const int slot = b->ring;
   GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
   WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->R;
   WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->R;
-  int nj = 0, tiles = 0, need_regions = 0;
+  int nj = 0, tiles = 0, need_region = 0;
   for (int r = 0; r < b->R; ++r) {
     BatchRep& br = b->reps[r];
     if (br.done) continue;
@@ -823,16 +757,10 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     const int ngen = end - br.generation;
     const int j = br.generation / br.chunk;
     WinRep& w = hr[nj++];
-    if (b->streamed) {
-      const int off = (j < b->nregions) ? b->region_off[static_cast<size_t>(r) * b->nregions + j] : -1;
-      if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
-      w.rec = static_cast<int>(b->region_base[j] + off + (br.generation - static_cast<long long>(j) * br.chunk));
-      need_regions = std::max(need_regions, j + 1);
-    } else {
-      if (br.filled < j) return fail(e, GF_ERR_STATE, "replicate %d: record chunk %d not resident", r, j);
-      w.rec = static_cast<int>((j % br.regions) * b->region_stride + br.rec0 +
-                               (br.generation - static_cast<long long>(j) * br.chunk));
-    }
+    const int off = (j < b->nregions) ? b->region_off[static_cast<size_t>(r) * b->nregions + j] : -1;
+    if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
+    w.rec = static_cast<int>(region_slot_base(b, j) + off + (br.generation - static_cast<long long>(j) * br.chunk));
+    need_region = std::max(need_region, j);
     w.base = br.base;
     w.capacity = br.capacity;
     w.ngen = ngen;
@@ -851,8 +779,8 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     if (active_out) *active_out = 0;
     return GF_OK;
   }
-  if (b->streamed) {
-    gf_status ust = stream_upload(e, b, need_regions);   // the records of this super-step, in stream order
+  {
+    gf_status ust = stream_upload(e, b, need_region);   // the records of this super-step, in stream order
     if (ust != GF_OK) return ust;
   }
   GF_CUDA(e, cudaMemcpyAsync(dr, hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));

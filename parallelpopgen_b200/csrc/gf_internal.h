@@ -141,10 +141,7 @@ struct BatchRep {
   int Nc = 0;               // Nchrom_e at `generation`
   int id_buf = 0;           // ID buffer holding its state
   int m_slot = 0;           // count array (d_M[m_slot]) holding its latest count
-  long long rec0 = -1;      // its offset inside each record region, or -1 (records not precomputed)
-  int chunk = 0;            // generations per record chunk (a multiple of its compaction cadence)
-  int regions = 1;          // 1: all its records resident; 2: chunks alternate between two regions
-  int filled = -1;          // highest chunk uploaded
+  int chunk = 0;            // generations per record slab (a multiple of its compaction cadence)
   bool done = false;
 };
 
@@ -180,22 +177,24 @@ struct Batch {
   WinRep* d_ring_all = nullptr;       // kRing tables of R entries, one allocation each side
   WinRep* h_ring_all = nullptr;
   cudaEvent_t ring_done[kRing] = {};
-  long long region_stride = 0;        // records per region (region k of replicate r: k * stride + rec0)
-  cudaEvent_t stage_done = nullptr;   // the last upload from the page-locked staging buffer
   int ring = 0;
   bool counts_stale = false;          // counts on the device are newer than reps[].M
   int* d_total_tiles = nullptr;       // tiles of the current super-step, assigned on the device
-  // streamed records: host threads draw the records region by region (region j holds slab j -- the
+  // generation records, drawn by host threads region by region (region j holds slab j -- the
   // generations (j * chunk, (j + 1) * chunk] -- of every replicate that runs that long) while the GPU
-  // runs the super-steps; each region is uploaded once all of its slabs are drawn
-  bool streamed = false;
+  // runs the super-steps; a region is uploaded once all of its slabs are drawn (batch.cu)
   int nregions = 0;
   int uploaded = 0;                           // regions uploaded so far
-  std::vector<long long> region_base;         // first record of region j (nregions + 1 entries)
+  int upload_done = 0;                        // regions whose upload has finished (ring mode)
+  int ring_slots = 0;                         // 0: all regions resident; K: regions cycle through K slots
+  long long slot_records = 0;                 // records per ring slot
+  std::vector<long long> region_base;         // first record of region j, resident layout (nregions + 1)
   std::vector<long long> region_jobs;         // slabs in region j
   std::vector<int> region_off;                // [r * nregions + j]: offset of replicate r's slab in region j
+  std::vector<cudaEvent_t> slot_upload;       // ring mode: the last upload from each staging slot
   std::unique_ptr<std::atomic<long long>[]> region_done;   // slabs drawn per region
   std::atomic<long long> next_job{0};         // producers' job counter (region-major over replicates)
+  std::atomic<int> producible{0};             // producers may draw regions below this
   std::atomic<bool> cancel{false};
   std::vector<std::thread> producers;
 };

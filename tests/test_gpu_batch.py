@@ -78,14 +78,15 @@ def test_batched_super_steps_are_resumable():
 
 
 def test_streamed_records_agree():
-    """A resident batch of at least 2**17 generation records has its records drawn by host threads
-    region by region while the super-steps run; it must give the same states as the chunked path
-    (a small budget) and the per-super-step path (budget 0), also when run in chunks of super-steps."""
+    """Generation records are drawn by host threads region by region while the super-steps run: all
+    regions resident (a large budget), a ring of a few regions (a budget of a few regions), a ring of
+    two (a tiny budget) and the per-super-step path (budget 0) must give the same states, also when
+    the batch runs in chunks of super-steps."""
     reps = make_replicates(64, seed=29, max_gens=4000)
     total = sum(r.num_generations for r in reps)
     assert total >= 1 << 17, total
     out = []
-    for budget, steps in ((1 << 26, 0), (1 << 26, 9), (600, 0), (0, 0)):
+    for budget, steps in ((1 << 26, 0), (1 << 26, 9), (100_000, 0), (600, 7), (0, 0)):
         with Engine() as e:
             e.batch_set_record_budget(budget)
             e.batch_begin(reps)
@@ -104,9 +105,9 @@ def test_streamed_records_agree():
 
 
 def test_record_paths_agree():
-    """All records resident, records in alternating chunks (a budget far below the batch's total), and
-    records built per super-step with a count read-back (budget 0) must give the same states, also
-    when the batch runs in chunks of super-steps."""
+    """All records resident, records cycling through a ring of regions (a budget far below the batch's
+    total), and records built per super-step with a count read-back (budget 0) must give the same
+    states, also when the batch runs in chunks of super-steps."""
     reps = make_replicates(6, seed=17, max_gens=700)
     out = []
     for budget in (1 << 26, 600, 0):
