@@ -1,7 +1,8 @@
 """Autotuner for the engine's launch choices and the batched engine's compaction cadence.
 
 Launch choices (`gf_tuning`: per-thread draws in lane order, warp-pooled draws or per-thread draws
-grouped by sampler branch; resident drift blocks per SM; window launches on/off) never change results; the tuner times a short calibration run per candidate
+grouped by sampler branch, or the normal approximation of a quad's four lanes first; resident drift
+blocks per SM; window launches on/off) never change results; the tuner times a short calibration run per candidate
 and keeps the fastest.  The compaction cadence of batched replicates does change results (the
 Philox counter of a mutation is its slot, and compaction moves slots), so it is tuned only when the
 caller asks for it -- batched statistics, where any cadence gives a valid, differently-seeded
@@ -27,6 +28,7 @@ LAUNCH_CANDIDATES = [
     {"draw_strategy": 0, "blocks_per_sm": 4, "windows": 1},
     {"draw_strategy": 1, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 2, "blocks_per_sm": 0, "windows": 1},
+    {"draw_strategy": 3, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 0, "blocks_per_sm": 0, "windows": 0},
     {"draw_strategy": 2, "blocks_per_sm": 0, "windows": 0},
 ]

@@ -645,6 +645,9 @@ static void launch_drift_c(Engine* e, int tiles_bound, int slot_in, int slot_out
   switch (e->draw_strategy) {
     case kDrawWarp: launch_drift_t<PT, NEUTRAL, FLAG, kDrawWarp>(e, tiles_bound, slot_in, slot_out, a); break;
     case kDrawGrouped: launch_drift_t<PT, NEUTRAL, FLAG, kDrawGrouped>(e, tiles_bound, slot_in, slot_out, a); break;
+    case kDrawNormalAll:
+      launch_drift_t<PT, NEUTRAL, FLAG, kDrawNormalAll>(e, tiles_bound, slot_in, slot_out, a);
+      break;
     default: launch_drift_t<PT, NEUTRAL, FLAG, kDrawLanes>(e, tiles_bound, slot_in, slot_out, a); break;
   }
 }
@@ -1497,7 +1500,7 @@ gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
   Engine* e = &g->impl;
   if (t->draw_strategy < 0 || t->draw_strategy >= kDrawStrategies || t->blocks_per_sm < 0 || t->windows < 0 ||
       t->windows > 1)
-    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2}, blocks_per_sm >= 0, windows in {0, 1}");
+    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2, 3}, blocks_per_sm >= 0, windows in {0, 1}");
   e->draw_strategy = t->draw_strategy;
   e->blocks_per_sm = t->blocks_per_sm;
   e->use_windows = t->windows != 0;

@@ -68,8 +68,9 @@ enum DrawStrategy : int {
   kDrawLanes = 0,    // each thread draws its needed lanes in lane order
   kDrawWarp = 1,     // the warp pools its draws in shared memory and runs them branch by branch
   kDrawGrouped = 2,  // each thread draws its normal-branch lanes first, then its search-branch lanes
+  kDrawNormalAll = 3,  // the normal approximation of all four lanes at once, then the search lanes
 };
-constexpr int kDrawStrategies = 3;
+constexpr int kDrawStrategies = 4;
 
 // Sampler branch of a lane (binom_draw_body): the sequential searches for mean <= 6 or
 // mean >= N - 6, the normal approximation otherwise.
@@ -101,6 +102,27 @@ __device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsi
 #pragma unroll
     for (int j = 0; j < 4; ++j)
       if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
+    return;
+  }
+  if (DRAW == kDrawNormalAll) {
+    // The normal-approximation branch of binom_draw_body for the four lanes without branches between
+    // them (independent chains the scheduler can interleave); lanes whose mean takes a search branch
+    // then replace their value.  Lanes that need no draw compute a value that is discarded.
+    if (!need) return;
+    float mean[4], var[4];
+    int nrm[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      mean[j] = xs[j] * N;
+      var[j] = (1.0f - xs[j]) * (xs[j] * N);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) nrm[j] = round(normcdfinv(u01(rb[j])) * sqrtf(var[j]) + mean[j]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (!((need >> j) & 1u)) continue;
+      res[j] = search_branch(mean[j], Nf) ? GF_LANE_DRAW(rb[j], mean[j], var[j], Nf) : nrm[j];
+    }
     return;
   }
   if (DRAW == kDrawGrouped) {

@@ -434,6 +434,7 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
   switch (e->draw_strategy) {
     case kDrawWarp: launch_window_kernel<kDrawWarp>(e, w); break;
     case kDrawGrouped: launch_window_kernel<kDrawGrouped>(e, w); break;
+    case kDrawNormalAll: launch_window_kernel<kDrawNormalAll>(e, w); break;
     default: launch_window_kernel<kDrawLanes>(e, w); break;
   }
   GF_CUDA(e, cudaGetLastError());
