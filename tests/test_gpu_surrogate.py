@@ -129,6 +129,46 @@ def test_surrogate_on_simulator_spectra():
         mlp.check()
 
 
+def test_trained_network_beats_answers_without_it():
+    """What the network adds over answering from the same simulated data without it: on held-out
+    parameter draws, its median per-bin relative error against 16-replicate simulator means must be
+    well below that of the training set's mean spectrum (one answer for every query) and that of the
+    nearest training draw's spectrum (a table lookup over the same simulations).  Measured on B200:
+    2.8 % against 84 % and 17 %."""
+    from parallelpopgen_b200 import Engine
+    from parallelpopgen_b200 import surrogate as sg
+
+    def small_n(p):
+        p[:, 0] = np.log(500.0) + (p[:, 0] - sg.LOW[0]) * 0.2      # N in [500, ~660]: quick runs
+        return p
+
+    with Engine() as e:
+        ptrain = small_n(sg.draw_parameters(2048, seed=31))
+        ptest = small_n(sg.draw_parameters(128, seed=32))
+        train_sims = sg.simulate_spectra(e, ptrain, reps=4, seed=2000)
+        truth = sg.simulate_spectra(e, ptest, reps=16, seed=9000)
+        targets = sg.spectra_to_targets(train_sims)
+        scale = sg.TargetScale.fit(targets)
+        X = torch.from_numpy(sg.encode(ptrain)).cuda()
+        T = torch.from_numpy(scale.apply(targets)).cuda()
+        mlp = sg.Mlp(capacity=2048, lr=1e-3)
+        mlp.set_params(sg.init_params(0))
+        sg.train(mlp, X, T, steps=3000, batch=512, lr=1e-3, log_every=1000)
+        net = sg.Surrogate(mlp, e, scale=scale).predict(ptest)
+        mlp.check()
+    train_p = train_sims / train_sims.sum(axis=1, keepdims=True)
+    constant = np.repeat(train_p.mean(axis=0, keepdims=True), len(ptest), axis=0)
+    xtr, xte = sg.encode(ptrain), sg.encode(ptest)
+    nearest = train_p[np.argmin(((xte[:, None, :] - xtr[None, :, :]) ** 2).sum(axis=2), axis=1)]
+    err_net = sg.median_relative_error(net, truth)[0]
+    err_const = sg.median_relative_error(constant, truth)[0]
+    err_nn = sg.median_relative_error(nearest, truth)[0]
+    print(f"median per-bin relative error: network {err_net:.4f}, training mean {err_const:.4f}, "
+          f"nearest training draw {err_nn:.4f}")
+    assert err_net < 0.5 * err_const, (err_net, err_const)
+    assert err_net < 0.5 * err_nn, (err_net, err_nn)
+
+
 def test_bounded_wait_reports_and_recovers():
     """Failure path without a GPU fault: an injected missing accumulator hand-off makes the GEMM's
     bounded wait run out; the kernel ends, the fault word reports it once, and the next pass is exact."""
