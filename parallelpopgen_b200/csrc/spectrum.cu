@@ -73,19 +73,54 @@ __global__ void hist_to_float_kernel(const unsigned* __restrict__ counts, int Nc
 constexpr int kProjThreads = 256;
 constexpr int kProjChunk = 256;
 
+// Per-class binomial terms c * C(n, k) p^k q^(n-k): a thread owns kper consecutive levels
+// [k0, k0 + kper); it evaluates the first in log space (one exp) and steps to the next with the pmf
+// ratio (n - k) / (k + 1) * p / q, so a class costs one exp per thread instead of one per level.
+// The recurrence adds ~1e-16 relative error per step (at most 7 steps); a first term that underflows
+// only drops terms below 1e-300.
+__device__ __forceinline__ void add_class_terms(double (&acc)[8], int k0, int kper, int levels, double c,
+                                                double lp, double lq, double pq, int n, double lg0,
+                                                const double (&ratio)[8]) {
+  if (k0 >= levels) return;
+  double t = c * exp(lg0 + k0 * lp + (n - k0) * lq);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    if (u >= kper) break;
+    if (k0 + u >= levels) break;
+    if (u > 0) t *= ratio[u - 1] * pq;
+    acc[u] += t;
+  }
+}
+
+// The per-thread constants of add_class_terms: log C(n, k0) and (n - k) / (k + 1) for its levels.
+__device__ __forceinline__ void thread_level_constants(const double* __restrict__ lgc, int n, int k0, int kper,
+                                                       double& lg0, double (&ratio)[8]) {
+  const int levels = n + 1;
+  lg0 = k0 < levels ? lgc[k0] : 0.0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int k = k0 + u;
+    ratio[u] = (u < kper && k < n) ? static_cast<double>(n - k) / static_cast<double>(k + 1) : 0.0;
+  }
+}
+
 // Partial projections: block b covers classes [j0, j1) and writes partial[b][k] for k in [0, n].
 __global__ void __launch_bounds__(kProjThreads)
     project_hist_kernel(const unsigned* __restrict__ counts, int Nc, int n, const double* __restrict__ lgc,
                         double* __restrict__ partial, int classes_per_block) {
   __shared__ double s_lp[kProjChunk];
   __shared__ double s_lq[kProjChunk];
+  __shared__ double s_pq[kProjChunk];
   __shared__ double s_c[kProjChunk];
   __shared__ int s_any;
   const int j0 = blockIdx.x * classes_per_block;
   const int j1 = min(Nc + 1, j0 + classes_per_block);
   const float Nf = static_cast<float>(Nc);
   const int levels = n + 1;
-  const int kper = (levels + kProjThreads - 1) / kProjThreads;  // levels per thread
+  const int kper = (levels + kProjThreads - 1) / kProjThreads;  // consecutive levels per thread
+  const int k0 = threadIdx.x * kper;
+  double lg0, ratio[8];
+  thread_level_constants(lgc, n, k0, kper, lg0, ratio);
   double acc[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) acc[u] = 0.0;
@@ -94,20 +129,23 @@ __global__ void __launch_bounds__(kProjThreads)
     __syncthreads();
     for (int t = threadIdx.x; t < kProjChunk; t += blockDim.x) {
       const int j = c0 + t;
-      double c = 0.0, lp = 0.0, lq = 0.0;
+      double c = 0.0, lp = 0.0, lq = 0.0, pq = 0.0;
       if (j < j1) {
         const float p = static_cast<float>(j) / Nf;
         const unsigned cnt = counts[j];
         if (cnt && p > 0.f && p < 1.f) {
+          const double pd = static_cast<double>(p);
           c = static_cast<double>(cnt);
-          lp = log(static_cast<double>(p));
-          lq = log1p(-static_cast<double>(p));
+          lp = log(pd);
+          lq = log1p(-pd);
+          pq = pd / (1.0 - pd);
           s_any = 1;
         }
       }
       s_c[t] = c;
       s_lp[t] = lp;
       s_lq[t] = lq;
+      s_pq[t] = pq;
     }
     __syncthreads();
     if (s_any) {
@@ -115,13 +153,7 @@ __global__ void __launch_bounds__(kProjThreads)
       for (int t = 0; t < cend; ++t) {
         const double c = s_c[t];
         if (c == 0.0) continue;
-        const double lp = s_lp[t], lq = s_lq[t];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          if (u >= kper) break;
-          const int k = threadIdx.x + u * kProjThreads;
-          if (k < levels) acc[u] += c * exp(lgc[k] + k * lp + (n - k) * lq);
-        }
+        add_class_terms(acc, k0, kper, levels, c, s_lp[t], s_lq[t], s_pq[t], n, lg0, ratio);
       }
     }
     __syncthreads();
@@ -129,7 +161,7 @@ __global__ void __launch_bounds__(kProjThreads)
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     if (u >= kper) break;
-    const int k = threadIdx.x + u * kProjThreads;
+    const int k = k0 + u;
     if (k < levels) partial[static_cast<long long>(blockIdx.x) * levels + k] = acc[u];
   }
 }
@@ -140,11 +172,15 @@ __global__ void __launch_bounds__(kProjThreads)
                           double* __restrict__ partial, int per_block, unsigned* __restrict__ nonseg) {
   __shared__ double s_lp[kProjChunk];
   __shared__ double s_lq[kProjChunk];
+  __shared__ double s_pq[kProjChunk];
   __shared__ double s_c[kProjChunk];
   const int i0 = blockIdx.x * per_block;
   const int i1 = min(M, i0 + per_block);
   const int levels = n + 1;
   const int kper = (levels + kProjThreads - 1) / kProjThreads;
+  const int k0 = threadIdx.x * kper;
+  double lg0, ratio[8];
+  thread_level_constants(lgc, n, k0, kper, lg0, ratio);
   double acc[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) acc[u] = 0.0;
@@ -152,13 +188,15 @@ __global__ void __launch_bounds__(kProjThreads)
   for (int c0 = i0; c0 < i1; c0 += kProjChunk) {
     for (int t = threadIdx.x; t < kProjChunk; t += blockDim.x) {
       const int i = c0 + t;
-      double c = 0.0, lp = 0.0, lq = 0.0;
+      double c = 0.0, lp = 0.0, lq = 0.0, pq = 0.0;
       if (i < i1) {
         const float p = freq[i];
         if (p > 0.f && p < 1.f) {
+          const double pd = static_cast<double>(p);
           c = 1.0;
-          lp = log(static_cast<double>(p));
-          lq = log1p(-static_cast<double>(p));
+          lp = log(pd);
+          lq = log1p(-pd);
+          pq = pd / (1.0 - pd);
         } else {
           ++ns;
         }
@@ -166,63 +204,76 @@ __global__ void __launch_bounds__(kProjThreads)
       s_c[t] = c;
       s_lp[t] = lp;
       s_lq[t] = lq;
+      s_pq[t] = pq;
     }
     __syncthreads();
     const int cend = min(kProjChunk, i1 - c0);
     for (int t = 0; t < cend; ++t) {
       if (s_c[t] == 0.0) continue;
-      const double lp = s_lp[t], lq = s_lq[t];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        if (u >= kper) break;
-        const int k = threadIdx.x + u * kProjThreads;
-        if (k < levels) acc[u] += exp(lgc[k] + k * lp + (n - k) * lq);
-      }
+      add_class_terms(acc, k0, kper, levels, s_c[t], s_lp[t], s_lq[t], s_pq[t], n, lg0, ratio);
     }
     __syncthreads();
   }
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     if (u >= kper) break;
-    const int k = threadIdx.x + u * kProjThreads;
+    const int k = k0 + u;
     if (k < levels) partial[static_cast<long long>(blockIdx.x) * levels + k] = acc[u];
   }
   if (ns) atomicAdd(nonseg, ns);
 }
 
 // Fixed-order reduction of the partials into float bins; k == n and every non-segregating mutation
-// fold into bin 0, plus the (num_sites - M) monomorphic sites (spectrum.cu:130-138).
-__global__ void sfs_finish_kernel(const double* __restrict__ partial, int nblocks, int n, double extra0,
-                                  const unsigned* __restrict__ nonseg_count, float* __restrict__ out) {
+// fold into bin 0, plus the (num_sites - M) monomorphic sites (spectrum.cu:130-138).  A block takes
+// 32 levels (one per lane); its 8 warps sum fixed, contiguous eighths of the partial blocks and the
+// eight sums are added in warp order, so the result does not depend on scheduling.
+constexpr int kFinishWarps = 8;
+
+__global__ void __launch_bounds__(32 * kFinishWarps)
+    sfs_finish_kernel(const double* __restrict__ partial, int nblocks, int n, double extra0,
+                      const unsigned* __restrict__ nonseg_count, float* __restrict__ out) {
+  __shared__ double s_sum[kFinishWarps][33];   // column 32: the top level k == n (block 0 only)
   const int levels = n + 1;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += blockDim.x * gridDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partial[static_cast<long long>(b) * levels + k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int k = blockIdx.x * 32 + lane;
+  const int per = (nblocks + kFinishWarps - 1) / kFinishWarps;
+  const int b0 = warp * per, b1 = min(nblocks, b0 + per);
+  double s = 0.0;
+  if (k < n)
+    for (int b = b0; b < b1; ++b) s += partial[static_cast<long long>(b) * levels + k];
+  s_sum[warp][lane] = s;
+  if (blockIdx.x == 0 && lane == 0) {
+    double top = 0.0;
+    for (int b = b0; b < b1; ++b) top += partial[static_cast<long long>(b) * levels + n];
+    s_sum[warp][32] = top;
+  }
+  __syncthreads();
+  if (warp == 0 && k < n) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kFinishWarps; ++w) t += s_sum[w][lane];
     if (k == 0) {
       double top = 0.0;
-      for (int b = 0; b < nblocks; ++b) top += partial[static_cast<long long>(b) * levels + n];
-      s += top + extra0 + static_cast<double>(*nonseg_count);
+#pragma unroll
+      for (int w = 0; w < kFinishWarps; ++w) top += s_sum[w][32];
+      t += top + extra0 + static_cast<double>(*nonseg_count);
     }
-    out[k] = static_cast<float>(s);
+    out[k] = static_cast<float>(t);
   }
 }
 
-// Non-segregating count from the histogram: classes whose p_j is not in (0, 1).
+// Non-segregating count from the histogram: classes whose p_j is not in (0, 1) -- only j == 0 and
+// j == Nc can be (tested with the same division as the projection).
 __global__ void nonseg_from_hist_kernel(const unsigned* __restrict__ counts, int Nc, unsigned* __restrict__ out) {
-  __shared__ unsigned s;
-  if (threadIdx.x == 0) s = 0;
-  __syncthreads();
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
   const float Nf = static_cast<float>(Nc);
-  unsigned local = 0;
-  for (int j = threadIdx.x; j <= Nc; j += blockDim.x) {
-    // only j == 0 and j == Nc can leave (0, 1); test them with the same division as the projection
-    if (j != 0 && j != Nc) continue;
+  unsigned total = 0;
+  for (int j : {0, Nc}) {
+    if (j == Nc && Nc == 0) break;   // one class only
     const float p = static_cast<float>(j) / Nf;
-    if (!(p > 0.f && p < 1.f)) local += counts[j];
+    if (!(p > 0.f && p < 1.f)) total += counts[j];
   }
-  atomicAdd(&s, local);
-  __syncthreads();
-  if (threadIdx.x == 0) *out = s;
+  *out = total;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -312,7 +363,7 @@ gf_status site_frequency_spectrum_device(Engine* e, const float* d_freq, int M, 
   const double extra0 = static_cast<double>(num_sites - M);
   int used_blocks;
   if (!h_mismatch) {
-    nonseg_from_hist_kernel<<<1, 256, 0, e->stream>>>(counts, Nc, nonseg);
+    nonseg_from_hist_kernel<<<1, 32, 0, e->stream>>>(counts, Nc, nonseg);
     project_hist_kernel<<<hist_nblocks, kProjThreads, 0, e->stream>>>(counts, Nc, n, lgc, partial, classes_per_block);
     used_blocks = hist_nblocks;
   } else {
@@ -323,7 +374,7 @@ gf_status site_frequency_spectrum_device(Engine* e, const float* d_freq, int M, 
     used_blocks = direct_nblocks;
   }
   GF_CUDA(e, cudaGetLastError());
-  sfs_finish_kernel<<<std::max(1, (n + 255) / 256), 256, 0, e->stream>>>(partial, used_blocks, n, extra0, nonseg, d_out);
+  sfs_finish_kernel<<<(n + 31) / 32, 32 * kFinishWarps, 0, e->stream>>>(partial, used_blocks, n, extra0, nonseg, d_out);
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += h_mismatch ? 2 : 3;
   return GF_OK;
@@ -503,7 +554,7 @@ gf_status gf_site_frequency_spectrum_noalloc(const float* d_freq, int32_t M, int
   if (!h_mismatch) {
     const int nb = std::max(1, std::min(kNoAllocMaxBlocks, (Nc + 1 + 255) / 256));
     const int per_block = (Nc + 1 + nb - 1) / nb;
-    nonseg_from_hist_kernel<<<1, 256, 0, stream>>>(counts, Nc, nonseg);
+    nonseg_from_hist_kernel<<<1, 32, 0, stream>>>(counts, Nc, nonseg);
     project_hist_kernel<<<nb, kProjThreads, 0, stream>>>(counts, Nc, n, lgc, partial, per_block);
     used_blocks = nb;
   } else {
@@ -513,7 +564,7 @@ gf_status gf_site_frequency_spectrum_noalloc(const float* d_freq, int32_t M, int
     used_blocks = nb;
   }
   GF_NA_CUDA(cudaGetLastError());
-  sfs_finish_kernel<<<std::max(1, (n + 255) / 256), 256, 0, stream>>>(partial, used_blocks, n,
+  sfs_finish_kernel<<<(n + 31) / 32, 32 * kFinishWarps, 0, stream>>>(partial, used_blocks, n,
                                                                       static_cast<double>(num_sites - M), nonseg, d_out);
   GF_NA_CUDA(cudaGetLastError());
   return GF_OK;
