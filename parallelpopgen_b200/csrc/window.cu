@@ -281,8 +281,10 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
   }
 }
 
-// One block per replicate: exclusive scan of its tile survivor counts, compacted count.
+// One block per replicate: exclusive scan of its tile survivor counts, compacted count.  Each thread
+// takes kSegScanItems consecutive tiles, so one pass covers 8,192 tiles (8.4 M slots).
 constexpr int kSegScanThreads = 1024;
+constexpr int kSegScanItems = 8;
 __global__ void __launch_bounds__(kSegScanThreads)
     seg_scan_kernel(const unsigned* __restrict__ tile_count, unsigned* __restrict__ tile_offset,
                     const WinRep* __restrict__ reps, const int* __restrict__ M_end, int* __restrict__ M_out) {
@@ -295,10 +297,16 @@ __global__ void __launch_bounds__(kSegScanThreads)
   const long long t0 = R.base / kWinTile;
   if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
-  for (int base = 0; base < n; base += kSegScanThreads) {
-    const int i = base + threadIdx.x;
-    const unsigned v = i < n ? tile_count[t0 + i] : 0u;
-    unsigned incl = v;
+  for (int base = 0; base < n; base += kSegScanThreads * kSegScanItems) {
+    const int first = base + threadIdx.x * kSegScanItems;
+    unsigned v[kSegScanItems];
+    unsigned sum = 0;
+#pragma unroll
+    for (int k = 0; k < kSegScanItems; ++k) {
+      v[k] = first + k < n ? tile_count[t0 + first + k] : 0u;
+      sum += v[k];
+    }
+    unsigned incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -317,17 +325,25 @@ __global__ void __launch_bounds__(kSegScanThreads)
       s_warp[lane] = wi - wv;
     }
     __syncthreads();
-    const unsigned excl = s_carry + s_warp[warp] + incl - v;
-    if (i < n) tile_offset[t0 + i] = excl;
+    unsigned run = s_carry + s_warp[warp] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kSegScanItems; ++k) {
+      if (first + k < n) tile_offset[t0 + first + k] = run;
+      run += v[k];
+    }
     __syncthreads();
-    if (threadIdx.x == kSegScanThreads - 1) s_carry = excl + v;
+    if (threadIdx.x == kSegScanThreads - 1) s_carry = run;
     __syncthreads();
   }
   if (threadIdx.x == 0) M_out[R.rep] = static_cast<int>(s_carry);
 }
 
 // Stable scatter of every compacting replicate's survivors (scatter_arrays, go_fish_impl.cu:147-189),
-// staged through shared memory into one contiguous run per tile.
+// staged through shared memory into one contiguous run per tile.  FUSED stages the frequency and
+// both ID words of a tile together (one barrier, the three loads in flight at once, 12 KB of staging)
+// -- faster for one large replicate; otherwise the arrays go one after the other through one 4 KB
+// buffer, which keeps more blocks resident for the many small tiles of a batch.
+template <bool FUSED>
 __global__ void __launch_bounds__(kWinThreads)
     seg_scatter_kernel(const float* __restrict__ src, float* __restrict__ dst, const int* __restrict__ gp_src,
                        const int* __restrict__ tid_src, int* __restrict__ gp_dst, int* __restrict__ tid_dst,
@@ -340,7 +356,7 @@ __global__ void __launch_bounds__(kWinThreads)
   load_tile0(s_tile0, reps, nreps);
   __shared__ unsigned s_words[32];
   __shared__ unsigned s_prefix[32];
-  __shared__ float s_stage[kWinTile];
+  __shared__ float s_stage[FUSED ? 3 * kWinTile : kWinTile];
   const int t = threadIdx.x;
   for (int gt = blockIdx.x; gt < ntiles_all; gt += gridDim.x) {
     if (t == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
@@ -371,6 +387,35 @@ __global__ void __launch_bounds__(kWinThreads)
     const int count = static_cast<int>(s_prefix[31] + __popc(s_words[31]));
     const long long out0 = R.base + tile_offset[atile];
     const long long in0 = R.base + static_cast<long long>(tile) * kWinTile + 4 * t;
+    if constexpr (FUSED) {
+      int* s_gstage = reinterpret_cast<int*>(s_stage + kWinTile);
+      int* s_tstage = s_gstage + kWinTile;
+      if (nib) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(src + in0));
+        const int4 g = __ldg(reinterpret_cast<const int4*>(gp_src + in0));
+        const int4 d = __ldg(reinterpret_cast<const int4*>(tid_src + in0));
+        const bool mark = R.preserve != 0;
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+        const int gg[4] = {g.x, g.y, g.z, g.w};
+        const int dd[4] = {d.x, d.y, d.z, d.w};
+        int k = local;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (!((nib >> j) & 1u)) continue;
+          s_stage[k] = vv[j];
+          s_gstage[k] = gg[j];
+          s_tstage[k++] = mark ? -abs(dd[j]) : dd[j];
+        }
+      }
+      __syncthreads();
+      for (int k = t; k < count; k += kWinThreads) {
+        dst[out0 + k] = s_stage[k];
+        gp_dst[out0 + k] = s_gstage[k];
+        tid_dst[out0 + k] = s_tstage[k];
+      }
+      __syncthreads();
+      continue;
+    }
     if (nib) {
       const float4 v = __ldg(reinterpret_cast<const float4*>(src + in0));
       int k = local;
@@ -444,10 +489,10 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
                                                                 w.M_out);
     GF_CUDA(e, cudaGetLastError());
     const int sblocks = std::max(1, std::min(w.total_tiles, e->num_sms * 8));
-    seg_scatter_kernel<<<sblocks, kWinThreads, 0, e->stream>>>(w.B, compact_dst, w.id_gp_cur, w.id_tid_cur,
-                                                               w.id_gp_next, w.id_tid_next, w.flags,
-                                                               w.tile_offset, w.reps, w.nreps, w.M_end,
-                                                               w.total_tiles, w.total_tiles_dev);
+    auto scatter = w.nreps == 1 ? seg_scatter_kernel<true> : seg_scatter_kernel<false>;
+    scatter<<<sblocks, kWinThreads, 0, e->stream>>>(w.B, compact_dst, w.id_gp_cur, w.id_tid_cur, w.id_gp_next,
+                                                    w.id_tid_next, w.flags, w.tile_offset, w.reps, w.nreps,
+                                                    w.M_end, w.total_tiles, w.total_tiles_dev);
     GF_CUDA(e, cudaGetLastError());
     e->kernel_launches += 2;
   }
