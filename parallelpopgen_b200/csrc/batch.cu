@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -484,7 +485,11 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   const long long want = std::max<long long>(1, total / 65536);
   const int workers = static_cast<int>(std::min<long long>(want, std::max(1u, std::min(hw / 2, 6u))));
   WinGen* stage = e->h_rec_stage;
-  for (int t = 0; t < workers; ++t) b->producers.emplace_back(produce_records, b, stage);
+  try {
+    for (int t = 0; t < workers; ++t) b->producers.emplace_back(produce_records, b, stage);
+  } catch (const std::exception&) {
+    if (b->producers.empty()) return fail(e, GF_ERR_STATE, "could not start a record producer thread");
+  }
   b->precomputed = true;
   GF_TRACE_POINT(e, "record producers started");
   return GF_OK;
