@@ -978,129 +978,141 @@ void gf_replicate_population_table(const gf_replicate* rep, int32_t first, int32
 }
 
 gf_status gf_batch_begin(gf_engine* g, const gf_replicate* reps, int32_t R) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  return batch_begin(&g->impl, reps, R);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    return batch_begin(&g->impl, reps, R);
+  });
 }
 
 gf_status gf_batch_set_record_budget(gf_engine* g, int64_t records) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  if (records < 0) return fail(&g->impl, GF_ERR_INVALID_ARGUMENT, "negative record budget");
-  g->impl.batch_record_budget = records;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    if (records < 0) return fail(&g->impl, GF_ERR_INVALID_ARGUMENT, "negative record budget");
+    g->impl.batch_record_budget = records;
+    return GF_OK;
+  });
 }
 
 gf_status gf_batch_run(gf_engine* g, int32_t max_super_steps, int32_t* out_active) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!e->batch) return fail(e, GF_ERR_STATE, "gf_batch_run before gf_batch_begin");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  int active = 1;
-  for (int s = 0; (max_super_steps <= 0 || s < max_super_steps) && active > 0; ++s) {
-    gf_status st = batch_super_step(e, &active);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->batch) return fail(e, GF_ERR_STATE, "gf_batch_run before gf_batch_begin");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    int active = 1;
+    for (int s = 0; (max_super_steps <= 0 || s < max_super_steps) && active > 0; ++s) {
+      gf_status st = batch_super_step(e, &active);
+      if (st != GF_OK) return st;
+    }
+    gf_status st = sync_counts(e);
     if (st != GF_OK) return st;
-  }
-  gf_status st = sync_counts(e);
-  if (st != GF_OK) return st;
-  if (out_active) {
-    int a = 0;
-    for (auto& br : e->batch->reps) a += br.done ? 0 : 1;
-    *out_active = a;
-  }
-  return GF_OK;
+    if (out_active) {
+      int a = 0;
+      for (auto& br : e->batch->reps) a += br.done ? 0 : 1;
+      *out_active = a;
+    }
+    return GF_OK;
+  });
 }
 
 gf_status gf_batch_read_state(gf_engine* g, int32_t r, float* freq_out, int32_t* ids_out, int32_t max_mutations,
                               int32_t* out_num, int32_t* out_generation) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  Batch* b = e->batch;
-  if (!b) return fail(e, GF_ERR_STATE, "no batch");
-  if (r < 0 || r >= b->R) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d outside [0, %d)", r, b->R);
-  GF_CUDA(e, cudaSetDevice(e->device));
-  {
-    gf_status st = sync_counts(e);
-    if (st != GF_OK) return st;
-  }
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  const BatchRep& br = b->reps[r];
-  if (out_num) *out_num = br.M;
-  if (out_generation) *out_generation = br.generation;
-  if (br.M > max_mutations) return fail(e, GF_ERR_CAPACITY, "replicate %d holds %d mutations", r, br.M);
-  if (br.M == 0) return GF_OK;
-  if (freq_out)
-    GF_CUDA(e, cudaMemcpy(freq_out, b->freq[0] + br.base, sizeof(float) * br.M, cudaMemcpyDeviceToHost));
-  if (ids_out) {
-    std::vector<int> gp(br.M), tid(br.M);
-    GF_CUDA(e, cudaMemcpy(gp.data(), b->id_gp[br.id_buf] + br.base, sizeof(int) * br.M, cudaMemcpyDeviceToHost));
-    GF_CUDA(e, cudaMemcpy(tid.data(), b->id_tid[br.id_buf] + br.base, sizeof(int) * br.M, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < br.M; ++i) {
-      ids_out[4 * i + 0] = gp[i] & 0xFFFFFF;
-      ids_out[4 * i + 1] = gp[i] >> 24;
-      ids_out[4 * i + 2] = tid[i];
-      ids_out[4 * i + 3] = 0;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    Batch* b = e->batch;
+    if (!b) return fail(e, GF_ERR_STATE, "no batch");
+    if (r < 0 || r >= b->R) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d outside [0, %d)", r, b->R);
+    GF_CUDA(e, cudaSetDevice(e->device));
+    {
+      gf_status st = sync_counts(e);
+      if (st != GF_OK) return st;
     }
-  }
-  return GF_OK;
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    const BatchRep& br = b->reps[r];
+    if (out_num) *out_num = br.M;
+    if (out_generation) *out_generation = br.generation;
+    if (br.M > max_mutations) return fail(e, GF_ERR_CAPACITY, "replicate %d holds %d mutations", r, br.M);
+    if (br.M == 0) return GF_OK;
+    if (freq_out)
+      GF_CUDA(e, cudaMemcpy(freq_out, b->freq[0] + br.base, sizeof(float) * br.M, cudaMemcpyDeviceToHost));
+    if (ids_out) {
+      std::vector<int> gp(br.M), tid(br.M);
+      GF_CUDA(e, cudaMemcpy(gp.data(), b->id_gp[br.id_buf] + br.base, sizeof(int) * br.M, cudaMemcpyDeviceToHost));
+      GF_CUDA(e, cudaMemcpy(tid.data(), b->id_tid[br.id_buf] + br.base, sizeof(int) * br.M, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < br.M; ++i) {
+        ids_out[4 * i + 0] = gp[i] & 0xFFFFFF;
+        ids_out[4 * i + 1] = gp[i] >> 24;
+        ids_out[4 * i + 2] = tid[i];
+        ids_out[4 * i + 3] = 0;
+      }
+    }
+    return GF_OK;
+  });
 }
 
 gf_status gf_batch_sfs(gf_engine* g, int32_t n, float* out) {
-  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  Batch* b = e->batch;
-  if (!b) return fail(e, GF_ERR_STATE, "no batch");
-  if (n < 1 || n + 1 > 8 * kBatchSfsThreads) return fail(e, GF_ERR_CAPACITY, "sample size %d outside [1, %d)", n, 8 * kBatchSfsThreads);
-  for (int r = 0; r < b->R; ++r)
-    if (n >= b->reps[r].Nc) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: sample size %d >= Nchrom_e %d", r, n, b->reps[r].Nc);
-  GF_CUDA(e, cudaSetDevice(e->device));
-  {
-    gf_status st = sync_counts(e);
-    if (st != GF_OK) return st;
-  }
-  std::vector<SfsRep> sr(b->R);
-  for (int r = 0; r < b->R; ++r) sr[r] = {b->reps[r].base, b->reps[r].M, b->reps[r].p.num_sites};
-  std::vector<double> lgc(n + 1);
-  const double ln = std::lgamma(n + 1.0);
-  for (int k = 0; k <= n; ++k) lgc[k] = ln - std::lgamma(k + 1.0) - std::lgamma(n - k + 1.0);
-  SfsRep* d_sr = nullptr;
-  double* d_lgc = nullptr;
-  float* d_out = nullptr;
-  {
-    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_sr), sizeof(SfsRep) * b->R);
-    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_lgc), sizeof(double) * (n + 1));
-    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_out), sizeof(float) * b->R * n);
-    if (ast != GF_OK) return ast;
-  }
-  GF_CUDA(e, cudaMemcpyAsync(d_sr, sr.data(), sizeof(SfsRep) * b->R, cudaMemcpyHostToDevice, e->stream));
-  GF_CUDA(e, cudaMemcpyAsync(d_lgc, lgc.data(), sizeof(double) * (n + 1), cudaMemcpyHostToDevice, e->stream));
-  batch_sfs_kernel<<<b->R, kBatchSfsThreads, 0, e->stream>>>(b->freq[0], d_sr, n, d_lgc, d_out);
-  GF_CUDA(e, cudaGetLastError());
-  e->kernel_launches += 1;
-  GF_CUDA(e, cudaMemcpyAsync(out, d_out, sizeof(float) * b->R * n, cudaMemcpyDeviceToHost, e->stream));
-  cudaFreeAsync(d_sr, e->stream);
-  cudaFreeAsync(d_lgc, e->stream);
-  cudaFreeAsync(d_out, e->stream);
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    Batch* b = e->batch;
+    if (!b) return fail(e, GF_ERR_STATE, "no batch");
+    if (n < 1 || n + 1 > 8 * kBatchSfsThreads) return fail(e, GF_ERR_CAPACITY, "sample size %d outside [1, %d)", n, 8 * kBatchSfsThreads);
+    for (int r = 0; r < b->R; ++r)
+      if (n >= b->reps[r].Nc) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: sample size %d >= Nchrom_e %d", r, n, b->reps[r].Nc);
+    GF_CUDA(e, cudaSetDevice(e->device));
+    {
+      gf_status st = sync_counts(e);
+      if (st != GF_OK) return st;
+    }
+    std::vector<SfsRep> sr(b->R);
+    for (int r = 0; r < b->R; ++r) sr[r] = {b->reps[r].base, b->reps[r].M, b->reps[r].p.num_sites};
+    std::vector<double> lgc(n + 1);
+    const double ln = std::lgamma(n + 1.0);
+    for (int k = 0; k <= n; ++k) lgc[k] = ln - std::lgamma(k + 1.0) - std::lgamma(n - k + 1.0);
+    SfsRep* d_sr = nullptr;
+    double* d_lgc = nullptr;
+    float* d_out = nullptr;
+    {
+      gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_sr), sizeof(SfsRep) * b->R);
+      if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_lgc), sizeof(double) * (n + 1));
+      if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_out), sizeof(float) * b->R * n);
+      if (ast != GF_OK) return ast;
+    }
+    GF_CUDA(e, cudaMemcpyAsync(d_sr, sr.data(), sizeof(SfsRep) * b->R, cudaMemcpyHostToDevice, e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(d_lgc, lgc.data(), sizeof(double) * (n + 1), cudaMemcpyHostToDevice, e->stream));
+    batch_sfs_kernel<<<b->R, kBatchSfsThreads, 0, e->stream>>>(b->freq[0], d_sr, n, d_lgc, d_out);
+    GF_CUDA(e, cudaGetLastError());
+    e->kernel_launches += 1;
+    GF_CUDA(e, cudaMemcpyAsync(out, d_out, sizeof(float) * b->R * n, cudaMemcpyDeviceToHost, e->stream));
+    cudaFreeAsync(d_sr, e->stream);
+    cudaFreeAsync(d_lgc, e->stream);
+    cudaFreeAsync(d_out, e->stream);
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    return GF_OK;
+  });
 }
 
 gf_status gf_batch_stats_read(gf_engine* g, gf_batch_stats* out) {
-  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  Batch* b = e->batch;
-  if (!b) return fail(e, GF_ERR_STATE, "no batch");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  unsigned long long st[2] = {0, 0};
-  GF_CUDA(e, cudaMemcpyAsync(st, e->d_stats, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  out->mutation_generations = static_cast<double>(st[0]);
-  out->generations = b->generations;
-  out->super_steps = b->super_steps;
-  out->replicates = b->R;
-  int a = 0;
-  for (auto& br : b->reps) a += br.done ? 0 : 1;
-  out->active = a;
-  out->arena_slots = b->arena;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    Batch* b = e->batch;
+    if (!b) return fail(e, GF_ERR_STATE, "no batch");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    unsigned long long st[2] = {0, 0};
+    GF_CUDA(e, cudaMemcpyAsync(st, e->d_stats, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    out->mutation_generations = static_cast<double>(st[0]);
+    out->generations = b->generations;
+    out->super_steps = b->super_steps;
+    out->replicates = b->R;
+    int a = 0;
+    for (auto& br : b->reps) a += br.done ? 0 : 1;
+    out->active = a;
+    out->arena_slots = b->arena;
+    return GF_OK;
+  });
 }
 
 }  // extern "C"

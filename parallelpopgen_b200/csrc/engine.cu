@@ -1196,7 +1196,8 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
   }
   if (device >= n) return GF_ERR_NO_DEVICE;
   if (cudaSetDevice(device) != cudaSuccess) return GF_ERR_NO_DEVICE;
-  gf_engine* g = new gf_engine();
+  gf_engine* g = new (std::nothrow) gf_engine();
+  if (!g) return GF_ERR_OUT_OF_MEMORY;
   Engine* e = &g->impl;
   e->device = device;
   if (cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || e->num_sms < 1) {
@@ -1278,10 +1279,12 @@ const char* gf_engine_last_error(const gf_engine* g) { return g ? g->impl.last_e
 int32_t gf_engine_device(const gf_engine* g) { return g ? g->impl.device : -1; }
 
 gf_status gf_engine_synchronize(gf_engine* g) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  GF_CUDA(e, cudaSetDevice(e->device));
-  return check_device_fault(e);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    GF_CUDA(e, cudaSetDevice(e->device));
+    return check_device_fault(e);
+  });
 }
 
 int32_t gf_new_mutation_count(int32_t seed1, int32_t seed2, float mu, int32_t Nchrom_e, float num_sites,
@@ -1290,221 +1293,237 @@ int32_t gf_new_mutation_count(int32_t seed1, int32_t seed2, float mu, int32_t Nc
 }
 
 gf_status gf_sim_begin_blank(gf_engine* g, const gf_sim_config* c, int32_t start_generation) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  (void)start_generation;
-  return begin_common(e, c, 0);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    (void)start_generation;
+    return begin_common(e, c, 0);
+  });
 }
 
 gf_status gf_sim_begin_from_state(gf_engine* g, const gf_sim_config* c, int32_t start_generation, const float* freq,
                                   const int32_t* mut_ids, int32_t num_mutations, const uint8_t* extinct,
                                   int32_t preserve) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  (void)start_generation;
-  (void)extinct;
-  if (num_mutations < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "num_mutations < 0");
-  if (num_mutations > 0 && (!freq || !mut_ids)) return fail(e, GF_ERR_INVALID_ARGUMENT, "freq / mut_ids is NULL");
-  gf_status st = begin_common(e, c, num_mutations);
-  if (st != GF_OK) return st;
-  if (num_mutations == 0) return GF_OK;
-  const int P = e->P;
-  GF_CUDA(e, cudaMemcpy2DAsync(e->freq[e->cur], sizeof(float) * e->capacity, freq, sizeof(float) * num_mutations,
-                               sizeof(float) * num_mutations, P, cudaMemcpyHostToDevice, e->stream));
-  for (int p = 0; p < P; ++p) {  // rows holding anything but +0.0 (bit pattern 0)
-    const uint32_t* row = reinterpret_cast<const uint32_t*>(freq + static_cast<size_t>(p) * num_mutations);
-    for (int i = 0; i < num_mutations; ++i)
-      if (row[i] != 0u) {
-        e->live_rows |= 1 << p;
-        break;
-      }
-  }
-  std::vector<int> gp(num_mutations), tid(num_mutations);
-  bool any_neg = false;
-  for (int i = 0; i < num_mutations; ++i) {
-    const int gen0 = mut_ids[4 * i + 0], pop0 = mut_ids[4 * i + 1];
-    if (gen0 < 0 || gen0 > GF_MAX_GENERATION || pop0 < 0 || pop0 >= 128)
-      return fail(e, GF_ERR_CAPACITY, "mutation %d: origin generation %d / population %d outside the packed ID range", i,
-                  gen0, pop0);
-    gp[i] = gen0 | (pop0 << 24);
-    tid[i] = preserve ? -std::abs(mut_ids[4 * i + 2]) : mut_ids[4 * i + 2];
-    any_neg |= tid[i] < 0;
-  }
-  GF_CUDA(e, cudaMemcpyAsync(e->id_gp[e->id_cur], gp.data(), sizeof(int) * num_mutations, cudaMemcpyHostToDevice, e->stream));
-  GF_CUDA(e, cudaMemcpyAsync(e->id_tid[e->id_cur], tid.data(), sizeof(int) * num_mutations, cudaMemcpyHostToDevice, e->stream));
-  const int M = num_mutations;
-  GF_CUDA(e, cudaMemcpyAsync(e->d_count, &M, sizeof(int), cudaMemcpyHostToDevice, e->stream));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));  // host vectors go out of scope
-  e->any_preserved = any_neg;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    (void)start_generation;
+    (void)extinct;
+    if (num_mutations < 0) return fail(e, GF_ERR_INVALID_ARGUMENT, "num_mutations < 0");
+    if (num_mutations > 0 && (!freq || !mut_ids)) return fail(e, GF_ERR_INVALID_ARGUMENT, "freq / mut_ids is NULL");
+    gf_status st = begin_common(e, c, num_mutations);
+    if (st != GF_OK) return st;
+    if (num_mutations == 0) return GF_OK;
+    const int P = e->P;
+    GF_CUDA(e, cudaMemcpy2DAsync(e->freq[e->cur], sizeof(float) * e->capacity, freq, sizeof(float) * num_mutations,
+                                 sizeof(float) * num_mutations, P, cudaMemcpyHostToDevice, e->stream));
+    for (int p = 0; p < P; ++p) {  // rows holding anything but +0.0 (bit pattern 0)
+      const uint32_t* row = reinterpret_cast<const uint32_t*>(freq + static_cast<size_t>(p) * num_mutations);
+      for (int i = 0; i < num_mutations; ++i)
+        if (row[i] != 0u) {
+          e->live_rows |= 1 << p;
+          break;
+        }
+    }
+    std::vector<int> gp(num_mutations), tid(num_mutations);
+    bool any_neg = false;
+    for (int i = 0; i < num_mutations; ++i) {
+      const int gen0 = mut_ids[4 * i + 0], pop0 = mut_ids[4 * i + 1];
+      if (gen0 < 0 || gen0 > GF_MAX_GENERATION || pop0 < 0 || pop0 >= 128)
+        return fail(e, GF_ERR_CAPACITY, "mutation %d: origin generation %d / population %d outside the packed ID range", i,
+                    gen0, pop0);
+      gp[i] = gen0 | (pop0 << 24);
+      tid[i] = preserve ? -std::abs(mut_ids[4 * i + 2]) : mut_ids[4 * i + 2];
+      any_neg |= tid[i] < 0;
+    }
+    GF_CUDA(e, cudaMemcpyAsync(e->id_gp[e->id_cur], gp.data(), sizeof(int) * num_mutations, cudaMemcpyHostToDevice, e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(e->id_tid[e->id_cur], tid.data(), sizeof(int) * num_mutations, cudaMemcpyHostToDevice, e->stream));
+    const int M = num_mutations;
+    GF_CUDA(e, cudaMemcpyAsync(e->d_count, &M, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));  // host vectors go out of scope
+    e->any_preserved = any_neg;
+    return GF_OK;
+  });
 }
 
 gf_status gf_sim_begin_mse(gf_engine* g, const gf_sim_config* c, const gf_mse_population* pops, int32_t preserve) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!c || !pops) return fail(e, GF_ERR_INVALID_ARGUMENT, "config / pops is NULL");
-  if (c->num_populations < 1 || c->num_populations > kMaxPops)
-    return fail(e, GF_ERR_INVALID_ARGUMENT, "num_populations %d outside [1, %d]", c->num_populations, kMaxPops);
-  const int P = c->num_populations;
-  MseClassRange cr;
-  std::memset(&cr, 0, sizeof(cr));
-  long long num_classes = 0;
-  for (int p = 0; p < P; ++p) {
-    cr.first_class[p] = static_cast<int>(num_classes);
-    cr.Nc[p] = pops[p].Nchrom_e;
-    if (pops[p].Nchrom_e > 1) num_classes += pops[p].Nchrom_e - 1;
-  }
-  for (int p = P; p <= kMaxPops; ++p) cr.first_class[p] = static_cast<int>(num_classes);
-  GF_CUDA(e, cudaSetDevice(e->device));
-  // class counts, then their exclusive scan; the total is read back once (as the reference does)
-  unsigned* d_counts = nullptr;
-  unsigned* d_starts = nullptr;
-  float* d_area = nullptr;
-  float* d_integral = nullptr;
-  int* d_total = nullptr;
-  const long long ncls = std::max<long long>(num_classes, 1);
-  long long max_nc = 1;
-  for (int p = 0; p < P; ++p) max_nc = std::max<long long>(max_nc, pops[p].Nchrom_e);
-  {
-    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_counts), sizeof(unsigned) * ncls);
-    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_starts), sizeof(unsigned) * ncls);
-    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_area), sizeof(float) * max_nc);
-    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_integral), sizeof(float) * max_nc);
-    if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_total), sizeof(int));
-    if (ast != GF_OK) {
-      for (void* q : {static_cast<void*>(d_counts), static_cast<void*>(d_starts), static_cast<void*>(d_area),
-                      static_cast<void*>(d_integral), static_cast<void*>(d_total)})
-        if (q) cudaFreeAsync(q, e->stream);
-      return ast;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!c || !pops) return fail(e, GF_ERR_INVALID_ARGUMENT, "config / pops is NULL");
+    if (c->num_populations < 1 || c->num_populations > kMaxPops)
+      return fail(e, GF_ERR_INVALID_ARGUMENT, "num_populations %d outside [1, %d]", c->num_populations, kMaxPops);
+    const int P = c->num_populations;
+    MseClassRange cr;
+    std::memset(&cr, 0, sizeof(cr));
+    long long num_classes = 0;
+    for (int p = 0; p < P; ++p) {
+      cr.first_class[p] = static_cast<int>(num_classes);
+      cr.Nc[p] = pops[p].Nchrom_e;
+      if (pops[p].Nchrom_e > 1) num_classes += pops[p].Nchrom_e - 1;
     }
-  }
-  GF_CUDA(e, cudaMemsetAsync(d_counts, 0, sizeof(unsigned) * ncls, e->stream));
-  for (int p = 0; p < P; ++p) {
-    const gf_mse_population& mp = pops[p];
-    const int Nc = mp.Nchrom_e;
-    if (Nc <= 1) continue;
-    const bool selected = (mp.sel_slope != 0.f || mp.sel_intercept != 0.f);
-    if (selected) {
-      mse_area_kernel<<<148, 1024, 0, e->stream>>>(d_area, Nc, 1.0f / Nc, mp.N_ind, mp.F, mp.h, mp.sel_slope,
-                                                    mp.sel_intercept);
-      mse_integral_kernel<<<1, 1024, 0, e->stream>>>(d_area, d_integral, Nc);
+    for (int p = P; p <= kMaxPops; ++p) cr.first_class[p] = static_cast<int>(num_classes);
+    GF_CUDA(e, cudaSetDevice(e->device));
+    // class counts, then their exclusive scan; the total is read back once (as the reference does)
+    unsigned* d_counts = nullptr;
+    unsigned* d_starts = nullptr;
+    float* d_area = nullptr;
+    float* d_integral = nullptr;
+    int* d_total = nullptr;
+    const long long ncls = std::max<long long>(num_classes, 1);
+    long long max_nc = 1;
+    for (int p = 0; p < P; ++p) max_nc = std::max<long long>(max_nc, pops[p].Nchrom_e);
+    {
+      gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_counts), sizeof(unsigned) * ncls);
+      if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_starts), sizeof(unsigned) * ncls);
+      if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_area), sizeof(float) * max_nc);
+      if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_integral), sizeof(float) * max_nc);
+      if (ast == GF_OK) ast = pool_alloc(e, reinterpret_cast<void**>(&d_total), sizeof(int));
+      if (ast != GF_OK) {
+        for (void* q : {static_cast<void*>(d_counts), static_cast<void*>(d_starts), static_cast<void*>(d_area),
+                        static_cast<void*>(d_integral), static_cast<void*>(d_total)})
+          if (q) cudaFreeAsync(q, e->stream);
+        return ast;
+      }
     }
-    mse_count_kernel<<<std::max(1, std::min(1184, (Nc + 255) / 256)), 256, 0, e->stream>>>(
-        d_counts, d_integral, cr.first_class[p], mp.mu, mp.N_ind, Nc, c->num_sites, mp.sel_slope, mp.sel_intercept,
-        mp.F, mp.h, c->seed1, c->seed2, p, selected ? 1 : 0);
+    GF_CUDA(e, cudaMemsetAsync(d_counts, 0, sizeof(unsigned) * ncls, e->stream));
+    for (int p = 0; p < P; ++p) {
+      const gf_mse_population& mp = pops[p];
+      const int Nc = mp.Nchrom_e;
+      if (Nc <= 1) continue;
+      const bool selected = (mp.sel_slope != 0.f || mp.sel_intercept != 0.f);
+      if (selected) {
+        mse_area_kernel<<<148, 1024, 0, e->stream>>>(d_area, Nc, 1.0f / Nc, mp.N_ind, mp.F, mp.h, mp.sel_slope,
+                                                      mp.sel_intercept);
+        mse_integral_kernel<<<1, 1024, 0, e->stream>>>(d_area, d_integral, Nc);
+      }
+      mse_count_kernel<<<std::max(1, std::min(1184, (Nc + 255) / 256)), 256, 0, e->stream>>>(
+          d_counts, d_integral, cr.first_class[p], mp.mu, mp.N_ind, Nc, c->num_sites, mp.sel_slope, mp.sel_intercept,
+          mp.F, mp.h, c->seed1, c->seed2, p, selected ? 1 : 0);
+      GF_CUDA(e, cudaGetLastError());
+      e->kernel_launches += selected ? 3 : 1;
+    }
+    e->kernel_launches += 2;  // class scan + slot fill
+    scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(d_counts, d_starts, static_cast<int>(num_classes), d_total,
+                                                              nullptr);
     GF_CUDA(e, cudaGetLastError());
-    e->kernel_launches += selected ? 3 : 1;
-  }
-  e->kernel_launches += 2;  // class scan + slot fill
-  scan_exclusive_kernel<<<1, kScanThreads, 0, e->stream>>>(d_counts, d_starts, static_cast<int>(num_classes), d_total,
-                                                            nullptr);
-  GF_CUDA(e, cudaGetLastError());
-  int M0 = 0;
-  GF_CUDA(e, cudaMemcpyAsync(&M0, d_total, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  gf_status st = begin_common(e, c, M0);
-  if (st == GF_OK && M0 > 0) {
-    mse_fill_kernel<<<std::max(1, std::min(148 * 8, (M0 + 255) / 256)), 256, 0, e->stream>>>(
-        e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], d_starts, static_cast<int>(num_classes), M0,
-        e->capacity, P, preserve ? 1 : 0, cr);
-    cudaError_t err = cudaGetLastError();
-    if (err != cudaSuccess) st = cuda_fail(e, err, "mse_fill_kernel");
-    if (st == GF_OK) {
-      err = cudaMemcpyAsync(e->d_count, &M0, sizeof(int), cudaMemcpyHostToDevice, e->stream);
-      if (err != cudaSuccess) st = cuda_fail(e, err, "cudaMemcpyAsync");
+    int M0 = 0;
+    GF_CUDA(e, cudaMemcpyAsync(&M0, d_total, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    gf_status st = begin_common(e, c, M0);
+    if (st == GF_OK && M0 > 0) {
+      mse_fill_kernel<<<std::max(1, std::min(148 * 8, (M0 + 255) / 256)), 256, 0, e->stream>>>(
+          e->freq[e->cur], e->id_gp[e->id_cur], e->id_tid[e->id_cur], d_starts, static_cast<int>(num_classes), M0,
+          e->capacity, P, preserve ? 1 : 0, cr);
+      cudaError_t err = cudaGetLastError();
+      if (err != cudaSuccess) st = cuda_fail(e, err, "mse_fill_kernel");
+      if (st == GF_OK) {
+        err = cudaMemcpyAsync(e->d_count, &M0, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        if (err != cudaSuccess) st = cuda_fail(e, err, "cudaMemcpyAsync");
+      }
+      e->any_preserved = preserve != 0;
+      for (int p = 0; p < P; ++p)  // populations with equilibrium mutations (the others' rows stay zero)
+        if (pops[p].Nchrom_e > 1) e->live_rows |= 1 << p;
     }
-    e->any_preserved = preserve != 0;
-    for (int p = 0; p < P; ++p)  // populations with equilibrium mutations (the others' rows stay zero)
-      if (pops[p].Nchrom_e > 1) e->live_rows |= 1 << p;
-  }
-  cudaFreeAsync(d_counts, e->stream);
-  cudaFreeAsync(d_starts, e->stream);
-  cudaFreeAsync(d_area, e->stream);
-  cudaFreeAsync(d_integral, e->stream);
-  cudaFreeAsync(d_total, e->stream);
-  return st;
+    cudaFreeAsync(d_counts, e->stream);
+    cudaFreeAsync(d_starts, e->stream);
+    cudaFreeAsync(d_area, e->stream);
+    cudaFreeAsync(d_integral, e->stream);
+    cudaFreeAsync(d_total, e->stream);
+    return st;
+  });
 }
 
 gf_status gf_sim_run(gf_engine* g, const gf_generation* gens, int32_t n) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!e->active) return fail(e, GF_ERR_STATE, "gf_sim_run before gf_sim_begin_*");
-  if (n < 0 || (n > 0 && !gens)) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad generation table");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  if (n == 0) return GF_OK;
-  return run_batch(e, gens, n);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->active) return fail(e, GF_ERR_STATE, "gf_sim_run before gf_sim_begin_*");
+    if (n < 0 || (n > 0 && !gens)) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad generation table");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    if (n == 0) return GF_OK;
+    return run_batch(e, gens, n);
+  });
 }
 
 gf_status gf_sim_num_mutations(gf_engine* g, int32_t* out) {
-  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  int M = 0;
-  gf_status st = current_count(e, &M);
-  if (st != GF_OK) return st;
-  *out = M;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    int M = 0;
+    gf_status st = current_count(e, &M);
+    if (st != GF_OK) return st;
+    *out = M;
+    return GF_OK;
+  });
 }
 
 gf_status gf_sim_read_state(gf_engine* g, float* freq_out, int32_t* ids_out, int32_t max_mutations,
                             int32_t* out_num) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  int M = 0;
-  gf_status st = current_count(e, &M);
-  if (st != GF_OK) return st;
-  if (out_num) *out_num = M;
-  if (M > max_mutations) return fail(e, GF_ERR_CAPACITY, "state holds %d mutations, caller buffer %d", M, max_mutations);
-  if (M == 0) return GF_OK;
-  if (freq_out) {
-    GF_CUDA(e, cudaMemcpy2DAsync(freq_out, sizeof(float) * M, e->freq[e->cur], sizeof(float) * e->capacity,
-                                 sizeof(float) * M, e->P, cudaMemcpyDeviceToHost, e->stream));
-  }
-  if (ids_out) {
-    // the reference's int4 IDs (generation, population, threadID, 0) are assembled on the device from
-    // the packed words and copied out in one transfer
-    int4* d_ids = nullptr;
-    gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_ids), sizeof(int4) * static_cast<size_t>(M));
-    if (ast != GF_OK) return ast;
-    expand_ids_kernel<<<std::min(148 * 8, (M + 255) / 256), 256, 0, e->stream>>>(e->id_gp[e->id_cur],
-                                                                               e->id_tid[e->id_cur], M, d_ids);
-    cudaError_t err = cudaGetLastError();
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(ids_out, d_ids, sizeof(int4) * static_cast<size_t>(M), cudaMemcpyDeviceToHost, e->stream);
-    cudaFreeAsync(d_ids, e->stream);
-    if (err != cudaSuccess) return cuda_fail(e, err, "reading mutation IDs");
-  }
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    int M = 0;
+    gf_status st = current_count(e, &M);
+    if (st != GF_OK) return st;
+    if (out_num) *out_num = M;
+    if (M > max_mutations) return fail(e, GF_ERR_CAPACITY, "state holds %d mutations, caller buffer %d", M, max_mutations);
+    if (M == 0) return GF_OK;
+    if (freq_out) {
+      GF_CUDA(e, cudaMemcpy2DAsync(freq_out, sizeof(float) * M, e->freq[e->cur], sizeof(float) * e->capacity,
+                                   sizeof(float) * M, e->P, cudaMemcpyDeviceToHost, e->stream));
+    }
+    if (ids_out) {
+      // the reference's int4 IDs (generation, population, threadID, 0) are assembled on the device from
+      // the packed words and copied out in one transfer
+      int4* d_ids = nullptr;
+      gf_status ast = pool_alloc(e, reinterpret_cast<void**>(&d_ids), sizeof(int4) * static_cast<size_t>(M));
+      if (ast != GF_OK) return ast;
+      expand_ids_kernel<<<std::min(148 * 8, (M + 255) / 256), 256, 0, e->stream>>>(e->id_gp[e->id_cur],
+                                                                                 e->id_tid[e->id_cur], M, d_ids);
+      cudaError_t err = cudaGetLastError();
+      if (err == cudaSuccess)
+        err = cudaMemcpyAsync(ids_out, d_ids, sizeof(int4) * static_cast<size_t>(M), cudaMemcpyDeviceToHost, e->stream);
+      cudaFreeAsync(d_ids, e->stream);
+      if (err != cudaSuccess) return cuda_fail(e, err, "reading mutation IDs");
+    }
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    return GF_OK;
+  });
 }
 
 gf_status gf_sim_stats_read(gf_engine* g, gf_sim_stats* out) {
-  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  GF_CUDA(e, cudaSetDevice(e->device));
-  unsigned long long st[2] = {0, 0};
-  GF_CUDA(e, cudaMemcpyAsync(st, e->d_stats, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  out->mutation_generations = static_cast<double>(st[0]);
-  out->generations = static_cast<int64_t>(st[1]);
-  out->compactions = e->compactions;
-  out->kernel_launches = e->kernel_launches;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    GF_CUDA(e, cudaSetDevice(e->device));
+    unsigned long long st[2] = {0, 0};
+    GF_CUDA(e, cudaMemcpyAsync(st, e->d_stats, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    out->mutation_generations = static_cast<double>(st[0]);
+    out->generations = static_cast<int64_t>(st[1]);
+    out->compactions = e->compactions;
+    out->kernel_launches = e->kernel_launches;
+    return GF_OK;
+  });
 }
 
 gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
-  if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (t->draw_strategy < 0 || t->draw_strategy >= kDrawStrategies || t->blocks_per_sm < 0 || t->windows < 0 ||
-      t->windows > 1)
-    return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2, 3}, blocks_per_sm >= 0, windows in {0, 1}");
-  e->draw_strategy = t->draw_strategy;
-  e->blocks_per_sm = t->blocks_per_sm;
-  e->use_windows = t->windows != 0;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !t) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (t->draw_strategy < 0 || t->draw_strategy >= kDrawStrategies || t->blocks_per_sm < 0 || t->windows < 0 ||
+        t->windows > 1)
+      return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2, 3}, blocks_per_sm >= 0, windows in {0, 1}");
+    e->draw_strategy = t->draw_strategy;
+    e->blocks_per_sm = t->blocks_per_sm;
+    e->use_windows = t->windows != 0;
+    return GF_OK;
+  });
 }
 
 gf_status gf_engine_get_tuning(const gf_engine* g, gf_tuning* t) {
@@ -1516,47 +1535,53 @@ gf_status gf_engine_get_tuning(const gf_engine* g, gf_tuning* t) {
 }
 
 gf_status gf_engine_set_profiling(gf_engine* g, int32_t enable) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  g->impl.profiling = enable != 0;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    g->impl.profiling = enable != 0;
+    return GF_OK;
+  });
 }
 
 gf_status gf_engine_read_profile(gf_engine* g, gf_kernel_times* out) {
-  if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  GF_CUDA(e, cudaSetDevice(e->device));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  auto sum = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, double* ms, int64_t* n) -> gf_status {
-    double t = 0;
-    for (auto& pr : v) {
-      float x = 0.f;
-      GF_CUDA(e, cudaEventElapsedTime(&x, pr.first, pr.second));
-      t += x;
-      e->prof_pool.push_back(pr.first);
-      e->prof_pool.push_back(pr.second);
-    }
-    *ms = t;
-    *n = static_cast<int64_t>(v.size());
-    v.clear();
-    return GF_OK;
-  };
-  gf_status st = sum(e->prof_drift, &out->drift_ms, &out->drift_launches);
-  if (st != GF_OK) return st;
-  return sum(e->prof_compact, &out->compact_ms, &out->compactions);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    GF_CUDA(e, cudaSetDevice(e->device));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    auto sum = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, double* ms, int64_t* n) -> gf_status {
+      double t = 0;
+      for (auto& pr : v) {
+        float x = 0.f;
+        GF_CUDA(e, cudaEventElapsedTime(&x, pr.first, pr.second));
+        t += x;
+        e->prof_pool.push_back(pr.first);
+        e->prof_pool.push_back(pr.second);
+      }
+      *ms = t;
+      *n = static_cast<int64_t>(v.size());
+      v.clear();
+      return GF_OK;
+    };
+    gf_status st = sum(e->prof_drift, &out->drift_ms, &out->drift_launches);
+    if (st != GF_OK) return st;
+    return sum(e->prof_compact, &out->compact_ms, &out->compactions);
+  });
 }
 
 gf_status gf_sim_device_state(gf_engine* g, const float** out_freq, int32_t* out_stride, int32_t* out_num) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  int M = 0;
-  gf_status st = current_count(e, &M);
-  if (st != GF_OK) return st;
-  if (out_freq) *out_freq = e->freq[e->cur];
-  if (out_stride) *out_stride = static_cast<int32_t>(e->capacity);
-  if (out_num) *out_num = M;
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    int M = 0;
+    gf_status st = current_count(e, &M);
+    if (st != GF_OK) return st;
+    if (out_freq) *out_freq = e->freq[e->cur];
+    if (out_stride) *out_stride = static_cast<int32_t>(e->capacity);
+    if (out_num) *out_num = M;
+    return GF_OK;
+  });
 }
 
 }  // extern "C"

@@ -320,3 +320,21 @@ void release_batch(Engine* e);
 struct gf_engine {
   gf::Engine impl;
 };
+
+#include <new>
+#include <exception>
+
+namespace gf {
+// No host exception crosses the C ABI: a failed host allocation or thread start inside an entry
+// point becomes a status (with the message on the engine).
+template <typename F>
+gf_status guard_host(gf_engine* g, F&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return g ? fail(&g->impl, GF_ERR_OUT_OF_MEMORY, "host allocation failed") : GF_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& ex) {
+    return g ? fail(&g->impl, GF_ERR_STATE, "host error: %s", ex.what()) : GF_ERR_STATE;
+  }
+}
+}  // namespace gf

@@ -190,42 +190,46 @@ extern "C" {
 gf_status gf_joint_site_frequency_spectrum_device(gf_engine* g, const float* d_freq_a, const float* d_freq_b,
                                                   int32_t M, int32_t n_a, int32_t n_b, float num_sites,
                                                   float* d_out) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  GF_CUDA(e, cudaSetDevice(e->device));
-  return joint_sfs_device(e, d_freq_a, d_freq_b, M, n_a, n_b, num_sites, d_out);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    GF_CUDA(e, cudaSetDevice(e->device));
+    return joint_sfs_device(e, d_freq_a, d_freq_b, M, n_a, n_b, num_sites, d_out);
+  });
 }
 
 gf_status gf_joint_site_frequency_spectrum(gf_engine* g, const float* freq_a, const float* freq_b, int32_t M,
                                            int32_t n_a, int32_t n_b, float num_sites, float* out) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (M < 0 || (M > 0 && (!freq_a || !freq_b)) || !out) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad buffers");
-  if (n_a < 1 || n_b < 1 || n_a > kJMaxN || n_b > kJMaxN)
-    return fail(e, GF_ERR_INVALID_ARGUMENT, "sample sizes %d, %d outside [1, %d]", n_a, n_b, kJMaxN);
-  GF_CUDA(e, cudaSetDevice(e->device));
-  const long long bins = static_cast<long long>(n_a + 1) * (n_b + 1);
-  float* d = nullptr;
-  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&d), sizeof(float) * (2ll * std::max(M, 1) + bins));
-  if (st != GF_OK) return st;
-  float* d_fa = d;
-  float* d_fb = d + std::max(M, 1);
-  float* d_out = d + 2ll * std::max(M, 1);
-  cudaError_t err = cudaSuccess;
-  if (M > 0) {
-    err = cudaMemcpyAsync(d_fa, freq_a, sizeof(float) * M, cudaMemcpyHostToDevice, e->stream);
-    if (err == cudaSuccess) err = cudaMemcpyAsync(d_fb, freq_b, sizeof(float) * M, cudaMemcpyHostToDevice, e->stream);
-  }
-  if (err == cudaSuccess) {
-    st = joint_sfs_device(e, d_fa, d_fb, M, n_a, n_b, num_sites, d_out);
-    if (st == GF_OK)
-      err = cudaMemcpyAsync(out, d_out, sizeof(float) * bins, cudaMemcpyDeviceToHost, e->stream);
-  }
-  cudaFreeAsync(d, e->stream);
-  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
-  if (st != GF_OK) return st;
-  if (err != cudaSuccess) return cuda_fail(e, err, "joint SFS transfer");
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (M < 0 || (M > 0 && (!freq_a || !freq_b)) || !out) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad buffers");
+    if (n_a < 1 || n_b < 1 || n_a > kJMaxN || n_b > kJMaxN)
+      return fail(e, GF_ERR_INVALID_ARGUMENT, "sample sizes %d, %d outside [1, %d]", n_a, n_b, kJMaxN);
+    GF_CUDA(e, cudaSetDevice(e->device));
+    const long long bins = static_cast<long long>(n_a + 1) * (n_b + 1);
+    float* d = nullptr;
+    gf_status st = pool_alloc(e, reinterpret_cast<void**>(&d), sizeof(float) * (2ll * std::max(M, 1) + bins));
+    if (st != GF_OK) return st;
+    float* d_fa = d;
+    float* d_fb = d + std::max(M, 1);
+    float* d_out = d + 2ll * std::max(M, 1);
+    cudaError_t err = cudaSuccess;
+    if (M > 0) {
+      err = cudaMemcpyAsync(d_fa, freq_a, sizeof(float) * M, cudaMemcpyHostToDevice, e->stream);
+      if (err == cudaSuccess) err = cudaMemcpyAsync(d_fb, freq_b, sizeof(float) * M, cudaMemcpyHostToDevice, e->stream);
+    }
+    if (err == cudaSuccess) {
+      st = joint_sfs_device(e, d_fa, d_fb, M, n_a, n_b, num_sites, d_out);
+      if (st == GF_OK)
+        err = cudaMemcpyAsync(out, d_out, sizeof(float) * bins, cudaMemcpyDeviceToHost, e->stream);
+    }
+    cudaFreeAsync(d, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (st != GF_OK) return st;
+    if (err != cudaSuccess) return cuda_fail(e, err, "joint SFS transfer");
+    return GF_OK;
+  });
 }
 
 }  // extern "C"

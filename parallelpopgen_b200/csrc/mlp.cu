@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -927,7 +928,8 @@ gf_status gf_mlp_create(int32_t device, void* stream, const gf_mlp_config* confi
   }
   if (config->batch_capacity <= 0 || config->batch_capacity % BM != 0) return GF_ERR_INVALID_ARGUMENT;
   if (!encode_fn()) return GF_ERR_CUDA;
-  auto* m = new gf_mlp();
+  auto* m = new (std::nothrow) gf_mlp();
+  if (!m) return GF_ERR_OUT_OF_MEMORY;
   m->device = device;
   m->cfg = *config;
   m->cap = config->batch_capacity;
@@ -1042,7 +1044,12 @@ gf_status gf_mlp_set_params(gf_mlp* m, const float* params, int64_t count) {
     return mlp_fail(m, GF_ERR_INVALID_ARGUMENT, "expected %lld parameters, got %lld",
                     static_cast<long long>(gf_mlp_param_count()), static_cast<long long>(count));
   MLP_CUDA(m, cudaSetDevice(m->device));
-  std::vector<float> h(m->n_params_padded, 0.f);
+  std::vector<float> h;
+  try {
+    h.assign(m->n_params_padded, 0.f);
+  } catch (const std::bad_alloc&) {
+    return mlp_fail(m, GF_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
   const float* p = params;
   for (int l = 0; l < GF_MLP_LAYERS; ++l) {
     for (int r = 0; r < m->rows_true[l]; ++r)
@@ -1061,7 +1068,12 @@ gf_status gf_mlp_set_params(gf_mlp* m, const float* params, int64_t count) {
 }
 
 static gf_status unpad_to_host(gf_mlp* m, const float* d_all, float* out) {
-  std::vector<float> h(m->n_params_padded);
+  std::vector<float> h;
+  try {
+    h.resize(m->n_params_padded);
+  } catch (const std::bad_alloc&) {
+    return mlp_fail(m, GF_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
   MLP_CUDA(m, cudaMemcpyAsync(h.data(), d_all, h.size() * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
   MLP_CUDA(m, cudaStreamSynchronize(m->stream));
   float* p = out;

@@ -396,52 +396,60 @@ using namespace gf;
 extern "C" {
 
 gf_status gf_population_histogram_device(gf_engine* g, const float* d_freq, int32_t M, int32_t Nc, float L, float* d_out) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  GF_CUDA(e, cudaSetDevice(e->device));
-  return population_histogram_device(e, d_freq, M, Nc, L, d_out);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    GF_CUDA(e, cudaSetDevice(e->device));
+    return population_histogram_device(e, d_freq, M, Nc, L, d_out);
+  });
 }
 
 gf_status gf_site_frequency_spectrum_device(gf_engine* g, const float* d_freq, int32_t M, int32_t Nc, int32_t n, float L,
                                             float* d_out) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  GF_CUDA(e, cudaSetDevice(e->device));
-  return site_frequency_spectrum_device(e, d_freq, M, Nc, n, L, d_out);
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    GF_CUDA(e, cudaSetDevice(e->device));
+    return site_frequency_spectrum_device(e, d_freq, M, Nc, n, L, d_out);
+  });
 }
 
 gf_status gf_population_histogram(gf_engine* g, const float* freq, int32_t M, int32_t Nc, float L, float* out) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!out || (M > 0 && !freq)) return fail(e, GF_ERR_INVALID_ARGUMENT, "NULL buffer");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  const float* d_freq = nullptr;
-  gf_status st = stage_input(e, freq, M, &d_freq);
-  if (st != GF_OK) return st;
-  st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_out), &e->spec_out_bytes, sizeof(float) * std::max(Nc, 1));
-  if (st != GF_OK) return st;
-  st = population_histogram_device(e, d_freq, M, Nc, L, e->spec_out);
-  if (st != GF_OK) return st;
-  GF_CUDA(e, cudaMemcpyAsync(out, e->spec_out, sizeof(float) * Nc, cudaMemcpyDeviceToHost, e->stream));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!out || (M > 0 && !freq)) return fail(e, GF_ERR_INVALID_ARGUMENT, "NULL buffer");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    const float* d_freq = nullptr;
+    gf_status st = stage_input(e, freq, M, &d_freq);
+    if (st != GF_OK) return st;
+    st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_out), &e->spec_out_bytes, sizeof(float) * std::max(Nc, 1));
+    if (st != GF_OK) return st;
+    st = population_histogram_device(e, d_freq, M, Nc, L, e->spec_out);
+    if (st != GF_OK) return st;
+    GF_CUDA(e, cudaMemcpyAsync(out, e->spec_out, sizeof(float) * Nc, cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    return GF_OK;
+  });
 }
 
 gf_status gf_site_frequency_spectrum(gf_engine* g, const float* freq, int32_t M, int32_t Nc, int32_t n, float L, float* out) {
-  if (!g) return GF_ERR_INVALID_ARGUMENT;
-  Engine* e = &g->impl;
-  if (!out || (M > 0 && !freq)) return fail(e, GF_ERR_INVALID_ARGUMENT, "NULL buffer");
-  GF_CUDA(e, cudaSetDevice(e->device));
-  const float* d_freq = nullptr;
-  gf_status st = stage_input(e, freq, M, &d_freq);
-  if (st != GF_OK) return st;
-  st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_out), &e->spec_out_bytes, sizeof(float) * std::max(n, 1));
-  if (st != GF_OK) return st;
-  st = site_frequency_spectrum_device(e, d_freq, M, Nc, n, L, e->spec_out);
-  if (st != GF_OK) return st;
-  GF_CUDA(e, cudaMemcpyAsync(out, e->spec_out, sizeof(float) * n, cudaMemcpyDeviceToHost, e->stream));
-  GF_CUDA(e, cudaStreamSynchronize(e->stream));
-  return GF_OK;
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!out || (M > 0 && !freq)) return fail(e, GF_ERR_INVALID_ARGUMENT, "NULL buffer");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    const float* d_freq = nullptr;
+    gf_status st = stage_input(e, freq, M, &d_freq);
+    if (st != GF_OK) return st;
+    st = ensure_scratch(e, reinterpret_cast<void**>(&e->spec_out), &e->spec_out_bytes, sizeof(float) * std::max(n, 1));
+    if (st != GF_OK) return st;
+    st = site_frequency_spectrum_device(e, d_freq, M, Nc, n, L, e->spec_out);
+    if (st != GF_OK) return st;
+    GF_CUDA(e, cudaMemcpyAsync(out, e->spec_out, sizeof(float) * n, cudaMemcpyDeviceToHost, e->stream));
+    GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    return GF_OK;
+  });
 }
 
 }  // extern "C"
