@@ -501,6 +501,7 @@ def run_batched(args):
         "mutation_generations_per_step": st["mutation_generations"],
         "mutation_generations_per_s": st["mutation_generations"] / batch_s,
         "super_steps": st["super_steps"],
+        "record_wait_ms_per_batch": st["record_wait_ms"], "record_producers": st["record_producers"],
         "window_ms_per_step": prof["drift_ms"], "window_launches_per_step": prof["drift_launches"],
         "looped_plain": {"value": plain_rate, "unit": "simulations/s", "sample": len(prepared),
                          "speedup_batched_over_looped": value / plain_rate},

@@ -199,6 +199,9 @@ typedef struct gf_batch_stats {
   int32_t replicates;
   int32_t active;
   int64_t arena_slots;         /* device slots reserved for all replicates */
+  double record_wait_ms;       /* host time spent waiting for generation records to be drawn */
+  int32_t record_producers;    /* host threads drawing the records (0: none) */
+  int32_t reserved;
 } gf_batch_stats;
 gf_status gf_batch_stats_read(gf_engine* engine, gf_batch_stats* out);
 /* Generation records (one per replicate per generation, 36 bytes, page-locked on the host and on

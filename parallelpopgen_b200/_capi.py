@@ -71,7 +71,8 @@ class Replicate(ctypes.Structure):
 class BatchStats(ctypes.Structure):
     _fields_ = [("mutation_generations", ctypes.c_double), ("generations", ctypes.c_int64),
                 ("super_steps", ctypes.c_int64), ("replicates", ctypes.c_int32), ("active", ctypes.c_int32),
-                ("arena_slots", ctypes.c_int64)]
+                ("arena_slots", ctypes.c_int64), ("record_wait_ms", ctypes.c_double),
+                ("record_producers", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class SimConfig(ctypes.Structure):

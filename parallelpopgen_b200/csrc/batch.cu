@@ -286,6 +286,24 @@ __global__ void __launch_bounds__(kBatchSfsThreads)
 // ------------------------------------------------------------------------------------------------
 // host
 // ------------------------------------------------------------------------------------------------
+// Grow an engine-owned device buffer to `need` bytes (with a quarter of headroom); its previous
+// contents are not kept.  The stream is idle when this runs (a batch begins after the last one ended).
+static gf_status grow_device(Engine* e, void** mem, size_t* have, size_t need) {
+  if (*have >= need && *mem) return GF_OK;
+  if (*mem) GF_CUDA(e, cudaFree(*mem));
+  *mem = nullptr;
+  *have = 0;
+  const size_t bytes = need + need / 4;
+  const cudaError_t err = cudaMalloc(mem, bytes);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    *mem = nullptr;
+    return cuda_fail(e, err, "batched arena allocation");
+  }
+  *have = bytes;
+  return GF_OK;
+}
+
 void release_batch(Engine* e) {
   Batch* b = e->batch;
   if (!b) return;
@@ -293,31 +311,13 @@ void release_batch(Engine* e) {
   for (auto& t : b->producers) t.join();
   b->producers.clear();
   cudaStreamSynchronize(e->stream);
-  auto release = [e](void* p) {
-    if (p) cudaFreeAsync(p, e->stream);
-  };
-  for (int k = 0; k < 2; ++k) {
-    release(b->freq[k]);
-    release(b->id_gp[k]);
-    release(b->id_tid[k]);
-    release(b->d_M[k]);
-  }
-  release(b->flags);
-  release(b->tile_count);
-  release(b->tile_offset);
-  release(b->d_Mend);
-  release(b->d_all_recs);
-  release(b->d_total_tiles);
+  // the arena buffers and the record buffer are slices of engine-owned allocations (kept)
   cudaStreamSynchronize(e->stream);
-  if (b->h_M) cudaFreeHost(b->h_M);
+  // h_M, the replicate-table ring and its events belong to the engine (kept for the next batch)
   if (b->d_recs) cudaFree(b->d_recs);
   if (b->h_recs) cudaFreeHost(b->h_recs);
   if (b->d_reps) cudaFree(b->d_reps);
   if (b->h_reps) cudaFreeHost(b->h_reps);
-  if (b->d_ring_all) cudaFree(b->d_ring_all);
-  if (b->h_ring_all) cudaFreeHost(b->h_ring_all);
-  for (int k = 0; k < Batch::kRing; ++k)
-    if (b->ring_done[k]) cudaEventDestroy(b->ring_done[k]);
   for (cudaEvent_t ev : b->slot_upload)
     if (ev) cudaEventDestroy(ev);
   delete b;
@@ -424,6 +424,7 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   b->precomputed = false;
   if (e->batch_record_budget <= 0 || total == 0) return GF_OK;
   const int W = std::max(1, (kStreamSlab + cmax - 1) / cmax);
+  b->slab_windows = W;
   int nreg = 0;
   for (auto& br : b->reps) {
     br.chunk = W * std::max(br.p.compact_interval, 1);
@@ -466,8 +467,9 @@ static gf_status precompute_records(Engine* e, Batch* b) {
     GF_CUDA(e, cudaMallocHost(&e->h_rec_stage, sizeof(WinGen) * cap));
     e->h_rec_stage_cap = cap;
   }
-  gf_status st = pool_alloc(e, reinterpret_cast<void**>(&b->d_all_recs), sizeof(WinGen) * slots);
+  gf_status st = grow_device(e, &e->batch_recs_mem, &e->batch_recs_bytes, sizeof(WinGen) * slots);
   if (st != GF_OK) return st;
+  b->d_all_recs = static_cast<WinGen*>(e->batch_recs_mem);
   const int K = b->ring_slots > 0 ? b->ring_slots : nreg;
   b->slot_upload.assign(K, nullptr);
   for (int k = 0; k < K && b->ring_slots > 0; ++k)
@@ -491,6 +493,18 @@ static gf_status precompute_records(Engine* e, Batch* b) {
     if (b->producers.empty()) return fail(e, GF_ERR_STATE, "could not start a record producer thread");
   }
   b->precomputed = true;
+  // lock-step bookkeeping: replicate r's last window is super-step ceil(G_r / c_r) - 1
+  b->finish_at.clear();
+  for (int r = 0; r < b->R; ++r) {
+    const BatchRep& br = b->reps[r];
+    if (br.done) continue;
+    const int c = std::max(br.p.compact_interval, 1);
+    const int last = (br.p.num_generations + c - 1) / c - 1;
+    if (static_cast<int>(b->finish_at.size()) <= last) b->finish_at.resize(last + 1);
+    b->finish_at[last].push_back(r);
+  }
+  b->active_dirty = true;
+  for (int& v : b->slot_version) v = -1;
   GF_TRACE_POINT(e, "record producers started");
   return GF_OK;
 }
@@ -511,7 +525,14 @@ static gf_status stream_upload(Engine* e, Batch* b, int need) {
   };
   const auto t0 = std::chrono::steady_clock::now();
   auto progress = t0;
+  auto wait0 = t0;
+  bool waiting = false;
   long long last = -1;
+  auto account = [&]() {
+    if (waiting)
+      b->record_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wait0).count();
+    waiting = false;
+  };
   for (;;) {
     poll();
     const int j = b->uploaded;
@@ -528,14 +549,20 @@ static gf_status stream_upload(Engine* e, Batch* b, int need) {
     }
     if (j > need) break;   // not needed by this super-step
     const auto now = std::chrono::steady_clock::now();
+    if (!waiting) {
+      waiting = true;
+      wait0 = now;
+    }
     if (done != last) {
       last = done;
       progress = now;
     } else if (now - progress > std::chrono::seconds(120)) {
+      account();
       return fail(e, GF_ERR_STATE, "record producers made no progress on region %d for 120 s", j);
     }
     std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
+  account();
   return GF_OK;
 }
 
@@ -581,7 +608,6 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     m.class_off = class_total;
     area_total += std::max(m.Nc0, 1);
     class_total += std::max(m.Nc0 - 1, 0);
-    br.Nc = m.Nc0;
   }
   MseRep* d_mr = nullptr;
   float *d_area = nullptr, *d_integral = nullptr;
@@ -624,9 +650,18 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
   }
   b->arena = arena;
   {
-    gf_status ast = GF_OK;
+    // slices of one engine-owned allocation, 256-byte aligned, laid out in a fixed order
+    size_t need = 0;
+    auto sz = [](size_t bytes) { return (bytes + 255) / 256 * 256; };
+    need += 2 * (sz(sizeof(float) * arena) + 2 * sz(sizeof(int) * arena) + sz(sizeof(int) * R));
+    need += sz(sizeof(unsigned) * (arena / 32)) + 2 * sz(sizeof(unsigned) * (arena / kBatchTile));
+    need += sz(sizeof(int) * R) + sz(sizeof(int));
+    gf_status ast = grow_device(e, &e->batch_arena_mem, &e->batch_arena_bytes, need);
+    if (ast != GF_OK) return ast;
+    char* cur = static_cast<char*>(e->batch_arena_mem);
     auto pa = [&](void** p, size_t bytes) {
-      if (ast == GF_OK) ast = pool_alloc(e, p, bytes);
+      *p = cur;
+      cur += sz(bytes);
     };
     for (int k = 0; k < 2; ++k) {
       pa(reinterpret_cast<void**>(&b->freq[k]), sizeof(float) * arena);
@@ -639,13 +674,32 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     pa(reinterpret_cast<void**>(&b->tile_offset), sizeof(unsigned) * (arena / kBatchTile));
     pa(reinterpret_cast<void**>(&b->d_Mend), sizeof(int) * R);
     pa(reinterpret_cast<void**>(&b->d_total_tiles), sizeof(int));
-    if (ast != GF_OK) return ast;
   }
-  GF_CUDA(e, cudaMallocHost(&b->h_M, sizeof(int) * 2 * R));
-  GF_CUDA(e, cudaMalloc(&b->d_ring_all, sizeof(WinRep) * R * Batch::kRing));
-  GF_CUDA(e, cudaMallocHost(&b->h_ring_all, sizeof(WinRep) * R * Batch::kRing));
+  static_assert(Batch::kRing == sizeof(Engine::batch_ring_done) / sizeof(cudaEvent_t), "ring events");
+  if (e->batch_h_M_cap < static_cast<size_t>(2 * R)) {
+    if (e->batch_h_M) GF_CUDA(e, cudaFreeHost(e->batch_h_M));
+    e->batch_h_M = nullptr;
+    e->batch_h_M_cap = 0;
+    GF_CUDA(e, cudaMallocHost(&e->batch_h_M, sizeof(int) * 2 * R));
+    e->batch_h_M_cap = 2 * R;
+  }
+  if (e->batch_ring_reps < static_cast<size_t>(R)) {
+    if (e->batch_d_ring) GF_CUDA(e, cudaFree(e->batch_d_ring));
+    if (e->batch_h_ring) GF_CUDA(e, cudaFreeHost(e->batch_h_ring));
+    e->batch_d_ring = nullptr;
+    e->batch_h_ring = nullptr;
+    e->batch_ring_reps = 0;
+    GF_CUDA(e, cudaMalloc(&e->batch_d_ring, sizeof(WinRep) * R * Batch::kRing));
+    GF_CUDA(e, cudaMallocHost(&e->batch_h_ring, sizeof(WinRep) * R * Batch::kRing));
+    e->batch_ring_reps = R;
+  }
   for (int k = 0; k < Batch::kRing; ++k)
-    GF_CUDA(e, cudaEventCreateWithFlags(&b->ring_done[k], cudaEventDisableTiming));
+    if (!e->batch_ring_done[k]) GF_CUDA(e, cudaEventCreateWithFlags(&e->batch_ring_done[k], cudaEventDisableTiming));
+  b->h_M = e->batch_h_M;
+  b->d_ring_all = e->batch_d_ring;
+  b->h_ring_all = e->batch_h_ring;
+  b->ring_stride = e->batch_ring_reps;
+  for (int k = 0; k < Batch::kRing; ++k) b->ring_done[k] = e->batch_ring_done[k];
   GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
@@ -747,45 +801,81 @@ static gf_status sync_counts(Engine* e) {
 // read-back (a one-block kernel assigns each replicate's tiles from its device-side count; tiles past
 // a replicate's end-of-window count return at once).  The replicate table goes through a ring of
 // pinned/device slots, each reused only after the launch that read it has finished.
+// Fields of unfinished replicates after k lock-step super-steps (finished ones are final already).
+static void sync_progress(Batch* b) {
+  if (!b->precomputed) return;
+  const long long k = b->super_steps;
+  for (int r : b->active) {
+    BatchRep& br = b->reps[r];
+    if (br.done) continue;
+    br.generation = static_cast<int>(k * br.p.compact_interval);
+    br.next_compact = br.generation + br.p.compact_interval;
+    br.id_buf = b->id_cur;
+    br.m_slot = b->mslot;
+  }
+}
+
 static gf_status batch_super_step(Engine* e, int* active_out) {
   Batch* b = e->batch;
   if (!b->precomputed) return batch_super_step_fallback(e, active_out);
-  const int slot = b->ring;
-  GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
-  WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->R;
-  WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->R;
-  int nj = 0, tiles = 0, need_region = 0;
-  for (int r = 0; r < b->R; ++r) {
-    BatchRep& br = b->reps[r];
-    if (br.done) continue;
-    const int end = std::min(br.next_compact, br.p.num_generations);
-    const int ngen = end - br.generation;
-    const int j = br.generation / br.chunk;
-    WinRep& w = hr[nj++];
-    const int off = (j < b->nregions) ? b->region_off[static_cast<size_t>(r) * b->nregions + j] : -1;
-    if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
-    w.rec = static_cast<int>(region_slot_base(b, j) + off + (br.generation - static_cast<long long>(j) * br.chunk));
-    need_region = std::max(need_region, j);
-    w.base = br.base;
-    w.capacity = br.capacity;
-    w.ngen = ngen;
-    w.tile0 = tiles;
-    w.ntiles = static_cast<int>(br.capacity / kBatchTile);
-    w.seed1 = br.p.seed1;
-    w.seed2 = br.p.seed2;
-    w.check_preserved = 0;
-    w.compact = 1;
-    w.preserve = 0;
-    w.rep = r;
-    w.births = 0;   // summed on the device from the records (batch_tiles_kernel)
-    tiles += w.ntiles;
+  if (b->active_dirty) {
+    b->active.clear();
+    b->active_tiles = 0;
+    b->active_cadence_sum = 0;
+    for (int r = 0; r < b->R; ++r) {
+      const BatchRep& br = b->reps[r];
+      if (br.done) continue;
+      b->active.push_back(r);
+      b->active_tiles += br.capacity / kBatchTile;
+      b->active_cadence_sum += br.p.compact_interval;
+    }
+    b->list_version += 1;
+    b->active_dirty = false;
   }
+  const int nj = static_cast<int>(b->active.size());
   if (nj == 0) {
     if (active_out) *active_out = 0;
     return GF_OK;
   }
+  const long long k = b->super_steps;
+  const int j = static_cast<int>(k / b->slab_windows);   // the record region of every active replicate
+  if (j >= b->nregions) return fail(e, GF_ERR_STATE, "super-step %lld beyond the record regions", k);
+  const int slot = b->ring;
+  GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
+  WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->ring_stride;
+  WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->ring_stride;
+  // a slot that last held this list only needs the per-step fields
+  const bool full = b->slot_version[slot] != b->list_version;
+  const long long region = region_slot_base(b, j);
+  int tiles = 0;
+  for (int i = 0; i < nj; ++i) {
+    const int r = b->active[i];
+    const BatchRep& br = b->reps[r];
+    const int c = br.p.compact_interval;
+    const long long gen = k * c;
+    const int off = b->region_off[static_cast<size_t>(r) * b->nregions + j];
+    if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
+    WinRep& w = hr[i];
+    w.rec = static_cast<int>(region + off + (gen - static_cast<long long>(j) * br.chunk));
+    w.ngen = static_cast<int>(std::min<long long>(c, br.p.num_generations - gen));
+    if (full) {
+      w.base = br.base;
+      w.capacity = br.capacity;
+      w.tile0 = tiles;
+      w.ntiles = static_cast<int>(br.capacity / kBatchTile);
+      w.seed1 = br.p.seed1;
+      w.seed2 = br.p.seed2;
+      w.check_preserved = 0;
+      w.compact = 1;
+      w.preserve = 0;
+      w.rep = r;
+      w.births = 0;   // summed on the device from the records (batch_tiles_kernel)
+      tiles += w.ntiles;
+    }
+  }
+  b->slot_version[slot] = b->list_version;
   {
-    gf_status ust = stream_upload(e, b, need_region);   // the records of this super-step, in stream order
+    gf_status ust = stream_upload(e, b, j);   // the records of this super-step, in stream order
     if (ust != GF_OK) return ust;
   }
   GF_CUDA(e, cudaMemcpyAsync(dr, hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));
@@ -809,7 +899,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   w.reps = dr;
   w.nreps = nj;
   w.recs = b->d_all_recs;
-  w.total_tiles = tiles;                 // segment tiles: an upper bound, sizes the grid
+  w.total_tiles = static_cast<int>(b->active_tiles);   // segment tiles: an upper bound, sizes the grid
   w.total_tiles_dev = b->d_total_tiles;
   w.any_compact = true;
   w.stats = e->d_stats;
@@ -832,19 +922,25 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   b->id_cur ^= 1;
   b->super_steps += 1;
   b->counts_stale = true;
-  int active = 0;
-  for (int j = 0; j < nj; ++j) {
-    BatchRep& br = b->reps[hr[j].rep];
-    br.generation += hr[j].ngen;
-    b->generations += hr[j].ngen;
-    br.next_compact = br.generation + br.p.compact_interval;
-    br.Nc = rep_nchrom(br.p, br.generation);
-    br.id_buf = b->id_cur;
-    br.m_slot = b->mslot;
-    if (br.generation >= br.p.num_generations) br.done = true;
-    else ++active;
+  // generations of this step: every active replicate's cadence, less what the finishing ones lack
+  long long gens = b->active_cadence_sum;
+  int finishing = 0;
+  if (k < static_cast<long long>(b->finish_at.size())) {
+    for (int r : b->finish_at[k]) {
+      BatchRep& br = b->reps[r];
+      const long long gen = k * br.p.compact_interval;
+      gens -= br.p.compact_interval - (br.p.num_generations - gen);
+      br.generation = br.p.num_generations;
+      br.next_compact = br.generation + br.p.compact_interval;
+      br.id_buf = b->id_cur;
+      br.m_slot = b->mslot;
+      br.done = true;
+      ++finishing;
+    }
+    if (finishing) b->active_dirty = true;
   }
-  if (active_out) *active_out = active;
+  b->generations += gens;
+  if (active_out) *active_out = nj - finishing;
   return GF_OK;
 }
 
@@ -952,7 +1048,6 @@ static gf_status batch_super_step_fallback(Engine* e, int* active_out) {
     br.generation += jobs[j].second;
     b->generations += jobs[j].second;
     br.next_compact = br.generation + br.p.compact_interval;
-    br.Nc = rep_nchrom(br.p, br.generation);
     br.id_buf = b->id_cur;
     br.m_slot = b->mslot;
     if (br.generation >= br.p.num_generations) br.done = true;
@@ -1002,8 +1097,12 @@ gf_status gf_batch_run(gf_engine* g, int32_t max_super_steps, int32_t* out_activ
     int active = 1;
     for (int s = 0; (max_super_steps <= 0 || s < max_super_steps) && active > 0; ++s) {
       gf_status st = batch_super_step(e, &active);
-      if (st != GF_OK) return st;
+      if (st != GF_OK) {
+        sync_progress(e->batch);
+        return st;
+      }
     }
+    sync_progress(e->batch);
     gf_status st = sync_counts(e);
     if (st != GF_OK) return st;
     if (out_active) {
@@ -1058,8 +1157,10 @@ gf_status gf_batch_sfs(gf_engine* g, int32_t n, float* out) {
     Batch* b = e->batch;
     if (!b) return fail(e, GF_ERR_STATE, "no batch");
     if (n < 1 || n + 1 > 8 * kBatchSfsThreads) return fail(e, GF_ERR_CAPACITY, "sample size %d outside [1, %d)", n, 8 * kBatchSfsThreads);
-    for (int r = 0; r < b->R; ++r)
-      if (n >= b->reps[r].Nc) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: sample size %d >= Nchrom_e %d", r, n, b->reps[r].Nc);
+    for (int r = 0; r < b->R; ++r) {
+      const int Nc = rep_nchrom(b->reps[r].p, b->reps[r].generation);   // Nchrom_e at its current generation
+      if (n >= Nc) return fail(e, GF_ERR_INVALID_ARGUMENT, "replicate %d: sample size %d >= Nchrom_e %d", r, n, Nc);
+    }
     GF_CUDA(e, cudaSetDevice(e->device));
     {
       gf_status st = sync_counts(e);
@@ -1110,6 +1211,9 @@ gf_status gf_batch_stats_read(gf_engine* g, gf_batch_stats* out) {
     int a = 0;
     for (auto& br : b->reps) a += br.done ? 0 : 1;
     out->active = a;
+    out->record_wait_ms = b->record_wait_ms;
+    out->record_producers = static_cast<int32_t>(b->producers.size());
+    out->reserved = 0;
     out->arena_slots = b->arena;
     return GF_OK;
   });

@@ -138,7 +138,6 @@ struct BatchRep {
   int generation = 0;       // last generation run
   int next_compact = 0;
   int M = 0;                // count after the last read-back
-  int Nc = 0;               // Nchrom_e at `generation`
   int id_buf = 0;           // ID buffer holding its state
   int m_slot = 0;           // count array (d_M[m_slot]) holding its latest count
   int chunk = 0;            // generations per record slab (a multiple of its compaction cadence)
@@ -174,8 +173,9 @@ struct Batch {
   // ring of per-super-step replicate tables: a slot is rewritten only after the launch that read it
   // (64 slots: the host may run that many super-steps ahead of the GPU)
   static constexpr int kRing = 64;
-  WinRep* d_ring_all = nullptr;       // kRing tables of R entries, one allocation each side
+  WinRep* d_ring_all = nullptr;       // kRing tables of ring_stride entries (the engine's buffers)
   WinRep* h_ring_all = nullptr;
+  size_t ring_stride = 0;
   cudaEvent_t ring_done[kRing] = {};
   int ring = 0;
   bool counts_stale = false;          // counts on the device are newer than reps[].M
@@ -197,6 +197,19 @@ struct Batch {
   std::atomic<int> producible{0};             // producers may draw regions below this
   std::atomic<bool> cancel{false};
   std::vector<std::thread> producers;
+  double record_wait_ms = 0.0;                // host time the super-steps waited for records
+  // Every replicate advances one window of its cadence per super-step from generation 0, so after k
+  // super-steps an unfinished replicate is at generation k * c_r and in record region k / slab_windows.
+  // The host keeps only the list of unfinished replicates and the replicates finishing at each step;
+  // their per-replicate fields are brought up to date when a run returns (sync_progress).
+  int slab_windows = 1;                       // windows per record slab
+  std::vector<int> active;                    // unfinished replicates, in index order
+  bool active_dirty = true;
+  int list_version = 0;
+  int slot_version[64];                       // list_version whose full entries a ring slot holds
+  long long active_tiles = 0;                 // segment tiles of the active replicates
+  long long active_cadence_sum = 0;           // sum of their cadences (generations per super-step)
+  std::vector<std::vector<int>> finish_at;    // [k]: replicates whose last window is super-step k
 };
 
 struct PendingCount {
@@ -279,6 +292,22 @@ struct Engine {
   // page-locked staging of batched generation records, kept across batches (grown on demand)
   WinGen* h_rec_stage = nullptr;
   size_t h_rec_stage_cap = 0;
+  // the batched engine's per-super-step replicate tables (a ring of 64, device and page-locked host),
+  // their events and the page-locked count read-back, kept across batches (grown on demand): pinning
+  // and freeing them per batch cost up to hundreds of milliseconds on a busy host
+  WinRep* batch_d_ring = nullptr;
+  WinRep* batch_h_ring = nullptr;
+  size_t batch_ring_reps = 0;                 // replicates per table
+  cudaEvent_t batch_ring_done[64] = {};
+  int* batch_h_M = nullptr;
+  size_t batch_h_M_cap = 0;
+  // the batched engine's device arena (state, IDs, flags, tile counts) and generation records, also
+  // kept across batches and grown on demand: carving a new batch's gigabytes out of the stream-ordered
+  // pool after its small temporaries fragmented it could map fresh memory (~0.5 s) every other batch
+  void* batch_arena_mem = nullptr;
+  size_t batch_arena_bytes = 0;
+  void* batch_recs_mem = nullptr;
+  size_t batch_recs_bytes = 0;
   void* spec_scratch = nullptr;
   size_t spec_scratch_bytes = 0;
   float* spec_in = nullptr;
