@@ -460,10 +460,19 @@ def run_batched(args):
             ev1.synchronize()
             times.append(ev0.elapsed_time(ev1) * 1e-3)
     batch_s = float(np.mean(times))
-    # one more batch with the window launches bracketed by CUDA events: device time of the drift work
+    # one more batch with the window launches bracketed by CUDA events (device time of the drift work)
+    # and host wall-clock phases, the device synchronised between them
     eng.set_profiling(True)
     eng.read_profile()
-    batch_step()
+    ph0 = time.perf_counter()
+    eng.batch_begin(reps)
+    eng.synchronize()
+    ph1 = time.perf_counter()
+    eng.batch_run()                      # returns after reading the counts back
+    ph2 = time.perf_counter()
+    eng.batch_sfs(n, len(reps))
+    ph3 = time.perf_counter()
+    phases = {"begin": 1e3 * (ph1 - ph0), "run": 1e3 * (ph2 - ph1), "sfs": 1e3 * (ph3 - ph2)}
     prof = eng.read_profile()
     eng.set_profiling(False)
     # the same replicates, one plain engine run each (a random sample, timed engine calls only)
@@ -502,6 +511,7 @@ def run_batched(args):
         "mutation_generations_per_s": st["mutation_generations"] / batch_s,
         "super_steps": st["super_steps"],
         "record_wait_ms_per_batch": st["record_wait_ms"], "record_producers": st["record_producers"],
+        "phases_ms_profiled_batch": phases,
         "window_ms_per_step": prof["drift_ms"], "window_launches_per_step": prof["drift_launches"],
         "looped_plain": {"value": plain_rate, "unit": "simulations/s", "sample": len(prepared),
                          "speedup_batched_over_looped": value / plain_rate},
