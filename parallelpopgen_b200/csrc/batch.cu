@@ -25,6 +25,7 @@
 #include "gf_drift.cuh"
 #include "gf_internal.h"
 #include "gf_mse.cuh"
+#include "gf_plan.h"
 
 #ifdef GF_TRACE
 #include <chrono>
@@ -387,19 +388,15 @@ static void make_record(const gf_replicate& p, int g, WinGen& w) {
 // order), and its slabs are drawn once the upload of region j - K has read the staging slot.
 constexpr int kStreamSlab = 512;
 
-static long long region_slot_base(const Batch* b, int j) {
-  return b->ring_slots > 0 ? static_cast<long long>(j % b->ring_slots) * b->slot_records : b->region_base[j];
-}
-
 static void produce_records(Batch* b, WinGen* stage) {
   const long long R = b->R;
-  const long long jobs = R * b->nregions;
+  const long long jobs = R * b->plan.nregions;
   for (;;) {
     if (b->cancel.load(std::memory_order_relaxed)) return;
     const long long i = b->next_job.fetch_add(1, std::memory_order_relaxed);
     if (i >= jobs) return;
     const int j = static_cast<int>(i / R), r = static_cast<int>(i % R);
-    const int off = b->region_off[static_cast<size_t>(r) * b->nregions + j];
+    const int off = b->plan.region_off[static_cast<size_t>(r) * b->plan.nregions + j];
     if (off < 0) continue;
     while (j >= b->producible.load(std::memory_order_acquire)) {   // its staging slot is still being read
       if (b->cancel.load(std::memory_order_relaxed)) return;
@@ -408,57 +405,25 @@ static void produce_records(Batch* b, WinGen* stage) {
     const BatchRep& br = b->reps[r];
     const int g0 = j * br.chunk;
     const int g1 = std::min(br.p.num_generations, g0 + br.chunk);
-    WinGen* out = stage + region_slot_base(b, j) + off;
+    WinGen* out = stage + b->plan.slot_base(j) + off;
     for (int g = g0 + 1; g <= g1; ++g) make_record(br.p, g, out[g - g0 - 1]);
     b->region_done[j].fetch_add(1, std::memory_order_release);
   }
 }
 
 static gf_status precompute_records(Engine* e, Batch* b) {
-  long long total = 0;
-  int cmax = 1;
-  for (auto& br : b->reps) {
-    total += br.p.num_generations;
-    cmax = std::max(cmax, br.p.compact_interval);
-  }
   b->precomputed = false;
+  long long total = 0;
+  for (auto& br : b->reps) total += br.p.num_generations;
   if (e->batch_record_budget <= 0 || total == 0) return GF_OK;
-  const int W = std::max(1, (kStreamSlab + cmax - 1) / cmax);
-  b->slab_windows = W;
-  int nreg = 0;
-  for (auto& br : b->reps) {
-    br.chunk = W * std::max(br.p.compact_interval, 1);
-    nreg = std::max(nreg, (br.p.num_generations + br.chunk - 1) / br.chunk);
-  }
-  b->nregions = nreg;
-  b->region_off.assign(static_cast<size_t>(b->R) * nreg, -1);
-  b->region_base.assign(nreg + 1, 0);
-  b->region_jobs.assign(nreg, 0);
-  long long off = 0, largest = 0;
-  for (int j = 0; j < nreg; ++j) {
-    b->region_base[j] = off;
-    for (int r = 0; r < b->R; ++r) {
-      const BatchRep& br = b->reps[r];
-      const int g0 = j * br.chunk;
-      if (g0 >= br.p.num_generations) continue;
-      b->region_off[static_cast<size_t>(r) * nreg + j] = static_cast<int>(off - b->region_base[j]);
-      off += std::min(br.p.num_generations, g0 + br.chunk) - g0;
-      b->region_jobs[j] += 1;
-    }
-    largest = std::max(largest, off - b->region_base[j]);
-  }
-  b->region_base[nreg] = off;
-  if (off != total) return fail(e, GF_ERR_STATE, "record layout holds %lld of %lld records", off, total);
-  long long slots = total;
-  b->ring_slots = 0;
-  if ((total > e->batch_record_budget || total >= (1ll << 31)) && nreg > 2) {   // record indices are int
-    const int K = static_cast<int>(std::min<long long>(nreg, std::max<long long>(2, e->batch_record_budget / largest)));
-    if (K < nreg) {
-      b->ring_slots = K;
-      b->slot_records = largest;
-      slots = K * largest;
-    }
-  }
+  std::vector<gf_replicate> ps(b->R);
+  for (int r = 0; r < b->R; ++r) ps[r] = b->reps[r].p;
+  b->plan = plan_records(ps.data(), b->R, e->batch_record_budget, kStreamSlab);
+  if (b->plan.region_base[b->plan.nregions] != total)
+    return fail(e, GF_ERR_STATE, "record layout holds %lld of %lld records", b->plan.region_base[b->plan.nregions], total);
+  for (int r = 0; r < b->R; ++r) b->reps[r].chunk = b->plan.chunk[r];
+  const int nreg = b->plan.nregions;
+  const long long slots = b->plan.slots;
   if (e->h_rec_stage_cap < static_cast<size_t>(slots)) {
     if (e->h_rec_stage) GF_CUDA(e, cudaFreeHost(e->h_rec_stage));
     e->h_rec_stage = nullptr;
@@ -470,9 +435,9 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   gf_status st = grow_device(e, &e->batch_recs_mem, &e->batch_recs_bytes, sizeof(WinGen) * slots);
   if (st != GF_OK) return st;
   b->d_all_recs = static_cast<WinGen*>(e->batch_recs_mem);
-  const int K = b->ring_slots > 0 ? b->ring_slots : nreg;
+  const int K = b->plan.ring_slots > 0 ? b->plan.ring_slots : nreg;
   b->slot_upload.assign(K, nullptr);
-  for (int k = 0; k < K && b->ring_slots > 0; ++k)
+  for (int k = 0; k < K && b->plan.ring_slots > 0; ++k)
     GF_CUDA(e, cudaEventCreateWithFlags(&b->slot_upload[k], cudaEventDisableTiming));
   b->region_done.reset(new std::atomic<long long>[nreg]);
   for (int j = 0; j < nreg; ++j) b->region_done[j].store(0);
@@ -480,7 +445,7 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   b->cancel.store(false);
   b->uploaded = 0;
   b->upload_done = 0;
-  b->producible.store(b->ring_slots > 0 ? b->ring_slots : nreg);
+  b->producible.store(b->plan.ring_slots > 0 ? b->plan.ring_slots : nreg);
   // A producer draws ~25 M records/s and the super-steps consume ~50 M/s at most, so a few producers
   // stay ahead of the GPU; more would take cores from the thread that enqueues the super-steps.
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
@@ -494,15 +459,7 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   }
   b->precomputed = true;
   // lock-step bookkeeping: replicate r's last window is super-step ceil(G_r / c_r) - 1
-  b->finish_at.clear();
-  for (int r = 0; r < b->R; ++r) {
-    const BatchRep& br = b->reps[r];
-    if (br.done) continue;
-    const int c = std::max(br.p.compact_interval, 1);
-    const int last = (br.p.num_generations + c - 1) / c - 1;
-    if (static_cast<int>(b->finish_at.size()) <= last) b->finish_at.resize(last + 1);
-    b->finish_at[last].push_back(r);
-  }
+  b->finish_at = plan_finish_steps(ps.data(), b->R);
   b->active_dirty = true;
   for (int& v : b->slot_version) v = -1;
   GF_TRACE_POINT(e, "record producers started");
@@ -514,14 +471,14 @@ static gf_status precompute_records(Engine* e, Batch* b) {
 // regions up to `need`.  Finished uploads free their staging slots for the producers.  A wait that
 // sees no progress for 120 s is reported as a state error.
 static gf_status stream_upload(Engine* e, Batch* b, int need) {
-  const int K = b->ring_slots > 0 ? b->ring_slots : b->nregions;
+  const int K = b->plan.ring_slots > 0 ? b->plan.ring_slots : b->plan.nregions;
   auto poll = [&]() {
-    if (b->ring_slots <= 0) return;
+    if (b->plan.ring_slots <= 0) return;
     while (b->upload_done < b->uploaded) {
       if (cudaEventQuery(b->slot_upload[b->upload_done % K]) != cudaSuccess) break;
       b->upload_done += 1;
     }
-    b->producible.store(std::min(b->nregions, b->upload_done + K), std::memory_order_release);
+    b->producible.store(std::min(b->plan.nregions, b->upload_done + K), std::memory_order_release);
   };
   const auto t0 = std::chrono::steady_clock::now();
   auto progress = t0;
@@ -536,14 +493,14 @@ static gf_status stream_upload(Engine* e, Batch* b, int need) {
   for (;;) {
     poll();
     const int j = b->uploaded;
-    if (j >= b->nregions || j >= need + K) break;
+    if (j >= b->plan.nregions || j >= need + K) break;
     const long long done = b->region_done[j].load(std::memory_order_acquire);
-    if (done == b->region_jobs[j]) {
-      const long long a = region_slot_base(b, j), n = b->region_base[j + 1] - b->region_base[j];
+    if (done == b->plan.region_jobs[j]) {
+      const long long a = b->plan.slot_base(j), n = b->plan.region_base[j + 1] - b->plan.region_base[j];
       if (n > 0)
         GF_CUDA(e, cudaMemcpyAsync(b->d_all_recs + a, e->h_rec_stage + a, sizeof(WinGen) * n, cudaMemcpyHostToDevice,
                                    e->stream));
-      if (b->ring_slots > 0) GF_CUDA(e, cudaEventRecord(b->slot_upload[j % K], e->stream));
+      if (b->plan.ring_slots > 0) GF_CUDA(e, cudaEventRecord(b->slot_upload[j % K], e->stream));
       b->uploaded += 1;
       continue;
     }
@@ -838,22 +795,22 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     return GF_OK;
   }
   const long long k = b->super_steps;
-  const int j = static_cast<int>(k / b->slab_windows);   // the record region of every active replicate
-  if (j >= b->nregions) return fail(e, GF_ERR_STATE, "super-step %lld beyond the record regions", k);
+  const int j = static_cast<int>(k / b->plan.slab_windows);   // the record region of every active replicate
+  if (j >= b->plan.nregions) return fail(e, GF_ERR_STATE, "super-step %lld beyond the record regions", k);
   const int slot = b->ring;
   GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
   WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->ring_stride;
   WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->ring_stride;
   // a slot that last held this list only needs the per-step fields
   const bool full = b->slot_version[slot] != b->list_version;
-  const long long region = region_slot_base(b, j);
+  const long long region = b->plan.slot_base(j);
   int tiles = 0;
   for (int i = 0; i < nj; ++i) {
     const int r = b->active[i];
     const BatchRep& br = b->reps[r];
     const int c = br.p.compact_interval;
     const long long gen = k * c;
-    const int off = b->region_off[static_cast<size_t>(r) * b->nregions + j];
+    const int off = b->plan.region_off[static_cast<size_t>(r) * b->plan.nregions + j];
     if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
     WinRep& w = hr[i];
     w.rec = static_cast<int>(region + off + (gen - static_cast<long long>(j) * br.chunk));

@@ -897,24 +897,10 @@ constexpr int kMaxWindow = kMaxWindowGenerations;
 // whose rows may hold a nonzero value, given the generations before this one).  Extinction
 // generations and every generation after an extinction run one launch each.
 static bool window_mp_eligible(const Engine* e, const gf_generation& g, int live) {
-  if (!e->use_windows || e->P < 2 || e->P > kMaxWindowPops) return false;
-  for (int p = 0; p < e->P; ++p) {
-    const gf_population_params& pp = g.pop[p];
-    if (pp.drift) {
-      if (pp.Nchrom_e <= 0) return false;
-    } else if ((live >> p) & 1) {
-      return false;
-    }
-  }
-  return true;
+  return e->use_windows && mp_window_generation_ok(g, e->P, live, kMaxWindowPops);
 }
 
-static int drift_bits(const gf_generation& g, int P) {
-  int m = 0;
-  for (int p = 0; p < P; ++p)
-    if (g.pop[p].drift) m |= 1 << p;
-  return m;
-}
+static int drift_bits(const gf_generation& g, int P) { return drifted_populations(g, P); }
 
 // Run generations [first, first + count) of the batch as one window launch.
 static gf_status launch_window(Engine* e, int b, int first, int count, const GenHost* gh) {

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/gofish_b200.h"
+#include "gf_plan.h"
 
 namespace gf {
 
@@ -183,14 +184,9 @@ struct Batch {
   // generation records, drawn by host threads region by region (region j holds slab j -- the
   // generations (j * chunk, (j + 1) * chunk] -- of every replicate that runs that long) while the GPU
   // runs the super-steps; a region is uploaded once all of its slabs are drawn (batch.cu)
-  int nregions = 0;
+  RecordPlan plan;                            // layout of the records (gf_plan.h)
   int uploaded = 0;                           // regions uploaded so far
   int upload_done = 0;                        // regions whose upload has finished (ring mode)
-  int ring_slots = 0;                         // 0: all regions resident; K: regions cycle through K slots
-  long long slot_records = 0;                 // records per ring slot
-  std::vector<long long> region_base;         // first record of region j, resident layout (nregions + 1)
-  std::vector<long long> region_jobs;         // slabs in region j
-  std::vector<int> region_off;                // [r * nregions + j]: offset of replicate r's slab in region j
   std::vector<cudaEvent_t> slot_upload;       // ring mode: the last upload from each staging slot
   std::unique_ptr<std::atomic<long long>[]> region_done;   // slabs drawn per region
   std::atomic<long long> next_job{0};         // producers' job counter (region-major over replicates)
@@ -202,7 +198,6 @@ struct Batch {
   // super-steps an unfinished replicate is at generation k * c_r and in record region k / slab_windows.
   // The host keeps only the list of unfinished replicates and the replicates finishing at each step;
   // their per-replicate fields are brought up to date when a run returns (sync_progress).
-  int slab_windows = 1;                       // windows per record slab
   std::vector<int> active;                    // unfinished replicates, in index order
   bool active_dirty = true;
   int list_version = 0;
