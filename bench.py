@@ -547,7 +547,7 @@ def run_surrogate(args):
         eng.synchronize()
         t_data = time.perf_counter() - t0
         peval = sg.draw_parameters(args.eval_draws, seed=202)
-        ref = sg.simulate_spectra(eng, peval, reps=64, seed=1 << 28)        # the judge: 64-replicate means
+        ref = sg.simulate_spectra(eng, peval, reps=64, seed=1 << 28)        # reference spectra: 64-replicate means
         if args.data_cache:
             np.savez(args.data_cache, ptrain=ptrain, train_sfs=train_sfs, peval=peval, ref=ref, t_data=t_data)
     # simulator throughput on the training distribution: 512 draws x 16 replicates, timed on its own
