@@ -5,6 +5,7 @@ from __future__ import annotations
 
 import os
 import socket
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -131,3 +132,21 @@ def test_multipop_bench_schedule():
                 assert abs(col - 1.0) < 1e-6
     assert whole[0]["pop"]["drift"][2] == 0 and whole[2500]["pop"]["drift"][2] == 1
     assert whole[2500]["pop"]["F"][2] == np.float32(0.1)
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (the CPU restatement timed on the host cores) prints one JSON line
+    with the metric, the `impl` tag, a `cpu_baseline` describing the run and an `e2e` with no copies."""
+    import json
+    import subprocess
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    out = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "mutation-generations/s"
+    assert line["value"] > 0 and line["higher_is_better"] is True and line["steps"] == 1
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
