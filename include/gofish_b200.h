@@ -248,12 +248,18 @@ gf_status gf_site_frequency_spectrum_device(gf_engine* engine, const float* d_fr
  * of GF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the process exits.
  *   Limits: Nchrom_e <= GF_NOALLOC_MAX_NCHROM, 1 <= n < Nchrom_e, n <= GF_NOALLOC_MAX_SAMPLE; larger
  *   sizes return GF_ERR_CAPACITY.
- *   The first call on a device looks the scratch array's address up (cudaGetSymbolAddress); make that
- *   first call before capturing a stream into a CUDA graph.
- *   All calls on a device share the scratch array: calls whose GPU work overlaps (two streams, two
- *   host threads) race; serialize them.  Each call clears what it accumulates into.
- *   The call synchronizes `cuda_stream` once (it reads back whether every frequency lies on the
- *   1/Nchrom_e grid).  Status codes only: there is no engine to hold a message. */
+ *   The first call on a device does that device's set-up: it looks the scratch array's address up
+ *   (cudaGetSymbolAddress) and sets the histogram kernel's shared-memory limit; make it before any
+ *   stream capture begins.  Under lazy module loading (the CUDA default) that first call may also load
+ *   the module, which is when the array takes its device memory; later calls take none.  The set-up
+ *   is kept for the life of the process and does not survive cudaDeviceReset: do not call this entry
+ *   point on a device after resetting it.
+ *   All calls on a device share the scratch array, which keeps the last call's contents: calls whose
+ *   GPU work overlaps (two streams, two host threads) race; serialize them.  Each call clears what it
+ *   accumulates into before using it.
+ *   Every call synchronizes `cuda_stream` once: it reads back whether every frequency lies on the
+ *   1/Nchrom_e grid to choose the projection.  Status codes only: there is no engine to hold a
+ *   message. */
 #define GF_NOALLOC_MAX_NCHROM (1 << 20)
 #define GF_NOALLOC_MAX_SAMPLE 1023
 #define GF_NOALLOC_SCRATCH_BYTES (4194560 + 256 + 8192 + 2097152)

@@ -492,8 +492,11 @@ __global__ void log_binomial_kernel(double* __restrict__ lgc, int n) {
   if (k <= n) lgc[k] = lgamma(n + 1.0) - lgamma(k + 1.0) - lgamma(n - k + 1.0);
 }
 
-// Device address of the scratch array on `device`, looked up once per device.  In host code the
-// array's name only stands for the symbol; kernels must be given this address.
+// Per-device set-up, done once per device by the first call on it (with that device current): the
+// scratch array's device address (in host code the array's name only stands for the symbol; kernels
+// must be given this address) and the histogram kernel's dynamic shared-memory limit.  Under lazy
+// module loading this first call may also load the module, which is when the array takes its device
+// memory.  The cached set-up does not survive cudaDeviceReset.
 static gf_status noalloc_scratch(int device, unsigned char** out) {
   static std::mutex mu;
   static unsigned char* addr[64] = {nullptr};
@@ -501,7 +504,10 @@ static gf_status noalloc_scratch(int device, unsigned char** out) {
   std::lock_guard<std::mutex> lock(mu);
   if (!addr[device]) {
     void* p = nullptr;
-    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err == cudaSuccess && p)
+      err = cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(unsigned) * kSmemBins));
     if (err != cudaSuccess || !p) {
       cudaGetLastError();
       return GF_ERR_CUDA;
@@ -549,8 +555,6 @@ gf_status gf_site_frequency_spectrum_noalloc(const float* d_freq, int32_t M, int
   GF_NA_CUDA(cudaGetLastError());
   if (M > 0) {
     const int smem_bins = std::min(kSmemBins, Nc + 1);
-    GF_NA_CUDA(cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(sizeof(unsigned) * kSmemBins)));
     hist_kernel<<<hist_blocks(M), kHistThreads, sizeof(unsigned) * smem_bins, stream>>>(d_freq, M, Nc, counts,
                                                                                        mismatch, smem_bins);
     GF_NA_CUDA(cudaGetLastError());
