@@ -1,12 +1,12 @@
 #!/usr/bin/env bash
-# Builds the reference (ParallelPopGen 3P, read-only at $REF) into oracle/_ref/ for use as a test
-# oracle.  Compiles the reference's own sources where they lie, with its own flags
+# Builds the reference (ParallelPopGen 3P, read-only at $REF; default: a checkout named `reference`
+# beside this repository) into oracle/_ref/ for use as a test oracle.  Compiles the reference's own sources where they lie, with its own flags
 # (examples/*/makefile: -O3 --use_fast_math, relocatable device code).  The reference's legacy
 # __shfl/__ballot calls only compile for a pre-Volta virtual architecture, so the PTX target is
 # compute_60 and ptxas lowers it to sm_100a machine code.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${REF:-/root/reference}"
+REF="${REF:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
 if [ ! -d "$REF/3P" ]; then

@@ -14,13 +14,15 @@ afterwards).
                                   examples/example_dadi/run_980.out (L = 2e9) and run_980_2.out
                                   (L = 2e8), and the diffusion expectation dadi_example.out.
 
-Usage:  python tests/golden/make_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_golden.py [--reference <reference checkout>]
+        (default: $REF, else a checkout named `reference` beside this repository)
 """
 from __future__ import annotations
 
 import argparse
 import hashlib
 import json
+import os
 import re
 import subprocess
 from pathlib import Path
@@ -105,7 +107,7 @@ def dadi(ref_root: Path) -> None:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("REF", str(ROOT.parent / "reference")))
     a = ap.parse_args()
     ref = Path(a.reference)
     hostrng(ref)
