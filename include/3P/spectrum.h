@@ -10,6 +10,8 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <utility>
 
 #include "../gofish_b200.h"
 #include "go_fish_data_struct.h"
@@ -34,6 +36,35 @@ struct SFS {
       : frequency_spectrum(NULL), populations(NULL), sample_size(NULL), num_populations(0), num_sites(0),
         num_mutations(0), sampled_generation(0) {}
   ~SFS() { clear(); }
+  /* Copies are deep.  The reference's SFS is copyable too (spectrum.h:24-37, implicit members), but
+   * its copies share the arrays that both destructors then delete; here each copy owns its own. */
+  SFS(const SFS& in)
+      : frequency_spectrum(NULL), populations(NULL), sample_size(NULL), num_populations(in.num_populations),
+        num_sites(in.num_sites), num_mutations(in.num_mutations), sampled_generation(in.sampled_generation) {
+    if (in.sample_size && in.num_populations > 0) {
+      sample_size = new int[in.num_populations];
+      std::memcpy(sample_size, in.sample_size, sizeof(int) * in.num_populations);
+    }
+    if (in.populations && in.num_populations > 0) {
+      populations = new int[in.num_populations];
+      std::memcpy(populations, in.populations, sizeof(int) * in.num_populations);
+    }
+    const size_t n = in.bins();
+    if (in.frequency_spectrum && n > 0) {
+      frequency_spectrum = new float[n];
+      std::memcpy(frequency_spectrum, in.frequency_spectrum, sizeof(float) * n);
+    }
+  }
+  SFS& operator=(SFS in) {
+    std::swap(frequency_spectrum, in.frequency_spectrum);
+    std::swap(populations, in.populations);
+    std::swap(sample_size, in.sample_size);
+    num_populations = in.num_populations;
+    num_sites = in.num_sites;
+    num_mutations = in.num_mutations;
+    sampled_generation = in.sampled_generation;
+    return *this;
+  }
   /* frees the arrays (the reference leaks them when an SFS is reused; this version frees first) */
   void clear() {
     delete[] frequency_spectrum;
@@ -45,8 +76,13 @@ struct SFS {
   }
 
  private:
-  SFS(const SFS&);
-  SFS& operator=(const SFS&);
+  /* floats in frequency_spectrum: the sample size of a single population's spectrum or histogram,
+   * (n_a + 1)(n_b + 1) for a joint spectrum of two populations */
+  size_t bins() const {
+    if (!sample_size || num_populations <= 0) return 0;
+    if (num_populations == 1) return static_cast<size_t>(sample_size[0]);
+    return static_cast<size_t>(sample_size[0] + 1) * static_cast<size_t>(sample_size[1] + 1);
+  }
 };
 
 }  // namespace Spectrum

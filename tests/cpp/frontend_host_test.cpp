@@ -93,5 +93,36 @@ int main() {
   std::ostringstream empty;
   empty << t;
   line("dump_empty_has_no_sim", empty.str().find("no simulation stored") != std::string::npos);
+
+  // Spectrum::SFS copies (deep: each copy owns its arrays; the program must end without a double free)
+  Spectrum::SFS sfs;
+  sfs.num_populations = 1;
+  sfs.sample_size = new int[1];
+  sfs.sample_size[0] = 5;
+  sfs.populations = new int[1];
+  sfs.populations[0] = 1;
+  sfs.frequency_spectrum = new float[5];
+  for (int i = 0; i < 5; ++i) sfs.frequency_spectrum[i] = 10.f * i;
+  sfs.num_sites = 100.f;
+  sfs.num_mutations = 100.f;
+  sfs.sampled_generation = 7;
+  Spectrum::SFS copy(sfs);
+  Spectrum::SFS assigned;
+  assigned = sfs;
+  sfs.frequency_spectrum[3] = -1.f;
+  line("sfs_copy_bin3", copy.frequency_spectrum[3]);
+  line("sfs_assigned_bin3", assigned.frequency_spectrum[3]);
+  line("sfs_copy_distinct", copy.frequency_spectrum != sfs.frequency_spectrum && assigned.populations != sfs.populations);
+  line("sfs_copy_fields", copy.sample_size[0] == 5 && copy.populations[0] == 1 && copy.sampled_generation == 7 &&
+                              assigned.num_sites == 100.f);
+  Spectrum::SFS joint;
+  joint.num_populations = 2;
+  joint.sample_size = new int[2];
+  joint.sample_size[0] = 2;
+  joint.sample_size[1] = 3;
+  joint.frequency_spectrum = new float[12];
+  for (int i = 0; i < 12; ++i) joint.frequency_spectrum[i] = static_cast<float>(i);
+  Spectrum::SFS joint_copy(joint);
+  line("sfs_joint_copy_last", joint_copy.frequency_spectrum[11]);
   return 0;
 }

@@ -80,3 +80,11 @@ def test_allele_trajectories_defaults(host_values):
     assert v["default_sites"] == 1000 and v["default_compact"] == 35 and v["default_init_mse"] == 1
     assert v["default_prev_sample"] == -1 and v["default_device"] == -1
     assert v["dump_empty_has_no_sim"] == 1
+
+
+def test_sfs_copies_are_deep(host_values):
+    """Spectrum::SFS is copyable as in the reference; here the copies own their arrays."""
+    v = host_values
+    assert v["sfs_copy_bin3"] == 30.0 and v["sfs_assigned_bin3"] == 30.0
+    assert v["sfs_copy_distinct"] == 1 and v["sfs_copy_fields"] == 1
+    assert v["sfs_joint_copy_last"] == 11.0
