@@ -313,7 +313,7 @@ def run_b200(args, rank, local_rank, world):
         "roofline": {
             "bound": "hbm",
             "kernel": "window_kernel (every generation of a compaction window per launch: selection, drift, "
-                      "births, compaction flags) with its segmented scan and scatter",
+                      "births, compaction flags); its segmented scan and scatter are compact_ms_per_step",
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
@@ -329,6 +329,9 @@ def run_b200(args, rank, local_rank, world):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
+    # over the whole timed step (MSE start, windows, compactions, SFS, both halves at once)
+    line["roofline"]["step"] = {"achieved": ALG_BYTES_PER_MUTGEN * value / 1e9, "unit": "GB/s",
+                                "frac": ALG_BYTES_PER_MUTGEN * value / 1e9 / peak}
     # the kernel is issue-bound: its rate against the instruction-issue ceiling at full warps
     mhz = line["clocks"].get("sm_mhz") or 1965.0
     issue_ceiling = B200_SMS * SCHEDULERS_PER_SM * mhz * 1e6 * 32 / THREAD_INSTR_PER_MUTGEN
@@ -338,7 +341,30 @@ def run_b200(args, rank, local_rank, world):
             "ceiling": issue_ceiling, "unit": "mutation-generations/s",
             "frac": achieved * 1e9 / ALG_BYTES_PER_MUTGEN / issue_ceiling,
         }
+    if world == 1 and not args.no_workloads:
+        for e in engines:
+            e.close()
+        del flush
+        torch.cuda.empty_cache()
+        line["workloads"] = extra_workloads()
     print(json.dumps(line), flush=True)
+
+
+def extra_workloads() -> dict:
+    """The other measured configurations, each with its own fixed step counts (independent of --steps):
+    batched ragged replicates over the full N0 range with the looped plain engine beside them, the
+    three-population model, and surrogate inference."""
+    out = {}
+    t0 = time.perf_counter()
+    b = measure_batched(4096, 1e5, plain_sample=8, steps=1, warmup=1, profile=False)
+    b["wall_s"] = time.perf_counter() - t0
+    out["batched"] = b
+    t0 = time.perf_counter()
+    m = measure_multipop(MP_GENS, steps=2, warmup=1)
+    m["wall_s"] = time.perf_counter() - t0
+    out["multipop"] = m
+    out["surrogate_forward"] = measure_surrogate_forward(steps=50, warmup=10)
+    return out
 
 
 # ------------------------------------------------------------------------------------------------
@@ -351,36 +377,43 @@ def equilibrium_state(rng, Nc, L, mu):
 
 
 def cpu_sample(threads: int, gens: int, seed: int = 1):
+    """`gens` generations of each half (neutral, then gamma = -10 with h = 0.5) of the headline workload
+    from a synthetic neutral-equilibrium state of ~2.7 M mutations; returns (mutation-generations, s)."""
     import oracle.oracle as orc  # CPU restatement: the timed baseline, never the product
+    from parallelpopgen_b200 import ConstantModel
     Nc = 2 * N_IND
     x = equilibrium_state(np.random.default_rng(seed), Nc, L_HALF, MU)
-    t0 = time.perf_counter()
-    _, _, mg = orc.run_single(x, first_gen=0, num_gens=gens, Nc=Nc, F=0.0, h=H, s=0.0, mu=MU, num_sites=L_HALF,
-                              seed1=SEED1, seed2=SEED2, compact_interval=COMPACT, capacity=2 * len(x) + 4_000_000,
-                              threads=threads)
-    dt = time.perf_counter() - t0
-    return mg, dt
+    mg_all, dt_all = 0.0, 0.0
+    for sel in (0.0, ConstantModel.s_from_gamma(GAMMA_SEL, N_IND, 0.0)):
+        t0 = time.perf_counter()
+        _, _, mg = orc.run_single(x, first_gen=0, num_gens=gens, Nc=Nc, F=0.0, h=H, s=sel, mu=MU,
+                                  num_sites=L_HALF, seed1=SEED1, seed2=SEED2, compact_interval=COMPACT,
+                                  capacity=2 * len(x) + 4_000_000, threads=threads)
+        dt_all += time.perf_counter() - t0
+        mg_all += mg
+    return mg_all, dt_all
 
 
-def cpu_baseline_sample(threads: int, gens: int = 80, serial_gens: int = 8):
+def cpu_baseline_sample(threads: int, gens: int = 40, serial_gens: int = 4):
     """The CPU restatement on all host threads (the baseline) and, on a shorter sample, on one thread
     (about 20 core-seconds of work in all)."""
     mg, dt = cpu_sample(threads, gens)
     smg, sdt = cpu_sample(1, serial_gens)
     return {"value": mg / dt, "unit": "mutation-generations/s", "cores": threads, "kind": "port",
-            "sample": f"{gens} generations of the neutral half (Nchrom_e 400,000, L 2.5e8, ~2.7M mutations) "
-                      f"from a synthetic equilibrium state; {dt:.1f} s wall on {threads} threads",
+            "sample": f"{gens} generations of each half (neutral, and gamma = -10 with h = 0.5; Nchrom_e 400,000, "
+                      f"L 2.5e8, ~2.7M mutations) from a synthetic equilibrium state; {dt:.1f} s wall on "
+                      f"{threads} threads",
             "serial": {"value": smg / sdt, "cores": 1,
-                       "sample": f"{serial_gens} generations of the same state on one thread; {sdt:.1f} s"}}
+                       "sample": f"{serial_gens} generations of each half on one thread; {sdt:.1f} s"}}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    gens = 20
+    gens = 10
     for _ in range(args.warmup):
-        cpu_sample(threads, 2)
+        cpu_sample(threads, 1)
     total_mg, total_s = 0.0, 0.0
     for k in range(args.steps):
         mg, dt = cpu_sample(threads, gens, seed=k + 1)
@@ -396,9 +429,9 @@ def run_reference(args, rank, world):
                                "(neutral + gamma=-10, h=0.5), MSE start, 10,000 generations, compact every 25, "
                                "SFS n=1000", "parallelism": "CPU threads"},
         "cpu_baseline": {"value": v, "unit": "mutation-generations/s", "cores": threads, "kind": "port",
-                         "sample": f"{gens} generations of the neutral half per step (~2.7M mutations), "
-                                   "CPU restatement of the reference's per-generation update (the reference "
-                                   "ships no CPU implementation of this path)"},
+                         "sample": f"{gens} generations of each half (neutral, gamma = -10) per step from a "
+                                   "~2.7M-mutation equilibrium state, CPU restatement of the reference's "
+                                   "per-generation update (the reference ships no CPU implementation of this path)"},
         "e2e": {"value": v, "unit": "mutation-generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -428,6 +461,12 @@ def batched_replicates(R: int, n_max: float, seed: int = 2024):
 
 
 def run_batched(args):
+    print(json.dumps(measure_batched(args.replicates, args.n_max, args.plain_sample, args.steps, args.warmup)),
+          flush=True)
+
+
+def measure_batched(replicates: int, n_max: float, plain_sample: int, steps: int, warmup: int,
+                    profile: bool = True) -> dict:
     import torch
     from parallelpopgen_b200 import Engine, replicate_mse_pops, replicate_plain_generations, replicate_population
     from parallelpopgen_b200.autotune import tune_batch_cadence
@@ -435,7 +474,7 @@ def run_batched(args):
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     eng = Engine(device=0, stream=stream.cuda_stream)
-    reps = batched_replicates(args.replicates, args.n_max)
+    reps = batched_replicates(replicates, n_max)
     tuned = tune_batch_cadence(eng, reps, use_cache=False)
     for r in reps:
         r.compact_interval = tuned["compact_interval"]
@@ -447,11 +486,11 @@ def run_batched(args):
         sfs = eng.batch_sfs(n, len(reps))
         return eng.batch_stats(), sfs
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batch_step()
     times, st = [], None
     with ClockSampler(0) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             ev0 = torch.cuda.Event(enable_timing=True)
             ev1 = torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
@@ -460,24 +499,26 @@ def run_batched(args):
             ev1.synchronize()
             times.append(ev0.elapsed_time(ev1) * 1e-3)
     batch_s = float(np.mean(times))
-    # one more batch with the window launches bracketed by CUDA events (device time of the drift work)
-    # and host wall-clock phases, the device synchronised between them
-    eng.set_profiling(True)
-    eng.read_profile()
-    ph0 = time.perf_counter()
-    eng.batch_begin(reps)
-    eng.synchronize()
-    ph1 = time.perf_counter()
-    eng.batch_run()                      # returns after reading the counts back
-    ph2 = time.perf_counter()
-    eng.batch_sfs(n, len(reps))
-    ph3 = time.perf_counter()
-    phases = {"begin": 1e3 * (ph1 - ph0), "run": 1e3 * (ph2 - ph1), "sfs": 1e3 * (ph3 - ph2)}
-    prof = eng.read_profile()
-    eng.set_profiling(False)
+    phases, prof = None, {"drift_ms": None, "drift_launches": None}
+    if profile:
+        # one more batch with the window launches bracketed by CUDA events (device time of the drift
+        # work) and host wall-clock phases, the device synchronised between them
+        eng.set_profiling(True)
+        eng.read_profile()
+        ph0 = time.perf_counter()
+        eng.batch_begin(reps)
+        eng.synchronize()
+        ph1 = time.perf_counter()
+        eng.batch_run()                      # returns after reading the counts back
+        ph2 = time.perf_counter()
+        eng.batch_sfs(n, len(reps))
+        ph3 = time.perf_counter()
+        phases = {"begin": 1e3 * (ph1 - ph0), "run": 1e3 * (ph2 - ph1), "sfs": 1e3 * (ph3 - ph2)}
+        prof = eng.read_profile()
+        eng.set_profiling(False)
     # the same replicates, one plain engine run each (a random sample, timed engine calls only)
     rng = np.random.default_rng(7)
-    sample = rng.choice(len(reps), size=min(args.plain_sample, len(reps)), replace=False)
+    sample = rng.choice(len(reps), size=min(plain_sample, len(reps)), replace=False)
     prepared = [(reps[i], replicate_mse_pops(reps[i]), replicate_plain_generations(reps[i])) for i in sample]
     d_sfs = torch.empty(n, dtype=torch.float32, device="cuda")
     eng = Engine(device=0, stream=stream.cuda_stream)     # a fresh engine: no batch state alongside
@@ -498,11 +539,11 @@ def run_batched(args):
         plain_s += ev0.elapsed_time(ev1) * 1e-3
     plain_rate = len(prepared) / plain_s
     value = len(reps) / batch_s
-    print(json.dumps({
+    return {
         "metric": "simulations/s (batched ragged replicates)", "value": value, "unit": "simulations/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_s * 1e3,
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": batch_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{len(reps)} single-population replicates: N0 log-uniform [1e3, {args.n_max:g}], "
+        "config": {"workload": f"{len(reps)} single-population replicates: N0 log-uniform [1e3, {n_max:g}], "
                                "gamma U[-100, 10], h U[0, 1], F U[0, 0.5], growth r U[-0.001, 0.01] clamped to "
                                "[N0/10, 10 N0], mu 1e-9, L 1e7, 4 N0 generations, MSE start, SFS n=100",
                    "compact_interval": tuned["compact_interval"], "cadence_trials": tuned["trials"],
@@ -516,7 +557,7 @@ def run_batched(args):
         "looped_plain": {"value": plain_rate, "unit": "simulations/s", "sample": len(prepared),
                          "speedup_batched_over_looped": value / plain_rate},
         "clocks": clk.summary(),
-    }), flush=True)
+    }
 
 
 # ------------------------------------------------------------------------------------------------
@@ -642,30 +683,48 @@ def run_surrogate(args):
 def surrogate_inference_only(args):
     """Forward passes of the surrogate network with initial weights (throughput does not depend on them):
     the tensor-core kernels alone, for profiling."""
+    print(json.dumps(measure_surrogate_forward(args.steps, args.warmup)), flush=True)
+
+
+def measure_surrogate_forward(steps: int, warmup: int, B: int = 32768) -> dict:
     import torch
     from parallelpopgen_b200 import surrogate as sg
-    B = 32768
     mlp = sg.Mlp(capacity=B)
     mlp.set_params(sg.init_params(0))
     xq = torch.from_numpy(sg.encode(sg.draw_parameters(B, seed=303))).cuda()
     yq = torch.empty((B, 99), dtype=torch.float32, device="cuda")
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
     ev1.record()
     ev1.synchronize()
     mlp.check()
-    fwd_s = ev0.elapsed_time(ev1) * 1e-3 / args.steps
+    fwd_s = ev0.elapsed_time(ev1) * 1e-3 / steps
     flops = 2.0 * B * (6 * 512 + 3 * 512 * 512 + 512 * 99)
     peak, kind = tensor_peak()
     tf = flops / fwd_s / 1e12
-    print(json.dumps({"metric": "SFS queries/s (surrogate forward)", "value": B / fwd_s, "unit": "queries/s",
-                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "batch": B,
-                      "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "peak_kind": kind,
-                                   "unit": "TFLOP/s", "frac": tf / peak, "forward_us": fwd_s * 1e6}}), flush=True)
+    # end to end: host parameters in, host spectra out, through the network's pointer API
+    hx = torch.from_numpy(sg.encode(sg.draw_parameters(B, seed=304))).pin_memory()
+    hy = torch.empty((B, 99), dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        xq.copy_(hx, non_blocking=True)
+        mlp.forward_ptr(xq.data_ptr(), B, yq.data_ptr())
+        hy.copy_(yq, non_blocking=True)
+    e1.record()
+    e1.synchronize()
+    e2e_s = e0.elapsed_time(e1) * 1e-3 / steps
+    return {"metric": "SFS queries/s (surrogate forward)", "value": B / fwd_s, "unit": "queries/s",
+            "n_gpus": 1, "steps": steps, "warmup": warmup, "batch": B, "dtype": "bf16 (fp32 accumulate)",
+            "e2e": {"value": B / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(hx.numel() * 4),
+                    "d2h_bytes_per_step": int(hy.numel() * 4)},
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "peak_kind": kind,
+                         "unit": "TFLOP/s", "frac": tf / peak, "forward_us": fwd_s * 1e6}}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -738,13 +797,16 @@ def multipop_generations(first: int, last: int, sample_every: int = 500, compact
 
 
 def run_multipop(args):
+    print(json.dumps(measure_multipop(args.mp_gens, args.steps, args.warmup)), flush=True)
+
+
+def measure_multipop(total: int, steps: int, warmup: int) -> dict:
     import torch
     from parallelpopgen_b200 import Engine
     from parallelpopgen_b200._capi import MSE_DTYPE
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     eng = Engine(device=0, stream=stream.cuda_stream)
-    total = args.mp_gens
     segments = [multipop_generations(a, min(a + 499, total), last_generation=total) for a in range(1, total + 1, 500)]
     pops = np.zeros(3, dtype=MSE_DTYPE)
     pops[0] = (MP_N0, 2 * MP_N0, MP_MU, 0.0, MP_H, 0.0, np.float32(MP_GAMMA[0]) / np.float32(2 * MP_N0))
@@ -763,11 +825,11 @@ def run_multipop(args):
                 d2h += 3 * 4 * M + 16 * M
         return eng.stats()["mutation_generations"], d2h, M
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step(False)
     times, mg = [], 0.0
     with ClockSampler(0) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
             m, _, _ = step(False)
@@ -776,7 +838,7 @@ def run_multipop(args):
             times.append(ev0.elapsed_time(ev1))
             mg += m
     e2e_t, e2e_mg, d2h = [], 0.0, 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         m, d2h, M = step(True)
@@ -790,21 +852,24 @@ def run_multipop(args):
         e2e_t.append(ev0.elapsed_time(ev1))
         e2e_mg += m
     value = mg / (sum(times) * 1e-3)
-    print(json.dumps({
+    return {
         "metric": "mutation-generations/s (multi-population)", "value": value, "unit": "mutation-generations/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(times) / args.steps,
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": sum(times) / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "3 populations: ancestral N=1e4 (MSE start), population 1 founded at generation 1, "
                                "population 2 at 2000, exponential growth r=0.005 to 1e5 / 2.5e5 / 5e5, symmetric "
                                "migration 1e-4, gamma -5 -> +2 at 3000, h 0.3, F 0.1 in population 2, mu 1e-9, "
                                "L 2e8, 5000 generations, compaction every 35 and at every time sample (500)",
                    "kernel": "window_mp_kernel (P = 3: all generations of a compaction window per launch)"},
-        "mutation_generations_per_step": mg / args.steps,
+        "mutation_generations_per_step": mg / steps,
         "e2e": {"value": e2e_mg / (sum(e2e_t) * 1e-3), "unit": "mutation-generations/s",
                 "path": "10 time samples read into page-locked buffers, SFS n=200 of each population",
-                "d2h_bytes_per_step": d2h},
+                "h2d_bytes_per_step": int(sum(seg.nbytes for seg in segments)), "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "bytes_per_mutation_generation": 48,
+                     "achieved": 48 * value / 1e9, "unit": "GB/s", "peak": measured_peaks()[0],
+                     "frac": 48 * value / 1e9 / measured_peaks()[0]},
         "clocks": clk.summary(),
-    }), flush=True)
+    }
 
 
 def tensor_peak():
@@ -824,6 +889,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="plain workload only: leave out the batched, multi-population and surrogate sub-objects")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "surrogate", "multipop"],
                     help="plain: the headline single-population workload; batched: batched ragged replicates; "
                          "surrogate: the SFS surrogate network against the simulator")

@@ -25,12 +25,19 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <type_traits>
 #include <utility>
 #include <vector>
 
 #include "../gofish_b200.h"
 #include "go_fish_data_struct.h"
+
+namespace gofish_detail {
+/* selection_sine_wave's coefficient at t = generation - generation_shift, evaluated on the device
+ * (defined below) */
+inline float sine_selection(float A, float pi, float rho, float D, int t);
+}  // namespace gofish_detail
 
 #if defined(__CUDACC__)
 #define GF_HD __host__ __device__
@@ -103,9 +110,12 @@ struct selection_sine_wave {
   GF_HD inline float operator()(const int population, const int generation, const float freq) const {
     return A * std::sin(pi * (generation - generation_shift) + rho) + D;
   }
+  /* The reference evaluates this model inside its drift kernel under --use_fast_math, where sin is the
+   * hardware approximation; the engine's device evaluates the same expression for the front-end. */
   inline void gf_affine(int population, int generation, float& s, float& i) const {
+    (void)population;
     s = 0.f;
-    i = (*this)(population, generation, 0.f);
+    i = gofish_detail::sine_selection(A, pi, rho, D, generation - generation_shift);
   }
 };
 
@@ -429,6 +439,17 @@ inline void selection_affine(const Sel& sel, int pop, int gen, float& slope, flo
   affine_of<Sel>::get(sel, pop, gen, slope, intercept);
 }
 
+/* true when every leaf of the selection model exposes its coefficients exactly (gf_affine) */
+template <typename Sel>
+struct exact_affine : has_gf_affine<Sel> {};
+template <typename S, typename SP>
+struct exact_affine<Sim_Model::selection_population_specific<S, SP>>
+    : std::integral_constant<bool, exact_affine<S>::value && exact_affine<SP>::value> {};
+template <typename S1, typename S2>
+struct exact_affine<Sim_Model::selection_piecewise<S1, S2>>
+    : std::integral_constant<bool, exact_affine<S1>::value && exact_affine<S2>::value> {};
+
+
 /* ---- one engine per device, created on first use ---- */
 inline gf_engine* engine_for(int device) {
   static gf_engine* engines[64] = {NULL};
@@ -450,6 +471,179 @@ inline void check(gf_engine* e, gf_status st, const char* what) {
     std::exit(1);
   }
 }
+
+/* engine of the run_sim call in progress on this thread (model functions evaluated on its device) */
+inline gf_engine*& model_engine() {
+  static thread_local gf_engine* e = NULL;
+  return e;
+}
+
+/* Coefficients of selection_sine_wave come from gf_selection_sine_values in blocks of consecutive
+ * t, cached per thread and per parameter set (compared bit for bit). */
+inline float sine_selection(float A, float pi, float rho, float D, int t) {
+  struct Block {
+    float key[4];
+    int t0;
+    std::vector<float> v;
+  };
+  static thread_local std::vector<Block> blocks;
+  const float key[4] = {A, pi, rho, D};
+  Block* hit = NULL;
+  for (size_t b = 0; b < blocks.size(); ++b)
+    if (std::memcmp(blocks[b].key, key, sizeof(key)) == 0) {
+      hit = &blocks[b];
+      if (t >= hit->t0 && t < hit->t0 + static_cast<int>(hit->v.size())) return hit->v[t - hit->t0];
+      break;
+    }
+  if (!hit) {
+    if (blocks.size() >= 16) blocks.erase(blocks.begin());
+    blocks.push_back(Block());
+    hit = &blocks.back();
+    std::memcpy(hit->key, key, sizeof(key));
+  }
+  const int kBlock = 4096;
+  hit->t0 = t;
+  hit->v.assign(kBlock, 0.f);
+  gf_engine* e = model_engine() ? model_engine() : engine_for(-1);
+  check(e, gf_selection_sine_values(e, A, pi, rho, D, t, kBlock, hit->v.data()), "selection_sine_wave");
+  return hit->v[0];
+}
+
+#ifdef __CUDACC__
+/* ---- selection models evaluated on the device (translation units compiled by nvcc) ----
+ * A selection functor without exact affine coefficients is evaluated per mutation on the device, as
+ * the reference evaluates every selection functor inside migration_selection_drift
+ * (go_fish_impl.cuh:98-105): before each generation, selection_table_kernel -- instantiated here, in
+ * the user's translation unit, for the user's functor -- writes s(pop, generation, x_mig) for every
+ * mutation into the engine's selection table (gf_sim_selection_view), and the engine's drift reads it. */
+struct migration_matrix {
+  float m[GF_MAX_POPULATIONS * GF_MAX_POPULATIONS];
+};
+
+template <typename Functor_selection>
+__global__ void selection_table_kernel(const Functor_selection sel, const float* __restrict__ freq, long long stride,
+                                       const int* __restrict__ num_mutations, int P, unsigned drift_mask,
+                                       int generation, const migration_matrix mig, float* __restrict__ out,
+                                       long long out_stride) {
+  const int M = *num_mutations;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+    for (int p = 0; p < P; ++p) {
+      if (!((drift_mask >> p) & 1u)) continue;
+      // x_mig in the order and rounding of the engine's drift kernels (k order, fused multiply-add)
+      float x = 0.f;
+      for (int k = 0; k < P; ++k) x = __fmaf_rn(mig.m[k * GF_MAX_POPULATIONS + p], freq[k * stride + i], x);
+      out[p * out_stride + i] = sel(p, generation, x);
+    }
+  }
+}
+
+/* s(pop, gen, x) at x = 0, 1/2 and 1, evaluated on the device */
+template <typename Functor_selection>
+__global__ void selection_probe_kernel(const Functor_selection sel, int pop, int gen, float* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    out[0] = sel(pop, gen, 0.f);
+    out[1] = sel(pop, gen, 0.5f);
+    out[2] = sel(pop, gen, 1.f);
+  }
+}
+
+inline void cuda_check(cudaError_t err, const char* what) {
+  if (err != cudaSuccess) {
+    std::fprintf(stderr, "%s: CUDA error %s\n", what, cudaGetErrorString(err));
+    std::exit(1);
+  }
+}
+
+/* Fill the engine's selection table for generation G (the caller then runs G alone). */
+template <typename Functor_selection>
+inline void launch_selection_table(gf_engine* eng, const Functor_selection& sel, const gf_generation& G, int P) {
+  gf_selection_view v;
+  check(eng, gf_sim_selection_view(eng, &v), "run_sim");
+  migration_matrix mig;
+  std::memcpy(mig.m, G.migration, sizeof(mig.m));
+  unsigned mask = 0;
+  for (int p = 0; p < P; ++p)
+    if (G.pop[p].drift && G.pop[p].Nchrom_e > 0) mask |= 1u << p;
+  selection_table_kernel<Functor_selection><<<148 * 4, 256, 0, static_cast<cudaStream_t>(v.cuda_stream)>>>(
+      sel, v.freq, v.row_stride, v.num_mutations, P, mask, G.generation, mig, v.selection, v.selection_stride);
+  cuda_check(cudaGetLastError(), "run_sim: selection_table_kernel");
+}
+
+/* Affine coefficients of a device-evaluated model at (pop, gen), for the equilibrium start: the
+ * model must be affine in frequency at generation 0 there, as the engine's start integrates
+ * s(x) = slope x + intercept. */
+template <typename Functor_selection>
+inline void device_selection_affine(gf_engine* eng, const Functor_selection& sel, int pop, int gen, float& slope,
+                                    float& intercept) {
+  (void)eng;
+  float* d = NULL;
+  float h[3];
+  cuda_check(cudaMalloc(&d, sizeof(h)), "run_sim");
+  selection_probe_kernel<Functor_selection><<<1, 32>>>(sel, pop, gen, d);
+  cuda_check(cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost), "run_sim");
+  cudaFree(d);
+  const float a = h[2] - h[0];
+  if (std::fabs((h[0] + 0.5f * a) - h[1]) > 1e-6f * (1.f + std::fabs(h[1]))) {
+    std::fprintf(stderr,
+                 "run_sim error: the mutation-selection-equilibrium start needs a selection model that is affine in "
+                 "frequency at generation 0 (population %d); start from a blank state or from prev_sim instead\n",
+                 pop);
+    std::exit(1);
+  }
+  slope = a;
+  intercept = h[0];
+}
+#endif
+
+/* Where the coefficients of a selection model come from: the host (exact affine models, and every
+ * model in a translation unit not compiled by nvcc) or the device (other models under nvcc). */
+template <typename Sel>
+struct uses_device_selection
+#ifdef __CUDACC__
+    : std::integral_constant<bool, !exact_affine<Sel>::value> {
+#else
+    : std::false_type {
+#endif
+};
+
+template <bool DEVICE>
+struct selection_dispatch {
+  /* coefficients for the equilibrium start at generation 0 */
+  template <typename Sel>
+  static void start(gf_engine*, const Sel& sel, int pop, float& slope, float& intercept) {
+    selection_affine(sel, pop, 0, slope, intercept);
+  }
+  /* coefficients packed into a generation record */
+  template <typename Sel>
+  static void generation(const Sel& sel, int pop, int gen, float& slope, float& intercept) {
+    selection_affine(sel, pop, gen, slope, intercept);
+  }
+  /* a generation that needs the device: nothing to do on the host path */
+  template <typename Sel>
+  static void run_alone(gf_engine*, const Sel&, gf_generation&, int) {}
+};
+
+#ifdef __CUDACC__
+template <>
+struct selection_dispatch<true> {
+  template <typename Sel>
+  static void start(gf_engine* eng, const Sel& sel, int pop, float& slope, float& intercept) {
+    device_selection_affine(eng, sel, pop, 0, slope, intercept);
+  }
+  template <typename Sel>
+  static void generation(const Sel&, int, int, float& slope, float& intercept) {
+    slope = 0.f;
+    intercept = 0.f;
+  }
+  /* fill the selection table for G, then run G alone */
+  template <typename Sel>
+  static void run_alone(gf_engine* eng, const Sel& sel, gf_generation& G, int P) {
+    G.selection_table = 1;
+    launch_selection_table(eng, sel, G, P);
+    check(eng, gf_sim_run(eng, &G, 1), "run_sim");
+  }
+};
+#endif
 
 /* privileged access to allele_trajectories (a friend of it) */
 struct trajectory_access {
@@ -578,6 +772,9 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
     std::exit(1);
   }
   gf_engine* eng = gofish_detail::engine_for(input.device);
+  gofish_detail::model_engine() = eng;
+  typedef gofish_detail::selection_dispatch<gofish_detail::uses_device_selection<Functor_selection>::value> sel_path;
+  const bool device_selection = gofish_detail::uses_device_selection<Functor_selection>::value;
   all_results.sim_input_constants.device = input.device = gf_engine_device(eng);  // reported back, as set_cuda_device does
   std::vector<char> extinct_v(P, 0);
   bool* extinct = reinterpret_cast<bool*>(extinct_v.data());
@@ -605,7 +802,7 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
       pops[p].mu = mu_rate(p, 0);
       pops[p].F = F;
       pops[p].h = dominance(p, 0);
-      gofish_detail::selection_affine(sel_coeff, p, 0, pops[p].sel_slope, pops[p].sel_intercept);
+      sel_path::start(eng, sel_coeff, p, pops[p].sel_slope, pops[p].sel_intercept);
     }
     check(eng, gf_sim_begin_mse(eng, &cfg, pops.data(), (preserve_mutations(0) | take_sample(0)) ? 1 : 0), "run_sim");
   } else {
@@ -670,6 +867,13 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
       batch.clear();
     }
   };
+  // in device-selection mode every generation runs alone, so nothing is ever queued before it
+  auto flush_before_last = [&]() {
+    if (batch.size() > 1) {
+      check(eng, gf_sim_run(eng, batch.data(), static_cast<int32_t>(batch.size() - 1)), "run_sim");
+      batch.erase(batch.begin(), batch.end() - 1);
+    }
+  };
   while (generation + 1 <= final_generation) {
     ++generation;
     gofish_detail::check_sim_parameters(mu_rate, demography, mig_prop, FI, P, extinct, generation);
@@ -697,7 +901,7 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
       pp.mu = mu_rate(pop, generation);
       pp.F = F;
       pp.h = dominance(pop, generation);
-      gofish_detail::selection_affine(sel_coeff, pop, generation, pp.sel_slope, pp.sel_intercept);
+      sel_path::generation(sel_coeff, pop, generation, pp.sel_slope, pp.sel_intercept);
       for (int to = 0; to < P; ++to) G.migration[pop * GF_MAX_POPULATIONS + to] = mig_prop(pop, to, generation);
     }
     const bool preserve = preserve_mutations(generation) | take_sample(generation);
@@ -707,6 +911,11 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
     G.preserve = (compact && preserve) ? 1 : 0;
     if (compact) next_compact_generation = generation + compact_interval;
     const bool sample_now = take_sample(generation) && generation != final_generation;
+    if (device_selection) {  // the generation reads the selection table filled just before it
+      flush_before_last();
+      sel_path::run_alone(eng, sel_coeff, G, P);
+      batch.clear();
+    }
     if (sample_now || batch.size() >= 256) flush();
     if (sample_now) {
       TA::store(all_results, sample_index, eng, generation, false, extinct, demography, FI);

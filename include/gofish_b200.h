@@ -88,7 +88,10 @@ typedef struct gf_generation {
   int32_t generation;
   int32_t compact;   /* compact after this generation (:705) */
   int32_t preserve;  /* mark survivors of this compaction as preserved (:686, scatter_arrays) */
-  int32_t reserved;
+  int32_t selection_table; /* 1: the selection coefficient of every drifted (population, mutation) is
+                            * read from the table of gf_sim_selection_view, filled by the caller for
+                            * this generation (sel_slope / sel_intercept are ignored); such a
+                            * generation is passed to gf_sim_run alone */
   gf_population_params pop[GF_MAX_POPULATIONS];
   /* migration[from * GF_MAX_POPULATIONS + to]: proportion of chromosomes in `to` from `from`
    * (Functor_migration, go_fish.cuh:238). */
@@ -132,6 +135,30 @@ gf_status gf_sim_begin_mse(gf_engine* engine, const gf_sim_config* config, const
  * Asynchronous: returns once the work is queued on the engine's stream. */
 gf_status gf_sim_run(gf_engine* engine, const gf_generation* gens, int32_t num_generations);
 
+/* Selection models that are not affine in frequency.  The reference evaluates
+ * s = sel_coeff(pop, generation, x_mig) per mutation inside migration_selection_drift
+ * (go_fish_impl.cuh:98-105), with x_mig = sum over k of migration(k, pop, generation) * freq[k][i]
+ * accumulated in k order with fused multiply-adds.  For such a model the caller evaluates the model on
+ * the device before the generation: it computes x_mig the same way from `freq` and the generation's
+ * migration matrix and writes s (unclamped; the engine applies max(s, -1)) to
+ * selection[pop * selection_stride + i] for every drifted population and every i < *num_mutations,
+ * with a kernel launched on `cuda_stream`, then runs the generation with selection_table = 1.  The
+ * header front-end (include/3P/go_fish.cuh) does this with a kernel instantiated for the user's
+ * functor when the user's translation unit is compiled by nvcc.  The view is valid until the next
+ * gf_sim_* call. */
+typedef struct gf_selection_view {
+  const float* freq;               /* [num_populations][row_stride] frequencies the generation starts from */
+  int64_t row_stride;
+  const int32_t* num_mutations;    /* device word: mutations the generation starts from */
+  float* selection;                /* [num_populations][selection_stride] coefficients to write */
+  int64_t selection_stride;
+  int32_t num_populations;
+  int32_t reserved;
+  void* cuda_stream;               /* the engine's cudaStream_t */
+} gf_selection_view;
+
+gf_status gf_sim_selection_view(gf_engine* engine, gf_selection_view* out);
+
 /* Current number of mutations in the array (h_mutations_Index).  Synchronizes the stream. */
 gf_status gf_sim_num_mutations(gf_engine* engine, int32_t* out_num_mutations);
 
@@ -153,6 +180,16 @@ gf_status gf_sim_device_state(gf_engine* engine, const float** out_freq, int32_t
  * shared.cuh:251-256): max(Poisson~(mu * Nchrom_e * L), 0) with counter (1, generation, pop, 0). */
 int32_t gf_new_mutation_count(int32_t seed1, int32_t seed2, float mu, int32_t Nchrom_e, float num_sites,
                               int32_t generation, int32_t population);
+
+/* Selection coefficients of Sim_Model::selection_sine_wave, s = A sin(pi t + rho) + D for
+ * t = t0 .. t0 + count - 1 (t = generation - generation_shift), into host out[count].  The reference
+ * evaluates this expression inside its drift kernel under --use_fast_math
+ * (template_inline_simulation_functors.cuh:92), where the sine is the hardware approximation; this
+ * call evaluates it on the engine's device with the same expression and flags, so the per-generation
+ * intercept the caller passes in gf_population_params is the float the reference's kernel uses.
+ * Synchronizes the engine's stream. */
+gf_status gf_selection_sine_values(gf_engine* engine, float A, float pi, float rho, float D, int32_t t0, int32_t count,
+                                   float* out);
 
 /* ---------------------------------------------------------------------------------------------
  * Batched replicates (no reference counterpart: the reference runs one simulation per run_sim call,

@@ -16,9 +16,7 @@
 #include <string>
 #include <vector>
 
-#include "go_fish.cuh"
-#include "spectrum.h"
-#include "../tests/cpp/scenarios.h"
+#include "../tests/cpp/scenarios.h"  // includes the reference's go_fish.cuh and spectrum.h
 
 static std::vector<char> slurp(const char* path) {
   FILE* f = std::fopen(path, "rb");

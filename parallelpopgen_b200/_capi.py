@@ -35,7 +35,7 @@ POP_DTYPE = np.dtype([
     ("mu", "<f4"), ("F", "<f4"), ("h", "<f4"), ("sel_slope", "<f4"), ("sel_intercept", "<f4"),
 ])
 GEN_DTYPE = np.dtype([
-    ("generation", "<i4"), ("compact", "<i4"), ("preserve", "<i4"), ("reserved", "<i4"),
+    ("generation", "<i4"), ("compact", "<i4"), ("preserve", "<i4"), ("selection_table", "<i4"),
     ("pop", POP_DTYPE, (MAX_POPULATIONS,)),
     ("migration", "<f4", (MAX_POPULATIONS * MAX_POPULATIONS,)),
 ])
@@ -107,7 +107,9 @@ SIGNATURES = {
     "gf_sim_num_mutations": (_I, [_P, ctypes.POINTER(_I)]),
     "gf_sim_read_state": (_I, [_P, _P, _P, _I, ctypes.POINTER(_I)]),
     "gf_sim_device_state": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "gf_sim_selection_view": (_I, [_P, _P]),
     "gf_new_mutation_count": (_I, [_I, _I, _F, _I, _F, _I, _I]),
+    "gf_selection_sine_values": (_I, [_P, _F, _F, _F, _F, _I, _I, _P]),
     "gf_population_histogram": (_I, [_P, _P, _I, _I, _F, _P]),
     "gf_site_frequency_spectrum": (_I, [_P, _P, _I, _I, _I, _F, _P]),
     "gf_population_histogram_device": (_I, [_P, _P, _I, _I, _F, _P]),

@@ -143,10 +143,18 @@ __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
             xm.w += m * v.w;
           }
           const float F = a.F[p], h = a.h[p], sa = a.sel_a[p], sb = a.sel_b[p];
-          xs[0] = selected_freq<NEUTRAL>(xm.x, sa, sb, F, h);
-          xs[1] = selected_freq<NEUTRAL>(xm.y, sa, sb, F, h);
-          xs[2] = selected_freq<NEUTRAL>(xm.z, sa, sb, F, h);
-          xs[3] = selected_freq<NEUTRAL>(xm.w, sa, sb, F, h);
+          if (!NEUTRAL && a.sel_table) {  // s(x_mig) evaluated per slot by the caller's model
+            const float4 st = __ldg(reinterpret_cast<const float4*>(a.sel_table + p * a.sel_stride + base));
+            xs[0] = selection_step(xm.x, fmaxf(st.x, -1.f), F, h);
+            xs[1] = selection_step(xm.y, fmaxf(st.y, -1.f), F, h);
+            xs[2] = selection_step(xm.z, fmaxf(st.z, -1.f), F, h);
+            xs[3] = selection_step(xm.w, fmaxf(st.w, -1.f), F, h);
+          } else {
+            xs[0] = selected_freq<NEUTRAL>(xm.x, sa, sb, F, h);
+            xs[1] = selected_freq<NEUTRAL>(xm.y, sa, sb, F, h);
+            xs[2] = selected_freq<NEUTRAL>(xm.z, sa, sb, F, h);
+            xs[3] = selected_freq<NEUTRAL>(xm.w, sa, sb, F, h);
+          }
         }
         // lost (x == 0) and, for N > 6, fixed (x == 1) slots have a certain outcome
         int res[4];
@@ -196,7 +204,10 @@ __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
             const int N = a.Nc[p];
             float o = 0.f;
             if (N > 0) {
-              const float xs = selected_freq<NEUTRAL>(xm, a.sel_a[p], a.sel_b[p], a.F[p], a.h[p]);
+              const float xs =
+                  (!NEUTRAL && a.sel_table)
+                      ? selection_step(xm, fmaxf(a.sel_table[p * a.sel_stride + e], -1.f), a.F[p], a.h[p])
+                      : selected_freq<NEUTRAL>(xm, a.sel_a[p], a.sel_b[p], a.F[p], a.h[p]);
               o = static_cast<float>(clampi(drift_tail(a.seed1, a.seed2, e, g, p, xs, N), 0, N)) /
                   static_cast<float>(N);
             }
@@ -463,6 +474,9 @@ static void release_sim(Engine* e) {
     e->id_gp[b] = nullptr;
     e->id_tid[b] = nullptr;
   }
+  if (e->sel_table) cudaFreeAsync(e->sel_table, e->stream);
+  e->sel_table = nullptr;
+  e->sel_table_stride = 0;
   if (e->flags) cudaFreeAsync(e->flags, e->stream);
   if (e->tile_count) cudaFreeAsync(e->tile_count, e->stream);
   if (e->tile_offset) cudaFreeAsync(e->tile_offset, e->stream);
@@ -716,6 +730,7 @@ static gf_status build_args(Engine* e, const gf_generation& gen, GenArgs& a, Gen
     a.sel_a[p] = pp.sel_slope;
     a.sel_b[p] = pp.sel_intercept;
     if (pp.drift && (pp.sel_slope != 0.f || pp.sel_intercept != 0.f)) neutral = false;
+    if (pp.drift && gen.selection_table) neutral = false;
     int count = 0;
     if (pp.mutate && pp.Nchrom_e > 0) {
       count = host_new_mutation_count(e->seed1, e->seed2, pp.mu, pp.Nchrom_e, e->num_sites, gen.generation, p);
@@ -729,6 +744,13 @@ static gf_status build_args(Engine* e, const gf_generation& gen, GenArgs& a, Gen
   for (int p = P; p <= kMaxPops; ++p) a.new_offset[p] = a.new_offset[P];
   a.new_total = static_cast<int>(new_total);
   a.flag = (gen.compact || gen.preserve) && e->compact_interval > 0;
+  if (gen.selection_table) {
+    if (!e->sel_table)
+      return fail(e, GF_ERR_STATE, "generation %d reads a selection table that gf_sim_selection_view has not set up",
+                  gen.generation);
+    a.sel_table = e->sel_table;
+    a.sel_stride = e->sel_table_stride;
+  }
   gh.neutral = neutral;
   gh.preserve = gen.preserve != 0;
   return GF_OK;
@@ -887,7 +909,7 @@ static gf_status push_readback(Engine* e, int slot) {
 
 // Single-population generations a window may hold: drifted, no migration factor other than 1.
 static bool window_eligible(const Engine* e, const gf_generation& g) {
-  return e->use_windows && e->P == 1 && g.pop[0].drift == 1 && g.migration[0] == 1.0f;
+  return e->use_windows && e->P == 1 && g.pop[0].drift == 1 && g.migration[0] == 1.0f && !g.selection_table;
 }
 
 constexpr int kMaxWindow = kMaxWindowGenerations;
@@ -897,7 +919,7 @@ constexpr int kMaxWindow = kMaxWindowGenerations;
 // whose rows may hold a nonzero value, given the generations before this one).  Extinction
 // generations and every generation after an extinction run one launch each.
 static bool window_mp_eligible(const Engine* e, const gf_generation& g, int live) {
-  return e->use_windows && mp_window_generation_ok(g, e->P, live, kMaxWindowPops);
+  return e->use_windows && !g.selection_table && mp_window_generation_ok(g, e->P, live, kMaxWindowPops);
 }
 
 static int drift_bits(const gf_generation& g, int P) { return drifted_populations(g, P); }
@@ -947,17 +969,26 @@ static gf_status launch_window(Engine* e, int b, int first, int count, const Gen
   w.any_compact = R.compact != 0;
   w.stats = e->d_stats;
   w.fault = e->d_count + 2;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // profiling: the window kernel's time counts as drift, its segmented scan and scatter as compaction
+  cudaEvent_t ev0 = nullptr, evw = nullptr, evc = nullptr, ev1 = nullptr;
   if (e->profiling) {
     ev0 = prof_event(e);
+    evw = prof_event(e);
+    evc = prof_event(e);
     ev1 = prof_event(e);
     GF_CUDA(e, cudaEventRecord(ev0, e->stream));
   }
-  st = window_run(e, w, e->freq[e->cur]);
+  st = window_run(e, w, e->freq[e->cur], evw, evc);
   if (st != GF_OK) return st;
   if (e->profiling) {
     GF_CUDA(e, cudaEventRecord(ev1, e->stream));
-    e->prof_drift.emplace_back(ev0, ev1);
+    e->prof_drift.emplace_back(ev0, evw);
+    if (R.compact) {
+      e->prof_compact.emplace_back(evc, ev1);
+    } else {
+      e->prof_pool.push_back(evc);
+      e->prof_pool.push_back(ev1);
+    }
   }
   e->M_upper = need;
   for (auto& pc : e->pending) pc.added += news;
@@ -1433,9 +1464,41 @@ gf_status gf_sim_run(gf_engine* g, const gf_generation* gens, int32_t n) {
     Engine* e = &g->impl;
     if (!e->active) return fail(e, GF_ERR_STATE, "gf_sim_run before gf_sim_begin_*");
     if (n < 0 || (n > 0 && !gens)) return fail(e, GF_ERR_INVALID_ARGUMENT, "bad generation table");
+    for (int i = 0; i < n && n > 1; ++i)
+      if (gens[i].selection_table)
+        return fail(e, GF_ERR_INVALID_ARGUMENT,
+                    "generation %d reads a selection table: such a generation is run alone (one record per call)",
+                    gens[i].generation);
     GF_CUDA(e, cudaSetDevice(e->device));
     if (n == 0) return GF_OK;
     return run_batch(e, gens, n);
+  });
+}
+
+gf_status gf_sim_selection_view(gf_engine* g, gf_selection_view* out) {
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->active) return fail(e, GF_ERR_STATE, "gf_sim_selection_view before gf_sim_begin_*");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    if (!e->sel_table || e->sel_table_stride < e->capacity) {
+      if (e->sel_table) cudaFreeAsync(e->sel_table, e->stream);
+      e->sel_table = nullptr;
+      e->sel_table_stride = 0;
+      gf_status st = pool_alloc(e, reinterpret_cast<void**>(&e->sel_table),
+                                sizeof(float) * static_cast<size_t>(e->P) * static_cast<size_t>(e->capacity));
+      if (st != GF_OK) return st;
+      e->sel_table_stride = e->capacity;
+    }
+    out->freq = e->freq[e->cur];
+    out->row_stride = e->capacity;
+    out->num_mutations = e->d_count + e->count_slot;
+    out->selection = e->sel_table;
+    out->selection_stride = e->sel_table_stride;
+    out->num_populations = e->P;
+    out->reserved = 0;
+    out->cuda_stream = e->stream;
+    return GF_OK;
   });
 }
 

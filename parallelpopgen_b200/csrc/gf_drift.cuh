@@ -14,18 +14,31 @@
 #ifndef GF_WINDOW_MIN_BLOCKS
 #define GF_WINDOW_MIN_BLOCKS GF_DRIFT_MIN_BLOCKS
 #endif
+// 1: the window kernel stages a window's generation records in shared memory.
+#ifndef GF_WIN_STAGE_RECORDS
+#define GF_WIN_STAGE_RECORDS 1
+#endif
+// 1: the lane-order draw schedule walks a quad's lanes in a rolled loop (one inlined copy of the
+// sampler instead of four); 0: the loop is unrolled.
+#ifndef GF_LANES_ROLLED
+#define GF_LANES_ROLLED 0
+#endif
 
 namespace gf {
 
 
 // Frequency after selection (go_fish_impl.cuh:105 / :119).  With s == 0 the expression reduces to
 // x exactly, which the NEUTRAL instantiation uses directly.
+// The selection step for a given coefficient s (already clamped at -1).
+__device__ __forceinline__ float selection_step(float x, float s, float F, float h) {
+  return (s * x * x + x + (F + h - h * F) * s * x * (1 - x)) /
+         (x * x * s + (F + 2 * h - 2 * h * F) * s * x * (1 - x) + 1);
+}
+
 template <bool NEUTRAL>
 __device__ __forceinline__ float selected_freq(float x, float sa, float sb, float F, float h) {
   if (NEUTRAL) return x;
-  const float s = fmaxf(sa * x + sb, -1.f);
-  return (s * x * x + x + (F + h - h * F) * s * x * (1 - x)) /
-         (x * x * s + (F + 2 * h - 2 * h * F) * s * x * (1 - x) + 1);
+  return selection_step(x, fmaxf(sa * x + sb, -1.f), F, h);
 }
 
 // Drift of one quad lane: returns the new count j in [0, N].  Lost (x == 0) and, for N > 6, fixed
@@ -99,9 +112,23 @@ __device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsi
   const float Nf = static_cast<float>(N);
   const uint32_t rb[4] = {r.x, r.y, r.z, r.w};
   if (DRAW == kDrawLanes) {
+#if GF_LANES_ROLLED
+#pragma unroll 1
+    for (unsigned m = need; m; m &= m - 1u) {
+      const int j = __ffs(m) - 1;
+      const float x = j == 0 ? xs[0] : j == 1 ? xs[1] : j == 2 ? xs[2] : xs[3];
+      const uint32_t b = j == 0 ? rb[0] : j == 1 ? rb[1] : j == 2 ? rb[2] : rb[3];
+      const int d = GF_LANE_DRAW(b, x * N, (1.0f - x) * (x * N), Nf);
+      res[0] = j == 0 ? d : res[0];
+      res[1] = j == 1 ? d : res[1];
+      res[2] = j == 2 ? d : res[2];
+      res[3] = j == 3 ? d : res[3];
+    }
+#else
 #pragma unroll
     for (int j = 0; j < 4; ++j)
       if ((need >> j) & 1u) res[j] = GF_LANE_DRAW(rb[j], xs[j] * N, (1.0f - xs[j]) * (xs[j] * N), Nf);
+#endif
     return;
   }
   if (DRAW == kDrawNormalAll) {

@@ -50,6 +50,10 @@ struct GenArgs {
   int flag;                      // 1: write compaction flags and tile counts for this generation
   int check_preserved;           // 1: some mutation may carry the preserved mark
   float mig[kMaxPops * kMaxPops];  // [from * num_pops + to]
+  // per-slot selection coefficients s(pop, generation, x_mig) written by the caller before this
+  // generation ([P][sel_stride], slots below the generation's starting count); null: affine (sel_a, sel_b)
+  const float* sel_table;
+  long long sel_stride;
 };
 
 // One generation of one single-population replicate, as the window kernel reads it (36 B).
@@ -271,6 +275,10 @@ struct Engine {
   WinRep* h_wrep[2] = {nullptr, nullptr};
   size_t wtable_cap[2] = {0, 0};
   bool use_windows = true;   // single-population runs use the window kernel
+  // per-slot selection table of generations whose selection model is evaluated by the caller on the
+  // device (gf_sim_selection_view): [P][sel_table_stride] floats, grown with the state's capacity
+  float* sel_table = nullptr;
+  long long sel_table_stride = 0;
 
   // batched replicates (gf_batch_*)
   Batch* batch = nullptr;
@@ -327,7 +335,10 @@ gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
 // Window launch (+ segmented compaction into compact_dst), window.cu.
 void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
                         int* total_out);
-gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst);
+// after_window, before_compaction (either may be null): recorded on the stream between the window
+// kernel and its compaction (two events, so that each timing pair owns its own)
+gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaEvent_t after_window = nullptr,
+                     cudaEvent_t before_compaction = nullptr);
 // Multi-population window launch (window_mp.cu); P in [2, 4].
 gf_status window_mp_run(Engine* e, const WindowMpLaunch& w);
 constexpr int kMaxWindowPops = 4;

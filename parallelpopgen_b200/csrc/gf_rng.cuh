@@ -85,8 +85,8 @@ __host__ __device__ __forceinline__ float u01(uint32_t bits) {
     if (cdf >= r || ((CAP_MEAN) > 0 && mean <= (CAP_MEAN))) return J; \
   }
 
-// Poisson inverse CDF by sequential search (poiscdfinv, shared.cuh:168-249).
-__host__ __device__ __forceinline__ int pois_search(float r, float mean) {
+// Poisson inverse CDF by sequential search (poiscdfinv, shared.cuh:168-249), all 70 steps.
+static __host__ __device__ __noinline__ int pois_search_full(float r, float mean) {
   float emu = expf(-1 * mean);
   float cdf = emu;
   if (cdf >= r) return 0;
@@ -117,8 +117,36 @@ __host__ __device__ __forceinline__ int pois_search(float r, float mean) {
   return 70;
 }
 
-// Binomial inverse CDF by sequential search (binomcdfinv, shared.cuh:84-166); x = p, n = N.
-__host__ __device__ __forceinline__ int binom_search(float r, float mean, float x, float n) {
+// The same search for mean <= 6, the case every sampler branch reaches it with: step 24's cap exit
+// (`|| mean <= 6`) then always returns 24, so the steps after it never run and are left out.  The
+// result equals pois_search_full's for every such mean; the shorter body keeps the inlined sampler
+// small (instruction-cache footprint of the drift kernels).
+__host__ __device__ __forceinline__ int pois_search_upto6(float r, float mean) {
+  float emu = expf(-1 * mean);
+  float cdf = emu;
+  if (cdf >= r) return 0;
+#define GF_ITER(JF)          \
+  {                          \
+    emu *= mean / (JF);      \
+    cdf += emu;              \
+  }
+  GF_SEARCH_STEP(1, 0) GF_SEARCH_STEP(2, 0) GF_SEARCH_STEP(3, 0) GF_SEARCH_STEP(4, 0)
+  GF_SEARCH_STEP(5, 0) GF_SEARCH_STEP(6, 0) GF_SEARCH_STEP(7, 0) GF_SEARCH_STEP(8, 0)
+  GF_SEARCH_STEP(9, 0) GF_SEARCH_STEP(10, 0) GF_SEARCH_STEP(11, 1) GF_SEARCH_STEP(12, 0)
+  GF_SEARCH_STEP(13, 0) GF_SEARCH_STEP(14, 2) GF_SEARCH_STEP(15, 0) GF_SEARCH_STEP(16, 0)
+  GF_SEARCH_STEP(17, 3) GF_SEARCH_STEP(18, 0) GF_SEARCH_STEP(19, 0) GF_SEARCH_STEP(20, 4)
+  GF_SEARCH_STEP(21, 0) GF_SEARCH_STEP(22, 5) GF_SEARCH_STEP(23, 0)
+#undef GF_ITER
+  return 24;
+}
+
+__host__ __device__ __forceinline__ int pois_search(float r, float mean) {
+  if (mean <= kMeanBoundary) return pois_search_upto6(r, mean);
+  return pois_search_full(r, mean);
+}
+
+// Binomial inverse CDF by sequential search (binomcdfinv, shared.cuh:84-166); x = p, n = N; all 70 steps.
+static __host__ __device__ __noinline__ int binom_search_full(float r, float mean, float x, float n) {
   float emu = powf(1 - x, n);
   if (emu == 1) emu = expf(-1 * mean);
   float cdf = emu;
@@ -148,6 +176,32 @@ __host__ __device__ __forceinline__ int binom_search(float r, float mean, float 
   GF_SEARCH_STEP(69, 0)
 #undef GF_ITER
   return 70;
+}
+
+// The same search for mean <= 6 (see pois_search_upto6).
+__host__ __device__ __forceinline__ int binom_search_upto6(float r, float mean, float x, float n) {
+  float emu = powf(1 - x, n);
+  if (emu == 1) emu = expf(-1 * mean);
+  float cdf = emu;
+  if (cdf >= r) return 0;
+#define GF_ITER(JF)                                       \
+  {                                                       \
+    emu *= ((n + 1.f - (JF)) * x) / ((JF) * (1 - x));     \
+    cdf += emu;                                           \
+  }
+  GF_SEARCH_STEP(1, 0) GF_SEARCH_STEP(2, 0) GF_SEARCH_STEP(3, 0) GF_SEARCH_STEP(4, 0)
+  GF_SEARCH_STEP(5, 0) GF_SEARCH_STEP(6, 0) GF_SEARCH_STEP(7, 0) GF_SEARCH_STEP(8, 0)
+  GF_SEARCH_STEP(9, 0) GF_SEARCH_STEP(10, 0) GF_SEARCH_STEP(11, 1) GF_SEARCH_STEP(12, 0)
+  GF_SEARCH_STEP(13, 0) GF_SEARCH_STEP(14, 2) GF_SEARCH_STEP(15, 0) GF_SEARCH_STEP(16, 0)
+  GF_SEARCH_STEP(17, 3) GF_SEARCH_STEP(18, 0) GF_SEARCH_STEP(19, 0) GF_SEARCH_STEP(20, 4)
+  GF_SEARCH_STEP(21, 0) GF_SEARCH_STEP(22, 5) GF_SEARCH_STEP(23, 0)
+#undef GF_ITER
+  return 24;
+}
+
+__host__ __device__ __forceinline__ int binom_search(float r, float mean, float x, float n) {
+  if (mean <= kMeanBoundary) return binom_search_upto6(r, mean, x, n);
+  return binom_search_full(r, mean, x, n);
 }
 #undef GF_SEARCH_STEP
 

@@ -122,6 +122,12 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
   __shared__ unsigned s_warp[kWinThreads / 32];
   __shared__ int s_tile0[kRepCache];
   __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinThreads / 32 : 1];
+#if GF_WIN_STAGE_RECORDS
+  // the generation records of the replicate whose tile the block works on (every thread reads every
+  // record of the window; staged once per replicate instead of read from global memory per thread)
+  __shared__ WinGen s_rec[kMaxWindowGenerations];
+  int staged = -1;  // replicate whose records s_rec holds (block-uniform)
+#endif
   const int lane = threadIdx.x & 31;
   WarpDraws* wd = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
@@ -130,6 +136,17 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     if (threadIdx.x == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
     __syncthreads();
     const WinRep R = reps[s_rep];
+#if GF_WIN_STAGE_RECORDS
+    // every thread has finished the previous tile (the barrier above), so s_rec may be refilled
+    const int nstage = min(R.ngen, kMaxWindowGenerations);
+    if (s_rep != staged) {
+      const int* src = reinterpret_cast<const int*>(recs + R.rec);
+      int* dst = reinterpret_cast<int*>(s_rec);
+      const int words = nstage * static_cast<int>(sizeof(WinGen) / 4);
+      for (int i = threadIdx.x; i < words; i += kWinThreads) dst[i] = src[i];
+      staged = s_rep;
+    }
+#endif
     __syncthreads();
     const int t = gt - R.tile0;
     const int q = t * kWinThreads + threadIdx.x;  // quad within the replicate
@@ -156,7 +173,11 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     int alive = 1;
 #pragma unroll 1
     for (int k = 0; k < R.ngen; ++k) {
+#if GF_WIN_STAGE_RECORDS
+      const WinGen G = k < nstage ? s_rec[k] : recs[R.rec + k];
+#else
       const WinGen G = recs[R.rec + k];
+#endif
       const int N = G.Nc;
       const int g = G.generation;
       alive = G.alive;
@@ -475,7 +496,8 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
 
 // Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
 // and scatter into `compact_dst` (the other state buffer).
-gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
+gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaEvent_t after_window,
+                     cudaEvent_t before_compaction) {
   switch (e->draw_strategy) {
     case kDrawWarp: launch_window_kernel<kDrawWarp>(e, w); break;
     case kDrawGrouped: launch_window_kernel<kDrawGrouped>(e, w); break;
@@ -484,6 +506,8 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst) {
   }
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;
+  if (after_window) GF_CUDA(e, cudaEventRecord(after_window, e->stream));
+  if (before_compaction) GF_CUDA(e, cudaEventRecord(before_compaction, e->stream));
   if (w.any_compact) {
     seg_scan_kernel<<<w.nreps, kSegScanThreads, 0, e->stream>>>(w.tile_count, w.tile_offset, w.reps, w.M_end,
                                                                 w.M_out);

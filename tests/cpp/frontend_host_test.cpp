@@ -76,10 +76,10 @@ int main() {
   line("sel_ps_p1", b);
   gofish_detail::selection_affine(sps, 0, 7, a, b);
   line("sel_ps_p0", b);
+  // (run_sim takes the sine model's coefficient from the device, gf_selection_sine_values; the host
+  // operator() is the plain-C++ evaluation a user may call)
   selection_sine_wave ssw(0.01f, 0.1f, 0.001f);
-  gofish_detail::selection_affine(ssw, 0, 12, a, b);
-  line("sel_sine_slope", a);
-  line("sel_sine_g12", b);
+  line("sel_sine_g12", ssw(0, 12, 0.3f));
 
   // allele_trajectories: defaults, copy, dump, delete_time_sample
   GO_Fish::allele_trajectories t;

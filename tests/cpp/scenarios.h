@@ -8,21 +8,37 @@
 // tests/gfdump.py).
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
 #include <map>
+#include <sstream>
 #include <string>
 #include <vector>
 
+// Test harness only: both libraries keep the arrays of a time sample private, and the only public way
+// to start a run from a given state is prev_sim.  To start the reference and the drop-in from one
+// identical stored state (save_state / load_state below), the harness opens the private members of
+// allele_trajectories, whose names are the same in both header sets.  Nothing else depends on this.
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
+#define private public
 #include "go_fish.cuh"
 #include "spectrum.h"
+#undef private
 
 #ifdef __CUDACC__
 #define SCN_HD __host__ __device__
+#define SCN_D __device__
 #else
 #define SCN_HD
+#define SCN_D
 #endif
 
 namespace scn {
@@ -98,7 +114,37 @@ struct split_migration {
 // ---------------------------------------------------------------------------------------------
 // scenario "wf": one population (or several identical ones), constant size, constant selection
 // ---------------------------------------------------------------------------------------------
-inline void scenario_wf(GO_Fish::allele_trajectories& a, const Args& args) {
+template <typename Selection>
+inline void run_wf(GO_Fish::allele_trajectories& a, const Args& args, const GO_Fish::allele_trajectories* prev,
+                   const Sim_Model::F_mu_h_constant& mutation, const Sim_Model::demography_constant& demography,
+                   const Sim_Model::migration_constant_equal& migration, const Selection& selection,
+                   const Sim_Model::F_mu_h_constant& inbreeding, const Sim_Model::F_mu_h_constant& dominance) {
+  every_k sample(static_cast<int>(args.integer("sample_every", 0)), 0);
+  if (prev) {  // continue from sample 0 of a stored state (see load_state)
+    a.sim_input_constants.init_mse = false;
+    a.sim_input_constants.prev_sim_sample = 0;
+    GO_Fish::run_sim(a, mutation, demography, migration, selection, inbreeding, dominance, Sim_Model::bool_off(),
+                     sample, *prev);
+  } else {
+    GO_Fish::run_sim(a, mutation, demography, migration, selection, inbreeding, dominance, Sim_Model::bool_off(),
+                     sample);
+  }
+}
+
+// A user selection model that is not affine in frequency, s(x) = a x^2 + b, written against the
+// reference's functor contract (a __device__ call operator, template_inline_simulation_functors.cuh:36-38).
+struct quadratic_selection {
+  float a, b;
+  SCN_D float operator()(const int population, const int generation, const float freq) const {
+    return a * freq * freq + b;
+  }
+};
+
+// Selection is selection_constant(gamma); with sine_A != 0 the seasonal model
+// selection_sine_wave(sine_A, sine_pi, gamma, rho = sine_rho); with quad_a != 0 the user model
+// quadratic_selection(quad_a / 2N, gamma / 2N) -- all scaled by the population size.
+inline void scenario_wf(GO_Fish::allele_trajectories& a, const Args& args,
+                        const GO_Fish::allele_trajectories* prev = NULL) {
   using namespace Sim_Model;
   a.sim_input_constants.seed1 = static_cast<int>(args.integer("seed1", 0xbeef));
   a.sim_input_constants.seed2 = static_cast<int>(args.integer("seed2", 0xdecaf));
@@ -112,10 +158,22 @@ inline void scenario_wf(GO_Fish::allele_trajectories& a, const Args& args) {
   F_mu_h_constant inbreeding(static_cast<float>(args.num("F", 0.0)));
   demography_constant demography(static_cast<int>(args.integer("N", 10000)));
   migration_constant_equal migration(static_cast<float>(args.num("m", 0.0)), P);
-  selection_constant selection(static_cast<float>(args.num("gamma", 0.0)), demography, inbreeding);
   F_mu_h_constant dominance(static_cast<float>(args.num("h", 0.5)));
-  every_k sample(static_cast<int>(args.integer("sample_every", 0)), 0);
-  GO_Fish::run_sim(a, mutation, demography, migration, selection, inbreeding, dominance, bool_off(), sample);
+  const float gamma = static_cast<float>(args.num("gamma", 0.0));
+  const float sine_A = static_cast<float>(args.num("sine_A", 0.0));
+  const float quad_a = static_cast<float>(args.num("quad_a", 0.0));
+  if (quad_a != 0.f) {
+    const float twoN = 2.f * static_cast<float>(args.integer("N", 10000));
+    quadratic_selection selection = {quad_a / twoN, gamma / twoN};
+    run_wf(a, args, prev, mutation, demography, migration, selection, inbreeding, dominance);
+  } else if (sine_A != 0.f) {
+    selection_sine_wave selection(sine_A, static_cast<float>(args.num("sine_pi", 0.05)), gamma, demography, inbreeding,
+                                  static_cast<float>(args.num("sine_rho", 0.0)));
+    run_wf(a, args, prev, mutation, demography, migration, selection, inbreeding, dominance);
+  } else {
+    selection_constant selection(gamma, demography, inbreeding);
+    run_wf(a, args, prev, mutation, demography, migration, selection, inbreeding, dominance);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -183,6 +241,89 @@ inline void scenario_split3(GO_Fish::allele_trajectories& a, const Args& args) {
   F_mu_h_constant dominance(static_cast<float>(args.num("h", 0.3)));
   every_k sample(static_cast<int>(args.integer("sample_every", 500)), 0);
   GO_Fish::run_sim(a, mutation, dem, mig, selection, inbreeding, dominance, bool_off(), sample);
+}
+
+// Three populations: pop 0 exists from the start, pop 1 is founded at found1 and pop 2 at found2; each
+// starts at N0 individuals and grows exponentially at `rate` per generation until it reaches its cap.
+struct capped_growth_demography {
+  int N0;
+  float rate;
+  int found1, found2;
+  int cap0, cap1, cap2;
+  SCN_HD int operator()(const int pop, const int gen) const {
+    const int found = pop == 0 ? 0 : (pop == 1 ? found1 : found2);
+    const int cap = pop == 0 ? cap0 : (pop == 1 ? cap1 : cap2);
+    if (pop > 0 && gen < found) return 0;
+    const float n = static_cast<float>(N0) * expf(rate * static_cast<float>(gen - found));
+    return n >= static_cast<float>(cap) ? cap : static_cast<int>(roundf(n));
+  }
+};
+
+// Pop 1 is founded from pop 0 and pop 2 from pop 1 (all chromosomes of the founding generation come
+// from the parent); otherwise existing populations exchange migrants symmetrically at rate m.
+struct founder_migration {
+  float m;
+  int found1, found2;
+  SCN_HD bool exists(int pop, int gen) const { return pop == 0 || (pop == 1 ? gen >= found1 : gen >= found2); }
+  SCN_HD float operator()(const int from, const int to, const int gen) const {
+    if (!exists(to, gen)) return from == to ? 1.f : 0.f;
+    if (to == 1 && gen == found1) return from == 0 ? 1.f : 0.f;
+    if (to == 2 && gen == found2) return from == 1 ? 1.f : 0.f;
+    if (!exists(from, gen)) return 0.f;
+    int live = 0;
+    for (int p = 0; p < 3; ++p) live += exists(p, gen) ? 1 : 0;
+    if (from == to) return 1.f - (live - 1) * m;
+    return m;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// scenario "multipop": the three-population benchmark model -- an ancestral population of N0 = 1e4
+// at mutation-selection equilibrium, population 1 founded from it at generation 1 and population 2
+// from population 1 at generation 2000, each growing at r = 0.005 to a cap (1e5, 2.5e5, 5e5);
+// symmetric migration 1e-4, selection gamma -5 switching to +2 at generation 3000 (selection_constant
+// scaled by the ancestral size), h = 0.3, F = 0.1 in population 2, mu = 1e-9, L = 2e8, compaction
+// every 35 generations and a time sample every 500.  With a stored start (prev) the run continues
+// from that state's generation for `gens` more generations.
+// ---------------------------------------------------------------------------------------------
+inline void scenario_multipop(GO_Fish::allele_trajectories& a, const Args& args,
+                              const GO_Fish::allele_trajectories* prev = NULL) {
+  using namespace Sim_Model;
+  a.sim_input_constants.seed1 = static_cast<int>(args.integer("seed1", 0xbeef));
+  a.sim_input_constants.seed2 = static_cast<int>(args.integer("seed2", 0xdecaf));
+  a.sim_input_constants.num_generations = static_cast<int>(args.integer("gens", 5000));
+  a.sim_input_constants.num_sites = static_cast<float>(args.num("L", 2e8));
+  a.sim_input_constants.num_populations = 3;
+  a.sim_input_constants.init_mse = true;
+  a.sim_input_constants.compact_interval = static_cast<int>(args.integer("compact", 35));
+  capped_growth_demography dem;
+  dem.N0 = static_cast<int>(args.integer("N0", 10000));
+  dem.rate = static_cast<float>(args.num("rate", 0.005));
+  dem.found1 = static_cast<int>(args.integer("found1", 1));
+  dem.found2 = static_cast<int>(args.integer("found2", 2000));
+  dem.cap0 = static_cast<int>(args.integer("cap0", 100000));
+  dem.cap1 = static_cast<int>(args.integer("cap1", 250000));
+  dem.cap2 = static_cast<int>(args.integer("cap2", 500000));
+  founder_migration mig;
+  mig.m = static_cast<float>(args.num("m", 1e-4));
+  mig.found1 = dem.found1;
+  mig.found2 = dem.found2;
+  F_mu_h_constant mutation(static_cast<float>(args.num("mu", 1e-9)));
+  F_mu_h_population_specific<F_mu_h_constant, F_mu_h_constant> inbreeding(
+      F_mu_h_constant(0.f), F_mu_h_constant(static_cast<float>(args.num("F2", 0.1))), 2);
+  selection_piecewise<selection_constant, selection_constant> selection(
+      selection_constant(static_cast<float>(args.num("gamma1", -5.0)), dem, inbreeding),
+      selection_constant(static_cast<float>(args.num("gamma2", 2.0)), dem, inbreeding),
+      static_cast<int>(args.integer("switch_gen", 3000)));
+  F_mu_h_constant dominance(static_cast<float>(args.num("h", 0.3)));
+  every_k sample(static_cast<int>(args.integer("sample_every", 500)), 0);
+  if (prev) {
+    a.sim_input_constants.init_mse = false;
+    a.sim_input_constants.prev_sim_sample = 0;
+    GO_Fish::run_sim(a, mutation, dem, mig, selection, inbreeding, dominance, bool_off(), sample, *prev);
+  } else {
+    GO_Fish::run_sim(a, mutation, dem, mig, selection, inbreeding, dominance, bool_off(), sample);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -261,11 +402,89 @@ inline void dadi_table(const Args& args, const char* path) {
   std::fclose(f);
 }
 
+// ---------------------------------------------------------------------------------------------
+// stored states: the final time sample of a run, written so that another run -- of either library --
+// can start from exactly that state through prev_sim.  Format (int32 little-endian words, float32
+// arrays): 'GFS1' P num_sites(float) generation M Nc[P] extinct[P] freq[P*M] ids[M*4]; the IDs are
+// stored raw, with the sign that marks a preserved mutation.
+// ---------------------------------------------------------------------------------------------
+inline void put(FILE* f, int32_t v);
+
+inline void save_state(GO_Fish::allele_trajectories& a, const char* path) {
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    std::perror(path);
+    std::exit(2);
+  }
+  const int P = a.sim_run_constants.num_populations;
+  const int s = a.num_samples - 1;
+  const int M = a.time_samples[s]->num_mutations;
+  std::fwrite("GFS1", 1, 4, f);
+  put(f, P);
+  const float L = a.sim_run_constants.num_sites;
+  std::fwrite(&L, sizeof(float), 1, f);
+  put(f, a.time_samples[s]->sampled_generation);
+  put(f, M);
+  for (int p = 0; p < P; ++p) put(f, a.time_samples[s]->Nchrom_e[p]);
+  for (int p = 0; p < P; ++p) put(f, a.time_samples[s]->extinct[p] ? 1 : 0);
+  if (M) std::fwrite(a.time_samples[s]->mutations_freq, sizeof(float), static_cast<size_t>(P) * M, f);
+  if (M) std::fwrite(a.mutations_ID, sizeof(GO_Fish::mutID), M, f);
+  std::fclose(f);
+}
+
+inline void load_state(GO_Fish::allele_trajectories& a, const char* path) {
+  FILE* f = std::fopen(path, "rb");
+  char magic[4];
+  int32_t P, gen, M;
+  float L;
+  if (!f || std::fread(magic, 1, 4, f) != 4 || std::memcmp(magic, "GFS1", 4) != 0 || std::fread(&P, 4, 1, f) != 1 ||
+      std::fread(&L, 4, 1, f) != 1 || std::fread(&gen, 4, 1, f) != 1 || std::fread(&M, 4, 1, f) != 1) {
+    std::fprintf(stderr, "load_state: cannot read %s\n", path);
+    std::exit(2);
+  }
+  a.sim_input_constants.num_populations = P;
+  a.sim_input_constants.num_sites = L;
+  a.initialize_sim_result_vector(1);
+  GO_Fish::allele_trajectories::time_sample* t = a.time_samples[0];
+  t->sampled_generation = gen;
+  t->num_mutations = M;
+  t->Nchrom_e = new int[P];
+  t->extinct = new bool[P];
+  t->mutations_freq = new float[static_cast<size_t>(P) * std::max(M, 1)];
+  std::vector<int32_t> w(2 * static_cast<size_t>(P));
+  bool ok = std::fread(w.data(), 4, w.size(), f) == w.size();
+  for (int p = 0; p < P; ++p) {
+    t->Nchrom_e[p] = w[p];
+    t->extinct[p] = w[P + p] != 0;
+  }
+  ok = ok && std::fread(t->mutations_freq, sizeof(float), static_cast<size_t>(P) * M, f) == static_cast<size_t>(P) * M;
+  a.mutations_ID = static_cast<GO_Fish::mutID*>(std::malloc(sizeof(GO_Fish::mutID) * std::max(M, 1)));
+  ok = ok && std::fread(a.mutations_ID, sizeof(GO_Fish::mutID), M, f) == static_cast<size_t>(M);
+  a.all_mutations = M;
+  std::fclose(f);
+  if (!ok) {
+    std::fprintf(stderr, "load_state: %s is truncated\n", path);
+    std::exit(2);
+  }
+}
+
+// Runs a scenario.  key=value options shared by every scenario: state_in=<path> continues from a
+// stored state (scenarios wf and multipop), state_out=<path> stores the run's final sample.  The
+// stored state is loaded into the result object itself, which is then passed as prev_sim too, as the
+// reference's example_compilation does: the reference accepts prev_sim_sample only below the sample
+// count of the object receiving the results (go_fish_impl.cuh:602), so a fresh result object could
+// not continue from another object's sample there.
 inline bool run_scenario(const std::string& name, GO_Fish::allele_trajectories& a, const Args& args) {
-  if (name == "wf") scenario_wf(a, args);
+  const std::string state_in = args.str("state_in", "");
+  if (!state_in.empty()) load_state(a, state_in.c_str());
+  const GO_Fish::allele_trajectories* start = state_in.empty() ? NULL : &a;
+  if (name == "wf") scenario_wf(a, args, start);
+  else if (name == "multipop") scenario_multipop(a, args, start);
   else if (name == "compilation") scenario_compilation(a, args);
   else if (name == "split3") scenario_split3(a, args);
   else return false;
+  const std::string state_out = args.str("state_out", "");
+  if (!state_out.empty()) save_state(a, state_out.c_str());
   return true;
 }
 
@@ -279,6 +498,11 @@ inline bool run_scenario(const std::string& name, GO_Fish::allele_trajectories& 
 inline void put(FILE* f, int32_t v) { std::fwrite(&v, sizeof(v), 1, f); }
 
 inline void dump_results(GO_Fish::allele_trajectories& a, const Args& args, const char* path) {
+  const std::string text = args.str("text", "");
+  if (!text.empty()) {  // the library's own text dump, operator<<(ostream&, allele_trajectories&)
+    std::ofstream out(text.c_str());
+    out << a;
+  }
   FILE* f = std::fopen(path, "wb");
   if (!f) {
     std::perror(path);

@@ -69,7 +69,6 @@ def test_selection_models_and_affine_coefficients(host_values):
     assert v["sel_pw99_slope"] == 0.0 and v["sel_pw99_intercept"] == v["sel_const_s"]
     assert v["sel_pw100_slope"] == v["sel_lin_slope"]
     assert v["sel_ps_p1"] == float(F32(0.02)) and v["sel_ps_p0"] == 0.0
-    assert v["sel_sine_slope"] == 0.0
     assert abs(v["sel_sine_g12"] - (0.01 * math.sin(0.1 * 12) + 0.001)) < 1e-7
 
 

@@ -143,6 +143,8 @@ def test_cfg1_neutral_matches_reference(gofish_driver, ref_driver, tmp_path):
     ["gamma=5", "h=0.3", "F=0.1", "mse=0", "gens=2000", "compact=10"],
     ["N=40", "mse=0", "gens=3000", "L=2e8"],
     ["pops=2", "m=0.01", "mse=1", "gens=500"],
+    # seasonal selection: the sine is evaluated on the device, as the reference's kernel evaluates it
+    ["sine_A=20", "sine_pi=0.05", "sine_rho=0.3", "gamma=-2", "mse=0", "gens=2000", "compact=25"],
 ])
 def test_wf_variants_match_reference(gofish_driver, ref_driver, tmp_path, extra):
     args = ["N=5000", "L=1e7", "sfs_n=50", "hist=1", "sample_every=0", *extra]
@@ -151,13 +153,102 @@ def test_wf_variants_match_reference(gofish_driver, ref_driver, tmp_path, extra)
     assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
 
 
+@pytest.mark.parametrize("extra", [
+    ["quad_a=-40", "gamma=2", "gens=2000", "compact=25"],
+    ["quad_a=30", "gamma=-3", "pops=2", "m=0.01", "gens=1500", "compact=20"],
+])
+def test_user_device_selection_functor_matches_reference(gofish_driver_nvcc, ref_driver, tmp_path, extra):
+    """A user selection functor that is not affine in frequency (s = a x^2 + b, a __device__ call
+    operator as the reference's functor contract asks): in a translation unit compiled by nvcc the
+    front-end instantiates its selection kernel for the functor and the engine reads the per-mutation
+    coefficients it writes, so the run is bit-exact against the reference, with and without migration."""
+    args = ["N=5000", "L=1e7", "sfs_n=50", "hist=1", "sample_every=0", "mse=0", *extra]
+    mine = run_driver(gofish_driver_nvcc, "wf", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *args], check=True, capture_output=True)
+    ref = Dump(tmp_path / "ref.bin")
+    assert ref.samples[-1]["M"] > 1000
+    assert_dumps_equal(mine, ref)
+
+
+def test_user_selection_functor_limits(gofish_driver, gofish_driver_nvcc, tmp_path):
+    """Where the device path is not available the front-end says so: a plain C++ translation unit can
+    only use selection models that are affine in frequency, and the equilibrium start integrates an
+    affine model at generation 0."""
+    args = ["N=2000", "L=1e6", "gens=10", "quad_a=-40", "gamma=2"]
+    r = subprocess.run([str(gofish_driver), "wf", str(tmp_path / "a.bin"), *args, "mse=0"], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "not affine in frequency" in r.stderr
+    r = subprocess.run([str(gofish_driver_nvcc), "wf", str(tmp_path / "b.bin"), *args, "mse=1"], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "affine in frequency at generation 0" in r.stderr
+
+
 def test_resume_and_preserve_match_reference(gofish_driver, ref_driver, tmp_path):
-    """Two inbred populations: blank start, burn-in, resume from the burn-in sample, sampling the start."""
+    """Two inbred populations: blank start, burn-in, resume from the burn-in sample, sampling the start.
+    The text dump of operator<< (inline_go_fish_data_struct.hpp:208-267) must be byte-identical too."""
     args = ["gens1=3000", "gens2=500", "L=2e7", "sfs_n=20", "hist=1"]
-    mine = run_driver(gofish_driver, "compilation", tmp_path / "mine.bin", args)
-    subprocess.run([str(ref_driver), "sim", "compilation", str(tmp_path / "ref.bin"), *args], check=True,
-                   capture_output=True)
+    mine = run_driver(gofish_driver, "compilation", tmp_path / "mine.bin", [*args, f"text={tmp_path / 'mine.txt'}"])
+    subprocess.run([str(ref_driver), "sim", "compilation", str(tmp_path / "ref.bin"), *args,
+                    f"text={tmp_path / 'ref.txt'}"], check=True, capture_output=True)
     assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
+    ref_text = (tmp_path / "ref.txt").read_bytes()
+    assert ref_text.count(b"\n") > 100
+    assert (tmp_path / "mine.txt").read_bytes() == ref_text
+
+
+# The benchmarked single-population workload: one half of N = 2e5 diploids (Nchrom_e 4e5), L = 2.5e8,
+# compaction every 25 generations, SFS of a sample of 1000 and the full population histogram.  About
+# 2.7 M segregating mutations at the start and 2e5 new ones every generation, so the quad/tail split,
+# capacity growth and the mix of Poisson and normal draws are the ones the benchmark exercises.
+CFG2_HALF = ["N=200000", "L=2.5e8", "gens=300", "compact=25", "sfs_n=1000", "hist=1", "sample_every=0"]
+
+
+def test_cfg2_neutral_half_matches_reference(gofish_driver, ref_driver, tmp_path):
+    """The neutral half of the benchmark from its mutation-selection-equilibrium start (deterministic in
+    the reference when s = 0), 300 generations."""
+    args = [*CFG2_HALF, "mse=1"]
+    mine = run_driver(gofish_driver, "wf", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *args], check=True, capture_output=True)
+    ref = Dump(tmp_path / "ref.bin")
+    assert ref.samples[-1]["M"] > 2_000_000
+    assert_dumps_equal(mine, ref)
+
+
+def test_cfg2_selected_half_matches_reference(gofish_driver, ref_driver, tmp_path):
+    """The gamma = -10, h = 0.5 half of the benchmark.  The reference's equilibrium start with selection
+    sums floats in a nondeterministic order (a CUB scan, go_fish_impl.cu:13-32), so both programs
+    continue from one stored reference state: the reference's own equilibrium start run for 25
+    generations, then 300 generations in each program from that state (prev_sim, init_mse = false)."""
+    start = tmp_path / "start.bin"
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "stage1.bin"), *CFG2_HALF, "gens=25", "mse=1",
+                    "gamma=-10", "h=0.5", f"state_out={start}"], check=True, capture_output=True)
+    args = [*CFG2_HALF, "gamma=-10", "h=0.5", f"state_in={start}"]
+    mine = run_driver(gofish_driver, "wf", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *args], check=True, capture_output=True)
+    ref = Dump(tmp_path / "ref.bin")
+    assert ref.samples[-1]["generation"] == 325 and ref.samples[-1]["M"] > 1_000_000
+    assert_dumps_equal(mine, ref)
+
+
+def test_multipop_after_the_split_matches_reference(gofish_driver, ref_driver, tmp_path):
+    """The benchmarked three-population model (scenario multipop): growth to the caps, migration 1e-4,
+    F = 0.1 in population 2, L = 2e8, a time sample every 500 generations, through the switch from
+    gamma -5 to +2 at generation 3000.  Before population 2 is founded (generation 2000) the reference
+    never writes its rows, which then hold whatever its fresh device allocations held, and its migration
+    sum multiplies them by a zero rate (go_fish_impl.cuh:98-102, 651-656), so the reference is only well
+    defined once every population exists.  Both programs therefore continue from one stored state at
+    generation 2100, written by this library, for 1000 generations."""
+    start = tmp_path / "start.bin"
+    run_driver(gofish_driver, "multipop", tmp_path / "stage1.bin", ["gens=2100", "sample_every=0",
+                                                                    f"state_out={start}"])
+    args = ["gens=1000", "sample_every=500", "sfs_n=200", "hist=1", f"state_in={start}"]
+    mine = run_driver(gofish_driver, "multipop", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "multipop", str(tmp_path / "ref.bin"), *args], check=True,
+                   capture_output=True)
+    ref = Dump(tmp_path / "ref.bin")
+    assert [s["generation"] for s in ref.samples] == [2500, 3000, 3100]
+    assert ref.samples[-1]["M"] > 1_000_000 and (ref.samples[-1]["Nc"] > 0).all()
+    assert_dumps_equal(mine, ref)
 
 
 def test_split3_matches_reference(gofish_driver, ref_driver, tmp_path):
