@@ -576,10 +576,12 @@ def run_surrogate(args):
     cached = None
     if args.data_cache and os.path.exists(args.data_cache):
         cached = np.load(args.data_cache)
-        if len(cached["ptrain"]) != args.train_draws or len(cached["peval"]) != args.eval_draws:
+        if (len(cached["ptrain"]) != args.train_draws or len(cached["peval"]) != args.eval_draws
+                or "ref_var" not in cached):
             cached = None
     if cached is not None:
         ptrain, train_sfs, peval, ref = cached["ptrain"], cached["train_sfs"], cached["peval"], cached["ref"]
+        ref_var = cached["ref_var"]
         t_data = float(cached["t_data"]) if "t_data" in cached else None
     else:
         t0 = time.perf_counter()
@@ -588,9 +590,11 @@ def run_surrogate(args):
         eng.synchronize()
         t_data = time.perf_counter() - t0
         peval = sg.draw_parameters(args.eval_draws, seed=202)
-        ref = sg.simulate_spectra(eng, peval, reps=64, seed=1 << 28)        # reference spectra: 64-replicate means
+        # reference spectra: 64-replicate means, with their per-bin variance
+        ref, ref_var = sg.simulate_spectra(eng, peval, reps=64, seed=1 << 28, with_variance=True)
         if args.data_cache:
-            np.savez(args.data_cache, ptrain=ptrain, train_sfs=train_sfs, peval=peval, ref=ref, t_data=t_data)
+            np.savez(args.data_cache, ptrain=ptrain, train_sfs=train_sfs.astype(np.float32), peval=peval,
+                     ref=ref, ref_var=ref_var, t_data=t_data)
     # simulator throughput on the training distribution: 512 draws x 16 replicates, timed on its own
     # (after one untimed run, which sizes the engine's buffers)
     sg.simulate_spectra(eng, ptrain[:512], reps=16, seed=(1 << 29) + 3)
@@ -612,6 +616,10 @@ def run_surrogate(args):
     surr = sg.Surrogate(mlp, eng, scale=scale)
     pred = surr.predict(peval)
     err, used = sg.median_relative_error(pred, ref)
+    report = sg.error_report(pred, ref, ref_var, reps=64)
+    # queries from the batched workload's distribution (N0 up to 1e5): the share the network answers
+    queries = sg.draw_query_parameters(65536, seed=505)
+    coverage = float(sg.in_support(queries).mean())
     # the simulator's own error with k replicates per query (k = 16 from independent seeds; fewer from
     # subsets of them are not available without rerunning, so k < 16 are simulated separately)
     sim_err = {16: sg.median_relative_error(indep / indep.sum(axis=1, keepdims=True), ref)[0]}
@@ -660,12 +668,15 @@ def run_surrogate(args):
         "metric": "SFS queries/s (surrogate)", "value": q_per_s, "unit": "queries/s", "n_gpus": 1,
         "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (batched simulator)",
         "config": {"workload": "6->512x4->99 GELU MLP, per-bin standardised log-spectrum targets; train " f"{args.train_draws} draws x 16 replicates, "
-                               f"eval {args.eval_draws} draws x 64 replicates; support: logN [log 500, log 2000], "
-                               "gamma [-100, 10], h [0, 1], F [0, 0.5], r [-0.001, 0.01], T [0.05, 1]; "
+                               f"eval {args.eval_draws} draws x 64 replicates; support: logN [log 1e3, log 1e4], "
+                               "gamma [-100, 10], h [0, 1], F [0, 0.5], r [-0.001, 0.01], T [0.05, 2]; "
                                f"theta {sg.THETA:g}, L {sg.NUM_SITES:g}, n 100",
                    "train_steps": args.train_steps, "batch": args.batch, "lr": args.lr,
                    "weight_decay": args.weight_decay, "inference_batch": B},
-        "median_rel_error": err, "bins_used": used,
+        "median_rel_error": err, "bins_used": used, "error": report,
+        "queries_in_support": coverage,
+        "queries_routed_to_simulator": 1.0 - coverage,
+        "query_distribution": "log N0 U[log 1e3, log 1e5], the other parameters over the support",
         "simulator_median_rel_error": {str(k): v for k, v in sim_err.items()},
         "matched_replicates": k_match,
         "simulator_sims_per_s": sims_per_s,
@@ -896,7 +907,7 @@ def main():
                          "surrogate: the SFS surrogate network against the simulator")
     ap.add_argument("--mp-gens", type=int, default=MP_GENS, help="multipop workload: generations per run")
     ap.add_argument("--train-draws", type=int, default=65536)
-    ap.add_argument("--eval-draws", type=int, default=1024)
+    ap.add_argument("--eval-draws", type=int, default=4096)
     ap.add_argument("--train-steps", type=int, default=120000)
     ap.add_argument("--infer-only", action="store_true",
                     help="surrogate workload: time forward passes of batches of 32768 queries only")

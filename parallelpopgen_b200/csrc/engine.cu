@@ -969,6 +969,9 @@ static gf_status launch_window(Engine* e, int b, int first, int count, const Gen
   w.any_compact = R.compact != 0;
   w.stats = e->d_stats;
   w.fault = e->d_count + 2;
+  w.uniform_key = true;
+  w.seed1 = e->seed1;
+  w.seed2 = e->seed2;
   // profiling: the window kernel's time counts as drift, its segmented scan and scatter as compaction
   cudaEvent_t ev0 = nullptr, evw = nullptr, evc = nullptr, ev1 = nullptr;
   if (e->profiling) {

@@ -14,9 +14,9 @@
 #ifndef GF_WINDOW_MIN_BLOCKS
 #define GF_WINDOW_MIN_BLOCKS GF_DRIFT_MIN_BLOCKS
 #endif
-// 1: the window kernel stages a window's generation records in shared memory.
-#ifndef GF_WIN_STAGE_RECORDS
-#define GF_WIN_STAGE_RECORDS 1
+// 1: a single-replicate window launch takes its Philox round keys from the kernel parameters.
+#ifndef GF_WINDOW_UNIFORM_KEYS
+#define GF_WINDOW_UNIFORM_KEYS 1
 #endif
 // 1: the lane-order draw schedule walks a quad's lanes in a rolled loop (one inlined copy of the
 // sampler instead of four); 0: the loop is unrolled.

@@ -106,6 +106,10 @@ struct WindowLaunch {
   bool any_compact;
   unsigned long long* stats;
   int* fault;
+  // one replicate (the plain engine): its seeds, from which the launch passes the Philox round keys
+  // as kernel parameters
+  bool uniform_key = false;
+  int seed1 = 0, seed2 = 0;
 };
 
 // Longest window (generations per window launch).

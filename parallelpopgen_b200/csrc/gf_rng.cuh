@@ -35,8 +35,18 @@ constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;  // sqrt(3) - 1
 constexpr float kMeanBoundary = 6.0f;
 constexpr float kBinomNBoundary = 100.0f;
 
+// 1: the 32x32->64 multiply is written as one 64-bit product (a single wide multiply on the
+// device); 0: low and high halves as two multiplies.  Both give the same bits.
+#ifndef GF_PHILOX_WIDE
+#define GF_PHILOX_WIDE 0
+#endif
+
 __host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
-#ifdef __CUDA_ARCH__
+#if defined(__CUDA_ARCH__) && GF_PHILOX_WIDE
+  const uint64_t p = static_cast<uint64_t>(a) * b;
+  lo = static_cast<uint32_t>(p);
+  hi = static_cast<uint32_t>(p >> 32);
+#elif defined(__CUDA_ARCH__)
   lo = a * b;
   hi = __umulhi(a, b);
 #else
@@ -58,6 +68,40 @@ __host__ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, ui
     mulhilo32(kPhiloxM0, c.x, hi0, lo0);
     mulhilo32(kPhiloxM1, c.z, hi1, lo1);
     c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+  }
+  return c;
+}
+
+// The ten round keys of one key (seed1, seed2), for kernels whose key is the same for every thread:
+// passed by value as a kernel parameter they sit in the constant bank, so a round's key costs no
+// instruction.
+struct PhiloxKeys {
+  uint32_t k0[10];
+  uint32_t k1[10];
+};
+
+__host__ __device__ __forceinline__ PhiloxKeys philox_round_keys(int seed1, int seed2) {
+  PhiloxKeys K;
+  uint32_t k0 = static_cast<uint32_t>(seed1), k1 = static_cast<uint32_t>(seed2);
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += kPhiloxW0;
+      k1 += kPhiloxW1;
+    }
+    K.k0[r] = k0;
+    K.k1[r] = k1;
+  }
+  return K;
+}
+
+// philox4x32_10 with precomputed round keys (the same bijection).
+__host__ __device__ __forceinline__ uint4 philox4x32_10_keys(uint4 c, const PhiloxKeys& K) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(kPhiloxM0, c.x, hi0, lo0);
+    mulhilo32(kPhiloxM1, c.z, hi1, lo1);
+    c = make_uint4(hi1 ^ c.y ^ K.k0[r], lo1, hi0 ^ c.w ^ K.k1[r], lo0);
   }
   return c;
 }
@@ -85,68 +129,40 @@ __host__ __device__ __forceinline__ float u01(uint32_t bits) {
     if (cdf >= r || ((CAP_MEAN) > 0 && mean <= (CAP_MEAN))) return J; \
   }
 
-// Poisson inverse CDF by sequential search (poiscdfinv, shared.cuh:168-249), all 70 steps.
-static __host__ __device__ __noinline__ int pois_search_full(float r, float mean) {
-  float emu = expf(-1 * mean);
-  float cdf = emu;
-  if (cdf >= r) return 0;
-#define GF_ITER(JF)          \
-  {                          \
-    emu *= mean / (JF);      \
-    cdf += emu;              \
-  }
-  GF_SEARCH_STEP(1, 0) GF_SEARCH_STEP(2, 0) GF_SEARCH_STEP(3, 0) GF_SEARCH_STEP(4, 0)
-  GF_SEARCH_STEP(5, 0) GF_SEARCH_STEP(6, 0) GF_SEARCH_STEP(7, 0) GF_SEARCH_STEP(8, 0)
-  GF_SEARCH_STEP(9, 0) GF_SEARCH_STEP(10, 0) GF_SEARCH_STEP(11, 1) GF_SEARCH_STEP(12, 0)
-  GF_SEARCH_STEP(13, 0) GF_SEARCH_STEP(14, 2) GF_SEARCH_STEP(15, 0) GF_SEARCH_STEP(16, 0)
-  GF_SEARCH_STEP(17, 3) GF_SEARCH_STEP(18, 0) GF_SEARCH_STEP(19, 0) GF_SEARCH_STEP(20, 4)
-  GF_SEARCH_STEP(21, 0) GF_SEARCH_STEP(22, 5) GF_SEARCH_STEP(23, 0) GF_SEARCH_STEP(24, 6)
-  GF_SEARCH_STEP(25, 0) GF_SEARCH_STEP(26, 7) GF_SEARCH_STEP(27, 0) GF_SEARCH_STEP(28, 8)
-  GF_SEARCH_STEP(29, 0) GF_SEARCH_STEP(30, 9) GF_SEARCH_STEP(31, 0) GF_SEARCH_STEP(32, 10)
-  GF_SEARCH_STEP(33, 0) GF_SEARCH_STEP(34, 11) GF_SEARCH_STEP(35, 0) GF_SEARCH_STEP(36, 12)
-  GF_SEARCH_STEP(37, 0) GF_SEARCH_STEP(38, 13) GF_SEARCH_STEP(39, 0) GF_SEARCH_STEP(40, 14)
-  GF_SEARCH_STEP(41, 15) GF_SEARCH_STEP(42, 0) GF_SEARCH_STEP(43, 16) GF_SEARCH_STEP(44, 0)
-  GF_SEARCH_STEP(45, 17) GF_SEARCH_STEP(46, 18) GF_SEARCH_STEP(47, 0) GF_SEARCH_STEP(48, 19)
-  GF_SEARCH_STEP(49, 0) GF_SEARCH_STEP(50, 20) GF_SEARCH_STEP(51, 21) GF_SEARCH_STEP(52, 0)
-  GF_SEARCH_STEP(53, 22) GF_SEARCH_STEP(54, 0) GF_SEARCH_STEP(55, 23) GF_SEARCH_STEP(56, 24)
-  GF_SEARCH_STEP(57, 0) GF_SEARCH_STEP(58, 25) GF_SEARCH_STEP(59, 26) GF_SEARCH_STEP(60, 0)
-  GF_SEARCH_STEP(61, 27) GF_SEARCH_STEP(62, 28) GF_SEARCH_STEP(63, 0) GF_SEARCH_STEP(64, 29)
-  GF_SEARCH_STEP(65, 30) GF_SEARCH_STEP(66, 0) GF_SEARCH_STEP(67, 31) GF_SEARCH_STEP(68, 32)
-  GF_SEARCH_STEP(69, 0)
-#undef GF_ITER
-  return 70;
-}
-
-// The same search for mean <= 6, the case every sampler branch reaches it with: step 24's cap exit
-// (`|| mean <= 6`) then always returns 24, so the steps after it never run and are left out.  The
-// result equals pois_search_full's for every such mean; the shorter body keeps the inlined sampler
-// small (instruction-cache footprint of the drift kernels).
-__host__ __device__ __forceinline__ int pois_search_upto6(float r, float mean) {
-  float emu = expf(-1 * mean);
-  float cdf = emu;
-  if (cdf >= r) return 0;
-#define GF_ITER(JF)          \
-  {                          \
-    emu *= mean / (JF);      \
-    cdf += emu;              \
-  }
-  GF_SEARCH_STEP(1, 0) GF_SEARCH_STEP(2, 0) GF_SEARCH_STEP(3, 0) GF_SEARCH_STEP(4, 0)
-  GF_SEARCH_STEP(5, 0) GF_SEARCH_STEP(6, 0) GF_SEARCH_STEP(7, 0) GF_SEARCH_STEP(8, 0)
-  GF_SEARCH_STEP(9, 0) GF_SEARCH_STEP(10, 0) GF_SEARCH_STEP(11, 1) GF_SEARCH_STEP(12, 0)
-  GF_SEARCH_STEP(13, 0) GF_SEARCH_STEP(14, 2) GF_SEARCH_STEP(15, 0) GF_SEARCH_STEP(16, 0)
-  GF_SEARCH_STEP(17, 3) GF_SEARCH_STEP(18, 0) GF_SEARCH_STEP(19, 0) GF_SEARCH_STEP(20, 4)
-  GF_SEARCH_STEP(21, 0) GF_SEARCH_STEP(22, 5) GF_SEARCH_STEP(23, 0)
-#undef GF_ITER
-  return 24;
-}
-
+// Poisson inverse CDF by sequential search (poiscdfinv, shared.cuh:168-249).
 __host__ __device__ __forceinline__ int pois_search(float r, float mean) {
-  if (mean <= kMeanBoundary) return pois_search_upto6(r, mean);
-  return pois_search_full(r, mean);
+  float emu = expf(-1 * mean);
+  float cdf = emu;
+  if (cdf >= r) return 0;
+#define GF_ITER(JF)          \
+  {                          \
+    emu *= mean / (JF);      \
+    cdf += emu;              \
+  }
+  GF_SEARCH_STEP(1, 0) GF_SEARCH_STEP(2, 0) GF_SEARCH_STEP(3, 0) GF_SEARCH_STEP(4, 0)
+  GF_SEARCH_STEP(5, 0) GF_SEARCH_STEP(6, 0) GF_SEARCH_STEP(7, 0) GF_SEARCH_STEP(8, 0)
+  GF_SEARCH_STEP(9, 0) GF_SEARCH_STEP(10, 0) GF_SEARCH_STEP(11, 1) GF_SEARCH_STEP(12, 0)
+  GF_SEARCH_STEP(13, 0) GF_SEARCH_STEP(14, 2) GF_SEARCH_STEP(15, 0) GF_SEARCH_STEP(16, 0)
+  GF_SEARCH_STEP(17, 3) GF_SEARCH_STEP(18, 0) GF_SEARCH_STEP(19, 0) GF_SEARCH_STEP(20, 4)
+  GF_SEARCH_STEP(21, 0) GF_SEARCH_STEP(22, 5) GF_SEARCH_STEP(23, 0) GF_SEARCH_STEP(24, 6)
+  GF_SEARCH_STEP(25, 0) GF_SEARCH_STEP(26, 7) GF_SEARCH_STEP(27, 0) GF_SEARCH_STEP(28, 8)
+  GF_SEARCH_STEP(29, 0) GF_SEARCH_STEP(30, 9) GF_SEARCH_STEP(31, 0) GF_SEARCH_STEP(32, 10)
+  GF_SEARCH_STEP(33, 0) GF_SEARCH_STEP(34, 11) GF_SEARCH_STEP(35, 0) GF_SEARCH_STEP(36, 12)
+  GF_SEARCH_STEP(37, 0) GF_SEARCH_STEP(38, 13) GF_SEARCH_STEP(39, 0) GF_SEARCH_STEP(40, 14)
+  GF_SEARCH_STEP(41, 15) GF_SEARCH_STEP(42, 0) GF_SEARCH_STEP(43, 16) GF_SEARCH_STEP(44, 0)
+  GF_SEARCH_STEP(45, 17) GF_SEARCH_STEP(46, 18) GF_SEARCH_STEP(47, 0) GF_SEARCH_STEP(48, 19)
+  GF_SEARCH_STEP(49, 0) GF_SEARCH_STEP(50, 20) GF_SEARCH_STEP(51, 21) GF_SEARCH_STEP(52, 0)
+  GF_SEARCH_STEP(53, 22) GF_SEARCH_STEP(54, 0) GF_SEARCH_STEP(55, 23) GF_SEARCH_STEP(56, 24)
+  GF_SEARCH_STEP(57, 0) GF_SEARCH_STEP(58, 25) GF_SEARCH_STEP(59, 26) GF_SEARCH_STEP(60, 0)
+  GF_SEARCH_STEP(61, 27) GF_SEARCH_STEP(62, 28) GF_SEARCH_STEP(63, 0) GF_SEARCH_STEP(64, 29)
+  GF_SEARCH_STEP(65, 30) GF_SEARCH_STEP(66, 0) GF_SEARCH_STEP(67, 31) GF_SEARCH_STEP(68, 32)
+  GF_SEARCH_STEP(69, 0)
+#undef GF_ITER
+  return 70;
 }
 
-// Binomial inverse CDF by sequential search (binomcdfinv, shared.cuh:84-166); x = p, n = N; all 70 steps.
-static __host__ __device__ __noinline__ int binom_search_full(float r, float mean, float x, float n) {
+// Binomial inverse CDF by sequential search (binomcdfinv, shared.cuh:84-166); x = p, n = N.
+__host__ __device__ __forceinline__ int binom_search(float r, float mean, float x, float n) {
   float emu = powf(1 - x, n);
   if (emu == 1) emu = expf(-1 * mean);
   float cdf = emu;
@@ -176,32 +192,6 @@ static __host__ __device__ __noinline__ int binom_search_full(float r, float mea
   GF_SEARCH_STEP(69, 0)
 #undef GF_ITER
   return 70;
-}
-
-// The same search for mean <= 6 (see pois_search_upto6).
-__host__ __device__ __forceinline__ int binom_search_upto6(float r, float mean, float x, float n) {
-  float emu = powf(1 - x, n);
-  if (emu == 1) emu = expf(-1 * mean);
-  float cdf = emu;
-  if (cdf >= r) return 0;
-#define GF_ITER(JF)                                       \
-  {                                                       \
-    emu *= ((n + 1.f - (JF)) * x) / ((JF) * (1 - x));     \
-    cdf += emu;                                           \
-  }
-  GF_SEARCH_STEP(1, 0) GF_SEARCH_STEP(2, 0) GF_SEARCH_STEP(3, 0) GF_SEARCH_STEP(4, 0)
-  GF_SEARCH_STEP(5, 0) GF_SEARCH_STEP(6, 0) GF_SEARCH_STEP(7, 0) GF_SEARCH_STEP(8, 0)
-  GF_SEARCH_STEP(9, 0) GF_SEARCH_STEP(10, 0) GF_SEARCH_STEP(11, 1) GF_SEARCH_STEP(12, 0)
-  GF_SEARCH_STEP(13, 0) GF_SEARCH_STEP(14, 2) GF_SEARCH_STEP(15, 0) GF_SEARCH_STEP(16, 0)
-  GF_SEARCH_STEP(17, 3) GF_SEARCH_STEP(18, 0) GF_SEARCH_STEP(19, 0) GF_SEARCH_STEP(20, 4)
-  GF_SEARCH_STEP(21, 0) GF_SEARCH_STEP(22, 5) GF_SEARCH_STEP(23, 0)
-#undef GF_ITER
-  return 24;
-}
-
-__host__ __device__ __forceinline__ int binom_search(float r, float mean, float x, float n) {
-  if (mean <= kMeanBoundary) return binom_search_upto6(r, mean, x, n);
-  return binom_search_full(r, mean, x, n);
 }
 #undef GF_SEARCH_STEP
 

@@ -109,25 +109,21 @@ __global__ void __launch_bounds__(1024) batch_tiles_kernel(WinRep* __restrict__ 
   if (threadIdx.x == 0) *total = s_carry;
 }
 
-// DRAW: how a warp schedules its sampler draws (DrawStrategy).
-template <int DRAW>
+// DRAW: how a warp schedules its sampler draws (DrawStrategy).  KEYS: every replicate of the launch
+// has the seeds whose round keys `keys` holds (a plain-engine launch), so the quads' Philox blocks take
+// their round keys from the kernel parameters instead of deriving them from the replicate's seeds.
+template <int DRAW, bool KEYS>
 __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     window_kernel(const float* __restrict__ A, float* __restrict__ B, int* __restrict__ id_gp,
                   int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
                   const WinRep* __restrict__ reps, int nreps, const WinGen* __restrict__ recs, int total_tiles,
                   const int* __restrict__ total_dev, unsigned long long* __restrict__ stats,
-                  int* __restrict__ fault) {
+                  int* __restrict__ fault, const PhiloxKeys keys) {
   __shared__ int s_rep;
   __shared__ unsigned s_warp[kWinThreads / 32];
   __shared__ int s_tile0[kRepCache];
   __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinThreads / 32 : 1];
-#if GF_WIN_STAGE_RECORDS
-  // the generation records of the replicate whose tile the block works on (every thread reads every
-  // record of the window; staged once per replicate instead of read from global memory per thread)
-  __shared__ WinGen s_rec[kMaxWindowGenerations];
-  int staged = -1;  // replicate whose records s_rec holds (block-uniform)
-#endif
   const int lane = threadIdx.x & 31;
   WarpDraws* wd = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
@@ -136,17 +132,6 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     if (threadIdx.x == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
     __syncthreads();
     const WinRep R = reps[s_rep];
-#if GF_WIN_STAGE_RECORDS
-    // every thread has finished the previous tile (the barrier above), so s_rec may be refilled
-    const int nstage = min(R.ngen, kMaxWindowGenerations);
-    if (s_rep != staged) {
-      const int* src = reinterpret_cast<const int*>(recs + R.rec);
-      int* dst = reinterpret_cast<int*>(s_rec);
-      const int words = nstage * static_cast<int>(sizeof(WinGen) / 4);
-      for (int i = threadIdx.x; i < words; i += kWinThreads) dst[i] = src[i];
-      staged = s_rep;
-    }
-#endif
     __syncthreads();
     const int t = gt - R.tile0;
     const int q = t * kWinThreads + threadIdx.x;  // quad within the replicate
@@ -173,11 +158,7 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     int alive = 1;
 #pragma unroll 1
     for (int k = 0; k < R.ngen; ++k) {
-#if GF_WIN_STAGE_RECORDS
-      const WinGen G = k < nstage ? s_rec[k] : recs[R.rec + k];
-#else
       const WinGen G = recs[R.rec + k];
-#endif
       const int N = G.Nc;
       const int g = G.generation;
       alive = G.alive;
@@ -206,7 +187,10 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
           }
         }
         uint4 r = make_uint4(0u, 0u, 0u, 0u);
-        if (need) r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
+        if (need) {
+          if (KEYS) r = philox4x32_10_keys(make_uint4(static_cast<uint32_t>(q + 2), static_cast<uint32_t>(g), 0u, 0u), keys);
+          else r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
+        }
         if (DRAW == kDrawWarp) {
           draw_quad<kDrawWarp>(xs, r, need, N, lane, wd, res);
         } else if (need) {
@@ -475,12 +459,14 @@ void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, c
   e->kernel_launches += 1;
 }
 
-template <int DRAW>
+template <int DRAW, bool KEYS>
 static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
-  // resident blocks per SM, queried once per strategy (thread-safe initialisation; the same on every B200)
+  // resident blocks per SM, queried once per instantiation (thread-safe initialisation; the same on
+  // every B200)
   static const int occupancy = [] {
     int o = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel<DRAW>, kWinThreads, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel<DRAW, KEYS>, kWinThreads, 0) !=
+            cudaSuccess ||
         o < 1) {
       cudaGetLastError();
       o = 1;
@@ -489,9 +475,10 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
   }();
   const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
   const int blocks = std::max(1, std::min(w.total_tiles, e->num_sms * per_sm));
-  window_kernel<DRAW><<<blocks, kWinThreads, 0, e->stream>>>(
+  const PhiloxKeys keys = philox_round_keys(w.seed1, w.seed2);
+  window_kernel<DRAW, KEYS><<<blocks, kWinThreads, 0, e->stream>>>(
       w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count, w.M_in, w.M_end, w.M_next, w.reps, w.nreps,
-      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault);
+      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault, keys);
 }
 
 // Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
@@ -499,10 +486,13 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaEvent_t after_window,
                      cudaEvent_t before_compaction) {
   switch (e->draw_strategy) {
-    case kDrawWarp: launch_window_kernel<kDrawWarp>(e, w); break;
-    case kDrawGrouped: launch_window_kernel<kDrawGrouped>(e, w); break;
-    case kDrawNormalAll: launch_window_kernel<kDrawNormalAll>(e, w); break;
-    default: launch_window_kernel<kDrawLanes>(e, w); break;
+    case kDrawWarp: launch_window_kernel<kDrawWarp, false>(e, w); break;
+    case kDrawGrouped: launch_window_kernel<kDrawGrouped, false>(e, w); break;
+    case kDrawNormalAll: launch_window_kernel<kDrawNormalAll, false>(e, w); break;
+    default:
+      if (GF_WINDOW_UNIFORM_KEYS && w.uniform_key && w.nreps == 1) launch_window_kernel<kDrawLanes, true>(e, w);
+      else launch_window_kernel<kDrawLanes, false>(e, w);
+      break;
   }
   GF_CUDA(e, cudaGetLastError());
   e->kernel_launches += 1;

@@ -8,10 +8,12 @@ calls on the parameter family below; `simulate_spectra` is the simulator side (t
 whose replicates equal plain GO_Fish runs bit for bit).
 
 Parameter family (one population, MSE start at N0, then exponential growth for T*2*N0 generations):
-    log N0 in [log 500, log 2000]     gamma = 2 N s (selection_constant semantics) in [-100, 10]
+    log N0 in [log 1e3, log 1e4]      gamma = 2 N s (selection_constant semantics) in [-100, 10]
     h in [0, 1]                        F in [0, 0.5]
-    r in [-0.001, 0.01] per generation, N clamped to [N0/10, 10 N0]      T in [0.05, 1]
+    r in [-0.001, 0.01] per generation, N clamped to [N0/10, 10 N0]      T in [0.05, 2]
 theta = 4 N0 mu L is held at THETA (mu = THETA / (4 N0 L)), so spectra differ only through the shape.
+T = 2 is the batched replicates' run length (4 N0 generations); queries with N0 in (1e4, 1e5] (the
+upper half of that workload's range) are outside the support and go to the simulator.
 """
 from __future__ import annotations
 
@@ -35,12 +37,12 @@ GAMMA_SCALE = 5.0         # gamma enters the network as asinh(gamma / GAMMA_SCAL
 
 # name, low, high (inputs are scaled to [-1, 1] over these ranges)
 SUPPORT = (
-    ("logN", math.log(500.0), math.log(2000.0)),
+    ("logN", math.log(1e3), math.log(1e4)),
     ("gamma", -100.0, 10.0),
     ("h", 0.0, 1.0),
     ("F", 0.0, 0.5),
     ("r", -0.001, 0.01),
-    ("T", 0.05, 1.0),
+    ("T", 0.05, 2.0),
 )
 LOW = np.array([s[1] for s in SUPPORT])
 HIGH = np.array([s[2] for s in SUPPORT])
@@ -153,6 +155,16 @@ def in_support(params: np.ndarray) -> np.ndarray:
     return np.all((params >= LOW) & (params <= HIGH), axis=1)
 
 
+def draw_query_parameters(count: int, seed: int) -> np.ndarray:
+    """Queries from the batched-replicate workload's distribution: log N0 uniform in [log 1e3, log 1e5],
+    gamma, h, F, r as the support, T uniform over the support's range.  About half fall in the support
+    (N0 <= 1e4)."""
+    p = draw_parameters(count, seed)
+    rng = np.random.default_rng(seed + 0x9E3779B9)
+    p[:, 0] = rng.uniform(math.log(1e3), math.log(1e5), size=count)
+    return p
+
+
 def encode(params: np.ndarray) -> np.ndarray:
     """Network inputs: every parameter scaled linearly to [-1, 1] over the support, except gamma, which
     is scaled through asinh(gamma / 5) (the spectrum's dependence on strong selection is close to
@@ -175,11 +187,17 @@ def replicate_for(p: np.ndarray, seed1: int, seed2: int, compact_interval: int =
 
 
 def simulate_spectra(engine: Engine, params: np.ndarray, reps: int, seed: int, chunk: int = 8192,
-                     compact_interval: int = 25) -> np.ndarray:
+                     compact_interval: int = 25, with_variance: bool = False):
     """Mean SFS (bins 1..99, expected site counts) over `reps` replicates per parameter row, from the
-    batched engine.  Replicate k of row i uses seeds (seed + 2(i reps + k), seed + 2(i reps + k) + 1)."""
+    batched engine.  Replicate k of row i uses seeds (seed + 2(i reps + k), seed + 2(i reps + k) + 1).
+    Replicates are grouped into batches of similar length (generations), so that a batch does not wait
+    on a few long replicates; the result does not depend on the grouping.  with_variance: also return
+    the per-bin variance over the replicates (ddof = 1)."""
     out = np.zeros((len(params), OUTPUTS), np.float64)
-    jobs = [(i, k) for i in range(len(params)) for k in range(reps)]
+    sq = np.zeros((len(params), OUTPUTS), np.float64)
+    gens = np.exp(params[:, 0]) * params[:, 5]
+    order = np.argsort(gens, kind="stable")
+    jobs = [(int(i), k) for i in order for k in range(reps)]
     for c0 in range(0, len(jobs), chunk):
         part = jobs[c0:c0 + chunk]
         recs = []
@@ -190,8 +208,14 @@ def simulate_spectra(engine: Engine, params: np.ndarray, reps: int, seed: int, c
         engine.batch_run()
         sfs = engine.batch_sfs(N_SAMPLE, len(recs))
         for (i, _), row in zip(part, sfs):
-            out[i] += row[1:N_SAMPLE]
-    return out / reps
+            v = row[1:N_SAMPLE].astype(np.float64)
+            out[i] += v
+            sq[i] += v * v
+    mean = out / reps
+    if not with_variance:
+        return mean
+    var = np.maximum(sq - reps * mean * mean, 0.0) / max(reps - 1, 1)
+    return mean, var
 
 
 def spectra_to_targets(mean_sfs: np.ndarray) -> np.ndarray:
@@ -226,6 +250,25 @@ def median_relative_error(pred_p: np.ndarray, sim_mean: np.ndarray, min_count: f
     mask = sim_mean >= min_count
     rel = np.abs(pred_p - sim_p)[mask] / sim_p[mask]
     return float(np.median(rel)), float(mask.mean())
+
+
+def error_report(pred_p: np.ndarray, sim_mean: np.ndarray, sim_var: np.ndarray, reps: int,
+                 max_rel_se: float = 0.10) -> dict:
+    """Median per-bin relative error |pred - sim| / sim on normalised spectra:
+    * over every bin whose simulated mean is nonzero ("all"),
+    * over the bins the simulator's own mean resolves: standard error of the `reps`-replicate mean below
+      `max_rel_se` of the mean ("resolved"), with the fraction of bins that criterion keeps.
+    Bins with a zero simulated mean have no relative error and are counted separately."""
+    sim_p = sim_mean / sim_mean.sum(axis=1, keepdims=True)
+    nz = sim_mean > 0
+    rel = np.full(sim_mean.shape, np.nan)
+    rel[nz] = np.abs(pred_p[nz] - sim_p[nz]) / sim_p[nz]
+    se = np.sqrt(sim_var / reps)
+    resolved = nz & (se < max_rel_se * sim_mean)
+    return {"median_all": float(np.median(rel[nz])), "bins_nonzero": float(nz.mean()),
+            "median_resolved": float(np.median(rel[resolved])) if resolved.any() else None,
+            "bins_resolved": float(resolved.mean()), "resolved_criterion": f"SE of the {reps}-replicate mean "
+                                                                            f"< {max_rel_se:g} x mean"}
 
 
 # ------------------------------------------------------------------------------------------------

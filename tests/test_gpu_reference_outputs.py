@@ -55,9 +55,12 @@ def test_dadi_model_matches_reference_table(gofish_driver, tmp_path):
     assert np.all(sd > 0)
     z = (mean - bins[:, 1]) / np.sqrt(sd ** 2 / reps + bins[:, 2] ** 2 / reps)
     # neighbouring bins of a projected SFS are strongly correlated, so the checks are on the
-    # distribution of z over bins rather than a sum of squares: under the same model the median |z| is
-    # about 0.67 and no bin is far out
-    assert 0.35 < np.median(np.abs(z)) < 1.1, np.median(np.abs(z))
+    # distribution of z over bins rather than a sum of squares.  Both tables use the same replicate
+    # seeds, and the runs differ only where the reference's equilibrium start sums floats in another
+    # order (and in the GPU's fast-math code), so the two sets of replicates are strongly correlated and
+    # |z| is typically far below the 0.67 median of independent samples; the bounds are one-sided.
+    print(f"dadi table: median |z| {np.median(np.abs(z)):.3f}, max |z| {np.abs(z).max():.3f}")
+    assert np.median(np.abs(z)) < 1.1, np.median(np.abs(z))
     assert np.abs(z).max() < 5.0, (np.argmax(np.abs(z)) + 1, np.abs(z).max())
     assert abs(z.mean()) < 1.0, z.mean()
     # the normalised SFS sums to the reference's within its own replicate spread
