@@ -669,7 +669,7 @@ def run_surrogate(args):
         "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (batched simulator)",
         "config": {"workload": "6->512x4->99 GELU MLP, per-bin standardised log-spectrum targets; train " f"{args.train_draws} draws x 16 replicates, "
                                f"eval {args.eval_draws} draws x 64 replicates; support: logN [log 1e3, log 1e4], "
-                               "gamma [-100, 10], h [0, 1], F [0, 0.5], r [-0.001, 0.01], T [0.05, 2]; "
+                               "gamma [-100, 10], h [0, 1], F [0, 0.5], r [-0.001, 0.01], T [0.05, 1]; "
                                f"theta {sg.THETA:g}, L {sg.NUM_SITES:g}, n 100",
                    "train_steps": args.train_steps, "batch": args.batch, "lr": args.lr,
                    "weight_decay": args.weight_decay, "inference_batch": B},

@@ -861,6 +861,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   w.any_compact = true;
   w.stats = e->d_stats;
   w.fault = e->d_count + 2;
+  w.sched = e->d_count + kSchedWord;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (e->profiling) {
     cudaEventCreate(&ev0);
@@ -977,6 +978,7 @@ static gf_status batch_super_step_fallback(Engine* e, int* active_out) {
   w.any_compact = true;
   w.stats = e->d_stats;
   w.fault = e->d_count + 2;
+  w.sched = e->d_count + kSchedWord;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (e->profiling) {
     cudaEventCreate(&ev0);

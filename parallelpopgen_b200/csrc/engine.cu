@@ -589,7 +589,7 @@ static gf_status begin_common(Engine* e, const gf_sim_config* c, long long initi
                                                2 * initial_mutations + 65536, 65536});
   gf_status st = set_capacity(e, want, 0);
   if (st != GF_OK) return st;
-  GF_CUDA(e, cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream));
+  GF_CUDA(e, cudaMemsetAsync(e->d_count, 0, sizeof(int) * kCountWords, e->stream));
   GF_CUDA(e, cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream));
   e->compactions = 0;
   e->M_upper = initial_mutations;
@@ -969,6 +969,7 @@ static gf_status launch_window(Engine* e, int b, int first, int count, const Gen
   w.any_compact = R.compact != 0;
   w.stats = e->d_stats;
   w.fault = e->d_count + 2;
+  w.sched = e->d_count + kSchedWord;
   w.uniform_key = true;
   w.seed1 = e->seed1;
   w.seed2 = e->seed2;
@@ -1233,7 +1234,7 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
     }
     e->own_stream = true;
   }
-  if (cudaMalloc(&e->d_count, sizeof(int) * 4) != cudaSuccess ||
+  if (cudaMalloc(&e->d_count, sizeof(int) * kCountWords) != cudaSuccess ||
       cudaMalloc(&e->d_stats, sizeof(unsigned long long) * 2) != cudaSuccess ||
       cudaMallocHost(&e->h_pinned, sizeof(int) * e->pinned_slots) != cudaSuccess) {
     if (e->d_count) cudaFree(e->d_count);
@@ -1241,7 +1242,7 @@ gf_status gf_engine_create(int device, void* cuda_stream, gf_engine** out) {
     delete g;
     return GF_ERR_OUT_OF_MEMORY;
   }
-  cudaMemsetAsync(e->d_count, 0, sizeof(int) * 4, e->stream);
+  cudaMemsetAsync(e->d_count, 0, sizeof(int) * kCountWords, e->stream);
   cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 2, e->stream);
   {
     cudaMemPoolProps props;

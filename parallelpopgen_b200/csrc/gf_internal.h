@@ -106,11 +106,17 @@ struct WindowLaunch {
   bool any_compact;
   unsigned long long* stats;
   int* fault;
+  int* sched = nullptr;    // two zeroed device words: next tile to hand out, blocks finished (the
+                           // launch's last block sets both back to zero)
   // one replicate (the plain engine): its seeds, from which the launch passes the Philox round keys
   // as kernel parameters
   bool uniform_key = false;
   int seed1 = 0, seed2 = 0;
 };
+
+// Words of the engine's device counter block (d_count) and the first of the window scheduler's two.
+constexpr int kCountWords = 8;
+constexpr int kSchedWord = 4;
 
 // Longest window (generations per window launch).
 constexpr int kMaxWindowGenerations = 128;
@@ -255,7 +261,9 @@ struct Engine {
   unsigned* tile_count = nullptr;           // survivors per tile
   unsigned* tile_offset = nullptr;          // exclusive prefix of tile_count
   int cur = 0;                              // buffer holding the current generation
-  int* d_count = nullptr;                   // [0],[1]: mutation count ping-pong; [2]: device status
+  int* d_count = nullptr;                   // [0],[1]: mutation count ping-pong; [2]: device status;
+                                            // [3]: slots at the end of a launch; [4],[5]: window tile
+                                            // scheduler (kSchedWord); kCountWords words in all
   int* h_pinned = nullptr;                  // pinned readback slots
   int pinned_slots = 64;
   int next_slot = 0;

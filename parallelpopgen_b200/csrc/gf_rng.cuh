@@ -35,18 +35,8 @@ constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;  // sqrt(3) - 1
 constexpr float kMeanBoundary = 6.0f;
 constexpr float kBinomNBoundary = 100.0f;
 
-// 1: the 32x32->64 multiply is written as one 64-bit product (a single wide multiply on the
-// device); 0: low and high halves as two multiplies.  Both give the same bits.
-#ifndef GF_PHILOX_WIDE
-#define GF_PHILOX_WIDE 0
-#endif
-
 __host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
-#if defined(__CUDA_ARCH__) && GF_PHILOX_WIDE
-  const uint64_t p = static_cast<uint64_t>(a) * b;
-  lo = static_cast<uint32_t>(p);
-  hi = static_cast<uint32_t>(p >> 32);
-#elif defined(__CUDA_ARCH__)
+#ifdef __CUDA_ARCH__
   lo = a * b;
   hi = __umulhi(a, b);
 #else

@@ -119,8 +119,9 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
                   const WinRep* __restrict__ reps, int nreps, const WinGen* __restrict__ recs, int total_tiles,
                   const int* __restrict__ total_dev, unsigned long long* __restrict__ stats,
-                  int* __restrict__ fault, const PhiloxKeys keys) {
+                  int* __restrict__ fault, const PhiloxKeys keys, int* __restrict__ sched) {
   __shared__ int s_rep;
+  __shared__ int s_tile;
   __shared__ unsigned s_warp[kWinThreads / 32];
   __shared__ int s_tile0[kRepCache];
   __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinThreads / 32 : 1];
@@ -128,9 +129,18 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
   WarpDraws* wd = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
   load_tile0(s_tile0, reps, nreps);
-  for (int gt = blockIdx.x; gt < ntiles_all; gt += gridDim.x) {
-    if (threadIdx.x == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
+  // Tiles are handed out in order by an atomic counter, so a block that drew cheap tiles (slots born
+  // late in the window) takes more of them: the launch does not wait on the blocks that a fixed
+  // assignment would have given the most expensive tiles.
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int t = atomicAdd(sched, 1);
+      s_tile = t;
+      if (t < ntiles_all) s_rep = find_rep_cached(s_tile0, reps, nreps, t);
+    }
     __syncthreads();
+    const int gt = s_tile;
+    if (gt >= ntiles_all) break;   // block-uniform
     const WinRep R = reps[s_rep];
     __syncthreads();
     const int t = gt - R.tile0;
@@ -282,6 +292,16 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
       if (M > cap) atomicExch(fault, kFaultCapacity);
       M_end[R.rep] = Mw;
       if (M_next && !R.compact) M_next[R.rep] = Mw;
+    }
+  }
+  // every block has drawn past the last tile once it gets here; the last one resets the scheduler
+  // for the next launch on this stream
+  if (threadIdx.x == 0) {
+    __threadfence();   // this block's last draw from sched[0] is ordered before its count in sched[1]
+    const int finished = atomicAdd(sched + 1, 1);
+    if (finished == static_cast<int>(gridDim.x) - 1) {
+      sched[0] = 0;
+      sched[1] = 0;
     }
   }
 }
@@ -478,7 +498,7 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
   const PhiloxKeys keys = philox_round_keys(w.seed1, w.seed2);
   window_kernel<DRAW, KEYS><<<blocks, kWinThreads, 0, e->stream>>>(
       w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count, w.M_in, w.M_end, w.M_next, w.reps, w.nreps,
-      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault, keys);
+      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault, keys, w.sched);
 }
 
 // Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan

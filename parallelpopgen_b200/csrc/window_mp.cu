@@ -72,9 +72,11 @@ __global__ void __launch_bounds__(kMpThreads, GF_WINDOW_MP_MIN_BLOCKS)
                      int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                      int* __restrict__ d_count, int slot_in, int slot_out, long long capacity,
                      const GenArgs* __restrict__ table, int ngen, long long births, int compact, int check_preserved,
-                     int seed1, int seed2, unsigned long long* __restrict__ stats) {
+                     int seed1, int seed2, unsigned long long* __restrict__ stats, const PhiloxKeys keys) {
   __shared__ MpGen<P> s_gen[kMaxWindowGenerations];
   __shared__ unsigned s_warp[kMpThreads / 32];
+  __shared__ int s_tile;
+  int* const sched = d_count + kSchedWord;   // tile scheduler: next tile, blocks finished
   for (int k = threadIdx.x; k < ngen; k += kMpThreads) {
     const GenArgs& a = table[k];
     MpGen<P>& G = s_gen[k];
@@ -122,7 +124,13 @@ __global__ void __launch_bounds__(kMpThreads, GF_WINDOW_MP_MIN_BLOCKS)
     stats[1] += static_cast<unsigned long long>(ngen);
   }
 
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  // tiles handed out in order by an atomic counter (cheap tiles of late-born slots balance out)
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(sched, 1);
+    __syncthreads();
+    const int t = s_tile;
+    __syncthreads();
+    if (t >= ntiles) break;   // block-uniform
     const int q = t * kMpThreads + threadIdx.x;  // quad
     const int s0 = 4 * q;
     float x[P][4];
@@ -182,7 +190,9 @@ __global__ void __launch_bounds__(kMpThreads, GF_WINDOW_MP_MIN_BLOCKS)
               if (!(xs[j] == 0.f || (xs[j] == 1.f && N > 6))) need |= 1u << j;
             }
             if (need) {
-              const uint4 r = philox(seed1, seed2, q + 2, g, p, 0);
+              // round keys of (seed1, seed2) from the kernel parameters (constant bank)
+              const uint4 r = philox4x32_10_keys(
+                  make_uint4(static_cast<uint32_t>(q + 2), static_cast<uint32_t>(g), static_cast<uint32_t>(p), 0u), keys);
               draw_quad<kDrawLanes>(xs, r, need, N, lane, nullptr, res);
             }
             const float Nf = static_cast<float>(N);
@@ -291,6 +301,15 @@ __global__ void __launch_bounds__(kMpThreads, GF_WINDOW_MP_MIN_BLOCKS)
       __syncthreads();
     }
   }
+  // the last block to finish resets the scheduler for the next launch on this stream
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int finished = atomicAdd(sched + 1, 1);
+    if (finished == static_cast<int>(gridDim.x) - 1) {
+      sched[0] = 0;
+      sched[1] = 0;
+    }
+  }
 }
 
 template <int P>
@@ -309,7 +328,8 @@ static void launch_mp(Engine* e, const WindowMpLaunch& w) {
   const int blocks = std::max(1, std::min(w.tiles_bound, e->num_sms * per_sm));
   window_mp_kernel<P><<<blocks, kMpThreads, 0, e->stream>>>(
       w.A, w.B, w.stride, w.id_gp, w.id_tid, w.flags, w.tile_count, w.d_count, w.slot_in, w.slot_out, w.stride,
-      w.table, w.ngen, w.births, w.compact, w.check_preserved, w.seed1, w.seed2, w.stats);
+      w.table, w.ngen, w.births, w.compact, w.check_preserved, w.seed1, w.seed2, w.stats,
+      philox_round_keys(w.seed1, w.seed2));
 }
 
 gf_status window_mp_run(Engine* e, const WindowMpLaunch& w) {

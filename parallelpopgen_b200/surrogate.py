@@ -10,10 +10,10 @@ whose replicates equal plain GO_Fish runs bit for bit).
 Parameter family (one population, MSE start at N0, then exponential growth for T*2*N0 generations):
     log N0 in [log 1e3, log 1e4]      gamma = 2 N s (selection_constant semantics) in [-100, 10]
     h in [0, 1]                        F in [0, 0.5]
-    r in [-0.001, 0.01] per generation, N clamped to [N0/10, 10 N0]      T in [0.05, 2]
+    r in [-0.001, 0.01] per generation, N clamped to [N0/10, 10 N0]      T in [0.05, 1]
 theta = 4 N0 mu L is held at THETA (mu = THETA / (4 N0 L)), so spectra differ only through the shape.
-T = 2 is the batched replicates' run length (4 N0 generations); queries with N0 in (1e4, 1e5] (the
-upper half of that workload's range) are outside the support and go to the simulator.
+Queries with N0 in (1e4, 1e5] (the upper half of the batched-replicate workload's range) are outside
+the support and go to the simulator.
 """
 from __future__ import annotations
 
@@ -42,7 +42,7 @@ SUPPORT = (
     ("h", 0.0, 1.0),
     ("F", 0.0, 0.5),
     ("r", -0.001, 0.01),
-    ("T", 0.05, 2.0),
+    ("T", 0.05, 1.0),
 )
 LOW = np.array([s[1] for s in SUPPORT])
 HIGH = np.array([s[2] for s in SUPPORT])

@@ -112,7 +112,6 @@ def test_surrogate_on_simulator_spectra():
     with Engine() as e:
         ptrain = sg.draw_parameters(1024, seed=21)
         ptrain[:, 0] = sg.LOW[0] + (ptrain[:, 0] - sg.LOW[0]) * 0.1         # small N: quick
-        ptrain[:, 5] = np.minimum(ptrain[:, 5], 1.0)
         sims = sg.simulate_spectra(e, ptrain, reps=4, seed=1000)
         assert np.all(sims.sum(axis=1) > 0)
         X = torch.from_numpy(sg.encode(ptrain)).cuda()
@@ -141,7 +140,6 @@ def test_trained_network_beats_answers_without_it():
 
     def small_n(p):
         p[:, 0] = sg.LOW[0] + (p[:, 0] - sg.LOW[0]) * 0.1          # N in [1000, ~1260]: quick runs
-        p[:, 5] = np.minimum(p[:, 5], 1.0)
         return p
 
     with Engine() as e:
