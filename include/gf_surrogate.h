@@ -55,8 +55,11 @@ gf_status gf_mlp_get_params(gf_mlp* mlp, float* params, int64_t count);
 gf_status gf_mlp_set_learning_rate(gf_mlp* mlp, float lr);
 
 /* Inference: d_inputs [batch][6] fp32 -> d_outputs [batch][99] fp32 (device pointers; d_outputs
- * 16-byte aligned). */
+ * 16-byte aligned).  By default one fused kernel runs all five layers of each 128-row tile with the
+ * activations kept on chip; gf_mlp_set_fused_inference(mlp, 0) runs one tensor-core GEMM per layer
+ * instead (the same outputs, bit for bit). */
 gf_status gf_mlp_forward(gf_mlp* mlp, const float* d_inputs, int32_t batch, float* d_outputs);
+gf_status gf_mlp_set_fused_inference(gf_mlp* mlp, int32_t enable);
 
 /* Mean-squared-error gradients of the loss (1 / (batch * 99)) sum (out - target)^2 with respect to
  * the master parameters, without an update: host fp32 gradients in the parameter layout, and the
@@ -73,8 +76,8 @@ gf_status gf_mlp_train_step(gf_mlp* mlp, const float* d_inputs, const float* d_t
  * GF_ERR_DEVICE once per fault and clears the word; the network stays usable. */
 gf_status gf_mlp_check(gf_mlp* mlp);
 
-/* Failure-path testing: kind 1 arms the next inference pass so that its first GEMM withholds the
- * hand-off of one accumulator; the epilogue's bounded wait (about 2 ms under injection) runs out, the
+/* Failure-path testing: kind 1 arms the next inference pass so that its first GEMM (or the fused
+ * kernel's first layer) withholds the hand-off of one accumulator; the epilogue's bounded wait (about 2 ms under injection) runs out, the
  * kernel stops, drains what it issued, releases tensor memory and sets the fault word.  Outputs of
  * that pass are undefined.  kind 0 disarms. */
 gf_status gf_mlp_inject_fault(gf_mlp* mlp, int32_t kind);

@@ -139,6 +139,7 @@ SIGNATURES = {
     "gf_mlp_get_params": (_I, [_P, _P, ctypes.c_int64]),
     "gf_mlp_set_learning_rate": (_I, [_P, _F]),
     "gf_mlp_forward": (_I, [_P, _P, _I, _P]),
+    "gf_mlp_set_fused_inference": (_I, [_P, _I]),
     "gf_mlp_gradients": (_I, [_P, _P, _P, _I, _P, _P]),
     "gf_mlp_train_step": (_I, [_P, _P, _P, _I, _P]),
     "gf_mlp_check": (_I, [_P]),

@@ -438,6 +438,279 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
 }
 
 // ---------------------------------------------------------------------------------------------
+// Fused inference forward: all five layers of a 128-row tile in one CTA, the activations on chip.
+//
+// The layered path writes each hidden activation (batch x 512 bf16) to memory and reads it back in
+// the next layer's GEMM.  Here a CTA keeps its tile's activation H (128 x 512 bf16 = 128 KB) in
+// shared memory, in the 128-byte-swizzled K-major layout the MMA reads (eight 64-column K blocks of
+// 16 KB), and the layer's fp32 accumulator (128 x 512) in all 512 tensor-memory columns.  Per layer:
+// warp 1 issues the MMAs (A = H from shared memory, B = weight K-blocks streamed by warp 0's TMA
+// through a 3-stage ring from L2, where every CTA finds the 1.3 MB of weights), then 16 epilogue
+// warps drain the accumulator (bias, GELU, bf16) back into H for the next layer; the last layer's
+// epilogue writes acc + bias to the caller's [batch][99] array.  Each layer's MMAs run in the order
+// of the layered GEMMs (N halves of 256, K blocks 0..7, four 16-wide slices each; layer 5 one
+// 128-wide N tile), so the outputs are bit-identical to the layered path.
+// ---------------------------------------------------------------------------------------------
+constexpr int FF_EPI_WARPS = 16;                          // four per tensor-memory lane quarter
+constexpr int FF_THREADS = 64 + 32 * FF_EPI_WARPS;        // TMA warp, MMA warp, 16 epilogue warps
+constexpr int FF_WSTAGES = 3;
+constexpr int FF_KB_BYTES = BM * BK * 2;                  // one 128 x 64 bf16 K block of H: 16 KB
+constexpr int FF_H_BYTES = BM * HID * 2;                  // H: 128 KB
+constexpr int FF_WSTAGE_BYTES = 256 * BK * 2;             // a 256-row x 64 weight block: 32 KB
+constexpr int FF_BAR_OFFSET = FF_H_BYTES + FF_WSTAGES * FF_WSTAGE_BYTES;
+constexpr int FF_SMEM = FF_BAR_OFFSET + 256 + 1024;       // + barriers and flags, + base alignment
+static_assert(FF_SMEM <= SMEM_LIMIT, "fused forward shared memory");
+constexpr int FF_STAGES_PER_TILE = 2 + 3 * 16 + 8;        // weight blocks streamed per tile (58)
+
+// Weight block `i` of a tile's stream: layer, the N offset of its rows, the K block, its rows.
+struct FfBlock {
+  int layer, n0, kb, rows;
+};
+__device__ __forceinline__ FfBlock ff_block(int i) {
+  if (i < 2) return {0, 256 * i, 0, 256};                           // layer 1: K = 64, two N halves
+  if (i < 50) {                                                      // layers 2-4: N halves x 8 K blocks
+    const int j = i - 2;
+    return {1 + j / 16, 256 * ((j % 16) / 8), j % 8, 256};
+  }
+  return {4, 0, i - 50, OUT_PAD};                                    // layer 5: 128 rows x 8 K blocks
+}
+
+__global__ void __launch_bounds__(FF_THREADS, 1)
+fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_constant__ CUtensorMap tma_w1,
+                     const __grid_constant__ CUtensorMap tma_w2, const __grid_constant__ CUtensorMap tma_w3,
+                     const __grid_constant__ CUtensorMap tma_w4, const __grid_constant__ CUtensorMap tma_w5,
+                     const float* __restrict__ b1, const float* __restrict__ b2, const float* __restrict__ b3,
+                     const float* __restrict__ b4, const float* __restrict__ b5, float* __restrict__ out,
+                     int batch, int m_tiles, long long wait_limit, int inject, int* fault) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* H = smem;
+  uint8_t* W = smem + FF_H_BYTES;
+  uint64_t* wfull = reinterpret_cast<uint64_t*>(smem + FF_BAR_OFFSET);
+  uint64_t* wempty = wfull + FF_WSTAGES;
+  uint64_t* xfull = wempty + FF_WSTAGES;   // the tile's inputs have landed in H's first K block
+  uint64_t* accfull = xfull + 1;           // a layer's accumulator is complete (MMA -> epilogue)
+  uint64_t* hready = accfull + 1;          // H written and the accumulator drained (epilogue -> MMA)
+  uint64_t* hfree = hready + 1;            // the tile's last MMAs have read H (MMA -> producer)
+  uint64_t* drain = hfree + 1;             // MMA completion before tensor memory is released (abort)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  int* flags = reinterpret_cast<int*>(tmem_slot + 1);
+  volatile int* abort_flag = flags;        // [0] a wait ran out; [1] epilogue verdict; [2] consumed
+  int* epi_fail = flags + 1;
+  int* consumed_s = flags + 2;             // weight blocks the MMA thread received (for the drain)
+  int* x_consumed_s = flags + 3;           // input tiles the MMA thread received
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (*abort_flag) return false;
+    const uint32_t addr = smem_u32(bar);
+    const long long t0 = clock64();
+    while (!mbar_try_wait(addr, parity)) {
+      if (*abort_flag) return false;
+      if (clock64() - t0 > wait_limit) {
+        *abort_flag = 1;
+        return false;
+      }
+    }
+    return true;
+  };
+
+  if (threadIdx.x == 0) {
+    tma_prefetch_desc(&tma_x);
+    for (int s = 0; s < FF_WSTAGES; ++s) {
+      mbar_init(&wfull[s], 1);
+      mbar_init(&wempty[s], 1);
+    }
+    mbar_init(xfull, 1);
+    mbar_init(accfull, 1);
+    mbar_init(hready, FF_EPI_WARPS);
+    mbar_init(hfree, 1);
+    mbar_init(drain, 1);
+    flags[0] = flags[1] = flags[2] = flags[3] = 0;
+    mbar_fence_init();
+  }
+  __syncwarp();
+  if (warp == 1) tmem_alloc(tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool late = false;
+  int issued = 0, x_issued = 0;
+
+  if (warp == 0) {
+    // ---- producer: the tile's inputs, then its 58 weight blocks in the order the MMAs use them ----
+    if (lane == 0) {
+      int it = 0, local = 0;
+      for (int tile = blockIdx.x; tile < m_tiles; tile += gridDim.x, ++local) {
+        if (local > 0 && !wait(hfree, (local - 1) & 1)) {   // the previous tile's MMAs are done with H
+          late = true;
+          break;
+        }
+        mbar_arrive_expect_tx(xfull, FF_KB_BYTES);
+        tma_load_2d(H, &tma_x, 0, tile * BM, xfull);
+        ++x_issued;
+        bool stop = false;
+        for (int i = 0; i < FF_STAGES_PER_TILE; ++i, ++it) {
+          const int s = it % FF_WSTAGES;
+          if (!wait(&wempty[s], ((it / FF_WSTAGES) & 1) ^ 1)) {
+            stop = true;
+            break;
+          }
+          const FfBlock blk = ff_block(i);
+          const CUtensorMap* map = blk.layer == 0 ? &tma_w1 : blk.layer == 1 ? &tma_w2 : blk.layer == 2 ? &tma_w3
+                                   : blk.layer == 3 ? &tma_w4 : &tma_w5;
+          mbar_arrive_expect_tx(&wfull[s], blk.rows * BK * 2);
+          tma_load_2d(W + s * FF_WSTAGE_BYTES, map, blk.kb * BK, blk.n0, &wfull[s]);
+        }
+        if (stop) {
+          late = true;
+          break;
+        }
+      }
+      issued = it;
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---- MMA issue (one thread) ----
+    if (lane == 0) {
+      constexpr uint32_t idesc256 = bf16_idesc(BM, 256);
+      constexpr uint32_t idesc128 = bf16_idesc(BM, OUT_PAD);
+      int it = 0, local = 0, hwaits = 0, xs = 0;
+      const uint32_t h_addr = smem_u32(H);
+      for (int tile = blockIdx.x; tile < m_tiles && !late; tile += gridDim.x, ++local) {
+        if (!wait(xfull, local & 1)) {
+          late = true;
+          break;
+        }
+        ++xs;
+        int i = 0;
+        for (int layer = 0; layer < GF_MLP_LAYERS; ++layer) {
+          // H holds this layer's input and the accumulator has been drained (not before the very first)
+          if (local > 0 || layer > 0) {
+            if (!wait(hready, hwaits & 1)) {
+              late = true;
+              break;
+            }
+            ++hwaits;
+          }
+          tc_fence_after();
+          const int nblocks = layer == 0 ? 2 : layer < 4 ? 16 : 8;
+          for (int b = 0; b < nblocks; ++b, ++i, ++it) {
+            const int s = it % FF_WSTAGES;
+            if (!wait(&wfull[s], (it / FF_WSTAGES) & 1)) {
+              late = true;
+              break;
+            }
+            tc_fence_after();
+            const FfBlock blk = ff_block(i);
+            const uint32_t w_addr = smem_u32(W + s * FF_WSTAGE_BYTES);
+            const uint32_t a_addr = h_addr + blk.kb * FF_KB_BYTES;
+            const uint32_t d = tmem + static_cast<uint32_t>(blk.n0);
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+              umma_bf16(d, sw128_kmajor_desc(a_addr + kk * 32), sw128_kmajor_desc(w_addr + kk * 32),
+                        layer == 4 ? idesc128 : idesc256, (blk.kb | kk) != 0);
+            umma_commit(&wempty[s]);
+          }
+          if (late) break;
+          // fault injection for tests: withhold the first accumulator hand-off
+          if (!((inject & 1) && local == 0 && layer == 0)) umma_commit(accfull);
+        }
+        if (late) break;
+        umma_commit(hfree);
+      }
+      *consumed_s = it;
+      *x_consumed_s = xs;
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: lane quarter qd of tensor memory, column group cg of the layer's outputs ----
+    const int qd = warp & 3;
+    const int cg = (warp - 2) >> 2;
+    const int r = qd * 32 + lane;                 // row within the tile
+    int accs = 0;
+    for (int tile = blockIdx.x; tile < m_tiles; tile += gridDim.x) {
+      bool stop = false;
+      for (int layer = 0; layer < GF_MLP_LAYERS; ++layer, ++accs) {
+        if (lane == 0 && !mbar_wait(accfull, accs & 1, wait_limit)) atomicOr(epi_fail, 1);
+        named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every epilogue warp has its verdict
+        if (*reinterpret_cast<volatile int*>(epi_fail)) {
+          stop = true;
+          break;
+        }
+        __syncwarp();
+        tc_fence_after();
+        const uint32_t tbase = tmem + (static_cast<uint32_t>(qd * 32) << 16);
+        if (layer < 4) {
+          const float* bias = layer == 0 ? b1 : layer == 1 ? b2 : layer == 2 ? b3 : b4;
+#pragma unroll 1
+          for (int c0 = cg * 128; c0 < cg * 128 + 128; c0 += 32) {
+            float v[32];
+            tmem_ld_32cols(tbase + c0, v);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] = gelu(v[j] + __ldg(bias + c0 + j));
+            // row r, columns c0 .. c0+31 of H: K block c0 / 64, 16-byte units (c0 % 64) / 8 + q,
+            // placed at unit ^ (r % 8) of the row (128-byte swizzle)
+            uint8_t* rowp = H + (c0 >> 6) * FF_KB_BYTES + r * 128;
+            const int u0 = (c0 & 63) >> 3;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              uint32_t w4[4];
+#pragma unroll
+              for (int t = 0; t < 4; ++t) {
+                __nv_bfloat162 pr = __floats2bfloat162_rn(v[q * 8 + 2 * t], v[q * 8 + 2 * t + 1]);
+                w4[t] = *reinterpret_cast<uint32_t*>(&pr);
+              }
+              *reinterpret_cast<uint4*>(rowp + (((u0 + q) ^ (r & 7)) << 4)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+            }
+          }
+          fence_proxy_async_smem();   // H is read by the tensor cores (async proxy)
+        } else {
+          // layer 5: 128 padded outputs, one 32-column chunk per warp; the first 99 go to the caller
+          const int c0 = cg * 32;
+          float v[32];
+          tmem_ld_32cols(tbase + c0, v);
+          const int grow = tile * BM + r;
+          if (grow < batch) {
+            float* o = out + static_cast<long long>(grow) * GF_MLP_OUTPUTS;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j < GF_MLP_OUTPUTS) o[c0 + j] = v[j] + __ldg(b5 + c0 + j);
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(hready);
+      }
+      if (stop) {
+        late = true;
+        break;
+      }
+    }
+  }
+
+  tc_fence_before();
+  if (late) *abort_flag = 1;
+  __syncthreads();
+  if (*abort_flag) {
+    // a wait ran out: every load and MMA this CTA issued completes before its shared and tensor memory
+    // are released (each wait again bounded)
+    if (threadIdx.x == 0) {
+      for (int it = *consumed_s; it < issued; ++it)
+        mbar_wait(&wfull[it % FF_WSTAGES], (it / FF_WSTAGES) & 1, wait_limit);
+      for (int x = *x_consumed_s; x < x_issued; ++x) mbar_wait(xfull, x & 1, wait_limit);
+      if (fault) atomicOr(fault, 1);
+    } else if (threadIdx.x == 32) {
+      umma_commit(drain);
+      mbar_wait(drain, 0, wait_limit);
+    }
+    __syncthreads();
+  }
+  if (warp == 1) tmem_dealloc(tmem, 512);
+}
+
+// ---------------------------------------------------------------------------------------------
 // small kernels
 // ---------------------------------------------------------------------------------------------
 
@@ -678,6 +951,25 @@ cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtens
   return cudaGetLastError();
 }
 
+cudaError_t launch_fused_forward(const CUtensorMap& x, const CUtensorMap* w256, const CUtensorMap& w5,
+                                 float* const* bias, float* out, int batch, cudaStream_t stream, int inject,
+                                 int* fault) {
+  static std::atomic<bool> attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    cudaError_t err = cudaFuncSetAttribute(fused_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FF_SMEM);
+    if (err != cudaSuccess) return err;
+    attr_set[dev] = true;
+  }
+  const int m_tiles = batch / BM;
+  const int grid = m_tiles < sm_count() ? m_tiles : sm_count();
+  fused_forward_kernel<<<grid, FF_THREADS, FF_SMEM, stream>>>(
+      x, w256[0], w256[1], w256[2], w256[3], w5, bias[0], bias[1], bias[2], bias[3], bias[4], out, batch, m_tiles,
+      inject ? INJECT_WAIT_LIMIT : WAIT_LIMIT, inject, fault);
+  return cudaGetLastError();
+}
+
 // Split count for a weight-gradient GEMM: enough CTAs to cover the SMs, each split a whole number
 // of 64-wide K blocks.
 int choose_splits(int tiles, int K) {
@@ -743,6 +1035,7 @@ struct gf_mlp {
 
   std::vector<void*> allocations;
   int inject = 0;   // fault injection armed for the next forward pass (tests)
+  int fused = 1;    // inference runs the fused five-layer kernel (0: one GEMM per layer)
 };
 
 namespace {
@@ -834,6 +1127,13 @@ gf_status run_forward(gf_mlp* m, const float* d_inputs, int batch, bool train, f
   encode_inputs_kernel<<<(batch + 255) / 256, 256, 0, m->stream>>>(d_inputs, batch, m->x0, m->x0t, m->cap,
                                                                   train ? 1 : 0);
   MLP_CUDA(m, cudaGetLastError());
+  if (!train && m->fused) {
+    cudaError_t err = launch_fused_forward(m->fwd_a[0], m->fwd_b256, m->fwd_b[4], m->b, d_out, batch, m->stream,
+                                           m->inject, m->fault);
+    m->inject = 0;
+    if (err != cudaSuccess) return mlp_fail(m, GF_ERR_CUDA, "fused forward: %s", cudaGetErrorString(err));
+    return GF_OK;
+  }
   for (int l = 0; l < GF_MLP_LAYERS; ++l) {
     EpiArgs ep{};
     ep.bias = m->b[l];
@@ -1156,6 +1456,12 @@ gf_status gf_mlp_check(gf_mlp* m) {
     MLP_CUDA(m, cudaStreamSynchronize(m->stream));
     return mlp_fail(m, GF_ERR_DEVICE, "a tensor-core GEMM wait ran out of time");
   }
+  return GF_OK;
+}
+
+gf_status gf_mlp_set_fused_inference(gf_mlp* m, int32_t enable) {
+  if (!m || enable < 0 || enable > 1) return GF_ERR_INVALID_ARGUMENT;
+  m->fused = enable;
   return GF_OK;
 }
 

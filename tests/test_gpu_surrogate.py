@@ -60,6 +60,25 @@ def test_forward_matches_oracle():
     assert _rel(y, exact) < 3e-2, _rel(y, exact)
 
 
+@pytest.mark.parametrize("B", [512, 4096, 148 * 128 + 256])
+def test_fused_forward_equals_layered_forward(B):
+    """The fused five-layer inference kernel issues each layer's MMAs in the layered GEMMs' order and
+    rounds the activations at the same points, so its outputs equal the one-GEMM-per-layer path bit for
+    bit (batches of one tile per CTA, several tiles per CTA, and more tiles than SMs)."""
+    from parallelpopgen_b200 import _capi
+    mlp, vec, x, _ = _net(7, B)
+    xs = torch.from_numpy(x).cuda()
+    fused = mlp.forward(xs).cpu().numpy()
+    mlp.check()
+    lib = _capi.load()
+    assert lib.gf_mlp_set_fused_inference(mlp.h, 0) == 0
+    layered = mlp.forward(xs).cpu().numpy()
+    mlp.check()
+    assert lib.gf_mlp_set_fused_inference(mlp.h, 1) == 0
+    assert np.isfinite(fused).all()
+    assert np.array_equal(fused.view(np.uint32), layered.view(np.uint32))
+
+
 def test_gradients_match_oracle():
     mlp, vec, x, t = _net(3, 512)
     g, loss = mlp.gradients(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
