@@ -14,14 +14,6 @@
 #ifndef GF_WINDOW_MIN_BLOCKS
 #define GF_WINDOW_MIN_BLOCKS GF_DRIFT_MIN_BLOCKS
 #endif
-// Quads per thread of the window kernel (1 or 2), and the resident 128-thread blocks per SM the
-// register allocation must allow with two.
-#ifndef GF_WIN_QPT
-#define GF_WIN_QPT 1
-#endif
-#ifndef GF_WINDOW_QPT2_MIN_BLOCKS
-#define GF_WINDOW_QPT2_MIN_BLOCKS 8
-#endif
 // 1: a single-replicate window launch takes its Philox round keys from the kernel parameters.
 #ifndef GF_WINDOW_UNIFORM_KEYS
 #define GF_WINDOW_UNIFORM_KEYS 1

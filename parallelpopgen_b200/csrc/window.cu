@@ -112,27 +112,19 @@ __global__ void __launch_bounds__(1024) batch_tiles_kernel(WinRep* __restrict__ 
 // DRAW: how a warp schedules its sampler draws (DrawStrategy).  KEYS: every replicate of the launch
 // has the seeds whose round keys `keys` holds (a plain-engine launch), so the quads' Philox blocks take
 // their round keys from the kernel parameters instead of deriving them from the replicate's seeds.
-// A tile is 1024 slots = 256 quads; a block of kWinThreads / GF_WIN_QPT threads works on it, each
-// thread on GF_WIN_QPT quads (quads i and i + 128 with two), so one thread's per-generation control
-// serves more slots and its quads' independent draws can be interleaved.
-constexpr int kWinQpt = GF_WIN_QPT;
-constexpr int kWinBlock = kWinThreads / kWinQpt;
-constexpr int kWinMinBlocks = kWinQpt == 1 ? GF_WINDOW_MIN_BLOCKS : GF_WINDOW_QPT2_MIN_BLOCKS;
-
 template <int DRAW, bool KEYS>
-__global__ void __launch_bounds__(kWinBlock, kWinMinBlocks)
+__global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     window_kernel(const float* __restrict__ A, float* __restrict__ B, int* __restrict__ id_gp,
                   int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
                   const WinRep* __restrict__ reps, int nreps, const WinGen* __restrict__ recs, int total_tiles,
                   const int* __restrict__ total_dev, unsigned long long* __restrict__ stats,
                   int* __restrict__ fault, const PhiloxKeys keys, int* __restrict__ sched) {
-  constexpr int QPT = kWinQpt;
   __shared__ int s_rep;
   __shared__ int s_tile;
-  __shared__ unsigned s_warp[kWinBlock / 32];
+  __shared__ unsigned s_warp[kWinThreads / 32];
   __shared__ int s_tile0[kRepCache];
-  __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinBlock / 32 : 1];
+  __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinThreads / 32 : 1];
   const int lane = threadIdx.x & 31;
   WarpDraws* wd = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
@@ -152,6 +144,8 @@ __global__ void __launch_bounds__(kWinBlock, kWinMinBlocks)
     const WinRep R = reps[s_rep];
     __syncthreads();
     const int t = gt - R.tile0;
+    const int q = t * kWinThreads + threadIdx.x;  // quad within the replicate
+    const int s0 = 4 * q;
     const int cap = static_cast<int>(R.capacity);
     const int M0 = M_in[R.rep];
     // a tile past the replicate's end-of-window count has nothing to do (tile 0 keeps the bookkeeping)
@@ -161,19 +155,13 @@ __global__ void __launch_bounds__(kWinBlock, kWinMinBlocks)
     int* const gp = id_gp + R.base;
     int* const tid = id_tid + R.base;
 
-    int q[QPT], s0[QPT];
-    float x[QPT][4];
+    float x[4];
+    if (s0 + 3 < M0) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(rowA + s0));
+      x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+    } else {
 #pragma unroll
-    for (int u = 0; u < QPT; ++u) {
-      q[u] = t * kWinThreads + u * kWinBlock + threadIdx.x;  // quad within the replicate
-      s0[u] = 4 * q[u];
-      if (s0[u] + 3 < M0) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(rowA + s0[u]));
-        x[u][0] = v.x; x[u][1] = v.y; x[u][2] = v.z; x[u][3] = v.w;
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) x[u][j] = (s0[u] + j < M0) ? rowA[s0[u] + j] : 0.f;
-      }
+      for (int j = 0; j < 4; ++j) x[j] = (s0 + j < M0) ? rowA[s0 + j] : 0.f;
     }
 
     int M = M0;
@@ -187,113 +175,97 @@ __global__ void __launch_bounds__(kWinBlock, kWinMinBlocks)
       if (N <= 0) {
         // extinction generation: the population's row is cleared
 #pragma unroll
-        for (int u = 0; u < QPT; ++u)
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (s0[u] + j < M) x[u][j] = 0.f;
+        for (int j = 0; j < 4; ++j)
+          if (s0 + j < M) x[j] = 0.f;
       } else {
         // whole quad: Philox (q + 2, g, 0, 0), lanes x, y, z, w.  Every lane of the warp reaches the
         // draw (N and the loop are uniform over the block), as the warp-pooled strategy requires.
+        const bool quad = q < (M >> 2);
         const bool neutral = (G.sel_a == 0.f && G.sel_b == 0.f);
+        float xs[4] = {0.f, 0.f, 0.f, 0.f};
+        int res[4] = {0, 0, 0, 0};
+        unsigned need = 0;
+        if (quad) {
 #pragma unroll
-        for (int u = 0; u < QPT; ++u) {
-          const bool quad = q[u] < (M >> 2);
-          float xs[4] = {0.f, 0.f, 0.f, 0.f};
-          int res[4] = {0, 0, 0, 0};
-          unsigned need = 0;
-          if (quad) {
+          for (int j = 0; j < 4; ++j)
+            xs[j] = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
+                            : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-              xs[j] = neutral ? selected_freq<true>(x[u][j], 0.f, 0.f, 0.f, 0.f)
-                              : selected_freq<false>(x[u][j], G.sel_a, G.sel_b, G.F, G.h);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              res[j] = (xs[j] == 1.f && N > 6) ? N : 0;
-              if (!(xs[j] == 0.f || (xs[j] == 1.f && N > 6))) need |= 1u << j;
-            }
+          for (int j = 0; j < 4; ++j) {
+            res[j] = (xs[j] == 1.f && N > 6) ? N : 0;
+            if (!(xs[j] == 0.f || (xs[j] == 1.f && N > 6))) need |= 1u << j;
           }
-          uint4 r = make_uint4(0u, 0u, 0u, 0u);
-          if (need) {
-            if (KEYS) r = philox4x32_10_keys(make_uint4(static_cast<uint32_t>(q[u] + 2), static_cast<uint32_t>(g), 0u, 0u), keys);
-            else r = philox(R.seed1, R.seed2, q[u] + 2, g, 0, 0);
-          }
-          if (DRAW == kDrawWarp) {
-            draw_quad<kDrawWarp>(xs, r, need, N, lane, wd, res);
-          } else if (need) {
-            draw_quad<DRAW>(xs, r, need, N, lane, wd, res);
-          }
-          if (quad) {
-            const float Nf = static_cast<float>(N);
+        }
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);
+        if (need) {
+          if (KEYS) r = philox4x32_10_keys(make_uint4(static_cast<uint32_t>(q + 2), static_cast<uint32_t>(g), 0u, 0u), keys);
+          else r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
+        }
+        if (DRAW == kDrawWarp) {
+          draw_quad<kDrawWarp>(xs, r, need, N, lane, wd, res);
+        } else if (need) {
+          draw_quad<DRAW>(xs, r, need, N, lane, wd, res);
+        }
+        if (quad) {
+          const float Nf = static_cast<float>(N);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) x[u][j] = static_cast<float>(clampi(res[j], 0, N)) / Nf;
-          } else if (s0[u] < M) {
-            // scalar tail: Philox (slot + 2, g, 0, 0) lane x, variance in double
+          for (int j = 0; j < 4; ++j) x[j] = static_cast<float>(clampi(res[j], 0, N)) / Nf;
+        } else if (s0 < M) {
+          // scalar tail: Philox (slot + 2, g, 0, 0) lane x, variance in double
 #pragma unroll 1
-            for (int j = 0; j < 4; ++j) {
-              const int e = s0[u] + j;
-              if (e >= M) break;
-              const float xs1 = neutral ? selected_freq<true>(x[u][j], 0.f, 0.f, 0.f, 0.f)
-                                        : selected_freq<false>(x[u][j], G.sel_a, G.sel_b, G.F, G.h);
-              x[u][j] = static_cast<float>(clampi(drift_tail(R.seed1, R.seed2, e, g, 0, xs1, N), 0, N)) /
-                        static_cast<float>(N);
-            }
+          for (int j = 0; j < 4; ++j) {
+            const int e = s0 + j;
+            if (e >= M) break;
+            const float xs1 = neutral ? selected_freq<true>(x[j], 0.f, 0.f, 0.f, 0.f)
+                                      : selected_freq<false>(x[j], G.sel_a, G.sel_b, G.F, G.h);
+            x[j] = static_cast<float>(clampi(drift_tail(R.seed1, R.seed2, e, g, 0, xs1, N), 0, N)) /
+                   static_cast<float>(N);
           }
         }
       }
       // births: slots [M, M + new_count) start at 1/Nc with ID (g, 0, slot - M + 1)
       const int Mn = M + G.new_count;
+      if (s0 + 3 >= M && s0 < Mn) {
 #pragma unroll
-      for (int u = 0; u < QPT; ++u) {
-        if (s0[u] + 3 >= M && s0[u] < Mn) {
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int e = s0[u] + j;
-            if (e >= M && e < Mn && e < cap) {
-              x[u][j] = G.new_freq;
-              gp[e] = g;
-              tid[e] = e - M + 1;
-            }
+        for (int j = 0; j < 4; ++j) {
+          const int e = s0 + j;
+          if (e >= M && e < Mn && e < cap) {
+            x[j] = G.new_freq;
+            gp[e] = g;
+            tid[e] = e - M + 1;
           }
         }
       }
       M = Mn;
     }
     const int Mw = min(M, cap);
+    if (s0 + 3 < Mw) {
+      *reinterpret_cast<float4*>(rowB + s0) = make_float4(x[0], x[1], x[2], x[3]);
+    } else {
 #pragma unroll
-    for (int u = 0; u < QPT; ++u) {
-      if (s0[u] + 3 < Mw) {
-        *reinterpret_cast<float4*>(rowB + s0[u]) = make_float4(x[u][0], x[u][1], x[u][2], x[u][3]);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (s0[u] + j < Mw) rowB[s0[u] + j] = x[u][j];
-      }
+      for (int j = 0; j < 4; ++j)
+        if (s0 + j < Mw) rowB[s0 + j] = x[j];
     }
 
     if (R.compact) {
       // flag_segregating_mutations for one population: keep unless lost or fixed (when alive), or
       // if preserved
-      unsigned c = 0;
+      unsigned keep = 0;
 #pragma unroll
-      for (int u = 0; u < QPT; ++u) {
-        unsigned keep = 0;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int e = s0[u] + j;
-          if (e >= Mw) continue;
-          // lost or fixed in the (only) population -- or the population is not alive -- removes it
-          bool kp = alive && !(x[u][j] <= 0.f || x[u][j] >= 1.f);
-          if (R.check_preserved && e < M0 && tid[e] < 0) kp = true;
-          if (kp) keep |= 1u << j;
-        }
-        // 8 consecutive threads own the 32 slots of one flag word
-        unsigned word = keep << ((lane & 7) * 4);
-        word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);
-        word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);
-        word |= __shfl_xor_sync(0xFFFFFFFFu, word, 4);
-        if ((lane & 7) == 0) flags[(R.base + s0[u]) >> 5] = word;
-        c += __popc(keep);
+      for (int j = 0; j < 4; ++j) {
+        const int e = s0 + j;
+        if (e >= Mw) continue;
+        // lost or fixed in the (only) population -- or the population is not alive -- removes it
+        bool k = alive && !(x[j] <= 0.f || x[j] >= 1.f);
+        if (R.check_preserved && e < M0 && tid[e] < 0) k = true;
+        if (k) keep |= 1u << j;
       }
+      unsigned word = keep << ((lane & 7) * 4);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 1);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 2);
+      word |= __shfl_xor_sync(0xFFFFFFFFu, word, 4);
+      if ((lane & 7) == 0) flags[(R.base + s0) >> 5] = word;
+      unsigned c = __popc(keep);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
       if (lane == 0) s_warp[threadIdx.x >> 5] = c;
@@ -301,7 +273,7 @@ __global__ void __launch_bounds__(kWinBlock, kWinMinBlocks)
       if (threadIdx.x == 0) {
         unsigned tot = 0;
 #pragma unroll
-        for (int w = 0; w < kWinBlock / 32; ++w) tot += s_warp[w];
+        for (int w = 0; w < kWinThreads / 32; ++w) tot += s_warp[w];
         tile_count[R.base / kWinTile + t] = tot;
       }
       __syncthreads();
@@ -513,7 +485,7 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
   // every B200)
   static const int occupancy = [] {
     int o = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel<DRAW, KEYS>, kWinBlock, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, window_kernel<DRAW, KEYS>, kWinThreads, 0) !=
             cudaSuccess ||
         o < 1) {
       cudaGetLastError();
@@ -524,7 +496,7 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
   const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
   const int blocks = std::max(1, std::min(w.total_tiles, e->num_sms * per_sm));
   const PhiloxKeys keys = philox_round_keys(w.seed1, w.seed2);
-  window_kernel<DRAW, KEYS><<<blocks, kWinBlock, 0, e->stream>>>(
+  window_kernel<DRAW, KEYS><<<blocks, kWinThreads, 0, e->stream>>>(
       w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count, w.M_in, w.M_end, w.M_next, w.reps, w.nreps,
       w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault, keys, w.sched);
 }
