@@ -56,6 +56,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   return true;
 }
 
+// The same, for a thread with nothing else to do meanwhile: it sleeps briefly between polls, so that
+// the warps sharing its scheduler get the issue slots.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, long long limit) {
+  const uint32_t addr = smem_u32(bar);
+  const long long t0 = clock64();
+  while (!mbar_try_wait(addr, parity)) {
+    if (clock64() - t0 > limit) return false;
+    __nanosleep(64);
+  }
+  return true;
+}
+
 // ---------------------------------------------------------------------------------------------
 // TMA: 2-D tiled load global -> shared, completion counted on an mbarrier (no multicast)
 // ---------------------------------------------------------------------------------------------

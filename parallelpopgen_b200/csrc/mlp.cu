@@ -457,8 +457,11 @@ constexpr int FF_WSTAGES = 3;
 constexpr int FF_KB_BYTES = BM * BK * 2;                  // one 128 x 64 bf16 K block of H: 16 KB
 constexpr int FF_H_BYTES = BM * HID * 2;                  // H: 128 KB
 constexpr int FF_WSTAGE_BYTES = 256 * BK * 2;             // a 256-row x 64 weight block: 32 KB
-constexpr int FF_BAR_OFFSET = FF_H_BYTES + FF_WSTAGES * FF_WSTAGE_BYTES;
-constexpr int FF_SMEM = FF_BAR_OFFSET + 256 + 1024;       // + barriers and flags, + base alignment
+constexpr int FF_BIAS_OFFSET = FF_H_BYTES + FF_WSTAGES * FF_WSTAGE_BYTES;   // the layer's bias (512 fp32)
+constexpr int FF_BAR_OFFSET = FF_BIAS_OFFSET + HID * 4;
+constexpr int FF_ALIGN_SLACK = 256;   // dynamic shared memory starts 1024-aligned when a kernel has no static
+                                      // shared memory; up to this much misalignment is absorbed, more is a fault
+constexpr int FF_SMEM = FF_BAR_OFFSET + 256 + FF_ALIGN_SLACK;   // + barriers and flags
 static_assert(FF_SMEM <= SMEM_LIMIT, "fused forward shared memory");
 constexpr int FF_STAGES_PER_TILE = 2 + 3 * 16 + 8;        // weight blocks streamed per tile (58)
 
@@ -484,8 +487,13 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
                      int batch, int m_tiles, long long wait_limit, int inject, int* fault) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  if (smem - smem_raw > FF_ALIGN_SLACK) {   // the layout would not fit (uniform over the CTA)
+    if (threadIdx.x == 0 && fault) atomicOr(fault, 1);
+    return;
+  }
   uint8_t* H = smem;
   uint8_t* W = smem + FF_H_BYTES;
+  float* s_bias = reinterpret_cast<float*>(smem + FF_BIAS_OFFSET);
   uint64_t* wfull = reinterpret_cast<uint64_t*>(smem + FF_BAR_OFFSET);
   uint64_t* wempty = wfull + FF_WSTAGES;
   uint64_t* xfull = wempty + FF_WSTAGES;   // the tile's inputs have landed in H's first K block
@@ -633,8 +641,16 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
     for (int tile = blockIdx.x; tile < m_tiles; tile += gridDim.x) {
       bool stop = false;
       for (int layer = 0; layer < GF_MLP_LAYERS; ++layer, ++accs) {
-        if (lane == 0 && !mbar_wait(accfull, accs & 1, wait_limit)) atomicOr(epi_fail, 1);
-        named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every epilogue warp has its verdict
+        // the layer's bias into shared memory while its MMAs run (the previous layer's epilogue is done
+        // with the buffer: every epilogue warp passed the barrier below before arriving on hready)
+        {
+          const float* bias = layer == 0 ? b1 : layer == 1 ? b2 : layer == 2 ? b3 : layer == 3 ? b4 : b5;
+          const int nb = layer < 4 ? HID : OUT_PAD;
+          const int et = threadIdx.x - 64;
+          if (et < nb) s_bias[et] = __ldg(bias + et);
+        }
+        if (lane == 0 && !mbar_wait_sleep(accfull, accs & 1, wait_limit)) atomicOr(epi_fail, 1);
+        named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every epilogue warp has its verdict (and the bias)
         if (*reinterpret_cast<volatile int*>(epi_fail)) {
           stop = true;
           break;
@@ -643,13 +659,19 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
         tc_fence_after();
         const uint32_t tbase = tmem + (static_cast<uint32_t>(qd * 32) << 16);
         if (layer < 4) {
-          const float* bias = layer == 0 ? b1 : layer == 1 ? b2 : layer == 2 ? b3 : b4;
 #pragma unroll 1
           for (int c0 = cg * 128; c0 < cg * 128 + 128; c0 += 32) {
             float v[32];
             tmem_ld_32cols(tbase + c0, v);
+            const float4* b4v = reinterpret_cast<const float4*>(s_bias + c0);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) v[j] = gelu(v[j] + __ldg(bias + c0 + j));
+            for (int q4 = 0; q4 < 8; ++q4) {
+              const float4 bb = b4v[q4];
+              v[4 * q4] = gelu(v[4 * q4] + bb.x);
+              v[4 * q4 + 1] = gelu(v[4 * q4 + 1] + bb.y);
+              v[4 * q4 + 2] = gelu(v[4 * q4 + 2] + bb.z);
+              v[4 * q4 + 3] = gelu(v[4 * q4 + 3] + bb.w);
+            }
             // row r, columns c0 .. c0+31 of H: K block c0 / 64, 16-byte units (c0 % 64) / 8 + q,
             // placed at unit ^ (r % 8) of the row (128-byte swizzle)
             uint8_t* rowp = H + (c0 >> 6) * FF_KB_BYTES + r * 128;
@@ -676,11 +698,11 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
             float* o = out + static_cast<long long>(grow) * GF_MLP_OUTPUTS;
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-              if (c0 + j < GF_MLP_OUTPUTS) o[c0 + j] = v[j] + __ldg(b5 + c0 + j);
+              if (c0 + j < GF_MLP_OUTPUTS) o[c0 + j] = v[j] + s_bias[c0 + j];
           }
         }
         tc_fence_before();
-        __syncwarp();
+        named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every warp is done with s_bias before it is refilled
         if (lane == 0) mbar_arrive(hready);
       }
       if (stop) {

@@ -152,8 +152,8 @@ def test_trained_network_beats_answers_without_it():
     """What the network adds over answering from the same simulated data without it: on held-out
     parameter draws, its median per-bin relative error against 16-replicate simulator means must be
     well below that of the training set's mean spectrum (one answer for every query) and that of the
-    nearest training draw's spectrum (a table lookup over the same simulations).  Measured on B200:
-    2.8 % against 84 % and 17 %."""
+    nearest training draw's spectrum (a table lookup over the same simulations).  Measured on B200 with
+    N in [500, 660]: 2.8 % against 84 % and 17 %."""
     from parallelpopgen_b200 import Engine
     from parallelpopgen_b200 import surrogate as sg
 
