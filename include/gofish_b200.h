@@ -340,7 +340,9 @@ typedef struct gf_tuning {
   int32_t draw_strategy; /* 0: each thread draws its own four lanes in order; 1: warp-cooperative draws,
                             pooled in shared memory by sampler branch; 2: each thread draws its lanes
                             grouped by sampler branch (normal approximation first, then the searches);
-                            3: the normal approximation of all four lanes at once, then the searches */
+                            3: the normal approximation of all four lanes at once, then the searches;
+                            4: the normal approximation of all four lanes in each thread, then the
+                            warp's search-branch draws pooled in shared memory and run together */
   int32_t blocks_per_sm; /* resident drift blocks per SM (0: the occupancy maximum) */
   int32_t windows;       /* 1 (default): single-population generations between compactions run as one
                             window launch; 0: one launch per generation */

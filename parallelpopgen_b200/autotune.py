@@ -29,6 +29,7 @@ LAUNCH_CANDIDATES = [
     {"draw_strategy": 1, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 2, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 3, "blocks_per_sm": 0, "windows": 1},
+    {"draw_strategy": 4, "blocks_per_sm": 0, "windows": 1},
     {"draw_strategy": 0, "blocks_per_sm": 0, "windows": 0},
     {"draw_strategy": 2, "blocks_per_sm": 0, "windows": 0},
 ]

@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
                  int* __restrict__ d_count, unsigned long long* __restrict__ stats, long long stride, int slot_in,
                  int slot_out, long long capacity, const GenArgs* __restrict__ table) {
   __shared__ GenArgs a;
-  __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kDriftThreads / 32 : 1];
+  __shared__ WarpDraws s_draws[(DRAW == kDrawWarp || DRAW == kDrawPooledSearch) ? kDriftThreads / 32 : 1];
   __shared__ unsigned s_warp[kDriftThreads / 32];
   {
     const int* src = reinterpret_cast<const int*>(table);
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kDriftThreads, kDriftMinBlocks)
   const int P = (PT > 0) ? PT : a.num_pops;
   const int g = a.generation;
   const int lane = threadIdx.x & 31;
-  WarpDraws* w = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
+  WarpDraws* w = &s_draws[(DRAW == kDrawWarp || DRAW == kDrawPooledSearch) ? (threadIdx.x >> 5) : 0];
 
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     d_count[slot_out] = total;
@@ -661,6 +661,9 @@ static void launch_drift_c(Engine* e, int tiles_bound, int slot_in, int slot_out
     case kDrawGrouped: launch_drift_t<PT, NEUTRAL, FLAG, kDrawGrouped>(e, tiles_bound, slot_in, slot_out, a); break;
     case kDrawNormalAll:
       launch_drift_t<PT, NEUTRAL, FLAG, kDrawNormalAll>(e, tiles_bound, slot_in, slot_out, a);
+      break;
+    case kDrawPooledSearch:
+      launch_drift_t<PT, NEUTRAL, FLAG, kDrawPooledSearch>(e, tiles_bound, slot_in, slot_out, a);
       break;
     default: launch_drift_t<PT, NEUTRAL, FLAG, kDrawLanes>(e, tiles_bound, slot_in, slot_out, a); break;
   }
@@ -1578,7 +1581,7 @@ gf_status gf_engine_set_tuning(gf_engine* g, const gf_tuning* t) {
     Engine* e = &g->impl;
     if (t->draw_strategy < 0 || t->draw_strategy >= kDrawStrategies || t->blocks_per_sm < 0 || t->windows < 0 ||
         t->windows > 1)
-      return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2, 3}, blocks_per_sm >= 0, windows in {0, 1}");
+      return fail(e, GF_ERR_INVALID_ARGUMENT, "tuning: draw_strategy in {0, 1, 2, 3, 4}, blocks_per_sm >= 0, windows in {0, 1}");
     e->draw_strategy = t->draw_strategy;
     e->blocks_per_sm = t->blocks_per_sm;
     e->use_windows = t->windows != 0;

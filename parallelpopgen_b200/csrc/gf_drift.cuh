@@ -82,8 +82,10 @@ enum DrawStrategy : int {
   kDrawWarp = 1,     // the warp pools its draws in shared memory and runs them branch by branch
   kDrawGrouped = 2,  // each thread draws its normal-branch lanes first, then its search-branch lanes
   kDrawNormalAll = 3,  // the normal approximation of all four lanes at once, then the search lanes
+  kDrawPooledSearch = 4,  // the normal approximation of all four lanes in each thread, then the warp's
+                          // search-branch draws pooled in shared memory and run together
 };
-constexpr int kDrawStrategies = 4;
+constexpr int kDrawStrategies = 5;
 
 // Sampler branch of a lane (binom_draw_body): the sequential searches for mean <= 6 or
 // mean >= N - 6, the normal approximation otherwise.
@@ -150,6 +152,54 @@ __device__ __forceinline__ void draw_quad(const float xs[4], const uint4 r, unsi
       if (!((need >> j) & 1u)) continue;
       res[j] = search_branch(mean[j], Nf) ? GF_LANE_DRAW(rb[j], mean[j], var[j], Nf) : nrm[j];
     }
+    return;
+  }
+  if (DRAW == kDrawPooledSearch) {
+    // Every lane of the warp calls this together.  The normal approximation of a thread's four lanes
+    // runs without branches between them; the draws that take a sequential search (means within 6
+    // of 0 or N, about one lane in five) are pooled across the warp and run 32 at a time, so the warp
+    // runs the search code about once per quad position set instead of once per lane position.  Each
+    // pooled draw calls the same sampler on the same (bits, mean, var, N) as the lane-order schedule.
+    float mean[4], var[4];
+    unsigned search = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      mean[j] = xs[j] * N;
+      var[j] = (1.0f - xs[j]) * (xs[j] * N);
+      if (((need >> j) & 1u) && search_branch(mean[j], Nf)) search |= 1u << j;
+    }
+    if (need & ~search) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int nrm = round(normcdfinv(u01(rb[j])) * sqrtf(var[j]) + mean[j]);
+        if (((need & ~search) >> j) & 1u) res[j] = nrm;
+      }
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    int nS = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const bool mine = (search >> j) & 1u;
+      const unsigned b = __ballot_sync(0xFFFFFFFFu, mine);
+      if (mine) {
+        const int k = nS + __popc(b & lt);
+        w->bits[k] = rb[j];
+        w->mean[k] = mean[j];
+        w->var[k] = var[j];
+        w->slot[k] = static_cast<unsigned char>(4 * lane + j);
+      }
+      nS += __popc(b);
+    }
+    if (nS == 0) return;   // warp-uniform
+    __syncwarp();
+    for (int k = lane; k < nS; k += 32) w->res[w->slot[k]] = GF_LANE_DRAW(w->bits[k], w->mean[k], w->var[k], Nf);
+    __syncwarp();
+    if (search) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if ((search >> j) & 1u) res[j] = w->res[4 * lane + j];
+    }
+    __syncwarp();
     return;
   }
   if (DRAW == kDrawGrouped) {

@@ -124,9 +124,9 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
   __shared__ int s_tile;
   __shared__ unsigned s_warp[kWinThreads / 32];
   __shared__ int s_tile0[kRepCache];
-  __shared__ WarpDraws s_draws[DRAW == kDrawWarp ? kWinThreads / 32 : 1];
+  __shared__ WarpDraws s_draws[(DRAW == kDrawWarp || DRAW == kDrawPooledSearch) ? kWinThreads / 32 : 1];
   const int lane = threadIdx.x & 31;
-  WarpDraws* wd = &s_draws[DRAW == kDrawWarp ? (threadIdx.x >> 5) : 0];
+  WarpDraws* wd = &s_draws[(DRAW == kDrawWarp || DRAW == kDrawPooledSearch) ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
   load_tile0(s_tile0, reps, nreps);
   // Tiles are handed out in order by an atomic counter, so a block that drew cheap tiles (slots born
@@ -201,8 +201,8 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
           if (KEYS) r = philox4x32_10_keys(make_uint4(static_cast<uint32_t>(q + 2), static_cast<uint32_t>(g), 0u, 0u), keys);
           else r = philox(R.seed1, R.seed2, q + 2, g, 0, 0);
         }
-        if (DRAW == kDrawWarp) {
-          draw_quad<kDrawWarp>(xs, r, need, N, lane, wd, res);
+        if (DRAW == kDrawWarp || DRAW == kDrawPooledSearch) {
+          draw_quad<DRAW>(xs, r, need, N, lane, wd, res);   // every lane of the warp calls it
         } else if (need) {
           draw_quad<DRAW>(xs, r, need, N, lane, wd, res);
         }
@@ -505,12 +505,17 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
 // and scatter into `compact_dst` (the other state buffer).
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaEvent_t after_window,
                      cudaEvent_t before_compaction) {
+  const bool keys = GF_WINDOW_UNIFORM_KEYS && w.uniform_key && w.nreps == 1;
   switch (e->draw_strategy) {
     case kDrawWarp: launch_window_kernel<kDrawWarp, false>(e, w); break;
     case kDrawGrouped: launch_window_kernel<kDrawGrouped, false>(e, w); break;
     case kDrawNormalAll: launch_window_kernel<kDrawNormalAll, false>(e, w); break;
+    case kDrawPooledSearch:
+      if (keys) launch_window_kernel<kDrawPooledSearch, true>(e, w);
+      else launch_window_kernel<kDrawPooledSearch, false>(e, w);
+      break;
     default:
-      if (GF_WINDOW_UNIFORM_KEYS && w.uniform_key && w.nreps == 1) launch_window_kernel<kDrawLanes, true>(e, w);
+      if (keys) launch_window_kernel<kDrawLanes, true>(e, w);
       else launch_window_kernel<kDrawLanes, false>(e, w);
       break;
   }

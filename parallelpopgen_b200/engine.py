@@ -131,7 +131,8 @@ class Engine:
     def set_tuning(self, draw_strategy: int = 0, blocks_per_sm: int = 0, windows: int = 1) -> None:
         """Launch choices that never change results (gf_engine_set_tuning): draw_strategy 0 = each thread
         draws its lanes in order, 1 = warp-pooled draws, 2 = a thread's lanes grouped by sampler branch,
-        3 = the normal approximation of a quad's lanes first; blocks_per_sm caps the resident drift
+        3 = the normal approximation of a quad's lanes first, 4 = the normal approximation per thread
+        and the warp's search draws pooled; blocks_per_sm caps the resident drift
         blocks (0 = occupancy maximum); windows = 0 runs one launch per generation."""
         t = _capi.Tuning(int(draw_strategy), int(blocks_per_sm), int(windows))
         self._check(self.lib.gf_engine_set_tuning(self.h, ctypes.byref(t)))

@@ -357,8 +357,9 @@ def test_window_path_equals_per_generation_path(gamma, ci, mse):
 
 @pytest.mark.parametrize("pops", [1, 3])
 def test_draw_strategies_agree(pops):
-    """The four draw schedules (lane order, warp-pooled, grouped by sampler branch, normal
-    approximation of all lanes first) call the same sampler on the same inputs, so window and per-generation runs, single- and multi-population,
+    """The five draw schedules (lane order, warp-pooled, grouped by sampler branch, normal
+    approximation of all lanes first, normal approximation per thread with the search draws pooled
+    per warp) call the same sampler on the same inputs, so window and per-generation runs, single- and multi-population,
     give the same state bit for bit under every one of them."""
     N = 4000
     if pops == 1:
@@ -367,7 +368,7 @@ def test_draw_strategies_agree(pops):
         model = ConstantModel(N=N, s=ConstantModel.s_from_gamma(-4.0, N, 0.0), mu=2e-8, h=0.3, P=3, m=0.01)
     gens = constant_generations(model, 1, 200, 25)
     out = []
-    for strategy in (0, 1, 2, 3):
+    for strategy in (0, 1, 2, 3, 4):
         for windows in ((1, 0) if pops == 1 else (1,)):
             with Engine() as e:
                 e.set_tuning(draw_strategy=strategy, windows=windows)
