@@ -77,11 +77,13 @@ struct SFS {
 
  private:
   /* floats in frequency_spectrum: the sample size of a single population's spectrum or histogram,
-   * (n_a + 1)(n_b + 1) for a joint spectrum of two populations */
+   * the product of (n + 1) over the populations of a joint spectrum */
   size_t bins() const {
     if (!sample_size || num_populations <= 0) return 0;
     if (num_populations == 1) return static_cast<size_t>(sample_size[0]);
-    return static_cast<size_t>(sample_size[0] + 1) * static_cast<size_t>(sample_size[1] + 1);
+    size_t b = 1;
+    for (int i = 0; i < num_populations; ++i) b *= static_cast<size_t>(sample_size[i] + 1);
+    return b;
   }
 };
 
@@ -232,6 +234,56 @@ inline void joint_site_frequency_spectrum(SFS& mySFS, const GO_Fish::allele_traj
   mySFS.populations = new int[2];
   mySFS.populations[0] = population_a;
   mySFS.populations[1] = population_b;
+  mySFS.sampled_generation = generation;
+}
+
+/* Joint SFS of populations a, b and c at one time sample (the same extension):
+ * frequency_spectrum[(i * (n_b + 1) + j) * (n_c + 1) + k] = expected number of sites with i, j and k
+ * derived copies in samples of n_a, n_b and n_c from populations a, b and c, plus the monomorphic sites
+ * at (0, 0, 0).  Requires 1 <= n < Nchrom_e for each population, n <= 1023 and
+ * (n_a + 1)(n_b + 1)(n_c + 1) <= 2^24. */
+inline void joint_site_frequency_spectrum(SFS& mySFS, const GO_Fish::allele_trajectories& all_results,
+                                          const int sample_index, const int population_a, const int population_b,
+                                          const int population_c, const int sample_size_a, const int sample_size_b,
+                                          const int sample_size_c, int cuda_device = -1) {
+  GO_Fish::allele_trajectories& a = const_cast<GO_Fish::allele_trajectories&>(all_results);
+  const float *fa, *fb, *fc;
+  int M, Nca, Ncb, Ncc, generation;
+  float L;
+  gofish_detail::spectrum_access::row(a, sample_index, population_a, &fa, &M, &Nca, &generation, &L);
+  gofish_detail::spectrum_access::row(a, sample_index, population_b, &fb, &M, &Ncb, &generation, &L);
+  gofish_detail::spectrum_access::row(a, sample_index, population_c, &fc, &M, &Ncc, &generation, &L);
+  if (sample_size_a <= 0 || sample_size_a >= Nca || sample_size_b <= 0 || sample_size_b >= Ncb || sample_size_c <= 0 ||
+      sample_size_c >= Ncc) {
+    std::fprintf(stderr,
+                 "joint_site_frequency_spectrum error: requested sample sizes out of range: %d [1,%d), %d [1,%d), "
+                 "%d [1,%d)\n",
+                 sample_size_a, Nca, sample_size_b, Ncb, sample_size_c, Ncc);
+    std::exit(1);
+  }
+  gf_engine* e = gofish_detail::spectrum_engine(cuda_device);
+  const size_t bins = static_cast<size_t>(sample_size_a + 1) * (sample_size_b + 1) * (sample_size_c + 1);
+  float* h = new float[bins];
+  const gf_status st =
+      gf_joint3_site_frequency_spectrum(e, fa, fb, fc, M, sample_size_a, sample_size_b, sample_size_c, L, h);
+  if (st != GF_OK) {
+    delete[] h;
+    std::fprintf(stderr, "joint_site_frequency_spectrum error: %s\n", gf_engine_last_error(e));
+    std::exit(1);
+  }
+  mySFS.clear();
+  mySFS.frequency_spectrum = h;
+  mySFS.num_populations = 3;
+  mySFS.sample_size = new int[3];
+  mySFS.sample_size[0] = sample_size_a;
+  mySFS.sample_size[1] = sample_size_b;
+  mySFS.sample_size[2] = sample_size_c;
+  mySFS.num_sites = L;
+  mySFS.num_mutations = mySFS.num_sites - mySFS.frequency_spectrum[0];
+  mySFS.populations = new int[3];
+  mySFS.populations[0] = population_a;
+  mySFS.populations[1] = population_b;
+  mySFS.populations[2] = population_c;
   mySFS.sampled_generation = generation;
 }
 

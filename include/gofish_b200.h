@@ -335,6 +335,20 @@ gf_status gf_joint_site_frequency_spectrum_device(gf_engine* engine, const float
                                                   int32_t num_mutations, int32_t n_a, int32_t n_b,
                                                   float num_sites, float* d_out);
 
+/* Joint SFS of three populations (the same extension): out[(i * (n_b + 1) + j) * (n_c + 1) + k] =
+ * expected number of sites whose samples of n_a, n_b and n_c chromosomes from populations a, b and c
+ * hold i, j and k derived copies, each mutation contributing the product of its three binomial
+ * projections; the num_sites - M monomorphic sites go to (0, 0, 0).  Summed over k it is the joint SFS
+ * of a and b.  1 <= n_a, n_b, n_c <= 1023 and (n_a + 1)(n_b + 1)(n_c + 1) <= 2^24 bins (larger:
+ * GF_ERR_CAPACITY).  Computed in double, deterministic; the _device variant takes device pointers and
+ * runs asynchronously. */
+gf_status gf_joint3_site_frequency_spectrum(gf_engine* engine, const float* freq_a, const float* freq_b,
+                                            const float* freq_c, int32_t num_mutations, int32_t n_a, int32_t n_b,
+                                            int32_t n_c, float num_sites, float* out);
+gf_status gf_joint3_site_frequency_spectrum_device(gf_engine* engine, const float* d_freq_a, const float* d_freq_b,
+                                                   const float* d_freq_c, int32_t num_mutations, int32_t n_a,
+                                                   int32_t n_b, int32_t n_c, float num_sites, float* d_out);
+
 /* Launch choices of the drift pass (results do not depend on them). */
 typedef struct gf_tuning {
   int32_t draw_strategy; /* 0: each thread draws its own four lanes in order; 1: warp-cooperative draws,

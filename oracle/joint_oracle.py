@@ -1,5 +1,5 @@
-"""CPU restatement of the joint (two-population) SFS projection.  TEST INFRASTRUCTURE ONLY: imported by
-tests/ to check the GPU path, never by the product.
+"""CPU restatement of the joint (two- and three-population) SFS projection.  TEST INFRASTRUCTURE ONLY:
+imported by tests/ to check the GPU path, never by the product.
 
 The reference projects one population's frequency p onto a sample of n as C(n,k) p^k (1-p)^(n-k)
 (spectrum.cu:90-139, binom_coeff and binom); the joint form multiplies the two populations'
@@ -34,4 +34,16 @@ def joint_sfs(freq_a: np.ndarray, freq_b: np.ndarray, n_a: int, n_b: int, num_si
     B = sample_pmf(np.asarray(freq_b, dtype=np.float32), n_b)
     out = A.T @ B
     out[0, 0] += float(np.float32(num_sites)) - len(freq_a)
+    return out
+
+
+def joint3_sfs(freq_a: np.ndarray, freq_b: np.ndarray, freq_c: np.ndarray, n_a: int, n_b: int, n_c: int,
+               num_sites: float) -> np.ndarray:
+    """[n_a + 1][n_b + 1][n_c + 1] expected joint SFS of three populations (float64): every mutation
+    contributes the product of its three projections; the num_sites - M monomorphic sites go to (0, 0, 0)."""
+    A = sample_pmf(np.asarray(freq_a, dtype=np.float32), n_a)
+    B = sample_pmf(np.asarray(freq_b, dtype=np.float32), n_b)
+    C = sample_pmf(np.asarray(freq_c, dtype=np.float32), n_c)
+    out = np.einsum("mi,mj,mk->ijk", A, B, C, optimize=True)
+    out[0, 0, 0] += float(np.float32(num_sites)) - len(freq_a)
     return out

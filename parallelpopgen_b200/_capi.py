@@ -118,6 +118,8 @@ SIGNATURES = {
     "gf_sim_stats_read": (_I, [_P, ctypes.POINTER(SimStats)]),
     "gf_joint_site_frequency_spectrum": (_I, [_P, _P, _P, _I, _I, _I, _F, _P]),
     "gf_joint_site_frequency_spectrum_device": (_I, [_P, _P, _P, _I, _I, _I, _F, _P]),
+    "gf_joint3_site_frequency_spectrum": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _F, _P]),
+    "gf_joint3_site_frequency_spectrum_device": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _F, _P]),
     "gf_replicate_population": (_I, [ctypes.POINTER(Replicate), _I]),
     "gf_replicate_population_table": (None, [ctypes.POINTER(Replicate), _I, _I, _P]),
     "gf_batch_begin": (_I, [_P, _P, _I]),

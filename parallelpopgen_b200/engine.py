@@ -216,6 +216,19 @@ class Engine:
                                                               float(num_sites), ptr(out)))
         return out
 
+    def joint3_site_frequency_spectrum(self, freq_a: np.ndarray, freq_b: np.ndarray, freq_c: np.ndarray, n_a: int,
+                                       n_b: int, n_c: int, num_sites: float) -> np.ndarray:
+        """Expected joint SFS [n_a + 1][n_b + 1][n_c + 1] of three populations' rows of the same mutations."""
+        fa = np.ascontiguousarray(freq_a, dtype=np.float32)
+        fb = np.ascontiguousarray(freq_b, dtype=np.float32)
+        fc = np.ascontiguousarray(freq_c, dtype=np.float32)
+        if fa.shape != fb.shape or fa.shape != fc.shape:
+            raise ValueError("the three rows must hold the same mutations")
+        out = np.empty((n_a + 1, n_b + 1, n_c + 1), dtype=np.float32)
+        self._check(self.lib.gf_joint3_site_frequency_spectrum(self.h, ptr(fa), ptr(fb), ptr(fc), len(fa), int(n_a),
+                                                               int(n_b), int(n_c), float(num_sites), ptr(out)))
+        return out
+
     def joint_site_frequency_spectrum_device(self, d_freq_a: int, d_freq_b: int, M: int, n_a: int, n_b: int,
                                              num_sites: float, d_out: int) -> None:
         self._check(self.lib.gf_joint_site_frequency_spectrum_device(

@@ -169,7 +169,14 @@ inline void scenario_wf(GO_Fish::allele_trajectories& a, const Args& args,
   } else if (sine_A != 0.f) {
     selection_sine_wave selection(sine_A, static_cast<float>(args.num("sine_pi", 0.05)), gamma, demography, inbreeding,
                                   static_cast<float>(args.num("sine_rho", 0.0)));
-    run_wf(a, args, prev, mutation, demography, migration, selection, inbreeding, dominance);
+    const int sine_pop = static_cast<int>(args.integer("sine_pop", -1));
+    if (sine_pop >= 0) {  // seasonal selection in one population, constant in the others
+      selection_population_specific<selection_constant, selection_sine_wave> specific(
+          selection_constant(gamma, demography, inbreeding), selection, sine_pop);
+      run_wf(a, args, prev, mutation, demography, migration, specific, inbreeding, dominance);
+    } else {
+      run_wf(a, args, prev, mutation, demography, migration, selection, inbreeding, dominance);
+    }
   } else {
     selection_constant selection(gamma, demography, inbreeding);
     run_wf(a, args, prev, mutation, demography, migration, selection, inbreeding, dominance);
@@ -317,6 +324,21 @@ inline void scenario_multipop(GO_Fish::allele_trajectories& a, const Args& args,
       static_cast<int>(args.integer("switch_gen", 3000)));
   F_mu_h_constant dominance(static_cast<float>(args.num("h", 0.3)));
   every_k sample(static_cast<int>(args.integer("sample_every", 500)), 0);
+  const float quad_a = static_cast<float>(args.num("quad_a", 0.0));
+  if (quad_a != 0.f) {
+    // the user model s(x) = quad_a / 2N0 x^2 + gamma1 / 2N0 in every population (continuations only:
+    // the equilibrium start integrates affine models)
+    const float twoN = 2.f * static_cast<float>(dem.N0);
+    quadratic_selection user = {quad_a / twoN, static_cast<float>(args.num("gamma1", -5.0)) / twoN};
+    if (prev) {
+      a.sim_input_constants.init_mse = false;
+      a.sim_input_constants.prev_sim_sample = 0;
+      GO_Fish::run_sim(a, mutation, dem, mig, user, inbreeding, dominance, bool_off(), sample, *prev);
+    } else {
+      GO_Fish::run_sim(a, mutation, dem, mig, user, inbreeding, dominance, bool_off(), sample);
+    }
+    return;
+  }
   if (prev) {
     a.sim_input_constants.init_mse = false;
     a.sim_input_constants.prev_sim_sample = 0;

@@ -145,6 +145,9 @@ def test_cfg1_neutral_matches_reference(gofish_driver, ref_driver, tmp_path):
     ["pops=2", "m=0.01", "mse=1", "gens=500"],
     # seasonal selection: the sine is evaluated on the device, as the reference's kernel evaluates it
     ["sine_A=20", "sine_pi=0.05", "sine_rho=0.3", "gamma=-2", "mse=0", "gens=2000", "compact=25"],
+    # ... in one of two populations exchanging migrants (selection_population_specific around it)
+    ["sine_A=-30", "sine_pi=0.02", "gamma=1", "sine_pop=1", "pops=2", "m=0.005", "mse=0", "gens=1500",
+     "compact=30"],
 ])
 def test_wf_variants_match_reference(gofish_driver, ref_driver, tmp_path, extra):
     args = ["N=5000", "L=1e7", "sfs_n=50", "hist=1", "sample_every=0", *extra]
@@ -167,6 +170,22 @@ def test_user_device_selection_functor_matches_reference(gofish_driver_nvcc, ref
     subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *args], check=True, capture_output=True)
     ref = Dump(tmp_path / "ref.bin")
     assert ref.samples[-1]["M"] > 1000
+    assert_dumps_equal(mine, ref)
+
+
+def test_user_device_selection_functor_three_populations(gofish_driver_nvcc, ref_driver, tmp_path):
+    """The device-evaluated user functor with three populations exchanging migrants (the benchmark's
+    three-population model after its last founding, continued from one stored state for 300
+    generations): x_mig mixes three rows before the functor sees it."""
+    start = tmp_path / "start.bin"
+    run_driver(gofish_driver_nvcc, "multipop", tmp_path / "stage1.bin", ["gens=2100", "sample_every=0", "L=5e7",
+                                                                         f"state_out={start}"])
+    args = ["gens=300", "sample_every=0", "L=5e7", "quad_a=-60", "sfs_n=100", "hist=1", f"state_in={start}"]
+    mine = run_driver(gofish_driver_nvcc, "multipop", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "multipop", str(tmp_path / "ref.bin"), *args], check=True,
+                   capture_output=True)
+    ref = Dump(tmp_path / "ref.bin")
+    assert ref.samples[-1]["generation"] == 2400 and ref.samples[-1]["M"] > 100_000
     assert_dumps_equal(mine, ref)
 
 

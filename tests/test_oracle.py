@@ -179,3 +179,27 @@ def test_joint_oracle_matches_brute_force():
     got = joint_sfs(fa, fb, na, nb, L)
     np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
     assert abs(got.sum() - L) < 1e-9
+
+
+def test_joint3_oracle_matches_brute_force():
+    """The three-population joint-SFS restatement against an explicit loop."""
+    import math
+    from oracle.joint_oracle import joint3_sfs
+    rng = np.random.default_rng(9)
+    Nc = 40
+    f = [(rng.integers(0, Nc + 1, 25) / Nc).astype(np.float32) for _ in range(3)]
+    n, L = (3, 4, 2), 500.0
+    want = np.zeros((n[0] + 1, n[1] + 1, n[2] + 1))
+    want[0, 0, 0] = L - 25
+
+    def pmf(p, n_, k):
+        return math.comb(n_, k) * p ** k * (1 - p) ** (n_ - k)
+
+    for pa, pb, pc in zip(*(x.astype(np.float64) for x in f)):
+        for i in range(n[0] + 1):
+            for j in range(n[1] + 1):
+                for k in range(n[2] + 1):
+                    want[i, j, k] += pmf(pa, n[0], i) * pmf(pb, n[1], j) * pmf(pc, n[2], k)
+    got = joint3_sfs(*f, *n, L)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+    assert abs(got.sum() - L) < 1e-9
