@@ -113,9 +113,13 @@ __device__ __forceinline__ float tanh_hw(float x) {
   return y;
 }
 
+// Written as tanh(z (c + c a z^2)) and (z/2) t + z/2: six instructions, one of them on the MUFU pipe.
+// The fused forward's epilogue is bound by instruction issue, and this form issues two fewer than
+// c (z + a z^3) and (z/2)(1 + t).
 __device__ __forceinline__ float gelu(float z) {
-  const float t = tanh_hw(GELU_C * fmaf(GELU_A * z, z * z, z));
-  return 0.5f * z * (1.f + t);
+  const float t = tanh_hw(z * fmaf(GELU_C * GELU_A, z * z, GELU_C));
+  const float hz = 0.5f * z;
+  return fmaf(hz, t, hz);
 }
 
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -443,13 +447,16 @@ umma_gemm_kernel(const __grid_constant__ CUtensorMap tma_a, const __grid_constan
 // The layered path writes each hidden activation (batch x 512 bf16) to memory and reads it back in
 // the next layer's GEMM.  Here a CTA keeps its tile's activation H (128 x 512 bf16 = 128 KB) in
 // shared memory, in the 128-byte-swizzled K-major layout the MMA reads (eight 64-column K blocks of
-// 16 KB), and the layer's fp32 accumulator (128 x 512) in all 512 tensor-memory columns.  Per layer:
-// warp 1 issues the MMAs (A = H from shared memory, B = weight K-blocks streamed by warp 0's TMA
-// through a 3-stage ring from L2, where every CTA finds the 1.3 MB of weights), then 16 epilogue
-// warps drain the accumulator (bias, GELU, bf16) back into H for the next layer; the last layer's
-// epilogue writes acc + bias to the caller's [batch][99] array.  Each layer's MMAs run in the order
-// of the layered GEMMs (N halves of 256, K blocks 0..7, four 16-wide slices each; layer 5 one
-// 128-wide N tile), so the outputs are bit-identical to the layered path.
+// 16 KB), and the layer's fp32 accumulator (128 x 512) in all 512 tensor-memory columns: N half 0
+// in region A (columns 0-255), N half 1 in region B (256-511).  Warp 1 issues the MMAs (A = H from
+// shared memory, B = weight K-blocks streamed by warp 0's TMA through a 3-stage ring from L2, where
+// every CTA finds the 1.3 MB of weights); 16 epilogue warps drain the accumulators (bias, GELU, bf16)
+// back into H for the next layer, overlapped with the MMAs: region A while N half 1 accumulates
+// (staged in tensor memory, since H is still being read), region B while the next layer's first
+// K blocks accumulate.  The last layer's epilogue writes acc + bias to the caller's [batch][99]
+// array.  Each layer's MMAs run in the order of the layered GEMMs (N halves of 256, K blocks 0..7,
+// four 16-wide slices each; layer 5 one 128-wide N tile), so the outputs are bit-identical to the
+// layered path.
 // ---------------------------------------------------------------------------------------------
 constexpr int FF_EPI_WARPS = 16;                          // four per tensor-memory lane quarter
 constexpr int FF_THREADS = 64 + 32 * FF_EPI_WARPS;        // TMA warp, MMA warp, 16 epilogue warps
@@ -464,6 +471,8 @@ constexpr int FF_ALIGN_SLACK = 256;   // dynamic shared memory starts 1024-align
 constexpr int FF_SMEM = FF_BAR_OFFSET + 256 + FF_ALIGN_SLACK;   // + barriers and flags
 static_assert(FF_SMEM <= SMEM_LIMIT, "fused forward shared memory");
 constexpr int FF_STAGES_PER_TILE = 2 + 3 * 16 + 8;        // weight blocks streamed per tile (58)
+constexpr int kFfStoreThread = 64;                         // the epilogue thread that issues the output stores
+static_assert(BM * GF_MLP_OUTPUTS * 4 <= 4 * FF_KB_BYTES, "staged outputs fit in H's K blocks 1-4");
 
 // Weight block `i` of a tile's stream: layer, the N offset of its rows, the K block, its rows.
 struct FfBlock {
@@ -497,9 +506,11 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
   uint64_t* wfull = reinterpret_cast<uint64_t*>(smem + FF_BAR_OFFSET);
   uint64_t* wempty = wfull + FF_WSTAGES;
   uint64_t* xfull = wempty + FF_WSTAGES;   // the tile's inputs have landed in H's first K block
-  uint64_t* accfull = xfull + 1;           // a layer's accumulator is complete (MMA -> epilogue)
-  uint64_t* hready = accfull + 1;          // H written and the accumulator drained (epilogue -> MMA)
-  uint64_t* hfree = hready + 1;            // the tile's last MMAs have read H (MMA -> producer)
+  uint64_t* accA = xfull + 1;              // N half 0 (region A) accumulated (MMA -> epilogue)
+  uint64_t* accB = accA + 1;               // N half 1 (region B) accumulated: the layer's MMAs are done
+  uint64_t* hlo = accB + 1;                // H's K blocks 0-3 written, region A drained (epilogue -> MMA)
+  uint64_t* hhi = hlo + 1;                 // H's K blocks 4-7 written, region B drained (epilogue -> MMA)
+  uint64_t* hfree = hhi + 1;               // the tile's last MMAs have read H (MMA -> producer)
   uint64_t* drain = hfree + 1;             // MMA completion before tensor memory is released (abort)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   int* flags = reinterpret_cast<int*>(tmem_slot + 1);
@@ -530,8 +541,10 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
       mbar_init(&wempty[s], 1);
     }
     mbar_init(xfull, 1);
-    mbar_init(accfull, 1);
-    mbar_init(hready, FF_EPI_WARPS);
+    mbar_init(accA, 1);
+    mbar_init(accB, 1);
+    mbar_init(hlo, FF_EPI_WARPS);
+    mbar_init(hhi, FF_EPI_WARPS);
     mbar_init(hfree, 1);
     mbar_init(drain, 1);
     flags[0] = flags[1] = flags[2] = flags[3] = 0;
@@ -584,8 +597,24 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
     if (lane == 0) {
       constexpr uint32_t idesc256 = bf16_idesc(BM, 256);
       constexpr uint32_t idesc128 = bf16_idesc(BM, OUT_PAD);
-      int it = 0, local = 0, hwaits = 0, xs = 0;
+      int it = 0, local = 0, lo_waits = 0, hi_waits = 0, xs = 0;
       const uint32_t h_addr = smem_u32(H);
+      // the four MMAs of weight block i of the tile's stream (ring slot it % 3): A = H's K block
+      auto stage = [&](int i, uint32_t d, uint32_t idesc) -> bool {
+        const int s = it % FF_WSTAGES;
+        if (!wait(&wfull[s], (it / FF_WSTAGES) & 1)) return false;
+        tc_fence_after();
+        const FfBlock blk = ff_block(i);
+        const uint32_t w_addr = smem_u32(W + s * FF_WSTAGE_BYTES);
+        const uint32_t a_addr = h_addr + blk.kb * FF_KB_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk)
+          umma_bf16(d, sw128_kmajor_desc(a_addr + kk * 32), sw128_kmajor_desc(w_addr + kk * 32), idesc,
+                    (blk.kb | kk) != 0);
+        umma_commit(&wempty[s]);
+        ++it;
+        return true;
+      };
       for (int tile = blockIdx.x; tile < m_tiles && !late; tile += gridDim.x, ++local) {
         if (!wait(xfull, local & 1)) {
           late = true;
@@ -594,36 +623,40 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
         ++xs;
         int i = 0;
         for (int layer = 0; layer < GF_MLP_LAYERS; ++layer) {
-          // H holds this layer's input and the accumulator has been drained (not before the very first)
+          // region A drained (by the previous layer's staging copy, or the previous tile's output) and,
+          // from the second layer on, H's K blocks 0-3 written
           if (local > 0 || layer > 0) {
-            if (!wait(hready, hwaits & 1)) {
+            if (!wait(hlo, lo_waits & 1)) {
               late = true;
               break;
             }
-            ++hwaits;
+            ++lo_waits;
           }
           tc_fence_after();
-          const int nblocks = layer == 0 ? 2 : layer < 4 ? 16 : 8;
-          for (int b = 0; b < nblocks; ++b, ++i, ++it) {
-            const int s = it % FF_WSTAGES;
-            if (!wait(&wfull[s], (it / FF_WSTAGES) & 1)) {
-              late = true;
-              break;
+          const int kblocks = layer == 0 ? 1 : 8;
+          // N half 0 (the output layer's only N tile) into region A; K blocks 4-7 once H's K blocks 4-7
+          // are written (which also means region B is drained)
+          for (int kb = 0; kb < kblocks && !late; ++kb, ++i) {
+            if (kb == 4) {
+              if (!wait(hhi, hi_waits & 1)) {
+                late = true;
+                break;
+              }
+              ++hi_waits;
+              tc_fence_after();
             }
-            tc_fence_after();
-            const FfBlock blk = ff_block(i);
-            const uint32_t w_addr = smem_u32(W + s * FF_WSTAGE_BYTES);
-            const uint32_t a_addr = h_addr + blk.kb * FF_KB_BYTES;
-            const uint32_t d = tmem + static_cast<uint32_t>(blk.n0);
-#pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk)
-              umma_bf16(d, sw128_kmajor_desc(a_addr + kk * 32), sw128_kmajor_desc(w_addr + kk * 32),
-                        layer == 4 ? idesc128 : idesc256, (blk.kb | kk) != 0);
-            umma_commit(&wempty[s]);
+            if (!stage(i, tmem, layer == 4 ? idesc128 : idesc256)) late = true;
           }
           if (late) break;
           // fault injection for tests: withhold the first accumulator hand-off
-          if (!((inject & 1) && local == 0 && layer == 0)) umma_commit(accfull);
+          if (!((inject & 1) && local == 0 && layer == 0)) umma_commit(accA);
+          if (layer < 4) {
+            // N half 1 into region B, while the epilogue drains region A
+            for (int kb = 0; kb < kblocks && !late; ++kb, ++i)
+              if (!stage(i, tmem + 256, idesc256)) late = true;
+            if (late) break;
+            umma_commit(accB);   // also: every MMA of the layer has read H
+          }
         }
         if (late) break;
         umma_commit(hfree);
@@ -633,83 +666,149 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
     }
     __syncwarp();
   } else {
-    // ---- epilogue: lane quarter qd of tensor memory, column group cg of the layer's outputs ----
+    // ---- epilogue: lane quarter qd of tensor memory, column group cg of each N half ----
+    // A hidden layer's N half 0 (region A, tensor-memory columns 0-255) is drained while the MMAs of
+    // N half 1 run: bias + GELU, rounded to bf16 pairs and stored back into the first half of the
+    // warp's own region-A columns (H is still being read).  Once every MMA of the layer is done, the
+    // staged half is copied into H's K blocks 0-3, which releases region A and lets the next layer's
+    // MMAs start on K blocks 0-3 while N half 1 (region B) is drained straight into K blocks 4-7.
     const int qd = warp & 3;
     const int cg = (warp - 2) >> 2;
     const int r = qd * 32 + lane;                 // row within the tile
-    int accs = 0;
+    float* s_out = reinterpret_cast<float*>(H + FF_KB_BYTES);   // the last layer's staged outputs
+    const uint32_t tlane = tmem + (static_cast<uint32_t>(qd * 32) << 16);
+    int a_waits = 0, b_waits = 0;
+    // lane 0 of each warp waits for the MMA hand-off; every epilogue warp then learns the joint verdict
+    auto handoff = [&](uint64_t* bar, int& n, bool store_read) -> bool {
+      if (lane == 0 && !mbar_wait_sleep(bar, n & 1, wait_limit)) atomicOr(epi_fail, 1);
+      ++n;
+      // the previous tile's output store has read its staging rows before this tile writes H
+      if (store_read && threadIdx.x == kFfStoreThread) bulk_wait_read<0>();
+      named_barrier_sync(4, 32 * FF_EPI_WARPS);
+      if (*reinterpret_cast<volatile int*>(epi_fail)) return false;
+      __syncwarp();
+      tc_fence_after();
+      return true;
+    };
+    // bias + GELU of the 32 accumulator columns at tensor-memory column tcol (output columns c0 ..
+    // c0 + 31), rounded to 16 bf16 pairs
+    auto gelu_pack = [&](uint32_t tcol, int c0, uint32_t (&w)[16]) {
+      float v[32];
+      tmem_ld_32cols(tlane + tcol, v);
+      const float4* b4v = reinterpret_cast<const float4*>(s_bias + c0);
+#pragma unroll
+      for (int q4 = 0; q4 < 8; ++q4) {
+        const float4 bb = b4v[q4];
+        v[4 * q4] = gelu(v[4 * q4] + bb.x);
+        v[4 * q4 + 1] = gelu(v[4 * q4 + 1] + bb.y);
+        v[4 * q4 + 2] = gelu(v[4 * q4 + 2] + bb.z);
+        v[4 * q4 + 3] = gelu(v[4 * q4 + 3] + bb.w);
+      }
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        __nv_bfloat162 pr = __floats2bfloat162_rn(v[2 * t], v[2 * t + 1]);
+        w[t] = *reinterpret_cast<uint32_t*>(&pr);
+      }
+    };
+    // row r, output columns c0 .. c0+31 of H: K block c0 / 64, 16-byte units (c0 % 64) / 8 + q, placed
+    // at unit ^ (r % 8) of the row (128-byte swizzle)
+    auto store_h = [&](int c0, const uint32_t (&w)[16]) {
+      uint8_t* rowp = H + (c0 >> 6) * FF_KB_BYTES + r * 128;
+      const int u0 = (c0 & 63) >> 3;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        *reinterpret_cast<uint4*>(rowp + (((u0 + q) ^ (r & 7)) << 4)) =
+            make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    };
     for (int tile = blockIdx.x; tile < m_tiles; tile += gridDim.x) {
       bool stop = false;
-      for (int layer = 0; layer < GF_MLP_LAYERS; ++layer, ++accs) {
-        // the layer's bias into shared memory while its MMAs run (the previous layer's epilogue is done
-        // with the buffer: every epilogue warp passed the barrier below before arriving on hready)
+      for (int layer = 0; layer < GF_MLP_LAYERS; ++layer) {
+        // the layer's bias into shared memory while its MMAs run (every epilogue warp passed the
+        // barrier at the end of the previous layer, so the buffer is free)
         {
           const float* bias = layer == 0 ? b1 : layer == 1 ? b2 : layer == 2 ? b3 : layer == 3 ? b4 : b5;
           const int nb = layer < 4 ? HID : OUT_PAD;
           const int et = threadIdx.x - 64;
           if (et < nb) s_bias[et] = __ldg(bias + et);
         }
-        if (lane == 0 && !mbar_wait_sleep(accfull, accs & 1, wait_limit)) atomicOr(epi_fail, 1);
-        named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every epilogue warp has its verdict (and the bias)
-        if (*reinterpret_cast<volatile int*>(epi_fail)) {
+        if (!handoff(accA, a_waits, false)) {
           stop = true;
           break;
         }
-        __syncwarp();
-        tc_fence_after();
-        const uint32_t tbase = tmem + (static_cast<uint32_t>(qd * 32) << 16);
         if (layer < 4) {
+          // N half 0: output columns cg*64 .. cg*64+63, staged as bf16 pairs in tensor-memory columns
+          // cg*64 .. cg*64+31 (each chunk's pairs land on columns this warp has already read)
 #pragma unroll 1
-          for (int c0 = cg * 128; c0 < cg * 128 + 128; c0 += 32) {
+          for (int h = 0; h < 2; ++h) {
+            uint32_t w[16];
+            gelu_pack(cg * 64 + 32 * h, cg * 64 + 32 * h, w);
+            tmem_st_16cols(tlane + cg * 64 + 16 * h, w);
+          }
+          tmem_st_wait();
+          if (!handoff(accB, b_waits, layer == 0)) {   // every MMA of the layer is done with H
+            stop = true;
+            break;
+          }
+          {
             float v[32];
-            tmem_ld_32cols(tbase + c0, v);
-            const float4* b4v = reinterpret_cast<const float4*>(s_bias + c0);
+            tmem_ld_32cols(tlane + cg * 64, v);
+            uint32_t w0[16], w1[16];
 #pragma unroll
-            for (int q4 = 0; q4 < 8; ++q4) {
-              const float4 bb = b4v[q4];
-              v[4 * q4] = gelu(v[4 * q4] + bb.x);
-              v[4 * q4 + 1] = gelu(v[4 * q4 + 1] + bb.y);
-              v[4 * q4 + 2] = gelu(v[4 * q4 + 2] + bb.z);
-              v[4 * q4 + 3] = gelu(v[4 * q4 + 3] + bb.w);
+            for (int j = 0; j < 16; ++j) {
+              w0[j] = __float_as_uint(v[j]);
+              w1[j] = __float_as_uint(v[16 + j]);
             }
-            // row r, columns c0 .. c0+31 of H: K block c0 / 64, 16-byte units (c0 % 64) / 8 + q,
-            // placed at unit ^ (r % 8) of the row (128-byte swizzle)
-            uint8_t* rowp = H + (c0 >> 6) * FF_KB_BYTES + r * 128;
-            const int u0 = (c0 & 63) >> 3;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              uint32_t w4[4];
-#pragma unroll
-              for (int t = 0; t < 4; ++t) {
-                __nv_bfloat162 pr = __floats2bfloat162_rn(v[q * 8 + 2 * t], v[q * 8 + 2 * t + 1]);
-                w4[t] = *reinterpret_cast<uint32_t*>(&pr);
-              }
-              *reinterpret_cast<uint4*>(rowp + (((u0 + q) ^ (r & 7)) << 4)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
-            }
+            store_h(cg * 64, w0);
+            store_h(cg * 64 + 32, w1);
           }
           fence_proxy_async_smem();   // H is read by the tensor cores (async proxy)
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(hlo);   // H's K blocks 0-3 written, region A drained
+          // N half 1: output columns 256 + cg*64 .. +63 straight into H's K block 4 + cg
+#pragma unroll 1
+          for (int h = 0; h < 2; ++h) {
+            uint32_t w[16];
+            const int c0 = 256 + cg * 64 + 32 * h;
+            gelu_pack(c0, c0, w);
+            store_h(c0, w);
+          }
+          fence_proxy_async_smem();
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(hhi);   // H's K blocks 4-7 written, region B drained
         } else {
-          // layer 5: 128 padded outputs, one 32-column chunk per warp; the first 99 go to the caller
+          // layer 5: 128 padded outputs, one 32-column chunk per warp.  The first 99 of each row are
+          // staged in H's K blocks 1-4 (row stride 99 words: the lanes' rows fall in distinct banks), and
+          // the tile's rows, one contiguous span of the caller's [batch][99] array, leave in one bulk
+          // store.  K block 0 may already be receiving the next tile's inputs; blocks 1-7 are next
+          // written by the next tile's first epilogue, which waits until this store has read them.
           const int c0 = cg * 32;
           float v[32];
-          tmem_ld_32cols(tbase + c0, v);
-          const int grow = tile * BM + r;
-          if (grow < batch) {
-            float* o = out + static_cast<long long>(grow) * GF_MLP_OUTPUTS;
+          tmem_ld_32cols(tlane + c0, v);
+          float* o = s_out + r * GF_MLP_OUTPUTS;
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (c0 + j < GF_MLP_OUTPUTS) o[c0 + j] = v[j] + s_bias[c0 + j];
+          for (int j = 0; j < 32; ++j)
+            if (c0 + j < GF_MLP_OUTPUTS) o[c0 + j] = v[j] + s_bias[c0 + j];
+          fence_proxy_async_smem();   // the staged rows are read by the bulk copy (async proxy)
+          tc_fence_before();
+          named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every row is staged
+          if (threadIdx.x == kFfStoreThread) {
+            // batch is a multiple of 128 (checked by the caller): the tile's rows are all in range
+            bulk_store_1d(out + static_cast<long long>(tile) * BM * GF_MLP_OUTPUTS, s_out,
+                          BM * GF_MLP_OUTPUTS * 4);
+            bulk_commit();
           }
+          if (lane == 0) mbar_arrive(hlo);   // region A drained: the next tile's first MMAs may write it
         }
-        tc_fence_before();
         named_barrier_sync(4, 32 * FF_EPI_WARPS);   // every warp is done with s_bias before it is refilled
-        if (lane == 0) mbar_arrive(hready);
       }
       if (stop) {
         late = true;
         break;
       }
     }
+    if (threadIdx.x == kFfStoreThread) bulk_wait_all();   // the outputs are written before the CTA exits
   }
 
   tc_fence_before();
