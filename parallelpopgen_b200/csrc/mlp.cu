@@ -472,6 +472,7 @@ constexpr int FF_SMEM = FF_BAR_OFFSET + 256 + FF_ALIGN_SLACK;   // + barriers an
 static_assert(FF_SMEM <= SMEM_LIMIT, "fused forward shared memory");
 constexpr int FF_STAGES_PER_TILE = 2 + 3 * 16 + 8;        // weight blocks streamed per tile (58)
 constexpr int kFfStoreThread = 64;                         // the epilogue thread that issues the output stores
+constexpr int kFfPollThread = 64;                          // the epilogue thread that waits for the MMA hand-offs
 static_assert(BM * GF_MLP_OUTPUTS * 4 <= 4 * FF_KB_BYTES, "staged outputs fit in H's K blocks 1-4");
 
 // Weight block `i` of a tile's stream: layer, the N offset of its rows, the K block, its rows.
@@ -534,6 +535,23 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
     return true;
   };
 
+  // the same, sleeping between polls: for the producer, whose polls otherwise take issue slots and
+  // barrier accesses from the MMA thread (~2%)
+  auto wait_sleep = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (*abort_flag) return false;
+    const uint32_t addr = smem_u32(bar);
+    const long long t0 = clock64();
+    while (!mbar_try_wait(addr, parity)) {
+      if (*abort_flag) return false;
+      if (clock64() - t0 > wait_limit) {
+        *abort_flag = 1;
+        return false;
+      }
+      __nanosleep(32);
+    }
+    return true;
+  };
+
   if (threadIdx.x == 0) {
     tma_prefetch_desc(&tma_x);
     for (int s = 0; s < FF_WSTAGES; ++s) {
@@ -574,7 +592,7 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
         bool stop = false;
         for (int i = 0; i < FF_STAGES_PER_TILE; ++i, ++it) {
           const int s = it % FF_WSTAGES;
-          if (!wait(&wempty[s], ((it / FF_WSTAGES) & 1) ^ 1)) {
+          if (!wait_sleep(&wempty[s], ((it / FF_WSTAGES) & 1) ^ 1)) {
             stop = true;
             break;
           }
@@ -678,9 +696,10 @@ fused_forward_kernel(const __grid_constant__ CUtensorMap tma_x, const __grid_con
     float* s_out = reinterpret_cast<float*>(H + FF_KB_BYTES);   // the last layer's staged outputs
     const uint32_t tlane = tmem + (static_cast<uint32_t>(qd * 32) << 16);
     int a_waits = 0, b_waits = 0;
-    // lane 0 of each warp waits for the MMA hand-off; every epilogue warp then learns the joint verdict
+    // one thread waits for the MMA hand-off (sixteen pollers of the same barrier slow the MMAs down by
+    // ~5%); every epilogue warp then learns the verdict at the named barrier
     auto handoff = [&](uint64_t* bar, int& n, bool store_read) -> bool {
-      if (lane == 0 && !mbar_wait_sleep(bar, n & 1, wait_limit)) atomicOr(epi_fail, 1);
+      if (threadIdx.x == kFfPollThread && !mbar_wait_sleep(bar, n & 1, wait_limit)) atomicOr(epi_fail, 1);
       ++n;
       // the previous tile's output store has read its staging rows before this tile writes H
       if (store_read && threadIdx.x == kFfStoreThread) bulk_wait_read<0>();
