@@ -60,11 +60,11 @@ def test_forward_matches_oracle():
     assert _rel(y, exact) < 3e-2, _rel(y, exact)
 
 
-@pytest.mark.parametrize("B", [512, 4096, 148 * 128 + 256])
+@pytest.mark.parametrize("B", [128, 512, 4096, 148 * 128 + 256, 2 * 148 * 128 + 128])
 def test_fused_forward_equals_layered_forward(B):
     """The fused five-layer inference kernel issues each layer's MMAs in the layered GEMMs' order and
     rounds the activations at the same points, so its outputs equal the one-GEMM-per-layer path bit for
-    bit (batches of one tile per CTA, several tiles per CTA, and more tiles than SMs)."""
+    bit (one tile; one tile per CTA; more tiles than SMs; three tiles on some CTAs, two on the rest)."""
     from parallelpopgen_b200 import _capi
     mlp, vec, x, _ = _net(7, B)
     xs = torch.from_numpy(x).cuda()
