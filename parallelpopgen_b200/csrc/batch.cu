@@ -314,7 +314,7 @@ void release_batch(Engine* e) {
   cudaStreamSynchronize(e->stream);
   // the arena buffers and the record buffer are slices of engine-owned allocations (kept)
   cudaStreamSynchronize(e->stream);
-  // h_M, the replicate-table ring and its events belong to the engine (kept for the next batch)
+  // h_M and the device plan (replicate table, record offsets) belong to the engine (kept for the next batch)
   if (b->d_recs) cudaFree(b->d_recs);
   if (b->h_recs) cudaFreeHost(b->h_recs);
   if (b->d_reps) cudaFree(b->d_reps);
@@ -461,7 +461,54 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   // lock-step bookkeeping: replicate r's last window is super-step ceil(G_r / c_r) - 1
   b->finish_at = plan_finish_steps(ps.data(), b->R);
   b->active_dirty = true;
-  for (int& v : b->slot_version) v = -1;
+  // the device side of the plan: the replicate table (static fields), each replicate's cadence,
+  // generations and slab length, the region offsets and bases, and the super-step counter
+  {
+    const int R = b->R;
+    auto sz = [](size_t bytes) { return (bytes + 255) / 256 * 256; };
+    const size_t n_off = static_cast<size_t>(R) * nreg;
+    const size_t need = sz(sizeof(WinRep) * R) + sz(sizeof(StepRep) * R) + sz(sizeof(int) * n_off) +
+                        sz(sizeof(long long) * (nreg + 1)) + sz(sizeof(int));
+    st = grow_device(e, &e->batch_plan_mem, &e->batch_plan_bytes, need);
+    if (st != GF_OK) return st;
+    char* cur = static_cast<char*>(e->batch_plan_mem);
+    auto pa = [&](void** q, size_t bytes) {
+      *q = cur;
+      cur += sz(bytes);
+    };
+    pa(reinterpret_cast<void**>(&b->d_table), sizeof(WinRep) * R);
+    pa(reinterpret_cast<void**>(&b->d_steprep), sizeof(StepRep) * R);
+    pa(reinterpret_cast<void**>(&b->d_region_off), sizeof(int) * n_off);
+    pa(reinterpret_cast<void**>(&b->d_region_base), sizeof(long long) * (nreg + 1));
+    pa(reinterpret_cast<void**>(&b->d_step), sizeof(int));
+    std::vector<WinRep> table(R);
+    std::vector<StepRep> steprep(R);
+    b->all_tiles = 0;
+    for (int r = 0; r < R; ++r) {
+      const BatchRep& br = b->reps[r];
+      WinRep& w = table[r];
+      w = WinRep{};
+      w.base = br.base;
+      w.capacity = br.capacity;
+      w.seed1 = br.p.seed1;
+      w.seed2 = br.p.seed2;
+      w.check_preserved = 0;
+      w.compact = 0;
+      w.preserve = 0;
+      w.rep = r;
+      steprep[r] = StepRep{std::max(br.p.compact_interval, 1), std::max(br.p.num_generations, 0), br.chunk, 0};
+      b->all_tiles += br.capacity / kBatchTile;
+    }
+    // pageable sources: each copy returns once its source has been staged
+    GF_CUDA(e, cudaMemcpyAsync(b->d_table, table.data(), sizeof(WinRep) * R, cudaMemcpyHostToDevice, e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(b->d_steprep, steprep.data(), sizeof(StepRep) * R, cudaMemcpyHostToDevice, e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(b->d_region_off, b->plan.region_off.data(), sizeof(int) * n_off, cudaMemcpyHostToDevice,
+                               e->stream));
+    GF_CUDA(e, cudaMemcpyAsync(b->d_region_base, b->plan.region_base.data(), sizeof(long long) * (nreg + 1),
+                               cudaMemcpyHostToDevice, e->stream));
+    GF_CUDA(e, cudaMemsetAsync(b->d_step, 0, sizeof(int), e->stream));
+    b->step_plan = BatchStepPlan{b->plan.slab_windows, nreg, b->plan.ring_slots, 0, b->plan.slot_records};
+  }
   GF_TRACE_POINT(e, "record producers started");
   return GF_OK;
 }
@@ -632,7 +679,6 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     pa(reinterpret_cast<void**>(&b->d_Mend), sizeof(int) * R);
     pa(reinterpret_cast<void**>(&b->d_total_tiles), sizeof(int));
   }
-  static_assert(Batch::kRing == sizeof(Engine::batch_ring_done) / sizeof(cudaEvent_t), "ring events");
   if (e->batch_h_M_cap < static_cast<size_t>(2 * R)) {
     if (e->batch_h_M) GF_CUDA(e, cudaFreeHost(e->batch_h_M));
     e->batch_h_M = nullptr;
@@ -640,23 +686,7 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     GF_CUDA(e, cudaMallocHost(&e->batch_h_M, sizeof(int) * 2 * R));
     e->batch_h_M_cap = 2 * R;
   }
-  if (e->batch_ring_reps < static_cast<size_t>(R)) {
-    if (e->batch_d_ring) GF_CUDA(e, cudaFree(e->batch_d_ring));
-    if (e->batch_h_ring) GF_CUDA(e, cudaFreeHost(e->batch_h_ring));
-    e->batch_d_ring = nullptr;
-    e->batch_h_ring = nullptr;
-    e->batch_ring_reps = 0;
-    GF_CUDA(e, cudaMalloc(&e->batch_d_ring, sizeof(WinRep) * R * Batch::kRing));
-    GF_CUDA(e, cudaMallocHost(&e->batch_h_ring, sizeof(WinRep) * R * Batch::kRing));
-    e->batch_ring_reps = R;
-  }
-  for (int k = 0; k < Batch::kRing; ++k)
-    if (!e->batch_ring_done[k]) GF_CUDA(e, cudaEventCreateWithFlags(&e->batch_ring_done[k], cudaEventDisableTiming));
   b->h_M = e->batch_h_M;
-  b->d_ring_all = e->batch_d_ring;
-  b->h_ring_all = e->batch_h_ring;
-  b->ring_stride = e->batch_ring_reps;
-  for (int k = 0; k < Batch::kRing; ++k) b->ring_done[k] = e->batch_ring_done[k];
   GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
@@ -750,14 +780,14 @@ static gf_status sync_counts(Engine* e) {
   GF_CUDA(e, cudaStreamSynchronize(e->stream));
   for (int r = 0; r < b->R; ++r) b->reps[r].M = b->h_M[b->reps[r].m_slot * b->R + r];
   b->counts_stale = false;
-  if (fault) return fail(e, GF_ERR_DEVICE, "device status word reports fault %d (replicate capacity exceeded)", fault);
+  if (fault)
+    return fail(e, GF_ERR_DEVICE, "device status word reports fault %d (%s)", fault,
+                fault == kFaultCapacity  ? "replicate capacity exceeded"
+                : fault == kFaultRecords ? "a replicate's window has no generation records"
+                                         : "bounded wait expired");
   return GF_OK;
 }
 
-// One window of every active replicate from the precomputed records: no host record work and no
-// read-back (a one-block kernel assigns each replicate's tiles from its device-side count; tiles past
-// a replicate's end-of-window count return at once).  The replicate table goes through a ring of
-// pinned/device slots, each reused only after the launch that read it has finished.
 // Fields of unfinished replicates after k lock-step super-steps (finished ones are final already).
 static void sync_progress(Batch* b) {
   if (!b->precomputed) return;
@@ -772,21 +802,22 @@ static void sync_progress(Batch* b) {
   }
 }
 
+// One window of every unfinished replicate from the precomputed records: no host record work, no
+// upload and no read-back.  A one-block kernel derives each replicate's window (records, generations)
+// from the device's super-step counter and assigns its tiles from its device-side count; finished
+// replicates get none, and tiles past a replicate's end-of-window count return at once.
 static gf_status batch_super_step(Engine* e, int* active_out) {
   Batch* b = e->batch;
   if (!b->precomputed) return batch_super_step_fallback(e, active_out);
   if (b->active_dirty) {
     b->active.clear();
-    b->active_tiles = 0;
     b->active_cadence_sum = 0;
     for (int r = 0; r < b->R; ++r) {
       const BatchRep& br = b->reps[r];
       if (br.done) continue;
       b->active.push_back(r);
-      b->active_tiles += br.capacity / kBatchTile;
       b->active_cadence_sum += br.p.compact_interval;
     }
-    b->list_version += 1;
     b->active_dirty = false;
   }
   const int nj = static_cast<int>(b->active.size());
@@ -797,47 +828,13 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   const long long k = b->super_steps;
   const int j = static_cast<int>(k / b->plan.slab_windows);   // the record region of every active replicate
   if (j >= b->plan.nregions) return fail(e, GF_ERR_STATE, "super-step %lld beyond the record regions", k);
-  const int slot = b->ring;
-  GF_CUDA(e, cudaEventSynchronize(b->ring_done[slot]));
-  WinRep* hr = b->h_ring_all + static_cast<size_t>(slot) * b->ring_stride;
-  WinRep* dr = b->d_ring_all + static_cast<size_t>(slot) * b->ring_stride;
-  // a slot that last held this list only needs the per-step fields
-  const bool full = b->slot_version[slot] != b->list_version;
-  const long long region = b->plan.slot_base(j);
-  int tiles = 0;
-  for (int i = 0; i < nj; ++i) {
-    const int r = b->active[i];
-    const BatchRep& br = b->reps[r];
-    const int c = br.p.compact_interval;
-    const long long gen = k * c;
-    const int off = b->plan.region_off[static_cast<size_t>(r) * b->plan.nregions + j];
-    if (off < 0) return fail(e, GF_ERR_STATE, "replicate %d: no record slab %d", r, j);
-    WinRep& w = hr[i];
-    w.rec = static_cast<int>(region + off + (gen - static_cast<long long>(j) * br.chunk));
-    w.ngen = static_cast<int>(std::min<long long>(c, br.p.num_generations - gen));
-    if (full) {
-      w.base = br.base;
-      w.capacity = br.capacity;
-      w.tile0 = tiles;
-      w.ntiles = static_cast<int>(br.capacity / kBatchTile);
-      w.seed1 = br.p.seed1;
-      w.seed2 = br.p.seed2;
-      w.check_preserved = 0;
-      w.compact = 1;
-      w.preserve = 0;
-      w.rep = r;
-      w.births = 0;   // summed on the device from the records (batch_tiles_kernel)
-      tiles += w.ntiles;
-    }
-  }
-  b->slot_version[slot] = b->list_version;
   {
     gf_status ust = stream_upload(e, b, j);   // the records of this super-step, in stream order
     if (ust != GF_OK) return ust;
   }
-  GF_CUDA(e, cudaMemcpyAsync(dr, hr, sizeof(WinRep) * nj, cudaMemcpyHostToDevice, e->stream));
-  // each replicate's tiles from its device-side count: only its live slots are visited
-  assign_batch_tiles(e, dr, nj, b->d_M[b->mslot], b->d_all_recs, b->d_total_tiles);
+  // every replicate's window and tiles, derived on the device from the super-step counter
+  batch_step_tiles(e, b->d_table, b->R, b->d_M[b->mslot], b->d_all_recs, b->d_total_tiles, b->d_step, b->step_plan,
+                   b->d_region_off, b->d_region_base, b->d_steprep, e->d_count + 2);
   GF_CUDA(e, cudaGetLastError());
   WindowLaunch w;
   w.A = b->freq[0];
@@ -853,10 +850,10 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   w.M_end = b->d_Mend;
   w.M_next = nullptr;
   w.M_out = b->d_M[b->mslot ^ 1];
-  w.reps = dr;
-  w.nreps = nj;
+  w.reps = b->d_table;
+  w.nreps = b->R;
   w.recs = b->d_all_recs;
-  w.total_tiles = static_cast<int>(b->active_tiles);   // segment tiles: an upper bound, sizes the grid
+  w.total_tiles = static_cast<int>(std::min<long long>(b->all_tiles, INT32_MAX));   // sizes the grids
   w.total_tiles_dev = b->d_total_tiles;
   w.any_compact = true;
   w.stats = e->d_stats;
@@ -874,8 +871,6 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     GF_CUDA(e, cudaEventRecord(ev1, e->stream));
     e->prof_drift.emplace_back(ev0, ev1);
   }
-  GF_CUDA(e, cudaEventRecord(b->ring_done[slot], e->stream));
-  b->ring = (slot + 1) % Batch::kRing;
   b->mslot ^= 1;
   b->id_cur ^= 1;
   b->super_steps += 1;

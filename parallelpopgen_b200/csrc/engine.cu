@@ -1277,10 +1277,7 @@ void gf_engine_destroy(gf_engine* g) {
   if (e->batch_h_M) cudaFreeHost(e->batch_h_M);
   if (e->batch_arena_mem) cudaFree(e->batch_arena_mem);
   if (e->batch_recs_mem) cudaFree(e->batch_recs_mem);
-  if (e->batch_d_ring) cudaFree(e->batch_d_ring);
-  if (e->batch_h_ring) cudaFreeHost(e->batch_h_ring);
-  for (cudaEvent_t ev : e->batch_ring_done)
-    if (ev) cudaEventDestroy(ev);
+  if (e->batch_plan_mem) cudaFree(e->batch_plan_mem);
   if (e->pool) cudaMemPoolDestroy(e->pool);
   for (auto ev : e->free_events) cudaEventDestroy(ev);
   if (e->spec_scratch) cudaFree(e->spec_scratch);

@@ -32,6 +32,7 @@ enum DeviceFault : int {
   kFaultNone = 0,
   kFaultCapacity = 1,  // a kernel was asked to write beyond the allocated rows
   kFaultScanTimeout = 2,
+  kFaultRecords = 3,   // a batched replicate's window has no generation records (a planning error)
 };
 
 // Per-generation kernel arguments (passed by value; ~1.3 KB).
@@ -145,6 +146,23 @@ struct WindowMpLaunch {
   int tiles_bound;           // launch tiles (an upper bound of the end-of-window tiles)
 };
 
+// What a batched super-step derives each replicate's window from on the device (precomputed records):
+// super-step k runs generations (k c, min(G, (k + 1) c)] of a replicate with cadence c and G
+// generations, from record slab j = k / slab_windows.
+struct StepRep {
+  int cadence;
+  int gens;
+  int chunk;   // generations per slab
+  int pad;
+};
+struct BatchStepPlan {
+  int slab_windows;
+  int nregions;
+  int ring_slots;          // 0: every region resident at region_base[j]; else region j in slot j % ring_slots
+  int pad;
+  long long slot_records;  // records per ring slot
+};
+
 // Host record of one replicate of a batch.
 struct BatchRep {
   gf_replicate p;
@@ -185,14 +203,6 @@ struct Batch {
   // generation records of every replicate, computed once at begin (when they fit the budget)
   bool precomputed = false;
   WinGen* d_all_recs = nullptr;
-  // ring of per-super-step replicate tables: a slot is rewritten only after the launch that read it
-  // (64 slots: the host may run that many super-steps ahead of the GPU)
-  static constexpr int kRing = 64;
-  WinRep* d_ring_all = nullptr;       // kRing tables of ring_stride entries (the engine's buffers)
-  WinRep* h_ring_all = nullptr;
-  size_t ring_stride = 0;
-  cudaEvent_t ring_done[kRing] = {};
-  int ring = 0;
   bool counts_stale = false;          // counts on the device are newer than reps[].M
   int* d_total_tiles = nullptr;       // tiles of the current super-step, assigned on the device
   // generation records, drawn by host threads region by region (region j holds slab j -- the
@@ -214,11 +224,18 @@ struct Batch {
   // their per-replicate fields are brought up to date when a run returns (sync_progress).
   std::vector<int> active;                    // unfinished replicates, in index order
   bool active_dirty = true;
-  int list_version = 0;
-  int slot_version[64];                       // list_version whose full entries a ring slot holds
-  long long active_tiles = 0;                 // segment tiles of the active replicates
   long long active_cadence_sum = 0;           // sum of their cadences (generations per super-step)
   std::vector<std::vector<int>> finish_at;    // [k]: replicates whose last window is super-step k
+  // precomputed records: a replicate table of all R replicates in index order, whose per-window fields
+  // (records, generations, tiles, births; none once finished) a kernel derives from the super-step
+  // counter on the device, so a super-step needs no host table and no upload
+  WinRep* d_table = nullptr;
+  StepRep* d_steprep = nullptr;
+  int* d_region_off = nullptr;                // [r * nregions + j]
+  long long* d_region_base = nullptr;         // [j], resident layout
+  int* d_step = nullptr;                      // super-steps launched (advanced by the step kernel)
+  BatchStepPlan step_plan{};
+  long long all_tiles = 0;                    // segment tiles of all replicates (the launch bound)
 };
 
 struct PendingCount {
@@ -307,13 +324,8 @@ struct Engine {
   // page-locked staging of batched generation records, kept across batches (grown on demand)
   WinGen* h_rec_stage = nullptr;
   size_t h_rec_stage_cap = 0;
-  // the batched engine's per-super-step replicate tables (a ring of 64, device and page-locked host),
-  // their events and the page-locked count read-back, kept across batches (grown on demand): pinning
-  // and freeing them per batch cost up to hundreds of milliseconds on a busy host
-  WinRep* batch_d_ring = nullptr;
-  WinRep* batch_h_ring = nullptr;
-  size_t batch_ring_reps = 0;                 // replicates per table
-  cudaEvent_t batch_ring_done[64] = {};
+  // the batched engine's page-locked count read-back, kept across batches (grown on demand): pinning
+  // and freeing it per batch cost up to hundreds of milliseconds on a busy host
   int* batch_h_M = nullptr;
   size_t batch_h_M_cap = 0;
   // the batched engine's device arena (state, IDs, flags, tile counts) and generation records, also
@@ -323,6 +335,8 @@ struct Engine {
   size_t batch_arena_bytes = 0;
   void* batch_recs_mem = nullptr;
   size_t batch_recs_bytes = 0;
+  void* batch_plan_mem = nullptr;             // the replicate table and the record plan on the device
+  size_t batch_plan_bytes = 0;
   void* spec_scratch = nullptr;
   size_t spec_scratch_bytes = 0;
   float* spec_in = nullptr;
@@ -347,6 +361,11 @@ gf_status ensure_scratch(Engine* e, void** ptr, size_t* have, size_t need);
 // Window launch (+ segmented compaction into compact_dst), window.cu.
 void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
                         int* total_out);
+// Super-step *d_step of a batch with precomputed records: every replicate's window fields and tiles
+// in d_table (all R replicates; finished ones get none), then *d_step + 1.
+void batch_step_tiles(Engine* e, WinRep* d_table, int R, const int* M_in, const WinGen* recs, int* total_out,
+                      int* d_step, const BatchStepPlan& plan, const int* region_off, const long long* region_base,
+                      const StepRep* steprep, int* fault);
 // after_window, before_compaction (either may be null): recorded on the stream between the window
 // kernel and its compaction (two events, so that each timing pair owns its own)
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaEvent_t after_window = nullptr,

@@ -109,6 +109,95 @@ __global__ void __launch_bounds__(1024) batch_tiles_kernel(WinRep* __restrict__ 
   if (threadIdx.x == 0) *total = s_carry;
 }
 
+// Tiles of super-step k = *step of a batch with precomputed records, and every replicate's window
+// derived on the device: replicate r (cadence c, G generations) runs generations (k c, min(G, (k+1) c)]
+// from record slab j = k / slab_windows at its offset in region j; a finished replicate gets no tiles
+// (the window, scan and scatter kernels then never visit it, so its state and counts stay as they
+// are).  The others get ceil((M_in + births) / 1024) tiles (at least one, at most their segment), in
+// replicate order.  One block; thread 0 advances the counter once every thread has read it.
+__global__ void __launch_bounds__(1024) batch_step_kernel(WinRep* __restrict__ reps, int R,
+                                                          const int* __restrict__ M_in,
+                                                          const WinGen* __restrict__ recs, int* __restrict__ total,
+                                                          int* __restrict__ step, const BatchStepPlan plan,
+                                                          const int* __restrict__ region_off,
+                                                          const long long* __restrict__ region_base,
+                                                          const StepRep* __restrict__ steprep, int* __restrict__ fault) {
+  __shared__ int s_warp[32];
+  __shared__ int s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int k = *step;
+  const int j = k / plan.slab_windows;
+  const bool in_plan = j < plan.nregions;
+  const long long slot_base = !in_plan              ? 0
+                              : plan.ring_slots > 0 ? static_cast<long long>(j % plan.ring_slots) * plan.slot_records
+                                                    : region_base[j];
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();   // every thread has read *step
+  for (int base = 0; base < R; base += 1024) {
+    const int r = base + threadIdx.x;
+    int need = 0;
+    if (r < R) {
+      const StepRep sr = steprep[r];
+      const long long gen = static_cast<long long>(k) * sr.cadence;
+      int ngen = 0, rec = 0;
+      long long births = 0;
+      if (in_plan && gen < sr.gens) {
+        const int off = region_off[static_cast<size_t>(r) * plan.nregions + j];
+        if (off < 0) {
+          atomicExch(fault, kFaultRecords);
+        } else {
+          ngen = static_cast<int>(min(static_cast<long long>(sr.cadence), sr.gens - gen));
+          rec = static_cast<int>(slot_base + off + (gen - static_cast<long long>(j) * sr.chunk));
+          // the window's new-mutation counts, eight independent loads at a time
+          for (int g0 = 0; g0 < ngen; g0 += 8) {
+            int c[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) c[i] = g0 + i < ngen ? recs[rec + g0 + i].new_count : 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) births += c[i];
+          }
+          const long long end = static_cast<long long>(M_in[r]) + births;
+          const long long cap_tiles = reps[r].capacity / kWinTile;
+          need = static_cast<int>(max(1ll, min(cap_tiles, (end + kWinTile - 1) / kWinTile)));
+        }
+      }
+      WinRep& W = reps[r];
+      W.rec = rec;
+      W.ngen = ngen;
+      W.births = births;
+      W.compact = need > 0 ? 1 : 0;
+      W.ntiles = need;
+    }
+    int incl = need;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      int w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const int before = s_carry + (warp > 0 ? s_warp[warp - 1] : 0) + incl - need;
+    if (r < R) reps[r].tile0 = before;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += s_warp[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *total = s_carry;
+    *step = k + 1;
+  }
+}
+
 // DRAW: how a warp schedules its sampler draws (DrawStrategy).  KEYS: every replicate of the launch
 // has the seeds whose round keys `keys` holds (a plain-engine launch), so the quads' Philox blocks take
 // their round keys from the kernel parameters instead of deriving them from the replicate's seeds.
@@ -476,6 +565,14 @@ __global__ void __launch_bounds__(kWinThreads)
 void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, const WinGen* recs,
                         int* total_out) {
   batch_tiles_kernel<<<1, 1024, 0, e->stream>>>(d_reps, nreps, M_in, recs, total_out);
+  e->kernel_launches += 1;
+}
+
+void batch_step_tiles(Engine* e, WinRep* d_table, int R, const int* M_in, const WinGen* recs, int* total_out,
+                      int* d_step, const BatchStepPlan& plan, const int* region_off, const long long* region_base,
+                      const StepRep* steprep, int* fault) {
+  batch_step_kernel<<<1, 1024, 0, e->stream>>>(d_table, R, M_in, recs, total_out, d_step, plan, region_off,
+                                               region_base, steprep, fault);
   e->kernel_launches += 1;
 }
 
