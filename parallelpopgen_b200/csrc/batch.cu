@@ -315,6 +315,8 @@ void release_batch(Engine* e) {
   // the arena buffers and the record buffer are slices of engine-owned allocations (kept)
   cudaStreamSynchronize(e->stream);
   // h_M and the device plan (replicate table, record offsets) belong to the engine (kept for the next batch)
+  for (auto& g : b->slab_graph)
+    if (g) cudaGraphExecDestroy(g);
   if (b->d_recs) cudaFree(b->d_recs);
   if (b->h_recs) cudaFreeHost(b->h_recs);
   if (b->d_reps) cudaFree(b->d_reps);
@@ -446,11 +448,12 @@ static gf_status precompute_records(Engine* e, Batch* b) {
   b->uploaded = 0;
   b->upload_done = 0;
   b->producible.store(b->plan.ring_slots > 0 ? b->plan.ring_slots : nreg);
-  // A producer draws ~25 M records/s and the super-steps consume ~50 M/s at most, so a few producers
-  // stay ahead of the GPU; more would take cores from the thread that enqueues the super-steps.
+  // A producer draws ~25 M records/s; the super-steps, replayed a slab at a time, consume them faster
+  // than six producers drew them at the start of a batch, and the thread that enqueues the super-steps
+  // mostly waits on events, so the producers get all but two host threads (at most twelve).
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const long long want = std::max<long long>(1, total / 65536);
-  const int workers = static_cast<int>(std::min<long long>(want, std::max(1u, std::min(hw / 2, 6u))));
+  const int workers = static_cast<int>(std::min<long long>(want, std::max(1u, std::min(hw > 2 ? hw - 2 : 1u, 12u))));
   WinGen* stage = e->h_rec_stage;
   try {
     for (int t = 0; t < workers; ++t) b->producers.emplace_back(produce_records, b, stage);
@@ -468,7 +471,7 @@ static gf_status precompute_records(Engine* e, Batch* b) {
     auto sz = [](size_t bytes) { return (bytes + 255) / 256 * 256; };
     const size_t n_off = static_cast<size_t>(R) * nreg;
     const size_t need = sz(sizeof(WinRep) * R) + sz(sizeof(StepRep) * R) + sz(sizeof(int) * n_off) +
-                        sz(sizeof(long long) * (nreg + 1)) + sz(sizeof(int));
+                        sz(sizeof(long long) * (nreg + 1)) + sz(sizeof(int)) + 2 * sz(sizeof(int) * R) + sz(sizeof(int));
     st = grow_device(e, &e->batch_plan_mem, &e->batch_plan_bytes, need);
     if (st != GF_OK) return st;
     char* cur = static_cast<char*>(e->batch_plan_mem);
@@ -481,6 +484,9 @@ static gf_status precompute_records(Engine* e, Batch* b) {
     pa(reinterpret_cast<void**>(&b->d_region_off), sizeof(int) * n_off);
     pa(reinterpret_cast<void**>(&b->d_region_base), sizeof(long long) * (nreg + 1));
     pa(reinterpret_cast<void**>(&b->d_step), sizeof(int));
+    pa(reinterpret_cast<void**>(&b->d_list_rep), sizeof(int) * R);
+    pa(reinterpret_cast<void**>(&b->d_list_tile0), sizeof(int) * R);
+    pa(reinterpret_cast<void**>(&b->d_list_count), sizeof(int));
     std::vector<WinRep> table(R);
     std::vector<StepRep> steprep(R);
     b->all_tiles = 0;
@@ -687,6 +693,10 @@ static gf_status batch_begin(Engine* e, const gf_replicate* in, int R) {
     e->batch_h_M_cap = 2 * R;
   }
   b->h_M = e->batch_h_M;
+  for (cudaEvent_t& ev : e->batch_ahead)
+    if (!ev) GF_CUDA(e, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  b->step_ev = e->batch_ahead;
+  b->slab_ev = e->batch_ahead + 64;
   GF_CUDA(e, cudaMemsetAsync(b->freq[0], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemsetAsync(b->freq[1], 0, sizeof(float) * arena, e->stream));
   GF_CUDA(e, cudaMemcpyAsync(b->d_M[0], M0.data(), sizeof(int) * R, cudaMemcpyHostToDevice, e->stream));
@@ -802,39 +812,28 @@ static void sync_progress(Batch* b) {
   }
 }
 
-// One window of every unfinished replicate from the precomputed records: no host record work, no
-// upload and no read-back.  A one-block kernel derives each replicate's window (records, generations)
-// from the device's super-step counter and assigns its tiles from its device-side count; finished
-// replicates get none, and tiles past a replicate's end-of-window count return at once.
-static gf_status batch_super_step(Engine* e, int* active_out) {
-  Batch* b = e->batch;
-  if (!b->precomputed) return batch_super_step_fallback(e, active_out);
-  if (b->active_dirty) {
-    b->active.clear();
-    b->active_cadence_sum = 0;
-    for (int r = 0; r < b->R; ++r) {
-      const BatchRep& br = b->reps[r];
-      if (br.done) continue;
-      b->active.push_back(r);
-      b->active_cadence_sum += br.p.compact_interval;
-    }
-    b->active_dirty = false;
+static void refresh_active(Batch* b) {
+  if (!b->active_dirty) return;
+  b->active.clear();
+  b->active_cadence_sum = 0;
+  for (int r = 0; r < b->R; ++r) {
+    const BatchRep& br = b->reps[r];
+    if (br.done) continue;
+    b->active.push_back(r);
+    b->active_cadence_sum += br.p.compact_interval;
   }
-  const int nj = static_cast<int>(b->active.size());
-  if (nj == 0) {
-    if (active_out) *active_out = 0;
-    return GF_OK;
-  }
-  const long long k = b->super_steps;
-  const int j = static_cast<int>(k / b->plan.slab_windows);   // the record region of every active replicate
-  if (j >= b->plan.nregions) return fail(e, GF_ERR_STATE, "super-step %lld beyond the record regions", k);
-  {
-    gf_status ust = stream_upload(e, b, j);   // the records of this super-step, in stream order
-    if (ust != GF_OK) return ust;
-  }
-  // every replicate's window and tiles, derived on the device from the super-step counter
+  b->active_dirty = false;
+}
+
+// The launches of one super-step at the batch's current buffer parity (precomputed records): a
+// one-block kernel derives each replicate's window (records, generations) from the device's super-step
+// counter and assigns its tiles from its device-side count (finished replicates get none; tiles past a
+// replicate's end-of-window count return at once), then the window kernel and its compaction.  No
+// host record work, no upload and no read-back.
+static gf_status enqueue_step(Engine* e, Batch* b) {
   batch_step_tiles(e, b->d_table, b->R, b->d_M[b->mslot], b->d_all_recs, b->d_total_tiles, b->d_step, b->step_plan,
-                   b->d_region_off, b->d_region_base, b->d_steprep, e->d_count + 2);
+                   b->d_region_off, b->d_region_base, b->d_steprep, e->d_count + 2, b->d_list_rep, b->d_list_tile0,
+                   b->d_list_count);
   GF_CUDA(e, cudaGetLastError());
   WindowLaunch w;
   w.A = b->freq[0];
@@ -859,18 +858,18 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
   w.stats = e->d_stats;
   w.fault = e->d_count + 2;
   w.sched = e->d_count + kSchedWord;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  if (e->profiling) {
-    cudaEventCreate(&ev0);
-    cudaEventCreate(&ev1);
-    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
-  }
-  gf_status st = window_run(e, w, b->freq[0]);
-  if (st != GF_OK) return st;
-  if (e->profiling) {
-    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
-    e->prof_drift.emplace_back(ev0, ev1);
-  }
+  w.list.rep = b->d_list_rep;
+  w.list.tile0 = b->d_list_tile0;
+  w.list.count = b->d_list_count;
+  return window_run(e, w, b->freq[0]);
+}
+constexpr int kLaunchesPerStep = 4;   // step kernel, window, segmented scan, scatter
+
+// Host bookkeeping of the super-step just enqueued: buffer parity, generations, finished replicates.
+// Returns how many replicates finished with it.
+static int account_step(Batch* b) {
+  refresh_active(b);
+  const long long k = b->super_steps;
   b->mslot ^= 1;
   b->id_cur ^= 1;
   b->super_steps += 1;
@@ -893,7 +892,110 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
     if (finishing) b->active_dirty = true;
   }
   b->generations += gens;
+  return finishing;
+}
+
+static gf_status batch_super_step(Engine* e, int* active_out) {
+  Batch* b = e->batch;
+  if (!b->precomputed) return batch_super_step_fallback(e, active_out);
+  refresh_active(b);
+  const int nj = static_cast<int>(b->active.size());
+  if (nj == 0) {
+    if (active_out) *active_out = 0;
+    return GF_OK;
+  }
+  const long long k = b->super_steps;
+  const int j = static_cast<int>(k / b->plan.slab_windows);   // the record region of every active replicate
+  if (j >= b->plan.nregions) return fail(e, GF_ERR_STATE, "super-step %lld beyond the record regions", k);
+  {
+    gf_status ust = stream_upload(e, b, j);   // the records of this super-step, in stream order
+    if (ust != GF_OK) return ust;
+  }
+  cudaEvent_t& ahead = b->step_ev[b->steps_enqueued % 64];
+  GF_CUDA(e, cudaEventSynchronize(ahead));   // the step enqueued 64 steps ago has run
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e->profiling) {
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    GF_CUDA(e, cudaEventRecord(ev0, e->stream));
+  }
+  gf_status st = enqueue_step(e, b);
+  if (st != GF_OK) return st;
+  if (e->profiling) {
+    GF_CUDA(e, cudaEventRecord(ev1, e->stream));
+    e->prof_drift.emplace_back(ev0, ev1);
+  }
+  GF_CUDA(e, cudaEventRecord(ahead, e->stream));
+  b->steps_enqueued += 1;
+  const int finishing = account_step(b);
   if (active_out) *active_out = nj - finishing;
+  return GF_OK;
+}
+
+// The super-steps of one record slab (slab_windows of them, all in record region j) replayed as one
+// CUDA graph: the steps read their window from the device's super-step counter, so the same launches
+// serve every slab that starts at the same buffer parity (one graph per parity, captured on first use
+// and again after the draw tuning changes).  Taken only at a slab's first step, after the first slab
+// (which runs step by step, so launch set-up never happens inside a capture), when the whole slab
+// lies before the batch's last super-step, and never while profiling; `*ran` says whether it ran.
+static gf_status batch_slab(Engine* e, int* active_out, bool* ran) {
+  *ran = false;
+  Batch* b = e->batch;
+  if (!b->precomputed || e->profiling || !e->stream) return GF_OK;
+  refresh_active(b);
+  const long long k = b->super_steps;
+  const int W = b->plan.slab_windows;
+  if (b->active.empty() || k == 0 || k % W != 0 || k + W > static_cast<long long>(b->finish_at.size())) return GF_OK;
+  const int j = static_cast<int>(k / W);
+  if (j >= b->plan.nregions) return GF_OK;
+  {
+    gf_status ust = stream_upload(e, b, j);
+    if (ust != GF_OK) return ust;
+  }
+  const int parity = b->mslot;
+  if (b->slab_graph[parity] &&
+      (b->graph_draw[parity] != e->draw_strategy || b->graph_blocks[parity] != e->blocks_per_sm)) {
+    cudaGraphExecDestroy(b->slab_graph[parity]);
+    b->slab_graph[parity] = nullptr;
+  }
+  if (!b->slab_graph[parity]) {
+    const long long launches0 = e->kernel_launches;
+    const int m0 = b->mslot, i0 = b->id_cur;
+    GF_CUDA(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    gf_status st = GF_OK;
+    for (int i = 0; i < W && st == GF_OK; ++i) {
+      st = enqueue_step(e, b);
+      b->mslot ^= 1;
+      b->id_cur ^= 1;
+    }
+    b->mslot = m0;
+    b->id_cur = i0;
+    e->kernel_launches = launches0;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t cerr = cudaStreamEndCapture(e->stream, &graph);
+    if (st != GF_OK || cerr != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (st != GF_OK) return st;
+      return cuda_fail(e, cerr, "capturing a record slab's super-steps");
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ierr = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ierr != cudaSuccess) return cuda_fail(e, ierr, "instantiating a record slab's graph");
+    b->slab_graph[parity] = exec;
+    b->graph_draw[parity] = e->draw_strategy;
+    b->graph_blocks[parity] = e->blocks_per_sm;
+  }
+  cudaEvent_t& ahead = b->slab_ev[b->slabs_enqueued % 2];
+  GF_CUDA(e, cudaEventSynchronize(ahead));   // the slab enqueued two slabs ago has run
+  GF_CUDA(e, cudaGraphLaunch(b->slab_graph[parity], e->stream));
+  GF_CUDA(e, cudaEventRecord(ahead, e->stream));
+  b->slabs_enqueued += 1;
+  e->kernel_launches += static_cast<long long>(kLaunchesPerStep) * W;
+  for (int i = 0; i < W; ++i) account_step(b);
+  refresh_active(b);
+  if (active_out) *active_out = static_cast<int>(b->active.size());
+  *ran = true;
   return GF_OK;
 }
 
@@ -1049,12 +1151,26 @@ gf_status gf_batch_run(gf_engine* g, int32_t max_super_steps, int32_t* out_activ
     if (!e->batch) return fail(e, GF_ERR_STATE, "gf_batch_run before gf_batch_begin");
     GF_CUDA(e, cudaSetDevice(e->device));
     int active = 1;
-    for (int s = 0; (max_super_steps <= 0 || s < max_super_steps) && active > 0; ++s) {
+    const int W = e->batch->precomputed ? e->batch->plan.slab_windows : 1;
+    for (int s = 0; (max_super_steps <= 0 || s < max_super_steps) && active > 0;) {
+      if (max_super_steps <= 0 || max_super_steps - s >= W) {
+        bool ran = false;
+        gf_status st = batch_slab(e, &active, &ran);   // a whole record slab as one graph, where it may
+        if (st != GF_OK) {
+          sync_progress(e->batch);
+          return st;
+        }
+        if (ran) {
+          s += W;
+          continue;
+        }
+      }
       gf_status st = batch_super_step(e, &active);
       if (st != GF_OK) {
         sync_progress(e->batch);
         return st;
       }
+      ++s;
     }
     sync_progress(e->batch);
     gf_status st = sync_counts(e);

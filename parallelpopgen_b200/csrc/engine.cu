@@ -1278,6 +1278,8 @@ void gf_engine_destroy(gf_engine* g) {
   if (e->batch_arena_mem) cudaFree(e->batch_arena_mem);
   if (e->batch_recs_mem) cudaFree(e->batch_recs_mem);
   if (e->batch_plan_mem) cudaFree(e->batch_plan_mem);
+  for (cudaEvent_t ev : e->batch_ahead)
+    if (ev) cudaEventDestroy(ev);
   if (e->pool) cudaMemPoolDestroy(e->pool);
   for (auto ev : e->free_events) cudaEventDestroy(ev);
   if (e->spec_scratch) cudaFree(e->spec_scratch);

@@ -84,6 +84,15 @@ struct WinRep {
   long long births;     // new mutations over the window: tiles at or beyond M0 + births hold nothing
 };
 
+// Which table entries a batched launch visits: by default all nreps in order; a batch with
+// precomputed records passes the list of its unfinished replicates, built on the device each
+// super-step (their table indices, first tiles and count), so that finished ones cost nothing.
+struct RepList {
+  const int* rep = nullptr;     // [i] table index of the i-th listed replicate (null: i)
+  const int* tile0 = nullptr;   // [i] its first tile (null: the table's tile0 of entry i)
+  const int* count = nullptr;   // how many are listed, on the device (null: nreps)
+};
+
 // Pointers and sizes of one window launch plus its optional compaction.
 struct WindowLaunch {
   const float* A;          // state at the window start
@@ -113,6 +122,7 @@ struct WindowLaunch {
   // as kernel parameters
   bool uniform_key = false;
   int seed1 = 0, seed2 = 0;
+  RepList list{};
 };
 
 // Words of the engine's device counter block (d_count) and the first of the window scheduler's two.
@@ -234,8 +244,19 @@ struct Batch {
   int* d_region_off = nullptr;                // [r * nregions + j]
   long long* d_region_base = nullptr;         // [j], resident layout
   int* d_step = nullptr;                      // super-steps launched (advanced by the step kernel)
+  int* d_list_rep = nullptr;                  // the step's unfinished replicates (RepList), built by the
+  int* d_list_tile0 = nullptr;                // step kernel
+  int* d_list_count = nullptr;
   BatchStepPlan step_plan{};
   long long all_tiles = 0;                    // segment tiles of all replicates (the launch bound)
+  // one record slab's super-steps as a CUDA graph, per starting buffer parity, and the draw tuning
+  // it was captured with
+  cudaGraphExec_t slab_graph[2] = {nullptr, nullptr};
+  int graph_draw[2] = {-1, -1};
+  int graph_blocks[2] = {-1, -1};
+  cudaEvent_t* step_ev = nullptr;             // 64 (the engine's batch_ahead[0..63])
+  cudaEvent_t* slab_ev = nullptr;             // 2 (batch_ahead[64..65])
+  long long steps_enqueued = 0, slabs_enqueued = 0;
 };
 
 struct PendingCount {
@@ -328,6 +349,9 @@ struct Engine {
   // and freeing it per batch cost up to hundreds of milliseconds on a busy host
   int* batch_h_M = nullptr;
   size_t batch_h_M_cap = 0;
+  // events that keep the batched engine's host at most 64 super-steps (or two graph-replayed slabs)
+  // ahead of the GPU, so record uploads are not queued far behind the launches that precede them
+  cudaEvent_t batch_ahead[66] = {};
   // the batched engine's device arena (state, IDs, flags, tile counts) and generation records, also
   // kept across batches and grown on demand: carving a new batch's gigabytes out of the stream-ordered
   // pool after its small temporaries fragmented it could map fresh memory (~0.5 s) every other batch
@@ -365,7 +389,7 @@ void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, c
 // in d_table (all R replicates; finished ones get none), then *d_step + 1.
 void batch_step_tiles(Engine* e, WinRep* d_table, int R, const int* M_in, const WinGen* recs, int* total_out,
                       int* d_step, const BatchStepPlan& plan, const int* region_off, const long long* region_base,
-                      const StepRep* steprep, int* fault);
+                      const StepRep* steprep, int* fault, int* list_rep, int* list_tile0, int* list_count);
 // after_window, before_compaction (either may be null): recorded on the stream between the window
 // kernel and its compaction (two events, so that each timing pair owns its own)
 gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaEvent_t after_window = nullptr,

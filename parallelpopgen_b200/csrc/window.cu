@@ -23,25 +23,31 @@ namespace gf {
 constexpr int kWinThreads = 256;
 constexpr int kWinTile = kWinThreads * 4;
 
-// replicate owning launch tile `gt` (last replicate whose tile0 <= gt)
-__device__ __forceinline__ int find_rep(const WinRep* __restrict__ reps, int nreps, int gt) {
-  int lo = 0, hi = nreps - 1;
+__device__ __forceinline__ int list_count(const RepList& L, int nreps) { return L.count ? *L.count : nreps; }
+__device__ __forceinline__ int list_rep(const RepList& L, int i) { return L.rep ? L.rep[i] : i; }
+__device__ __forceinline__ int list_tile0(const RepList& L, const WinRep* __restrict__ reps, int i) {
+  return L.tile0 ? L.tile0[i] : reps[i].tile0;
+}
+
+// listed replicate owning launch tile `gt` (the last one whose tile0 <= gt)
+__device__ __forceinline__ int find_rep(const RepList& L, const WinRep* __restrict__ reps, int n, int gt) {
+  int lo = 0, hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (reps[mid].tile0 <= gt) lo = mid;
+    if (list_tile0(L, reps, mid) <= gt) lo = mid;
     else hi = mid - 1;
   }
   return lo;
 }
 
-// Shared-memory copy of the replicates' first tiles (batches of up to kRepCache replicates), so the
-// per-tile owner search does not chase global memory.
+// Shared-memory copy of the listed replicates' first tiles (up to kRepCache of them), so the per-tile
+// owner search does not chase global memory.
 constexpr int kRepCache = 4096;
 
-__device__ __forceinline__ int find_rep_cached(const int* s_tile0, const WinRep* __restrict__ reps, int nreps,
-                                               int gt) {
-  if (nreps > kRepCache) return find_rep(reps, nreps, gt);
-  int lo = 0, hi = nreps - 1;
+__device__ __forceinline__ int find_rep_cached(const int* s_tile0, const RepList& L, const WinRep* __restrict__ reps,
+                                               int n, int gt) {
+  if (n > kRepCache) return find_rep(L, reps, n, gt);
+  int lo = 0, hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (s_tile0[mid] <= gt) lo = mid;
@@ -50,9 +56,9 @@ __device__ __forceinline__ int find_rep_cached(const int* s_tile0, const WinRep*
   return lo;
 }
 
-__device__ __forceinline__ void load_tile0(int* s_tile0, const WinRep* __restrict__ reps, int nreps) {
-  if (nreps <= kRepCache)
-    for (int j = threadIdx.x; j < nreps; j += blockDim.x) s_tile0[j] = reps[j].tile0;
+__device__ __forceinline__ void load_tile0(int* s_tile0, const RepList& L, const WinRep* __restrict__ reps, int n) {
+  if (n <= kRepCache)
+    for (int j = threadIdx.x; j < n; j += blockDim.x) s_tile0[j] = list_tile0(L, reps, j);
   __syncthreads();
 }
 
@@ -111,19 +117,22 @@ __global__ void __launch_bounds__(1024) batch_tiles_kernel(WinRep* __restrict__ 
 
 // Tiles of super-step k = *step of a batch with precomputed records, and every replicate's window
 // derived on the device: replicate r (cadence c, G generations) runs generations (k c, min(G, (k+1) c)]
-// from record slab j = k / slab_windows at its offset in region j; a finished replicate gets no tiles
-// (the window, scan and scatter kernels then never visit it, so its state and counts stay as they
-// are).  The others get ceil((M_in + births) / 1024) tiles (at least one, at most their segment), in
-// replicate order.  One block; thread 0 advances the counter once every thread has read it.
+// from record slab j = k / slab_windows at its offset in region j; a finished replicate gets no tiles.
+// The others get ceil((M_in + births) / 1024) tiles (at least one, at most their segment), in replicate
+// order, and are listed (table index, first tile, count) for the window, scan and scatter kernels, which
+// then never visit a finished replicate (its state and counts stay as they are).  One block; thread 0
+// advances the counter once every thread has read it.
 __global__ void __launch_bounds__(1024) batch_step_kernel(WinRep* __restrict__ reps, int R,
                                                           const int* __restrict__ M_in,
                                                           const WinGen* __restrict__ recs, int* __restrict__ total,
                                                           int* __restrict__ step, const BatchStepPlan plan,
                                                           const int* __restrict__ region_off,
                                                           const long long* __restrict__ region_base,
-                                                          const StepRep* __restrict__ steprep, int* __restrict__ fault) {
-  __shared__ int s_warp[32];
-  __shared__ int s_carry;
+                                                          const StepRep* __restrict__ steprep, int* __restrict__ fault,
+                                                          int* __restrict__ list_rep, int* __restrict__ list_tile0,
+                                                          int* __restrict__ list_count) {
+  __shared__ int s_tiles[32], s_listed[32];
+  __shared__ int s_carry_tiles, s_carry_listed;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int k = *step;
   const int j = k / plan.slab_windows;
@@ -131,7 +140,10 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(WinRep* __restrict__ r
   const long long slot_base = !in_plan              ? 0
                               : plan.ring_slots > 0 ? static_cast<long long>(j % plan.ring_slots) * plan.slot_records
                                                     : region_base[j];
-  if (threadIdx.x == 0) s_carry = 0;
+  if (threadIdx.x == 0) {
+    s_carry_tiles = 0;
+    s_carry_listed = 0;
+  }
   __syncthreads();   // every thread has read *step
   for (int base = 0; base < R; base += 1024) {
     const int r = base + threadIdx.x;
@@ -168,32 +180,55 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(WinRep* __restrict__ r
       W.compact = need > 0 ? 1 : 0;
       W.ntiles = need;
     }
-    int incl = need;
+    // exclusive scans of the tiles and of the listed (unfinished) replicates over the block
+    const int listed = need > 0 ? 1 : 0;
+    int incl_t = need, incl_l = listed;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += y;
+      const int yt = __shfl_up_sync(0xFFFFFFFFu, incl_t, o);
+      const int yl = __shfl_up_sync(0xFFFFFFFFu, incl_l, o);
+      if (lane >= o) {
+        incl_t += yt;
+        incl_l += yl;
+      }
     }
-    if (lane == 31) s_warp[warp] = incl;
+    if (lane == 31) {
+      s_tiles[warp] = incl_t;
+      s_listed[warp] = incl_l;
+    }
     __syncthreads();
     if (warp == 0) {
-      int w = s_warp[lane];
+      int wt = s_tiles[lane], wl = s_listed[lane];
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-        if (lane >= o) w += y;
+        const int yt = __shfl_up_sync(0xFFFFFFFFu, wt, o);
+        const int yl = __shfl_up_sync(0xFFFFFFFFu, wl, o);
+        if (lane >= o) {
+          wt += yt;
+          wl += yl;
+        }
       }
-      s_warp[lane] = w;
+      s_tiles[lane] = wt;
+      s_listed[lane] = wl;
     }
     __syncthreads();
-    const int before = s_carry + (warp > 0 ? s_warp[warp - 1] : 0) + incl - need;
-    if (r < R) reps[r].tile0 = before;
+    const int tile0 = s_carry_tiles + (warp > 0 ? s_tiles[warp - 1] : 0) + incl_t - need;
+    const int pos = s_carry_listed + (warp > 0 ? s_listed[warp - 1] : 0) + incl_l - listed;
+    if (r < R) reps[r].tile0 = tile0;
+    if (listed) {
+      list_rep[pos] = r;
+      list_tile0[pos] = tile0;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) s_carry += s_warp[31];
+    if (threadIdx.x == 0) {
+      s_carry_tiles += s_tiles[31];
+      s_carry_listed += s_listed[31];
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    *total = s_carry;
+    *total = s_carry_tiles;
+    *list_count = s_carry_listed;
     *step = k + 1;
   }
 }
@@ -208,7 +243,7 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
                   const WinRep* __restrict__ reps, int nreps, const WinGen* __restrict__ recs, int total_tiles,
                   const int* __restrict__ total_dev, unsigned long long* __restrict__ stats,
-                  int* __restrict__ fault, const PhiloxKeys keys, int* __restrict__ sched) {
+                  int* __restrict__ fault, const PhiloxKeys keys, int* __restrict__ sched, const RepList list) {
   __shared__ int s_rep;
   __shared__ int s_tile;
   __shared__ unsigned s_warp[kWinThreads / 32];
@@ -217,7 +252,8 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
   const int lane = threadIdx.x & 31;
   WarpDraws* wd = &s_draws[(DRAW == kDrawWarp || DRAW == kDrawPooledSearch) ? (threadIdx.x >> 5) : 0];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
-  load_tile0(s_tile0, reps, nreps);
+  const int nlist = list_count(list, nreps);
+  load_tile0(s_tile0, list, reps, nlist);
   // Tiles are handed out in order by an atomic counter, so a block that drew cheap tiles (slots born
   // late in the window) takes more of them: the launch does not wait on the blocks that a fixed
   // assignment would have given the most expensive tiles.
@@ -225,7 +261,7 @@ __global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
     if (threadIdx.x == 0) {
       const int t = atomicAdd(sched, 1);
       s_tile = t;
-      if (t < ntiles_all) s_rep = find_rep_cached(s_tile0, reps, nreps, t);
+      if (t < ntiles_all) s_rep = list_rep(list, find_rep_cached(s_tile0, list, reps, nlist, t));
     }
     __syncthreads();
     const int gt = s_tile;
@@ -401,8 +437,10 @@ constexpr int kSegScanThreads = 1024;
 constexpr int kSegScanItems = 8;
 __global__ void __launch_bounds__(kSegScanThreads)
     seg_scan_kernel(const unsigned* __restrict__ tile_count, unsigned* __restrict__ tile_offset,
-                    const WinRep* __restrict__ reps, const int* __restrict__ M_end, int* __restrict__ M_out) {
-  const WinRep R = reps[blockIdx.x];
+                    const WinRep* __restrict__ reps, const int* __restrict__ M_end, int* __restrict__ M_out,
+                    const RepList list) {
+  if (list.count && static_cast<int>(blockIdx.x) >= *list.count) return;
+  const WinRep R = reps[list_rep(list, blockIdx.x)];
   if (!R.compact) return;
   __shared__ unsigned s_warp[kSegScanThreads / 32];
   __shared__ unsigned s_carry;
@@ -463,17 +501,18 @@ __global__ void __launch_bounds__(kWinThreads)
                        const int* __restrict__ tid_src, int* __restrict__ gp_dst, int* __restrict__ tid_dst,
                        const unsigned* __restrict__ flags, const unsigned* __restrict__ tile_offset,
                        const WinRep* __restrict__ reps, int nreps, const int* __restrict__ M_end, int total_tiles,
-                       const int* __restrict__ total_dev) {
+                       const int* __restrict__ total_dev, const RepList list) {
   __shared__ int s_rep;
   __shared__ int s_tile0[kRepCache];
   const int ntiles_all = total_dev ? *total_dev : total_tiles;
-  load_tile0(s_tile0, reps, nreps);
+  const int nlist = list_count(list, nreps);
+  load_tile0(s_tile0, list, reps, nlist);
   __shared__ unsigned s_words[32];
   __shared__ unsigned s_prefix[32];
   __shared__ float s_stage[FUSED ? 3 * kWinTile : kWinTile];
   const int t = threadIdx.x;
   for (int gt = blockIdx.x; gt < ntiles_all; gt += gridDim.x) {
-    if (t == 0) s_rep = find_rep_cached(s_tile0, reps, nreps, gt);
+    if (t == 0) s_rep = list_rep(list, find_rep_cached(s_tile0, list, reps, nlist, gt));
     __syncthreads();
     const WinRep R = reps[s_rep];
     __syncthreads();
@@ -570,9 +609,9 @@ void assign_batch_tiles(Engine* e, WinRep* d_reps, int nreps, const int* M_in, c
 
 void batch_step_tiles(Engine* e, WinRep* d_table, int R, const int* M_in, const WinGen* recs, int* total_out,
                       int* d_step, const BatchStepPlan& plan, const int* region_off, const long long* region_base,
-                      const StepRep* steprep, int* fault) {
+                      const StepRep* steprep, int* fault, int* list_rep, int* list_tile0, int* list_count) {
   batch_step_kernel<<<1, 1024, 0, e->stream>>>(d_table, R, M_in, recs, total_out, d_step, plan, region_off,
-                                               region_base, steprep, fault);
+                                               region_base, steprep, fault, list_rep, list_tile0, list_count);
   e->kernel_launches += 1;
 }
 
@@ -595,7 +634,7 @@ static void launch_window_kernel(Engine* e, const WindowLaunch& w) {
   const PhiloxKeys keys = philox_round_keys(w.seed1, w.seed2);
   window_kernel<DRAW, KEYS><<<blocks, kWinThreads, 0, e->stream>>>(
       w.A, w.B, w.id_gp_cur, w.id_tid_cur, w.flags, w.tile_count, w.M_in, w.M_end, w.M_next, w.reps, w.nreps,
-      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault, keys, w.sched);
+      w.recs, w.total_tiles, w.total_tiles_dev, w.stats, w.fault, keys, w.sched, w.list);
 }
 
 // Launch a window over w.nreps replicates and, for the replicates that compact, the segmented scan
@@ -622,13 +661,13 @@ gf_status window_run(Engine* e, const WindowLaunch& w, float* compact_dst, cudaE
   if (before_compaction) GF_CUDA(e, cudaEventRecord(before_compaction, e->stream));
   if (w.any_compact) {
     seg_scan_kernel<<<w.nreps, kSegScanThreads, 0, e->stream>>>(w.tile_count, w.tile_offset, w.reps, w.M_end,
-                                                                w.M_out);
+                                                                w.M_out, w.list);
     GF_CUDA(e, cudaGetLastError());
     const int sblocks = std::max(1, std::min(w.total_tiles, e->num_sms * 8));
     auto scatter = w.nreps == 1 ? seg_scatter_kernel<true> : seg_scatter_kernel<false>;
     scatter<<<sblocks, kWinThreads, 0, e->stream>>>(w.B, compact_dst, w.id_gp_cur, w.id_tid_cur, w.id_gp_next,
                                                     w.id_tid_next, w.flags, w.tile_offset, w.reps, w.nreps,
-                                                    w.M_end, w.total_tiles, w.total_tiles_dev);
+                                                    w.M_end, w.total_tiles, w.total_tiles_dev, w.list);
     GF_CUDA(e, cudaGetLastError());
     e->kernel_launches += 2;
   }
