@@ -77,6 +77,35 @@ def test_batched_super_steps_are_resumable():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+def test_slab_graphs_equal_single_steps():
+    """A record slab's super-steps replayed as one CUDA graph give the same states, counts and statistics
+    as the same super-steps launched one at a time (profiling mode launches them one at a time), whether
+    the batch runs to completion or in chunks that start slabs at both buffer parities; the batch is long
+    enough for many slabs (the graphs are used from the second one on)."""
+    reps = make_replicates(24, seed=21, max_gens=3000)
+    runs = []
+    for profiling, chunk in ((True, 0), (False, 0), (False, 53)):
+        with Engine() as e:
+            e.set_profiling(profiling)
+            e.batch_begin(reps)
+            if chunk:
+                while e.batch_run(chunk) > 0:
+                    pass
+            else:
+                assert e.batch_run() == 0
+            st = e.batch_stats()
+            runs.append(([e.batch_read_state(r) for r in range(len(reps))], st["generations"], st["super_steps"],
+                         st["mutation_generations"]))
+    (ref, gens, steps, mg) = runs[0]
+    assert steps >= 100   # slabs of 512 / (largest cadence) super-steps: many of them
+    for states, g, k, m in runs[1:]:
+        assert g == gens and k == steps and m == mg
+        for (fa, ia, ga), (fb, ib, gb) in zip(ref, states):
+            assert ga == gb
+            assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
+            assert np.array_equal(ia, ib)
+
+
 def test_streamed_records_agree():
     """Generation records are drawn by host threads region by region while the super-steps run: all
     regions resident (a large budget), a ring of a few regions (a budget of a few regions), a ring of
