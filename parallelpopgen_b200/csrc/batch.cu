@@ -327,15 +327,24 @@ void release_batch(Engine* e) {
   e->batch = nullptr;
 }
 
-// Upper bound on a replicate's slots: neutral equilibrium of its largest population plus one window
+// Upper bound on a replicate's slots: the equilibrium count of its largest population plus one window
 // of new mutations with 7-sigma margins (set_Index_Length's margin, go_fish_impl.cuh:235), with room
-// to spare; selection only lowers the count.
+// to spare.  The neutral equilibrium count theta (ln Nc + 0.58) is scaled by how far the replicate's
+// own mutation-selection-equilibrium start exceeds it at the initial size: positive selection raises
+// the count (up to about twice the neutral one, the high-frequency classes filling up), by a factor
+// that to first order does not depend on N, so a beneficial-allele replicate that grows keeps room for
+// its larger equilibrium; negative selection only lowers it (factor 1).
 static long long replicate_capacity(const gf_replicate& p, int M0) {
+  auto neutral_eq = [&](int nc) {
+    const double theta = 2.0 * p.mu * p.num_sites * nc;
+    return theta * (std::log(std::max(nc, 2)) + 0.58);
+  };
   int ncmax = 0;
   for (int g : {0, p.num_generations}) ncmax = std::max(ncmax, rep_nchrom(p, g));
   if (p.growth_rate != 0.f) ncmax = std::max(ncmax, static_cast<int>(2 * p.N_max / (1 + p.F)));
-  const double theta = 2.0 * p.mu * p.num_sites * ncmax;
-  const double eq = theta * (std::log(std::max(ncmax, 2)) + 0.58);
+  const double eq0 = neutral_eq(rep_nchrom(p, 0));
+  const double factor = eq0 > 0.0 ? std::max(1.0, M0 / eq0) : 1.0;
+  const double eq = factor * neutral_eq(ncmax);
   const double lam = static_cast<double>(p.mu) * ncmax * p.num_sites;
   const double window = p.compact_interval * (lam + 7.0 * std::sqrt(lam + 1.0));
   const double want = std::max<double>(M0, 1.5 * eq + 10.0 * std::sqrt(eq + 1.0)) + 2.0 * window + 1024.0;

@@ -106,6 +106,25 @@ def test_slab_graphs_equal_single_steps():
             assert np.array_equal(ia, ib)
 
 
+def test_beneficial_growing_replicate_fits_its_segment():
+    """Positive selection raises the equilibrium count of segregating sites above the neutral one, and a
+    growing population carries that excess to its larger size.  This replicate (gamma = +10 at N0, h =
+    0.875, tenfold growth, cadence 5; one of the benchmark's full-range draws) overflowed a segment sized
+    from the neutral count (20,546 slots against 20,480); sized from its own equilibrium start it runs
+    and equals the plain run."""
+    rep = replicate(seed1=52533, seed2=908905, num_sites=1e7, mu=1e-9, F=0.14773035049438477,
+                    h=0.8749696016311646, s=0.0025522892829030752, N0=2246, growth_rate=0.0009652790613472462,
+                    N_min=224, N_max=22460, num_generations=8984, compact_interval=5)
+    with Engine() as e:
+        e.batch_begin([rep])
+        assert e.batch_run() == 0
+        f_b, ids_b, gen = e.batch_read_state(0)
+    assert gen == rep.num_generations
+    f_p, ids_p = plain_run(rep)
+    assert np.array_equal(f_b.view(np.uint32), f_p.view(np.uint32))
+    assert np.array_equal(ids_b, ids_p)
+
+
 def test_streamed_records_agree():
     """Generation records are drawn by host threads region by region while the super-steps run: all
     regions resident (a large budget), a ring of a few regions (a budget of a few regions), a ring of
