@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(WinRep* __restrict__ r
 // has the seeds whose round keys `keys` holds (a plain-engine launch), so the quads' Philox blocks take
 // their round keys from the kernel parameters instead of deriving them from the replicate's seeds.
 template <int DRAW, bool KEYS>
-__global__ void __launch_bounds__(kWinThreads, GF_WINDOW_MIN_BLOCKS)
+__global__ void __launch_bounds__(kWinThreads, KEYS ? GF_WINDOW_MIN_BLOCKS_KEYS : GF_WINDOW_MIN_BLOCKS)
     window_kernel(const float* __restrict__ A, float* __restrict__ B, int* __restrict__ id_gp,
                   int* __restrict__ id_tid, unsigned* __restrict__ flags, unsigned* __restrict__ tile_count,
                   const int* __restrict__ M_in, int* __restrict__ M_end, int* __restrict__ M_next,
