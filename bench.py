@@ -829,19 +829,26 @@ def measure_multipop(total: int, steps: int, warmup: int) -> dict:
     pops = np.zeros(3, dtype=MSE_DTYPE)
     pops[0] = (MP_N0, 2 * MP_N0, MP_MU, 0.0, MP_H, 0.0, np.float32(MP_GAMMA[0]) / np.float32(2 * MP_N0))
     reserve = 48_000_000     # time samples preserve their survivors: the state grows past 25 M slots
-    h_freq = torch.empty(3 * reserve, dtype=torch.float32, pin_memory=True).numpy()
-    h_ids = torch.empty((reserve, 4), dtype=torch.int32, pin_memory=True).numpy()
+    # two page-locked sample buffers, used in turn: a sample's copy runs while the next segment does
+    bufs = [(torch.empty(3 * reserve, dtype=torch.float32, pin_memory=True).numpy(),
+             torch.empty((reserve, 4), dtype=torch.int32, pin_memory=True).numpy()) for _ in range(2)]
     n = 200
 
     def step(samples: bool):
         eng.begin_mse(pops, seed1=SEED1, seed2=SEED2, num_sites=MP_L, compact_interval=35, reserve=reserve)
-        d2h, M = 0, 0
-        for seg in segments:
+        d2h, M, last = 0, 0, None
+        for k, seg in enumerate(segments):
             eng.run(seg)
             if samples:     # the time sample taken at the segment's last generation (rows packed [3][M])
-                M = eng.read_state_into(h_freq, h_ids)
-                d2h += 3 * 4 * M + 16 * M
-        return eng.stats()["mutation_generations"], d2h, M
+                if last is not None:
+                    M, nbytes = eng.sample_wait(with_bytes=True)
+                    d2h += nbytes
+                last = bufs[k % 2]
+                eng.sample_begin(*last)
+        if samples:
+            M, nbytes = eng.sample_wait(with_bytes=True)
+            d2h += nbytes
+        return eng.stats()["mutation_generations"], d2h, M, (last[0] if last is not None else None)
 
     for _ in range(warmup):
         step(False)
@@ -850,7 +857,7 @@ def measure_multipop(total: int, steps: int, warmup: int) -> dict:
         for _ in range(steps):
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
-            m, _, _ = step(False)
+            m, _, _, _ = step(False)
             ev1.record(stream)
             ev1.synchronize()
             times.append(ev0.elapsed_time(ev1))
@@ -859,7 +866,7 @@ def measure_multipop(total: int, steps: int, warmup: int) -> dict:
     for _ in range(steps):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        m, d2h, M = step(True)
+        m, d2h, M, h_freq = step(True)
         # the final sample's SFS of a sample of 200 in each population
         for p in range(3):
             Nc = int(np.float32(2 * multipop_size(p, total)) / np.float32(1 + np.float32(0.1 if p == 2 else 0.0)))
@@ -881,7 +888,8 @@ def measure_multipop(total: int, steps: int, warmup: int) -> dict:
                    "kernel": "window_mp_kernel (P = 3: all generations of a compaction window per launch)"},
         "mutation_generations_per_step": mg / steps,
         "e2e": {"value": e2e_mg / (sum(e2e_t) * 1e-3), "unit": "mutation-generations/s",
-                "path": "10 time samples read into page-locked buffers, SFS n=200 of each population",
+                "path": "10 time samples copied into page-locked buffers while the next segment runs "
+                        "(gf_sim_sample_begin / _wait), SFS n=200 of each population",
                 "h2d_bytes_per_step": int(sum(seg.nbytes for seg in segments)), "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "bytes_per_mutation_generation": 48,
                      "achieved": 48 * value / 1e9, "unit": "GB/s", "peak": measured_peaks()[0],

@@ -170,6 +170,19 @@ gf_status gf_sim_num_mutations(gf_engine* engine, int32_t* out_num_mutations);
 gf_status gf_sim_read_state(gf_engine* engine, float* freq_out, int32_t* ids_out, int32_t max_mutations,
                             int32_t* out_num_mutations);
 
+/* The same copy without stopping the run (the time-sample pipeline: store_time_sample's copy into
+ * the trajectory, go_fish_impl.cuh:477-501).  gf_sim_sample_begin packs the state on the device at this
+ * point of the engine's stream into engine-owned scratch and returns; the caller may enqueue more
+ * generations.  gf_sim_sample_wait copies the packed rows into freq_out ([num_populations][M]) and the
+ * IDs into ids_out ([M][4]) on a second stream, exactly M of them, while the engine's stream runs what
+ * was enqueued after the begin, and returns M (and, out_bytes_copied may be NULL, the bytes moved).
+ * Page-locked arrays (cudaMallocHost / cudaHostRegister) keep the copies direct.  max_mutations must
+ * cover the count at the begin (checked against the engine's upper bound on it, read exactly if that
+ * bound is larger; GF_ERR_CAPACITY otherwise).  One sample may be in flight per engine, and the
+ * caller's arrays must stay untouched until its wait returns. */
+gf_status gf_sim_sample_begin(gf_engine* engine, float* freq_out, int32_t* ids_out, int32_t max_mutations);
+gf_status gf_sim_sample_wait(gf_engine* engine, int32_t* out_num_mutations, int64_t* out_bytes_copied);
+
 /* Device pointer to the current frequency rows ([P][stride] floats) and their row stride, for
  * device-side consumers (valid until the next gf_sim_* call). */
 gf_status gf_sim_device_state(gf_engine* engine, const float** out_freq, int32_t* out_row_stride,

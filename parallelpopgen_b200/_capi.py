@@ -106,6 +106,8 @@ SIGNATURES = {
     "gf_sim_run": (_I, [_P, _P, _I]),
     "gf_sim_num_mutations": (_I, [_P, ctypes.POINTER(_I)]),
     "gf_sim_read_state": (_I, [_P, _P, _P, _I, ctypes.POINTER(_I)]),
+    "gf_sim_sample_begin": (_I, [_P, _P, _P, _I]),
+    "gf_sim_sample_wait": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_int64)]),
     "gf_sim_device_state": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "gf_sim_selection_view": (_I, [_P, _P]),
     "gf_new_mutation_count": (_I, [_I, _I, _F, _I, _F, _I, _I]),

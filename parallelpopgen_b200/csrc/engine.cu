@@ -464,6 +464,25 @@ __global__ void expand_ids_kernel(const int* __restrict__ gp, const int* __restr
   }
 }
 
+// A time sample packed at this point of the stream: the count M (from the device) and the rows
+// [P][M] and int4 IDs of the first M slots, into scratch of `bound` slots (M > bound reports -1).
+__global__ void pack_sample_kernel(const float* __restrict__ freq, long long capacity, int P,
+                                   const int* __restrict__ gp, const int* __restrict__ tid,
+                                   const int* __restrict__ count, int bound, float* __restrict__ out_freq,
+                                   int4* __restrict__ out_ids, int* __restrict__ out_count) {
+  const int M = *count;
+  if (M > bound) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = -1;
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = M;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+    for (int p = 0; p < P; ++p) out_freq[static_cast<long long>(p) * M + i] = freq[p * capacity + i];
+    const int w = gp[i];
+    out_ids[i] = make_int4(w & 0xFFFFFF, w >> 24, tid[i], 0);
+  }
+}
+
 static void release_sim(Engine* e) {
   // stream-ordered frees: the memory returns to the engine's pool for the next simulation
   for (int b = 0; b < 2; ++b) {
@@ -1270,6 +1289,14 @@ void gf_engine_destroy(gf_engine* g) {
   Engine* e = &g->impl;
   cudaSetDevice(e->device);
   cudaStreamSynchronize(e->stream);
+  if (e->copy_stream) {
+    cudaStreamSynchronize(e->copy_stream);
+    cudaStreamDestroy(e->copy_stream);
+    cudaEventDestroy(e->sample_packed);
+    cudaEventDestroy(e->sample_done);
+    cudaFreeHost(e->h_sample_count);
+    if (e->sample_scratch) cudaFree(e->sample_scratch);
+  }
   release_sim(e);
   release_batch(e);
   cudaStreamSynchronize(e->stream);
@@ -1554,6 +1581,101 @@ gf_status gf_sim_read_state(gf_engine* g, float* freq_out, int32_t* ids_out, int
       if (err != cudaSuccess) return cuda_fail(e, err, "reading mutation IDs");
     }
     GF_CUDA(e, cudaStreamSynchronize(e->stream));
+    return GF_OK;
+  });
+}
+
+gf_status gf_sim_sample_begin(gf_engine* g, float* freq_out, int32_t* ids_out, int32_t max_mutations) {
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || max_mutations < 0) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->active) return fail(e, GF_ERR_STATE, "no simulation");
+    if (e->sample_in_flight) return fail(e, GF_ERR_STATE, "a time sample is already in flight");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    poll_pending(e, false);
+    long long bound = e->M_upper;
+    if (bound > max_mutations) {   // the bound is loose: read the count itself
+      int M = 0;
+      gf_status st = current_count(e, &M);
+      if (st != GF_OK) return st;
+      if (M > max_mutations)
+        return fail(e, GF_ERR_CAPACITY, "state holds %d mutations, caller buffer %d", M, max_mutations);
+      bound = M;
+    }
+    if (!e->copy_stream) {
+      GF_CUDA(e, cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+      GF_CUDA(e, cudaEventCreateWithFlags(&e->sample_packed, cudaEventDisableTiming));
+      GF_CUDA(e, cudaEventCreateWithFlags(&e->sample_done, cudaEventDisableTiming));
+      GF_CUDA(e, cudaMallocHost(&e->h_sample_count, sizeof(int)));
+    }
+    const int P = e->P;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t fbytes = sizeof(float) * static_cast<size_t>(P) * static_cast<size_t>(bound);
+    const size_t ibytes = sizeof(int4) * static_cast<size_t>(bound);
+    const size_t need = al(fbytes) + al(ibytes) + 256;
+    if (e->sample_scratch_bytes < need) {   // no sample in flight: the old scratch is free
+      GF_CUDA(e, cudaStreamSynchronize(e->copy_stream));
+      if (e->sample_scratch) GF_CUDA(e, cudaFree(e->sample_scratch));
+      e->sample_scratch = nullptr;
+      e->sample_scratch_bytes = 0;
+      const size_t bytes = need + need / 4;
+      GF_CUDA(e, cudaMalloc(&e->sample_scratch, bytes));
+      e->sample_scratch_bytes = bytes;
+    }
+    char* base = static_cast<char*>(e->sample_scratch);
+    float* d_freq = reinterpret_cast<float*>(base);
+    int4* d_ids = reinterpret_cast<int4*>(base + al(fbytes));
+    int* d_cnt = reinterpret_cast<int*>(base + al(fbytes) + al(ibytes));
+    e->sample_bound = bound;
+    const int blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(148 * 8, (bound + 255) / 256)));
+    pack_sample_kernel<<<blocks, 256, 0, e->stream>>>(e->freq[e->cur], e->capacity, P, e->id_gp[e->id_cur],
+                                                       e->id_tid[e->id_cur], e->d_count + e->count_slot,
+                                                       static_cast<int>(bound), d_freq, d_ids, d_cnt);
+    GF_CUDA(e, cudaGetLastError());
+    e->kernel_launches += 1;
+    GF_CUDA(e, cudaEventRecord(e->sample_packed, e->stream));
+    // the count follows on the copy stream; the rows and IDs are copied once it is known (at the
+    // wait), exactly M of them, while the engine's stream runs whatever was enqueued after this point
+    GF_CUDA(e, cudaStreamWaitEvent(e->copy_stream, e->sample_packed, 0));
+    GF_CUDA(e, cudaMemcpyAsync(e->h_sample_count, d_cnt, sizeof(int), cudaMemcpyDeviceToHost, e->copy_stream));
+    GF_CUDA(e, cudaEventRecord(e->sample_done, e->copy_stream));
+    e->sample_in_flight = true;
+    e->sample_freq_out = freq_out;
+    e->sample_ids_out = ids_out;
+    return GF_OK;
+  });
+}
+
+gf_status gf_sim_sample_wait(gf_engine* g, int32_t* out_num, int64_t* out_bytes) {
+  return guard_host(g, [&]() -> gf_status {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (!e->sample_in_flight) return fail(e, GF_ERR_STATE, "no time sample in flight");
+    GF_CUDA(e, cudaSetDevice(e->device));
+    e->sample_in_flight = false;
+    GF_CUDA(e, cudaEventSynchronize(e->sample_done));   // the sample is packed and its count is here
+    const int M = *e->h_sample_count;
+    if (M < 0) return fail(e, GF_ERR_STATE, "the count exceeded the engine's bound on it when the sample was packed");
+    const int P = e->P;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    // the begin's scratch layout: rows [P][M] packed at the front of a bound-sized area, then the IDs
+    char* base = static_cast<char*>(e->sample_scratch);
+    const size_t fbytes = sizeof(float) * static_cast<size_t>(P) * static_cast<size_t>(e->sample_bound);
+    const int4* d_ids = reinterpret_cast<const int4*>(base + al(fbytes));
+    long long bytes = sizeof(int);
+    if (M > 0 && e->sample_freq_out) {
+      GF_CUDA(e, cudaMemcpyAsync(e->sample_freq_out, base, sizeof(float) * static_cast<size_t>(P) * M,
+                                 cudaMemcpyDeviceToHost, e->copy_stream));
+      bytes += static_cast<long long>(sizeof(float)) * P * M;
+    }
+    if (M > 0 && e->sample_ids_out) {
+      GF_CUDA(e, cudaMemcpyAsync(e->sample_ids_out, d_ids, sizeof(int4) * static_cast<size_t>(M), cudaMemcpyDeviceToHost,
+                                 e->copy_stream));
+      bytes += static_cast<long long>(sizeof(int4)) * M;
+    }
+    GF_CUDA(e, cudaStreamSynchronize(e->copy_stream));
+    if (out_num) *out_num = M;
+    if (out_bytes) *out_bytes = bytes;
     return GF_OK;
   });
 }

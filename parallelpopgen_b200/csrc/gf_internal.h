@@ -309,6 +309,17 @@ struct Engine {
   // host tracking of the mutation count
   long long M_upper = 0;   // upper bound on the current count (exact when nothing is pending)
   bool M_exact = true;
+  // an asynchronous time sample (gf_sim_sample_begin / _wait): the state packed into device scratch on
+  // the engine's stream, copied to the caller's arrays on a second stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t sample_packed = nullptr, sample_done = nullptr;
+  void* sample_scratch = nullptr;
+  size_t sample_scratch_bytes = 0;
+  int* h_sample_count = nullptr;   // page-locked: the sample's count
+  bool sample_in_flight = false;
+  float* sample_freq_out = nullptr;   // the in-flight sample's destination arrays
+  int32_t* sample_ids_out = nullptr;
+  long long sample_bound = 0;         // slots its scratch was laid out for
   std::deque<PendingCount> pending;
   std::vector<cudaEvent_t> free_events;
 

@@ -115,6 +115,23 @@ class Engine:
         self._check(self.lib.gf_sim_read_state(self.h, ptr(freq_out), ptr(ids_out), int(cap), ctypes.byref(got)))
         return got.value
 
+    def sample_begin(self, freq_out: np.ndarray, ids_out: np.ndarray | None = None) -> None:
+        """Start copying the current state into caller-owned arrays while later generations run
+        (gf_sim_sample_begin): the rows arrive packed as [P][M] at the front of `freq_out`, the IDs in the
+        first M rows of `ids_out`.  Page-locked arrays keep the copies asynchronous; leave them untouched
+        until sample_wait, which returns M."""
+        cap = freq_out.size // max(self.P, 1)
+        if ids_out is not None and ids_out.shape[0] < cap:
+            cap = ids_out.shape[0]
+        self._check(self.lib.gf_sim_sample_begin(self.h, ptr(freq_out), ptr(ids_out), int(cap)))
+
+    def sample_wait(self, with_bytes: bool = False):
+        """M of the sample in flight (and, with_bytes, the bytes its copies moved)."""
+        got = ctypes.c_int32()
+        nbytes = ctypes.c_int64()
+        self._check(self.lib.gf_sim_sample_wait(self.h, ctypes.byref(got), ctypes.byref(nbytes)))
+        return (got.value, nbytes.value) if with_bytes else got.value
+
     def device_state(self):
         p = ctypes.c_void_p()
         stride = ctypes.c_int32()

@@ -149,3 +149,44 @@ def test_resumed_nonzero_row_of_an_unfounded_population():
     out = run_both(lambda e: e.begin_from_state(freq, ids, seed1=1, seed2=2, num_sites=2e6, compact_interval=25),
                    [gens])
     assert_same(out)
+
+
+@pytest.mark.parametrize("P", [1, 3])
+def test_async_time_samples_equal_synchronous_reads(P):
+    """Time samples copied while the next generations run (gf_sim_sample_begin / _wait, two page-locked
+    buffer sets used in turn) equal, bit for bit, the synchronous reads of an identical run at the same
+    generations: rows packed [P][M] and the mutation IDs."""
+    import torch
+    gens = schedule(P, 1, 300, sample_every=60)
+    segments = [gens[a:a + 60] for a in range(0, 300, 60)]
+    setup = (lambda e: e.begin_mse(mse_start(P), seed1=31, seed2=32, num_sites=4e6, compact_interval=25))
+    want = []
+    with Engine() as e:
+        setup(e)
+        for seg in segments:
+            e.run(seg)
+            want.append(e.read_state())
+    cap = 200_000
+    bufs = [(torch.empty(P * cap, dtype=torch.float32).pin_memory().numpy(),
+             torch.empty((cap, 4), dtype=torch.int32).pin_memory().numpy()) for _ in range(2)]
+    got = []
+    with Engine() as e:
+        setup(e)
+        pending = None
+        for k, seg in enumerate(segments):
+            e.run(seg)
+            if pending is not None:           # the previous sample's copy overlapped this segment
+                M = e.sample_wait()
+                f, ids = pending
+                got.append((f[:P * M].reshape(P, M).copy(), ids[:M].copy()))
+            f, ids = bufs[k % 2]
+            e.sample_begin(f, ids)
+            pending = (f, ids)
+        M = e.sample_wait()
+        f, ids = pending
+        got.append((f[:P * M].reshape(P, M).copy(), ids[:M].copy()))
+    assert len(got) == len(want)
+    for (fa, ia), (fb, ib) in zip(got, want):
+        assert fa.shape == fb.shape and fa.shape[1] > 100, (fa.shape, fb.shape)
+        assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
+        assert np.array_equal(ia, ib)
