@@ -190,3 +190,27 @@ def test_async_time_samples_equal_synchronous_reads(P):
         assert fa.shape == fb.shape and fa.shape[1] > 100, (fa.shape, fb.shape)
         assert np.array_equal(fa.view(np.uint32), fb.view(np.uint32))
         assert np.array_equal(ia, ib)
+
+
+def test_async_time_sample_misuse_is_reported():
+    """A wait with no sample in flight, a second begin while one is in flight, and caller arrays too small
+    for the state come back as status codes; the engine stays usable."""
+    import torch
+    from parallelpopgen_b200._capi import GoFishError
+    gens = schedule(2, 1, 60, sample_every=60)
+    with Engine() as e:
+        e.begin_mse(mse_start(2), seed1=41, seed2=42, num_sites=4e6, compact_interval=25)
+        e.run(gens)
+        with pytest.raises(GoFishError, match="no time sample in flight"):
+            e.sample_wait()
+        tiny = torch.empty(2 * 10, dtype=torch.float32).pin_memory().numpy()
+        with pytest.raises(GoFishError, match="GF_ERR_CAPACITY"):
+            e.sample_begin(tiny)
+        f = torch.empty(2 * 200_000, dtype=torch.float32).pin_memory().numpy()
+        e.sample_begin(f)
+        with pytest.raises(GoFishError, match="already in flight"):
+            e.sample_begin(f)
+        M = e.sample_wait()
+        want, _ = e.read_state()
+        assert want.shape[1] == M
+        assert np.array_equal(f[:2 * M].reshape(2, M).view(np.uint32), want.view(np.uint32))
