@@ -950,7 +950,7 @@ static gf_status batch_super_step(Engine* e, int* active_out) {
 static gf_status batch_slab(Engine* e, int* active_out, bool* ran) {
   *ran = false;
   Batch* b = e->batch;
-  if (!b->precomputed || e->profiling || !e->stream) return GF_OK;
+  if (!b->precomputed || e->profiling || !e->stream || b->graphs_off) return GF_OK;
   refresh_active(b);
   const long long k = b->super_steps;
   const int W = b->plan.slab_windows;
@@ -970,7 +970,11 @@ static gf_status batch_slab(Engine* e, int* active_out, bool* ran) {
   if (!b->slab_graph[parity]) {
     const long long launches0 = e->kernel_launches;
     const int m0 = b->mslot, i0 = b->id_cur;
-    GF_CUDA(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();   // a stream that cannot be captured: the batch runs step by step
+      b->graphs_off = true;
+      return GF_OK;
+    }
     gf_status st = GF_OK;
     for (int i = 0; i < W && st == GF_OK; ++i) {
       st = enqueue_step(e, b);
@@ -982,15 +986,18 @@ static gf_status batch_slab(Engine* e, int* active_out, bool* ran) {
     e->kernel_launches = launches0;
     cudaGraph_t graph = nullptr;
     const cudaError_t cerr = cudaStreamEndCapture(e->stream, &graph);
-    if (st != GF_OK || cerr != cudaSuccess) {
+    if (st != GF_OK) {
       if (graph) cudaGraphDestroy(graph);
-      if (st != GF_OK) return st;
-      return cuda_fail(e, cerr, "capturing a record slab's super-steps");
+      return st;
     }
     cudaGraphExec_t exec = nullptr;
-    const cudaError_t ierr = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ierr != cudaSuccess) return cuda_fail(e, ierr, "instantiating a record slab's graph");
+    const cudaError_t ierr = cerr == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cerr;
+    if (graph) cudaGraphDestroy(graph);
+    if (ierr != cudaSuccess) {   // nothing captured ran: the batch continues step by step
+      cudaGetLastError();
+      b->graphs_off = true;
+      return GF_OK;
+    }
     b->slab_graph[parity] = exec;
     b->graph_draw[parity] = e->draw_strategy;
     b->graph_blocks[parity] = e->blocks_per_sm;

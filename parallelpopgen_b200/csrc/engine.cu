@@ -1627,6 +1627,7 @@ gf_status gf_sim_sample_begin(gf_engine* g, float* freq_out, int32_t* ids_out, i
     int4* d_ids = reinterpret_cast<int4*>(base + al(fbytes));
     int* d_cnt = reinterpret_cast<int*>(base + al(fbytes) + al(ibytes));
     e->sample_bound = bound;
+    e->sample_P = P;
     const int blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(148 * 8, (bound + 255) / 256)));
     pack_sample_kernel<<<blocks, 256, 0, e->stream>>>(e->freq[e->cur], e->capacity, P, e->id_gp[e->id_cur],
                                                        e->id_tid[e->id_cur], e->d_count + e->count_slot,
@@ -1656,7 +1657,7 @@ gf_status gf_sim_sample_wait(gf_engine* g, int32_t* out_num, int64_t* out_bytes)
     GF_CUDA(e, cudaEventSynchronize(e->sample_done));   // the sample is packed and its count is here
     const int M = *e->h_sample_count;
     if (M < 0) return fail(e, GF_ERR_STATE, "the count exceeded the engine's bound on it when the sample was packed");
-    const int P = e->P;
+    const int P = e->sample_P;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     // the begin's scratch layout: rows [P][M] packed at the front of a bound-sized area, then the IDs
     char* base = static_cast<char*>(e->sample_scratch);

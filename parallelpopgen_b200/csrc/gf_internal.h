@@ -252,6 +252,7 @@ struct Batch {
   // one record slab's super-steps as a CUDA graph, per starting buffer parity, and the draw tuning
   // it was captured with
   cudaGraphExec_t slab_graph[2] = {nullptr, nullptr};
+  bool graphs_off = false;                    // the stream could not be captured: step by step
   int graph_draw[2] = {-1, -1};
   int graph_blocks[2] = {-1, -1};
   cudaEvent_t* step_ev = nullptr;             // 64 (the engine's batch_ahead[0..63])
@@ -320,6 +321,7 @@ struct Engine {
   float* sample_freq_out = nullptr;   // the in-flight sample's destination arrays
   int32_t* sample_ids_out = nullptr;
   long long sample_bound = 0;         // slots its scratch was laid out for
+  int sample_P = 0;                   // populations of the sampled state
   std::deque<PendingCount> pending;
   std::vector<cudaEvent_t> free_events;
 
