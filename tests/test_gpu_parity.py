@@ -156,6 +156,41 @@ def test_wf_variants_match_reference(gofish_driver, ref_driver, tmp_path, extra)
     assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
 
 
+def random_wf_cases(count: int, seed: int = 2026):
+    """Seeded draws over the single- and multi-population model space: population size (log-uniform
+    50 to 20,000), one to three populations with symmetric migration, selection, dominance, inbreeding,
+    mutation rate, sites, run length, compaction cadence and sampling.  Selected runs start blank: the
+    reference's selected equilibrium start is not deterministic (its float scan), so only neutral runs
+    start at equilibrium."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for _ in range(count):
+        pops = int(rng.choice([1, 1, 2, 3]))
+        gamma = 0.0 if rng.random() < 0.3 else float(np.round(rng.uniform(-50, 10), 2))
+        case = [f"seed1={int(rng.integers(1, 2**31 - 1))}", f"seed2={int(rng.integers(1, 2**31 - 1))}",
+                f"N={int(np.exp(rng.uniform(np.log(50), np.log(20000))))}", f"pops={pops}",
+                f"gamma={gamma}", f"h={float(np.round(rng.uniform(0, 1), 3))}",
+                f"F={0.0 if rng.random() < 0.5 else float(np.round(rng.uniform(0, 0.5), 3))}",
+                f"mu={float(rng.choice([1e-9, 1e-8]))}", f"L={float(np.round(np.exp(rng.uniform(np.log(1e6), np.log(5e7))), -3))}",
+                f"gens={int(rng.integers(200, 1500))}", f"compact={int(rng.integers(5, 50))}",
+                f"sample_every={int(rng.choice([0, 100, 250]))}", f"mse={1 if gamma == 0.0 else 0}"]
+        if pops > 1:
+            case.append(f"m={float(np.round(np.exp(rng.uniform(np.log(1e-4), np.log(0.02))), 6))}")
+        cases.append(case)
+    return cases
+
+
+@pytest.mark.parametrize("case", random_wf_cases(12), ids=lambda c: "-".join(x.split("=")[1] for x in c[2:5]))
+def test_random_wf_scenarios_match_reference(gofish_driver, ref_driver, tmp_path, case):
+    """Seeded random scenarios over the model space the reference's run_sim covers, each bit-exact
+    against the reference built and run on the same GPU (frequencies, IDs, histograms; SFS within the
+    tolerance)."""
+    args = ["sfs_n=50", "hist=1", *case]
+    mine = run_driver(gofish_driver, "wf", tmp_path / "mine.bin", args)
+    subprocess.run([str(ref_driver), "sim", "wf", str(tmp_path / "ref.bin"), *args], check=True, capture_output=True)
+    assert_dumps_equal(mine, Dump(tmp_path / "ref.bin"))
+
+
 @pytest.mark.parametrize("extra", [
     ["quad_a=-40", "gamma=2", "gens=2000", "compact=25"],
     ["quad_a=30", "gamma=-3", "pops=2", "m=0.01", "gens=1500", "compact=20"],
