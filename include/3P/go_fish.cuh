@@ -688,6 +688,35 @@ struct trajectory_access {
       ts->Nchrom_e[i] = 2 * demography(i, generation) / (1 + FI_(i, generation));
     }
   }
+
+  /* The same for a sample that is not the last, with its copy overlapped with the generations that
+   * follow: store_begin records the sample's generation, extinctions and sizes and has the engine pack
+   * its rows at this point of the run; store_finish, called once later generations are enqueued,
+   * copies them into the sample while those generations run. */
+  template <typename Dem, typename FI>
+  static void store_begin(AT& a, int s, gf_engine* e, int generation, const bool* extinct, Dem demography, FI FI_) {
+    const int P = a.sim_run_constants.num_populations;
+    AT::time_sample* ts = a.time_samples[s];
+    ts->sampled_generation = generation;
+    ts->extinct = new bool[P];
+    ts->Nchrom_e = new int[P];
+    for (int i = 0; i < P; ++i) {
+      ts->extinct[i] = extinct[i];
+      ts->Nchrom_e[i] = 2 * demography(i, generation) / (1 + FI_(i, generation));
+    }
+    check(e, gf_sim_sample_begin(e, NULL, NULL, 0x7fffffff), "store_time_sample");
+  }
+  static void store_finish(AT& a, int s, gf_engine* e) {
+    const int P = a.sim_run_constants.num_populations;
+    int M = 0;
+    check(e, gf_sim_sample_wait(e, &M, NULL), "store_time_sample");
+    const float* staged = NULL;
+    check(e, gf_sim_sample_staged(e, &staged), "store_time_sample");
+    AT::time_sample* ts = a.time_samples[s];
+    ts->num_mutations = M;
+    ts->mutations_freq = new float[static_cast<size_t>(P) * M];
+    if (M > 0) std::memcpy(ts->mutations_freq, staged, sizeof(float) * static_cast<size_t>(P) * M);
+  }
 };
 
 /* check_sim_parameters (go_fish_impl.cuh:431-452), with the reference's messages */
@@ -853,8 +882,16 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
   TA::init_results(all_results, new_length);
 
   int sample_index = 0;
+  int pending_sample = -1;   // a time sample whose copy overlaps the generations enqueued after it
+  auto finish_pending = [&]() {
+    if (pending_sample >= 0) {
+      TA::store_finish(all_results, pending_sample, eng);
+      pending_sample = -1;
+    }
+  };
   if (take_sample(generation) && generation != final_generation) {
-    TA::store(all_results, sample_index, eng, generation, false, extinct, demography, FI);
+    TA::store_begin(all_results, sample_index, eng, generation, extinct, demography, FI);
+    pending_sample = sample_index;
     ++sample_index;
   }
 
@@ -918,11 +955,14 @@ inline void run_sim(allele_trajectories& all_results, const Functor_mutation mu_
     }
     if (sample_now || batch.size() >= 256) flush();
     if (sample_now) {
-      TA::store(all_results, sample_index, eng, generation, false, extinct, demography, FI);
+      finish_pending();   // the previous sample's copy ran beside the generations just enqueued
+      TA::store_begin(all_results, sample_index, eng, generation, extinct, demography, FI);
+      pending_sample = sample_index;
       ++sample_index;
     }
   }
   flush();
+  finish_pending();
   TA::store(all_results, sample_index, eng, generation, true, extinct, demography, FI);
 }
 

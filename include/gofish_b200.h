@@ -179,9 +179,12 @@ gf_status gf_sim_read_state(gf_engine* engine, float* freq_out, int32_t* ids_out
  * Page-locked arrays (cudaMallocHost / cudaHostRegister) keep the copies direct.  max_mutations must
  * cover the count at the begin (checked against the engine's upper bound on it, read exactly if that
  * bound is larger; GF_ERR_CAPACITY otherwise).  One sample may be in flight per engine, and the
- * caller's arrays must stay untouched until its wait returns. */
+ * caller's arrays must stay untouched until its wait returns.  With freq_out and ids_out both NULL the
+ * wait copies the rows (not the IDs) into page-locked staging the engine owns, readable through
+ * gf_sim_sample_staged until the next begin. */
 gf_status gf_sim_sample_begin(gf_engine* engine, float* freq_out, int32_t* ids_out, int32_t max_mutations);
 gf_status gf_sim_sample_wait(gf_engine* engine, int32_t* out_num_mutations, int64_t* out_bytes_copied);
+gf_status gf_sim_sample_staged(gf_engine* engine, const float** out_freq);
 
 /* Device pointer to the current frequency rows ([P][stride] floats) and their row stride, for
  * device-side consumers (valid until the next gf_sim_* call). */

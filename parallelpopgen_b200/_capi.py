@@ -108,6 +108,7 @@ SIGNATURES = {
     "gf_sim_read_state": (_I, [_P, _P, _P, _I, ctypes.POINTER(_I)]),
     "gf_sim_sample_begin": (_I, [_P, _P, _P, _I]),
     "gf_sim_sample_wait": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_int64)]),
+    "gf_sim_sample_staged": (_I, [_P, ctypes.POINTER(_P)]),
     "gf_sim_device_state": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "gf_sim_selection_view": (_I, [_P, _P]),
     "gf_new_mutation_count": (_I, [_I, _I, _F, _I, _F, _I, _I]),

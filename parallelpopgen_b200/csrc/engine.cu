@@ -1296,6 +1296,7 @@ void gf_engine_destroy(gf_engine* g) {
     cudaEventDestroy(e->sample_done);
     cudaFreeHost(e->h_sample_count);
     if (e->sample_scratch) cudaFree(e->sample_scratch);
+    if (e->h_sample_stage) cudaFreeHost(e->h_sample_stage);
   }
   release_sim(e);
   release_batch(e);
@@ -1643,6 +1644,7 @@ gf_status gf_sim_sample_begin(gf_engine* g, float* freq_out, int32_t* ids_out, i
     e->sample_in_flight = true;
     e->sample_freq_out = freq_out;
     e->sample_ids_out = ids_out;
+    e->sample_to_stage = !freq_out && !ids_out;
     return GF_OK;
   });
 }
@@ -1664,6 +1666,18 @@ gf_status gf_sim_sample_wait(gf_engine* g, int32_t* out_num, int64_t* out_bytes)
     const size_t fbytes = sizeof(float) * static_cast<size_t>(P) * static_cast<size_t>(e->sample_bound);
     const int4* d_ids = reinterpret_cast<const int4*>(base + al(fbytes));
     long long bytes = sizeof(int);
+    if (e->sample_to_stage) {   // the engine's page-locked staging, grown to the sample with headroom
+      const size_t need = static_cast<size_t>(P) * static_cast<size_t>(std::max(M, 1));
+      if (e->sample_stage_cap < need) {
+        if (e->h_sample_stage) GF_CUDA(e, cudaFreeHost(e->h_sample_stage));
+        e->h_sample_stage = nullptr;
+        e->sample_stage_cap = 0;
+        const size_t cap = need + need / 4;
+        GF_CUDA(e, cudaMallocHost(&e->h_sample_stage, sizeof(float) * cap));
+        e->sample_stage_cap = cap;
+      }
+      e->sample_freq_out = e->h_sample_stage;
+    }
     if (M > 0 && e->sample_freq_out) {
       GF_CUDA(e, cudaMemcpyAsync(e->sample_freq_out, base, sizeof(float) * static_cast<size_t>(P) * M,
                                  cudaMemcpyDeviceToHost, e->copy_stream));
@@ -1677,6 +1691,17 @@ gf_status gf_sim_sample_wait(gf_engine* g, int32_t* out_num, int64_t* out_bytes)
     GF_CUDA(e, cudaStreamSynchronize(e->copy_stream));
     if (out_num) *out_num = M;
     if (out_bytes) *out_bytes = bytes;
+    return GF_OK;
+  });
+}
+
+gf_status gf_sim_sample_staged(gf_engine* g, const float** out_freq) {
+  return guard_host(g, [&]() -> gf_status {
+    if (!g || !out_freq) return GF_ERR_INVALID_ARGUMENT;
+    Engine* e = &g->impl;
+    if (e->sample_in_flight || !e->sample_to_stage || !e->h_sample_stage)
+      return fail(e, GF_ERR_STATE, "no staged time sample (begin with NULL arrays, then wait)");
+    *out_freq = e->h_sample_stage;
     return GF_OK;
   });
 }

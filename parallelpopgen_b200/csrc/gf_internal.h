@@ -322,6 +322,9 @@ struct Engine {
   int32_t* sample_ids_out = nullptr;
   long long sample_bound = 0;         // slots its scratch was laid out for
   int sample_P = 0;                   // populations of the sampled state
+  bool sample_to_stage = false;       // the wait copies into the engine's staging
+  float* h_sample_stage = nullptr;    // page-locked staging of a sample's rows
+  size_t sample_stage_cap = 0;        // in floats
   std::deque<PendingCount> pending;
   std::vector<cudaEvent_t> free_events;
 
