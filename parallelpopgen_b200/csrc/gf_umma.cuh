@@ -69,7 +69,7 @@ __device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, 
 }
 
 // ---------------------------------------------------------------------------------------------
-// TMA: 2-D tiled load global -> shared, completion counted on an mbarrier (no multicast)
+// TMA: 2-D tiled load global -> this CTA's shared memory, completion counted on an mbarrier
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void tma_load_2d(void* smem_dst, const void* tmap, int x, int y, uint64_t* bar) {
   asm volatile(
